@@ -1,0 +1,332 @@
+"""Benchmark of the B200 SPH step (particle-steps/s).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl ours|reference]
+
+One "step" is one SPHBase.step of the workload's scene(s) (neighbour search, DFSPH
+divergence and density solves, non-Newtonian implicit viscosity, elasticity,
+advection). `value` times K steps with the state resident in HBM (CUDA events,
+barrier + synchronize on both sides, max over ranks); `e2e` times the same steps
+through the public object API with the state copied from pinned host memory before
+each step and the positions read back after it. Inputs are synthetic (seeded numpy
+generators with the shapes of the benchmark scenes). `--impl reference` times the
+CPU restatement of the reference step (the reference itself is Python + Taichi, which
+is not installed) on all host cores over a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
+
+# Algorithmic bytes per particle of the passes (each field read or written once per
+# pass; neighbour gathers assumed served on chip; float4 position+volume and velocity):
+ALG_BYTES = {
+    "pressure_update": 16 + 16 + 4 + 4 + 16,      # pos4, vel4, kappa, flags -> vel4
+    "density_adv": 16 + 16 + 4 + 4 + 4 + 4 + 4,   # pos4, vel4, dens, alpha, flags -> rho_adv, kappa
+    "divergence_update": 16 + 16 + 4 + 4 + 16,
+    "density_change": 16 + 16 + 4 + 4 + 4 + 4,
+    "density_factor": 16 + 4 + 4 + 4,
+    "cg_matvec": 16 + 16 + 16 + 4 + 4 + 16,       # pos4, p, aux, mass, flags -> Ap
+}
+KERNEL_IDS = {"pressure_update": 0, "density_adv": 1, "divergence_update": 2, "density_change": 3,
+              "density_factor": 4, "build_lists": 5, "cg_matvec": 6, "nonpressure": 7}
+
+
+def step_bytes(iters_v, iters_p, iters_cg, f_el, implicit):
+    """Algorithmic bytes per particle-step of the whole step (frozen constants):
+    324 + 88 I_div + 88 I_p + [40 + 120 I_cg] + 600 f_el."""
+    b = 324 + 88 * iters_v + 88 * iters_p + 600 * f_el
+    if implicit:
+        b += 40 + 120 * iters_cg
+    return b
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d, "measured"
+    return PEAKS_FALLBACK, "fallback"
+
+
+def make_workload(name, seed=0):
+    from nonnewton_b200 import scene as S
+
+    if name == "roofline_2m":
+        return [S.roofline_scene(seed=seed)]
+    if name == "dam_break":
+        return [S.dam_break(seed=seed)]
+    if name == "shear_thinning_drop":
+        return [S.shear_thinning_drop(seed=seed)]
+    if name == "fluid_elastic":
+        return [S.fluid_elastic(seed=seed)]
+    raise SystemExit(f"unknown workload {name}")
+
+
+class ClockSampler:
+    def __init__(self, path):
+        self.path = path
+        self.p = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.path, "w")
+            dev = os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")[0] or "0"
+            self.p = subprocess.Popen(["nvidia-smi", "-i", dev, f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                       "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except Exception:
+                self.p.kill()
+            self.f.close()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        except Exception:
+            return None
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if len(r) > 5 + k and "Active" in r[5 + k]
+                          and "Not" not in r[5 + k]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup(args):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(v, world):
+    if world <= 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(v, world):
+    if world <= 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def cpu_baseline(scenes, budget_s=20.0, threads=None):
+    """The oracle (FP32 restatement of the reference step) on all host cores over a
+    bounded number of steps of the same scene."""
+    from oracle import oracle as O
+
+    O.build()
+    threads = threads or os.cpu_count()
+    O.set_threads(threads)
+    sc = scenes[0]
+    o = O.OracleSim(sc.particles, sc.param, "f32")
+    o.initialize()
+    t0 = time.perf_counter()
+    steps = 0
+    while True:
+        o.step(1)
+        steps += 1
+        el = time.perf_counter() - t0
+        if el > budget_s or steps >= 50:
+            break
+    n = sc.particles.n
+    return {"value": n * steps / el, "unit": "particle-steps/s", "cores": O.get_threads(), "kind": "port",
+            "sample": f"{steps} steps of {sc.name} ({n} particles), FP32 oracle, OpenMP {O.get_threads()} threads"}
+
+
+def run_reference(args):
+    world, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return
+    scenes = make_workload(args.workload)
+    budget = max(3.0, 60.0 / max(args.steps + args.warmup, 1))
+    vals = []
+    cb = None
+    for _ in range(args.warmup):
+        cpu_baseline(scenes, budget_s=budget / 4)
+    for _ in range(args.steps):
+        cb = cpu_baseline(scenes, budget_s=budget)
+        vals.append(cb["value"])
+    v = statistics.median(vals) if vals else 0.0
+    cb["value"] = v
+    print(json.dumps({"impl": "reference", "metric": "particle-steps/s", "value": v, "unit": "particle-steps/s",
+                      "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+                      "dtype": "f32", "data": "synthetic", "config": {"workload": args.workload},
+                      "cpu_baseline": cb,
+                      "e2e": {"value": v, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
+                              "d2h_bytes_per_step": 0}}))
+
+
+def run_ours(args):
+    import torch
+
+    from nonnewton_b200 import sph
+    from nonnewton_b200.config import SimConfig
+
+    world, rank, local = dist_setup(args)
+    scenes = make_workload(args.workload, seed=rank)
+    sc = scenes[0]
+    m = sph.initialize(SimConfig(config=sc.config), particles=sc.particles, quirks=sc.param.quirks)
+    solver = sph.build_solver()
+    solver.initialize()
+    n = sc.particles.n
+    eng = m.engine
+    stream = torch.cuda.current_stream()
+    # warm-up (also captures the step graphs)
+    solver.run(max(args.warmup, 1))
+    torch.cuda.synchronize()
+    barrier(world)
+    l0 = eng.launch_count()
+    clocks_path = os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else "",
+                               f"clocks_rank{rank}.csv")
+    # ---- device-resident timing: K steps, state in HBM, one graph replay per step
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    it_v = it_p = it_cg = 0
+    with ClockSampler(clocks_path) as cs:
+        torch.cuda.synchronize()
+        barrier(world)
+        e0.record(stream)
+        eng.step(args.steps, sync=False)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    launches = eng.launch_count() - l0
+    st = eng.stats(0)
+    barrier(world)
+    ms_max = max_over_ranks(ms, world)
+    total_ps = sum_over_ranks(float(n) * args.steps, world)
+    value = total_ps / (ms_max / 1e3)
+    # ---- roofline of the dominant kernel: timed live on the current slots
+    implicit = bool(sc.param.implicit_viscosity)
+    dom = "pressure_update"
+    kms = {}
+    for k in ("pressure_update", "density_adv", "build_lists", "density_factor", "divergence_update",
+              "density_change") + (("cg_matvec",) if implicit else ()):
+        kms[k] = eng.time_kernel(KERNEL_IDS[k], reps=10)
+    # ---- end to end through the public API: pinned host state in, positions out
+    pd = m.pd
+    h_x = torch.empty_like(pd.x, device="cpu").pin_memory()
+    h_v = torch.empty_like(pd.v, device="cpu").pin_memory()
+    h_out = torch.empty_like(pd.x, device="cpu").pin_memory()
+    h_x.copy_(pd.x)
+    h_v.copy_(pd.v)
+    torch.cuda.synchronize()
+    barrier(world)
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(args.steps):
+        pd.x.copy_(h_x, non_blocking=True)
+        pd.v.copy_(h_v, non_blocking=True)
+        solver.step()
+        h_out.copy_(pd.x, non_blocking=True)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(t0.elapsed_time(t1), world)
+    e2e_val = total_ps / (e2e_ms / 1e3)
+    peaks, peak_kind = load_peaks()
+    if rank != 0:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
+    ab = ALG_BYTES[dom] * n
+    achieved = ab / (kms[dom] / 1e3) / 1e9
+    hbm = peaks["hbm_gbs"]
+    bytes_step = step_bytes(st["iterations_v"] + 1, st["iterations"] + 1, st["cg_iterations"], 0.0, implicit)
+    line = {
+        "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded numpy scene generator)",
+        "config": {"workload": sc.name, "particles": n, "fluid": sc.particles.n_fluid,
+                   "parallelism": f"replicas{world}", "l2": "inputs larger than L2" if n * 48 > 126e6 else
+                   "inputs smaller than L2; not flushed", "step_graph": "CUDA graph with while-node solver loops"},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "peak_source": f"{peak_kind} hbm_gbs",
+                     "alg_bytes_per_launch": ab, "traffic": None,
+                     "kernel_ms": kms},
+        "step_alg_bytes_per_particle": bytes_step,
+        "step_roofline_frac": bytes_step * total_ps / (ms_max / 1e3) / 1e9 / hbm,
+        "solver": {k: st[k] for k in ("iterations_v", "iterations", "cg_iterations", "avg_density_err",
+                                      "max_neighbors_seen", "dt", "status")},
+        "gpu_launches": launches,
+        "e2e": {"value": e2e_val, "unit": "particle-steps/s", "h2d_bytes_per_step": int(24 * n),
+                "d2h_bytes_per_step": int(12 * n)},
+        "clocks": cs.summary(),
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(scenes, budget_s=args.cpu_budget)
+    print(json.dumps(line))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="roofline_2m")
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,253 @@
+/*
+ * nnsph.h — C ABI of the B200 SPH step (libnnsph.so).
+ *
+ * The reference (chunleili/nonNewton) has no FFI: its step is driven through the
+ * Python object API on the global `meta` (SPH/main.py:19-23) — `meta.pd` fields
+ * (SPH/main.py:697-723), `meta.ns` (SPH/main.py:764-853) and the solver returned by
+ * `build_solver()` (SPH/main.py:196-203). The Python package `nonnewton_b200`
+ * keeps that object API and binds the entry points below with ctypes; each entry
+ * point names the reference method it replaces.
+ *
+ * Conventions
+ *  - Every function returns an int status: NN_OK (0) or a negative NN_ERR_*.
+ *    No C++ exception crosses this boundary. nn_last_error() gives a message.
+ *  - Pointers in nn_state are DEVICE pointers owned by the caller (torch tensors),
+ *    laid out in particle-id order exactly like the reference's Taichi fields.
+ *    Several scenes may be packed one after another (segmented arrays); scene s
+ *    owns ids [start, start + n).
+ *  - The context owns every scratch buffer (sorted working set, cell table,
+ *    neighbour lists, solver vectors). They are allocated by nn_ctx_create /
+ *    nn_set_scenes only; stepping allocates nothing.
+ *  - All work is enqueued on the context's stream (nn_ctx_set_stream); calls on
+ *    one context are not thread-safe, calls on distinct contexts are.
+ */
+#ifndef NNSPH_H
+#define NNSPH_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NNSPH_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+#define NN_OK                     0
+#define NN_ERR_INVALID_ARG       -1
+#define NN_ERR_CUDA              -2
+#define NN_ERR_OOM               -3
+#define NN_ERR_NEIGHBOR_OVERFLOW -4  /* a particle had more neighbours than max_neighbors */
+#define NN_ERR_NOT_CONVERGED     -5  /* reported through nn_stats, not returned by nn_step */
+#define NN_ERR_NAN               -6  /* non-finite value found in the state */
+#define NN_ERR_STATE             -7  /* call out of order (e.g. no state bound) */
+#define NN_ERR_CAPACITY          -8  /* more particles / scenes / cells than the context holds */
+
+/* ---- materials, phases (SPH/main.py:26-39, 676) -------------------------- */
+#define NN_FLUID 0
+#define NN_SOLID 1
+/* phase_id ranges used by the reference loader (SPH/main.py:633-661):
+   fluid 0.., static 1000.., rigid 2000.., elastic 3000.. */
+#define NN_PHASE_STATIC_BASE  1000
+#define NN_PHASE_RIGID_BASE   2000
+#define NN_PHASE_ELASTIC_BASE 3000
+
+/* ---- feature flags of a scene ------------------------------------------ */
+#define NN_F_SURFACE_TENSION   (1u << 0) /* SurfaceTension, SPH/main.py:1378-1414 */
+#define NN_F_VISCOSITY         (1u << 1) /* explicit ViscosityModel, SPH/main.py:1417-1468 */
+#define NN_F_NONNEWTON         (1u << 2) /* NonNewton strain rate + law, SPH/main.py:332-492 */
+#define NN_F_IMPLICIT_VISCOSITY (1u << 3) /* Weiler 2018 CG (stub at SPH/main.py:1477-1513) */
+#define NN_F_ELASTICITY        (1u << 4) /* Becker 2009, SPH/main.py:1182-1375 */
+#define NN_F_DIVERGENCE        (1u << 5) /* divergence solve, SPH/main.py:1550 */
+#define NN_F_CFL               (1u << 6) /* CFL time step (extension: the reference has none) */
+#define NN_F_QUIRKS            (1u << 7) /* reproduce the reference's documented quirks */
+#define NN_F_CARREAU_TEXTBOOK  (1u << 8) /* (1+(K g)^2)^((n-1)/2) instead of SPH/main.py:431-437 */
+
+/* non-Newtonian laws, SPH/main.py:347-355 */
+#define NN_NEWTONIAN        0
+#define NN_POWER_LAW        1
+#define NN_CROSS            2
+#define NN_CASSON           3
+#define NN_CARREAU          4
+#define NN_BINGHAM          5
+#define NN_HERSCHEL_BULKLEY 6
+
+/* Parameters of one scene. Mirrors `Parameter` (SPH/main.py:594-621), the DFSPH
+   settings (SPH/main.py:1523-1535), NonNewton.initParameters (SPH/main.py:357-368),
+   Viscosity_Weiler2018 (SPH/main.py:1479-1485) and Elasticity (SPH/main.py:1188-1189).
+   Set `size` to sizeof(nn_scene_params). */
+typedef struct nn_scene_params {
+  uint32_t size;
+  uint32_t flags;                 /* NN_F_* */
+  double domain_start[3];         /* domainStart */
+  double domain_end[3];           /* domainEnd */
+  double particle_radius;         /* particleRadius; h = 4 r (SPH/main.py:606) */
+  double support_radius;          /* h */
+  double volume0;                 /* 0.8 (2r)^3 (SPH/main.py:607) */
+  double density0;                /* rho0 */
+  double gravity[3];              /* gravitation */
+  double dt;                      /* timeStepSize (initial step when NN_F_CFL) */
+  double sticky_coeff;            /* 0.999 */
+  double collision_coeff;         /* 0.5 */
+  double padding;                 /* = h (SPH/main.py:615) */
+  double viscosity;               /* explicit model coefficient (SPH/main.py:620-621) */
+  double boundary_viscosity;      /* boundaryViscosity */
+  double surface_tension;         /* 0.01 (SPH/main.py:1382) */
+  double eps;                     /* m_eps 1e-5 (SPH/main.py:1526) */
+  int32_t max_iterations_v;       /* maxIterationsV */
+  int32_t max_iterations;         /* maxIterations */
+  double max_error_v;             /* maxErrorV, percent */
+  double max_error;               /* maxError, percent */
+  /* non-Newtonian law */
+  int32_t nonnewton_method;       /* NN_NEWTONIAN.. */
+  int32_t pad0;
+  double power_index, consistency_index, viscosity0, viscosity_inf;
+  double critical_strain_rate, mu_c, yield_stress;
+  /* implicit viscosity (Weiler 2018) */
+  int32_t visco_max_iter;
+  int32_t pad1;
+  double visco_max_error;         /* relative residual of the CG */
+  double visco_boundary;          /* viscosityBoundary (kinematic, times rho0) */
+  /* elasticity */
+  double youngs_modulus, poisson_ratio;
+  /* CFL (extension) */
+  double cfl_factor, cfl_min_dt, cfl_max_dt;
+} nn_scene_params;
+
+/* One scene of a segmented particle array. */
+typedef struct nn_scene_desc {
+  uint32_t size;                  /* sizeof(nn_scene_desc) */
+  int32_t start;                  /* first particle id of the scene */
+  int32_t n;                      /* particles of the scene */
+  int32_t n_fluid;                /* fluid particles (ids start .. start+n_fluid-1) */
+  nn_scene_params params;
+} nn_scene_desc;
+
+/* Caller-owned device state, particle-id order (ParticleData, SPH/main.py:707-723).
+   vec3 fields are [n][3] float32, scalars [n]. Optional fields may be NULL. */
+typedef struct nn_state {
+  uint32_t size;                  /* sizeof(nn_state) */
+  int32_t n;
+  float* x;                       /* [n,3] */
+  float* x_0;                     /* [n,3] rest positions (elasticity) */
+  float* v;                       /* [n,3] */
+  float* acceleration;            /* [n,3] */
+  float* volume;                  /* [n] */
+  float* m;                       /* [n] */
+  float* density;                 /* [n] */
+  float* pressure;                /* [n] (unused by DFSPH, kept for the API) */
+  float* dfsph_factor;            /* [n] */
+  float* density_adv;             /* [n] */
+  int32_t* material;              /* [n] NN_FLUID / NN_SOLID */
+  int32_t* is_dynamic;            /* [n] */
+  int32_t* phase_id;              /* [n] */
+  /* optional outputs */
+  float* strain_rate_norm;        /* [n] NonNewton.strainRateNorm */
+  float* nonnewton_viscosity;     /* [n] NonNewton.nonNewtonViscosity */
+  float* stress;                  /* [n,6] Elasticity.m_stress (Voigt 00,11,22,01,02,12) */
+  float* rotations;               /* [n,9] Elasticity.m_rotations (row-major) */
+} nn_state;
+
+/* Per-scene statistics of the last step (SPH/main.py:1704, 1785 print these). */
+typedef struct nn_stats {
+  uint32_t size;
+  int32_t status;                 /* NN_OK or NN_ERR_* seen by the device */
+  int32_t iterations_v;           /* divergence solve: counter as printed at 1704 */
+  int32_t iterations;             /* pressure solve: counter as printed at 1785 */
+  int32_t cg_iterations;          /* implicit viscosity CG iterations */
+  int32_t max_neighbors_seen;
+  double avg_density_err_v;       /* last divergence error (FP64 reduction) */
+  double avg_density_err;         /* last pressure error (FP64 reduction) */
+  double cg_residual;             /* final relative CG residual */
+  double dt;                      /* time step used by the last step */
+  double max_density;             /* printed at SPH/main.py:1548 */
+  int64_t steps;                  /* steps taken since nn_initialize */
+} nn_stats;
+
+typedef struct nn_ctx nn_ctx;
+
+/* Passes of one step, each the sm_100a replacement of a reference method. */
+enum nn_pass {
+  NN_PASS_SEARCH = 0,                 /* NeighborhoodSearchSparse.run_search, 822-829 */
+  NN_PASS_STATIC_BOUNDARY_VOLUME,     /* SPHBase.compute_static_boundary_volume, 1010-1019 */
+  NN_PASS_MOVING_BOUNDARY_VOLUME,     /* SPHBase.compute_moving_boundary_volume, 1026-1035 */
+  NN_PASS_CLEAR_ACCELERATIONS,        /* SPHBase.clear_accelerations, 942-951 */
+  NN_PASS_DENSITIES,                  /* SPHBase.compute_densities, 975-984 */
+  NN_PASS_DFSPH_FACTOR,               /* DFSPHSolver.compute_DFSPH_factor, 1569-1593 */
+  NN_PASS_DIVERGENCE_SOLVE,           /* DFSPHSolver.divergence_solve, 1683-1713 */
+  NN_PASS_NON_PRESSURE_FORCES,        /* DFSPHSolver.compute_non_pressure_forces, 1557-1567 */
+  NN_PASS_NON_PRESSURE_ADVECT,        /* DFSPHSolver.non_pressure_advect, 1843-1848 */
+  NN_PASS_PRESSURE_SOLVE,             /* DFSPHSolver.pressure_solve, 1762-1791 */
+  NN_PASS_ELASTICITY,                 /* Elasticity.substep, 1241-1244 */
+  NN_PASS_ADVECT,                     /* SPHBase.advect, 1086-1093 */
+  NN_PASS_ENFORCE_BOUNDARY,           /* SPHBase.enforce_boundary_3D (FLUID then SOLID), 936-937 */
+  NN_PASS_SUBSTEP,                    /* DFSPHSolver.substep, 1546-1555 */
+  NN_PASS_COUNT
+};
+
+/* step flags */
+#define NN_STEP_SYNC_STATE  (1u << 0)  /* write the state back to nn_state after the last step */
+#define NN_STEP_HOST_LOOP   (1u << 1)  /* drive solver loops from the host (no CUDA graph) */
+
+/* ---- context ------------------------------------------------------------
+   Replaces: initialize() allocations (SPH/main.py:1870-1895) — ParticleData sizes,
+   NeighborhoodSearchSparse.__init__ (SPH/main.py:766-791). */
+int nn_ctx_create(int32_t max_particles, int32_t max_scenes, int32_t max_neighbors,
+                  int64_t max_cells, nn_ctx** out);
+int nn_ctx_destroy(nn_ctx* ctx);
+int nn_ctx_set_stream(nn_ctx* ctx, void* cuda_stream);
+const char* nn_last_error(const nn_ctx* ctx);
+int nn_abi_version(void);
+
+/* Bind caller-owned state (meta.pd). */
+int nn_bind_state(nn_ctx* ctx, const nn_state* state);
+/* Describe the scenes packed in the bound state (segmented arrays). */
+int nn_set_scenes(nn_ctx* ctx, int32_t nscenes, const nn_scene_desc* scenes);
+
+/* solver.initialize() (SPH/main.py:957-960) and, for elastic phases, the
+   Elasticity constructor (SPH/main.py:1186-1239): rest neighbourhoods and volumes. */
+int nn_initialize(nn_ctx* ctx);
+
+/* solver.step() (SPH/main.py:915-940), nsteps times. The state is read from
+   nn_state at the start; with NN_STEP_SYNC_STATE it is written back at the end. */
+int nn_step(nn_ctx* ctx, int32_t nsteps, uint32_t flags);
+
+/* One sub-step method on the bound state (reads and writes nn_state). */
+int nn_run_pass(nn_ctx* ctx, int32_t pass);
+
+/* meta.ns.num_neighbors / meta.ns.neighbors (SPH/main.py:780-781) materialised in
+   particle-id space, each row sorted by id and padded with -1. Device outputs:
+   num_neighbors [n] int32, neighbors [n, width] int32. */
+int nn_get_neighbors(nn_ctx* ctx, int32_t* num_neighbors, int32_t* neighbors, int32_t width);
+
+/* Statistics of scene `scene` (copies from the device; synchronises the stream). */
+int nn_get_stats(nn_ctx* ctx, int32_t scene, nn_stats* out);
+
+/* Kernel launches enqueued by this context since creation (for launch accounting). */
+int64_t nn_launch_count(const nn_ctx* ctx);
+
+/* Kernels of the step that nn_time_kernel can time on their own. */
+enum nn_kernel_id {
+  NN_K_PRESSURE_UPDATE = 0,   /* pressure_solve_iteration_kernel */
+  NN_K_DENSITY_ADV,           /* compute_density_adv + FP64 error reduction */
+  NN_K_DIVERGENCE_UPDATE,     /* divergence_solver_iteration_kernel */
+  NN_K_DENSITY_CHANGE,        /* compute_density_change + FP64 error reduction */
+  NN_K_DENSITY_FACTOR,        /* compute_densities + compute_DFSPH_factor */
+  NN_K_BUILD_LISTS,           /* store_neighbors */
+  NN_K_CG_MATVEC,             /* implicit viscosity matrix-vector product */
+  NN_K_NONPRESSURE,           /* surface tension + explicit viscosity */
+  NN_K_COUNT
+};
+/* Average duration in ms of `reps` launches of one kernel on the current slots,
+   timed with CUDA events on the context stream (measurement hook, no reference
+   counterpart). Solver masks are set to "iterating" first, so the kernel does its
+   full work; it mutates solver scratch and, for the update kernels, velocities. */
+int nn_time_kernel(nn_ctx* ctx, int32_t kernel, int32_t reps, float* ms_out);
+
+/* Autotuned launch shape: threads per block for the neighbour passes. 0 = default. */
+int nn_set_block_size(nn_ctx* ctx, int32_t threads);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NNSPH_H */

@@ -1,0 +1,281 @@
+// common.cuh — device data layout, SPH kernel functions and reductions shared by
+// every pass of the B200 SPH step.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/nnsph.h"
+
+#define NN_STRIPES 32          // striped FP64 accumulators per scene and quantity
+#define NN_SCENE_SHIFT 8       // slot flags: bits 0..7 particle class, 8.. scene index
+#define NN_CLS_SOLID 1u        // material == SOLID
+#define NN_CLS_DYNAMIC 2u      // is_dynamic
+#define NN_CLS_ELASTIC 4u      // member of the elastic model
+#define NN_CLS_VALID 8u        // slot holds a particle
+
+// Constants of one scene, derived once on the host (mirrors how Taichi folds the
+// reference's Python floats into f32 literals: SPH/main.py:859-905, 1044-1051).
+struct SceneDev {
+  uint32_t flags;
+  int32_t start, n, n_fluid;      // id range
+  int64_t cell_base;              // first cell key of the scene
+  int32_t gx, gy, gz, mbits;      // grid size; rows (y,z) are Morton-ordered with mbits per axis
+  float origin[3];
+  float cell;                     // cell edge (= h)
+  float h, k_w, k2_w, k_grad, W0; // cubic spline constants
+  float rho0, inv_rho0;
+  float g[3];
+  float eps;
+  float sigma, dia2, w_dia;       // surface tension
+  float visc, visc_b, c01h2;      // explicit viscosity
+  float xmin[3], xmax[3], cf, sticky;
+  double eta_v_fac;               // maxErrorV * 0.01 * rho0 (multiplied by 1/dt)
+  double eta_p;                   // maxError * 0.01 * rho0
+  int32_t max_iter_v, max_iter, visco_max_iter, nn_method;
+  double visco_tol;
+  float nn_n, nn_K, nn_mu0, nn_muinf, nn_gc, nn_muc, nn_tauy;
+  float mu_newton;                // viscosity * rho0 (implicit solver without a law)
+  float mu_b;                     // visco_boundary * rho0
+  float el_cd, el_co, el_cs;      // isotropic C of Becker 2009 (SPH/main.py:1276-1283)
+  int32_t el_mult;                // elastic substeps per step (quirk: one per elastic phase)
+  float cfl_factor, cfl_min_dt, cfl_max_dt, diameter;
+};
+
+// Mutable per-scene state on the device.
+struct SceneDyn {
+  float dt, inv_dt;               // time step and f32(1/dt)
+  float inv_dt2;                  // f32(1/(dt*dt))
+  int32_t it_v, it_p, it_cg;      // loop counters (reference semantics)
+  int32_t act_v, act_p, act_cg;   // 1 while the scene still iterates
+  int32_t status;                 // first NN_ERR_* seen
+  int32_t max_nb;                 // max neighbour count of the last search
+  uint32_t max_density_bits;      // float bits (densities are positive)
+  uint32_t vmax_bits;             // float bits of max |v| (CFL)
+  double avg_v, avg_p;            // last average density errors
+  double cg_rz, cg_bnorm2, cg_rel;
+  int32_t div_ran;                // divergence solve ran this step (alpha bookkeeping)
+  int32_t pad;
+  double cg_alpha, cg_beta;       // PCG scalars of the current iteration
+  int64_t steps;
+};
+
+// Accumulator slots per scene (each NN_STRIPES doubles).
+enum { ACC_ERR = 0, ACC_RZ, ACC_PAP, ACC_RR, ACC_BB, ACC_COUNT };
+
+struct Vec3 { float x, y, z; };
+__device__ __forceinline__ float3 f3(float4 a) { return make_float3(a.x, a.y, a.z); }
+__device__ __forceinline__ float3 operator-(float3 a, float3 b) { return make_float3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float3 operator+(float3 a, float3 b) { return make_float3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ float3 operator*(float3 a, float s) { return make_float3(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ float3 operator-(float3 a) { return make_float3(-a.x, -a.y, -a.z); }
+__device__ __forceinline__ void operator+=(float3& a, float3 b) { a.x += b.x; a.y += b.y; a.z += b.z; }
+__device__ __forceinline__ void operator-=(float3& a, float3 b) { a.x -= b.x; a.y -= b.y; a.z -= b.z; }
+__device__ __forceinline__ float dot3(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+
+// Exact f32 distance as the reference computes it for the in-range test:
+// (x_i - x_j).norm() < support_radius (SPH/main.py:845), no FMA contraction.
+__device__ __forceinline__ float exact_norm(float3 r) {
+  float s = __fadd_rn(__fadd_rn(__fmul_rn(r.x, r.x), __fmul_rn(r.y, r.y)), __fmul_rn(r.z, r.z));
+  return __fsqrt_rn(s);
+}
+
+// cubic_kernel, SPH/main.py:859-880
+__device__ __forceinline__ float kernel_w(float rn, const SceneDev& s) {
+  float q = rn / s.h;
+  float res = 0.f;
+  if (q <= 1.f) {
+    if (q <= 0.5f) {
+      float q2 = q * q;
+      float q3 = q2 * q;
+      res = s.k_w * (6.f * q3 - 6.f * q2 + 1.f);
+    } else {
+      float t = 1.f - q;
+      res = s.k2_w * (t * t * t);
+    }
+  }
+  return res;
+}
+
+// cubic_kernel_derivative, SPH/main.py:883-905 (rn = |r| passed in)
+__device__ __forceinline__ float3 kernel_grad(float3 r, float rn, const SceneDev& s) {
+  float q = rn / s.h;
+  float3 res = make_float3(0.f, 0.f, 0.f);
+  if (rn > 1e-5f && q <= 1.f) {
+    float den = rn * s.h;
+    float3 gq = make_float3(r.x / den, r.y / den, r.z / den);
+    float f;
+    if (q <= 0.5f) {
+      f = s.k_grad * q * (3.f * q - 2.f);
+    } else {
+      float t = 1.f - q;
+      f = s.k_grad * (-t * t);
+    }
+    res = gq * f;
+  }
+  return res;
+}
+
+__device__ __forceinline__ int slot_scene(uint32_t fl) { return (int)(fl >> NN_SCENE_SHIFT); }
+__device__ __forceinline__ bool cls_fluid(uint32_t fl) { return (fl & (NN_CLS_VALID | NN_CLS_SOLID)) == NN_CLS_VALID; }
+__device__ __forceinline__ bool cls_solid(uint32_t fl) { return (fl & NN_CLS_SOLID) != 0; }
+__device__ __forceinline__ bool cls_dyn_solid(uint32_t fl) { return (fl & (NN_CLS_SOLID | NN_CLS_DYNAMIC)) == (NN_CLS_SOLID | NN_CLS_DYNAMIC); }
+__device__ __forceinline__ bool cls_static_solid(uint32_t fl) { return (fl & (NN_CLS_SOLID | NN_CLS_DYNAMIC)) == NN_CLS_SOLID; }
+
+__device__ __forceinline__ void set_status(SceneDyn* dyn, int code) { atomicCAS(&dyn->status, 0, code); }
+
+// Per-scene FP64 sum of `val` over a warp: scene-uniform warps reduce with shuffles
+// and issue one atomic on a striped accumulator; mixed warps fall back to per-lane
+// atomics. Must be called by all 32 lanes (invalid lanes pass valid=false).
+__device__ __forceinline__ void scene_add(double* acc, int quantity, int nscenes_stride, int scene, bool valid,
+                                          double val) {
+  const unsigned full = 0xffffffffu;
+  int key = valid ? scene : -1;
+  int k0 = __shfl_sync(full, key, 0);
+  // find any valid scene in the warp to compare against
+  unsigned vb = __ballot_sync(full, valid);
+  if (vb == 0) return;
+  int leader = __ffs(vb) - 1;
+  int sl = __shfl_sync(full, key, leader);
+  bool uniform = __all_sync(full, !valid || key == sl);
+  (void)k0;
+  int lane = threadIdx.x & 31;
+  int stripe = ((blockIdx.x * (blockDim.x >> 5)) + (threadIdx.x >> 5)) & (NN_STRIPES - 1);
+  if (uniform) {
+    double v = valid ? val : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(full, v, o);
+    if (lane == leader) atomicAdd(&acc[((size_t)sl * ACC_COUNT + quantity) * NN_STRIPES + stripe], v);
+  } else if (valid) {
+    atomicAdd(&acc[((size_t)scene * ACC_COUNT + quantity) * NN_STRIPES + stripe], val);
+  }
+  (void)nscenes_stride;
+}
+
+// Warp-aggregated atomicMax: lanes that target the same address combine first.
+// Must be called by all 32 lanes.
+__device__ __forceinline__ void warp_max_to(unsigned* addr, unsigned val, bool valid) {
+  const unsigned full = 0xffffffffu;
+  unsigned long long key = valid ? (unsigned long long)addr : 0ull;
+  unsigned peers = __match_any_sync(full, key);
+  unsigned r = __reduce_max_sync(peers, valid ? val : 0u);
+  if (valid && (int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicMax(addr, r);
+}
+__device__ __forceinline__ void warp_max_to(int* addr, int val, bool valid) {
+  warp_max_to(reinterpret_cast<unsigned*>(addr), (unsigned)max(val, 0), valid);
+}
+
+__device__ __forceinline__ bool scene_implicit(const SceneDev& s) {
+  return (s.flags & NN_F_IMPLICIT_VISCOSITY) && !(s.flags & NN_F_QUIRKS);
+}
+
+__device__ __forceinline__ double acc_sum(const double* acc, int scene, int quantity) {
+  const double* a = &acc[((size_t)scene * ACC_COUNT + quantity) * NN_STRIPES];
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < NN_STRIPES; ++k) s += a[k];
+  return s;
+}
+__device__ __forceinline__ void acc_zero(double* acc, int scene, int quantity) {
+  double* a = &acc[((size_t)scene * ACC_COUNT + quantity) * NN_STRIPES];
+#pragma unroll
+  for (int k = 0; k < NN_STRIPES; ++k) a[k] = 0.0;
+}
+
+// Rotation of the polar decomposition (semantics of ti.polar_decompose used at
+// SPH/main.py:1273): SVD with U, V in SO(3), R = U V^T, computed in double with a
+// cyclic Jacobi eigen-decomposition of A^T A (same algorithm as the CPU oracle).
+__device__ inline void closest_rotation(const double A[3][3], double R[3][3]) {
+  double S[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) S[i][j] = A[0][i] * A[0][j] + A[1][i] * A[1][j] + A[2][i] * A[2][j];
+  double V[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+  for (int sweep = 0; sweep < 12; ++sweep) {
+    double off = S[0][1] * S[0][1] + S[0][2] * S[0][2] + S[1][2] * S[1][2];
+    double diag = S[0][0] * S[0][0] + S[1][1] * S[1][1] + S[2][2] * S[2][2];
+    if (off <= 1e-30 * diag || off == 0.0) break;
+#pragma unroll
+    for (int pq = 0; pq < 3; ++pq) {
+      const int p = pq == 2 ? 1 : 0;
+      const int q = pq == 0 ? 1 : 2;
+      double apq = S[p][q];
+      if (apq == 0.0) continue;
+      double theta = (S[q][q] - S[p][p]) / (2.0 * apq);
+      double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+      double c = 1.0 / sqrt(t * t + 1.0), sn = t * c;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        double skp = S[k][p], skq = S[k][q];
+        S[k][p] = c * skp - sn * skq;
+        S[k][q] = sn * skp + c * skq;
+      }
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        double spk = S[p][k], sqk = S[q][k];
+        S[p][k] = c * spk - sn * sqk;
+        S[q][k] = sn * spk + c * sqk;
+      }
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        double vkp = V[k][p], vkq = V[k][q];
+        V[k][p] = c * vkp - sn * vkq;
+        V[k][q] = sn * vkp + c * vkq;
+      }
+    }
+  }
+  double lam[3] = {S[0][0], S[1][1], S[2][2]};
+  int idx[3] = {0, 1, 2};
+  // order by descending eigenvalue (same comparisons as the CPU oracle)
+  for (int i = 0; i < 2; ++i)
+    for (int j = i + 1; j < 3; ++j)
+      if (lam[idx[j]] > lam[idx[i]]) { int t = idx[i]; idx[i] = idx[j]; idx[j] = t; }
+  double Vs[3][3], sig[3];
+  for (int c = 0; c < 3; ++c) {
+    sig[c] = sqrt(fmax(lam[idx[c]], 0.0));
+    for (int r = 0; r < 3; ++r) Vs[r][c] = V[r][idx[c]];
+  }
+  double detV = Vs[0][0] * (Vs[1][1] * Vs[2][2] - Vs[1][2] * Vs[2][1]) -
+                Vs[0][1] * (Vs[1][0] * Vs[2][2] - Vs[1][2] * Vs[2][0]) +
+                Vs[0][2] * (Vs[1][0] * Vs[2][1] - Vs[1][1] * Vs[2][0]);
+  if (detV < 0)
+    for (int r = 0; r < 3; ++r) Vs[r][2] = -Vs[r][2];
+  if (!(sig[0] > 1e-30)) {
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) R[i][j] = (i == j) ? 1.0 : 0.0;
+    return;
+  }
+  const double tiny = 1e-12 * sig[0];
+  double u0[3], u1[3], u2[3];
+  for (int r = 0; r < 3; ++r) u0[r] = (A[r][0] * Vs[0][0] + A[r][1] * Vs[1][0] + A[r][2] * Vs[2][0]) / sig[0];
+  double n0 = sqrt(u0[0] * u0[0] + u0[1] * u0[1] + u0[2] * u0[2]);
+  for (int r = 0; r < 3; ++r) u0[r] /= n0;
+  if (sig[1] > tiny) {
+    for (int r = 0; r < 3; ++r) u1[r] = A[r][0] * Vs[0][1] + A[r][1] * Vs[1][1] + A[r][2] * Vs[2][1];
+  } else {
+    int m = (fabs(u0[0]) < fabs(u0[1])) ? (fabs(u0[0]) < fabs(u0[2]) ? 0 : 2) : (fabs(u0[1]) < fabs(u0[2]) ? 1 : 2);
+    u1[0] = u1[1] = u1[2] = 0;
+    u1[m] = 1;
+  }
+  double d = u1[0] * u0[0] + u1[1] * u0[1] + u1[2] * u0[2];
+  for (int r = 0; r < 3; ++r) u1[r] -= d * u0[r];
+  double n1 = sqrt(u1[0] * u1[0] + u1[1] * u1[1] + u1[2] * u1[2]);
+  for (int r = 0; r < 3; ++r) u1[r] /= n1;
+  u2[0] = u0[1] * u1[2] - u0[2] * u1[1];
+  u2[1] = u0[2] * u1[0] - u0[0] * u1[2];
+  u2[2] = u0[0] * u1[1] - u0[1] * u1[0];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) R[i][j] = u0[i] * Vs[j][0] + u1[i] * Vs[j][1] + u2[i] * Vs[j][2];
+}
+
+// Morton interleave of two 16-bit row coordinates (y, z)
+__device__ __host__ __forceinline__ uint32_t morton2(uint32_t a, uint32_t b) {
+  auto spread = [](uint32_t v) {
+    v &= 0xffffu;
+    v = (v | (v << 8)) & 0x00ff00ffu;
+    v = (v | (v << 4)) & 0x0f0f0f0fu;
+    v = (v | (v << 2)) & 0x33333333u;
+    v = (v | (v << 1)) & 0x55555555u;
+    return v;
+  };
+  return spread(a) | (spread(b) << 1);
+}

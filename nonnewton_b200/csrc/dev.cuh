@@ -1,0 +1,71 @@
+// dev.cuh — device pointer bundle passed by value to every kernel.
+#pragma once
+#include "common.cuh"
+
+// Sorted working set: particles in cell order ("slots").
+struct WorkSet {
+  float4* pos;      // x, y, z, volume
+  float4* vel;      // v (w unused)
+  float* mass;
+  float* dens;
+  uint32_t* flags;  // class bits | scene << NN_SCENE_SHIFT
+  int32_t* id;      // particle id of the slot
+};
+
+// Caller-owned state in particle-id order (meta.pd).
+struct Truth {
+  float* x; float* x_0; float* v; float* a;
+  float* volume; float* m; float* density; float* dfsph_factor; float* density_adv;
+  int32_t* material; int32_t* is_dynamic; int32_t* phase_id;
+  float* srn; float* mu; float* stress; float* rot;
+};
+
+struct Dev {
+  // sizes (device-resident so a captured graph serves any batch composition)
+  const int32_t* d_n;          // [0] particles, [1] scenes, [2] total cells, [3] elastic particles
+  const SceneDev* sc;
+  SceneDyn* dyn;
+  double* acc;                 // [scene][ACC_COUNT][NN_STRIPES]
+  const int32_t* scene_of_id;  // scene of each particle id
+  Truth t;
+  WorkSet w;                   // current sorted set
+  WorkSet wo;                  // previous sorted set (resident re-sort source)
+  const int32_t* src_from_truth; // device flag: 1 = gather from Truth, 0 = from wo
+  float4* acc4;                // accelerations (slot order)
+  float* alpha;
+  float* rho_adv;
+  float* kappa;
+  int32_t* slot_of_id;
+  // neighbour search
+  uint32_t* key;               // per source index
+  uint32_t* rank;              // per source index
+  int32_t* src;                // source index of each new slot
+  uint32_t* cell_count;        // [cells + 1] counts, then exclusive starts
+  uint32_t* tile_sums;
+  int32_t* nbr;                // [max_nb][cap]
+  int32_t* nbr_cnt;            // [cap]
+  int32_t cap;                 // slot capacity (neighbour list stride)
+  int32_t max_nb;
+  // non-Newtonian
+  float* srn;
+  float* mu;
+  // implicit viscosity CG (slot order)
+  float4* cg_x; float4* cg_r; float4* cg_z; float4* cg_p; float4* cg_Ap; float4* cg_b;
+  float4* cg_aux;              // mu_i, m_i / rho_i
+  float* cg_pinv;              // [6][cap] symmetric inverse of the diagonal block
+  // elasticity (e-space: elastic particles in id order)
+  int32_t* el_id;              // [Ne] particle id
+  int32_t* el_slot;            // [Ne] current slot
+  int32_t* e_of_id;            // [cap] elastic index or -1
+  float4* el_x0;               // [Ne] rest position, rest volume
+  int32_t* el_nb;              // [rest_cap][Ne] rest neighbours (elastic indices)
+  int32_t* el_cnt;             // [Ne]
+  int32_t el_cap;              // rest list capacity
+  int32_t el_stride;           // Ne capacity
+  float* el_R;                 // [9][Ne]
+  float* el_S;                 // [6][Ne]
+  // loop control
+  int32_t* any_active;         // host-visible flag of the last check
+  unsigned long long loop_handle; // cudaGraphConditionalHandle (0 when not in a graph)
+  int32_t* body_count;         // [4] executed loop bodies (div, pressure, cg, elastic)
+};

@@ -1,0 +1,886 @@
+// nnsph.cu — libnnsph.so: context, C ABI (include/nnsph.h) and step orchestration.
+//
+// One step (SPHBase.step, SPH/main.py:915-940) is a fixed sequence of kernels; the
+// three data-dependent solver loops (divergence, implicit-viscosity CG, pressure)
+// become CUDA-graph while-nodes whose condition is set on the device by the loop's
+// check kernel, so a step runs without a host round-trip. A host-driven mode (one
+// stream sync per iteration, like the reference's Python loops) is kept for the
+// per-pass API and as a fallback.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "ns.cuh"
+#include "sph.cuh"
+
+namespace {
+
+constexpr double kPi = 3.14159265358979323846;
+
+enum SyncMask : uint32_t {
+  SM_X = 1, SM_V = 2, SM_A = 4, SM_VOL = 8, SM_DENS = 16, SM_ALPHA = 32, SM_RHOADV = 64, SM_NNV = 128, SM_MASS = 256,
+  SM_ALL = 511
+};
+
+template <typename T>
+cudaError_t dalloc(T** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) return cudaSuccess;
+  return cudaMalloc((void**)p, count * sizeof(T));
+}
+
+}  // namespace
+
+struct nn_ctx {
+  int cap = 0, max_scenes = 0, max_nb = 0;
+  int64_t max_cells = 0;
+  int dev_id = 0, sms = 148;
+  cudaStream_t stream = nullptr;      // caller stream (0 = legacy default)
+  cudaStream_t side = nullptr;        // capture stream for loop bodies
+  std::string err;
+  int64_t launches = 0;
+  int block = 256;
+  // state binding and scenes
+  nn_state state{};
+  bool bound = false;
+  std::vector<nn_scene_desc> scenes;
+  std::vector<SceneDev> sdev;
+  int n = 0, ncells = 0, ne = 0;
+  bool any_fluid = false, any_div = false, any_nonnewton = false, any_implicit = false, any_cfl = false;
+  int el_mult_max = 0;
+  // device buffers
+  WorkSet set[2]{};
+  int cur = 0;                         // set holding the current slots
+  bool searched = false;
+  int32_t* d_n = nullptr;
+  SceneDev* d_sc = nullptr;
+  SceneDyn* d_dyn = nullptr;
+  double* d_acc = nullptr;
+  int32_t* d_scene_of_id = nullptr;
+  int32_t* d_src_flag = nullptr;
+  float4* acc4 = nullptr;
+  float *alpha = nullptr, *rho_adv = nullptr, *kappa = nullptr, *srn = nullptr, *mu = nullptr;
+  int32_t* slot_of_id = nullptr;
+  uint32_t *key = nullptr, *rank = nullptr, *cell_count = nullptr, *tile_sums = nullptr;
+  int32_t *src = nullptr, *nbr = nullptr, *nbr_cnt = nullptr;
+  float4 *cg_x = nullptr, *cg_r = nullptr, *cg_z = nullptr, *cg_p = nullptr, *cg_Ap = nullptr, *cg_b = nullptr,
+         *cg_aux = nullptr;
+  float* cg_pinv = nullptr;
+  int el_cap = 64, el_stride = 0;
+  int32_t *el_id = nullptr, *el_slot = nullptr, *e_of_id = nullptr, *el_nb = nullptr, *el_cnt = nullptr;
+  float4* el_x0 = nullptr;
+  float *el_R = nullptr, *el_S = nullptr;
+  int32_t* d_any = nullptr;
+  int32_t* h_any = nullptr;            // pinned
+  int32_t* d_body = nullptr;
+  int64_t fixed_nodes_per_step = 0;    // kernel nodes outside loop bodies (graph mode)
+  int64_t graph_replays = 0;
+  int64_t body_nodes[3] = {3, 3, 5};   // kernels per loop body: divergence, pressure, CG
+  // graphs: [parity]
+  cudaGraphExec_t exec[2] = {nullptr, nullptr};
+  bool in_capture = false;
+  unsigned long long cur_handle = 0;
+  int64_t capture_nodes = 0;
+  std::map<const void*, int> occ;      // blocks per SM per kernel
+};
+
+static thread_local char g_err[512];
+
+static int fail(nn_ctx* c, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (c) c->err = buf;
+  snprintf(g_err, sizeof(g_err), "%s", buf);
+  return code;
+}
+
+#define CK(call)                                                                              \
+  do {                                                                                        \
+    cudaError_t _e = (call);                                                                  \
+    if (_e != cudaSuccess) return fail(c, NN_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(_e), __FILE__, __LINE__); \
+  } while (0)
+
+static Dev make_dev(nn_ctx* c, int cur) {
+  Dev d{};
+  d.d_n = c->d_n;
+  d.sc = c->d_sc;
+  d.dyn = c->d_dyn;
+  d.acc = c->d_acc;
+  d.scene_of_id = c->d_scene_of_id;
+  const nn_state& s = c->state;
+  d.t = Truth{s.x, s.x_0, s.v, s.acceleration, s.volume, s.m, s.density, s.dfsph_factor, s.density_adv,
+              s.material, s.is_dynamic, s.phase_id, s.strain_rate_norm, s.nonnewton_viscosity, s.stress, s.rotations};
+  d.w = c->set[cur];
+  d.wo = c->set[1 - cur];
+  d.src_from_truth = c->d_src_flag;
+  d.acc4 = c->acc4;
+  d.alpha = c->alpha;
+  d.rho_adv = c->rho_adv;
+  d.kappa = c->kappa;
+  d.slot_of_id = c->slot_of_id;
+  d.key = c->key;
+  d.rank = c->rank;
+  d.src = c->src;
+  d.cell_count = c->cell_count;
+  d.tile_sums = c->tile_sums;
+  d.nbr = c->nbr;
+  d.nbr_cnt = c->nbr_cnt;
+  d.cap = c->cap;
+  d.max_nb = c->max_nb;
+  d.srn = c->srn;
+  d.mu = c->mu;
+  d.cg_x = c->cg_x; d.cg_r = c->cg_r; d.cg_z = c->cg_z; d.cg_p = c->cg_p; d.cg_Ap = c->cg_Ap; d.cg_b = c->cg_b;
+  d.cg_aux = c->cg_aux;
+  d.cg_pinv = c->cg_pinv;
+  d.el_id = c->el_id; d.el_slot = c->el_slot; d.e_of_id = c->e_of_id; d.el_x0 = c->el_x0;
+  d.el_nb = c->el_nb; d.el_cnt = c->el_cnt; d.el_cap = c->el_cap; d.el_stride = c->el_stride;
+  d.el_R = c->el_R; d.el_S = c->el_S;
+  d.any_active = c->d_any;
+  d.loop_handle = c->cur_handle;
+  d.body_count = c->d_body;
+  return d;
+}
+
+// Launch helpers: grids are a multiple of the SM count (resident blocks per SM from
+// the occupancy calculator), capped by the work; kernels grid-stride over device sizes.
+template <typename... KArgs, typename... Args>
+static int launch(nn_ctx* c, cudaStream_t s, void (*k)(KArgs...), int block, int work, Args... args) {
+  auto it = c->occ.find((const void*)k);
+  int per_sm;
+  if (it == c->occ.end()) {
+    per_sm = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, block, 0);
+    per_sm = std::max(per_sm, 1);
+    c->occ[(const void*)k] = per_sm;
+  } else {
+    per_sm = it->second;
+  }
+  int64_t want = ((int64_t)std::max(work, 1) + block - 1) / block;
+  int grid = (int)std::min<int64_t>(want, (int64_t)c->sms * per_sm);
+  grid = std::max(grid, 1);
+  k<<<grid, block, 0, s>>>(args...);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(c, NN_ERR_CUDA, "kernel launch: %s", cudaGetErrorString(e));
+  if (c->in_capture) c->capture_nodes++;
+  else c->launches++;
+  return NN_OK;
+}
+template <typename... KArgs, typename... Args>
+static int launch1(nn_ctx* c, cudaStream_t s, void (*k)(KArgs...), Args... args) {
+  k<<<1, 256, 0, s>>>(args...);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(c, NN_ERR_CUDA, "kernel launch: %s", cudaGetErrorString(e));
+  if (c->in_capture) c->capture_nodes++;
+  else c->launches++;
+  return NN_OK;
+}
+
+#define RC(x)                 \
+  do {                        \
+    int _r = (x);             \
+    if (_r != NN_OK) return _r; \
+  } while (0)
+
+template <typename... KArgs, typename... Args>
+static int launch_g(nn_ctx* c, cudaStream_t s, void (*k)(KArgs...), int grid, int block, Args... args) {
+  k<<<std::max(grid, 1), block, 0, s>>>(args...);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(c, NN_ERR_CUDA, "kernel launch: %s", cudaGetErrorString(e));
+  if (c->in_capture) c->capture_nodes++;
+  else c->launches++;
+  return NN_OK;
+}
+
+// Data-dependent solver loop. In a capture, `pre` runs in the parent graph (it may
+// set the loop condition) and `body` becomes the body of a CUDA-graph while-node;
+// otherwise both run from the host with one synchronisation per iteration.
+// Body launches are counted per execution on the device (body_count).
+template <typename Pre, typename Body>
+static int solver_loop(nn_ctx* c, cudaStream_t s, bool check_first, Pre pre, Body body) {
+  if (c->in_capture) {
+    cudaStreamCaptureStatus st;
+    cudaGraph_t g;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    CK(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nd));
+    cudaGraphConditionalHandle h;
+    CK(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+    c->cur_handle = (unsigned long long)h;
+    int rc = pre(s);
+    if (rc != NN_OK) { c->cur_handle = 0; return rc; }
+    CK(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nd));
+    cudaGraphNodeParams p{};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = h;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    cudaGraphNode_t node;
+    CK(cudaGraphAddNode(&node, g, deps, nd, &p));
+    cudaGraph_t bodyg = p.conditional.phGraph_out[0];
+    CK(cudaStreamBeginCaptureToGraph(c->side, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    int64_t before = c->capture_nodes;
+    rc = body(c->side);
+    c->capture_nodes = before;
+    c->cur_handle = 0;
+    cudaGraph_t out;
+    cudaError_t e = cudaStreamEndCapture(c->side, &out);
+    if (rc != NN_OK) return rc;
+    if (e != cudaSuccess) return fail(c, NN_ERR_CUDA, "loop body capture: %s", cudaGetErrorString(e));
+    CK(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+    return NN_OK;
+  }
+  RC(pre(s));
+  if (check_first) {
+    CK(cudaMemcpyAsync(c->h_any, c->d_any, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (!*c->h_any) return NN_OK;
+  }
+  for (int it = 0; it < 1000000; ++it) {
+    int64_t before = c->launches;
+    RC(body(s));
+    c->launches = before;
+    CK(cudaMemcpyAsync(c->h_any, c->d_any, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (!*c->h_any) break;
+  }
+  return NN_OK;
+}
+
+// ---- pass sequences ---------------------------------------------------------------
+// NeighborhoodSearchSparse.run_search (SPH/main.py:822-829): the new slots go into the
+// other working set; the source (caller state or previous slots) is a device flag.
+static int enq_search(nn_ctx* c, cudaStream_t s) {
+  c->cur = 1 - c->cur;
+  Dev d = make_dev(c, c->cur);
+  const int B = 256;
+  const int tiles = (c->ncells + 1 + SCAN_TILE - 1) / SCAN_TILE;
+  RC(launch(c, s, k_zero_cells, B, c->ncells + 1, d));
+  RC(launch(c, s, k_keys, B, c->n, d));
+  RC(launch_g(c, s, k_scan_tiles, std::min(tiles, c->sms * 2), SCAN_THREADS, d));
+  RC(launch_g(c, s, k_scan_sums, 1, SCAN_THREADS, d));
+  RC(launch_g(c, s, k_scan_apply, std::min(tiles, c->sms * 2), SCAN_THREADS, d));
+  RC(launch(c, s, k_scatter, B, c->n, d));
+  RC(launch(c, s, k_cell_sort, B, c->ncells, d));
+  RC(launch(c, s, k_gather, B, c->n, d));
+  RC(launch(c, s, k_build_lists, c->block, c->n, d));
+  c->searched = true;
+  return NN_OK;
+}
+
+static int enq_divergence(nn_ctx* c, cudaStream_t s) {
+  Dev d = make_dev(c, c->cur);
+  const int B = c->block;
+  RC(launch1(c, s, k_solver_begin, d, 0));
+  RC(solver_loop(c, s, false,
+                 [&](cudaStream_t q) { return launch(c, q, k_density_change, B, c->n, make_dev(c, c->cur), 0); },
+                 [&](cudaStream_t q) {
+                   Dev e = make_dev(c, c->cur);
+                   RC(launch(c, q, k_divergence_update, B, c->n, e));
+                   RC(launch(c, q, k_density_change, B, c->n, e, 1));
+                   return launch1(c, q, k_solver_check, e, 0);
+                 }));
+  return launch(c, s, k_alpha_times_dt, 256, c->n, d);
+}
+
+static int enq_pressure(nn_ctx* c, cudaStream_t s) {
+  Dev d = make_dev(c, c->cur);
+  const int B = c->block;
+  RC(launch1(c, s, k_solver_begin, d, 1));
+  return solver_loop(c, s, false,
+                     [&](cudaStream_t q) { return launch(c, q, k_density_adv, B, c->n, make_dev(c, c->cur), 0); },
+                     [&](cudaStream_t q) {
+                       Dev e = make_dev(c, c->cur);
+                       RC(launch(c, q, k_pressure_update, B, c->n, e));
+                       RC(launch(c, q, k_density_adv, B, c->n, e, 1));
+                       return launch1(c, q, k_solver_check, e, 1);
+                     });
+}
+
+static int enq_nonpressure(nn_ctx* c, cudaStream_t s, int advect) {
+  Dev d = make_dev(c, c->cur);
+  const int B = c->block;
+  if (c->any_nonnewton) RC(launch(c, s, k_strain_rate, B, c->n, d));
+  RC(launch(c, s, k_nonpressure, B, c->n, d, advect));
+  if (c->any_implicit) {
+    RC(launch(c, s, k_cg_aux, 256, c->n, d));
+    RC(launch(c, s, k_cg_setup, B, c->n, d));
+    RC(solver_loop(c, s, true, [&](cudaStream_t q) { return launch1(c, q, k_cg_check0, make_dev(c, c->cur)); },
+                   [&](cudaStream_t q) {
+                     Dev e = make_dev(c, c->cur);
+                     RC(launch(c, q, k_cg_matvec, B, c->n, e));
+                     RC(launch1(c, q, k_cg_alpha, e));
+                     RC(launch(c, q, k_cg_update, 256, c->n, e));
+                     RC(launch1(c, q, k_cg_check, e));
+                     return launch(c, q, k_cg_pupdate, 256, c->n, e);
+                   }));
+    RC(launch(c, s, k_cg_finish, 256, c->n, d, advect));
+  }
+  return NN_OK;
+}
+
+static int enq_elastic(nn_ctx* c, cudaStream_t s) {
+  if (c->el_mult_max <= 0 || c->ne == 0) return NN_OK;
+  Dev d = make_dev(c, c->cur);
+  RC(launch(c, s, k_el_slots, 256, c->ne, d));
+  for (int rep = 0; rep < c->el_mult_max; ++rep) {
+    RC(launch(c, s, k_el_rotations, 128, c->ne, d, rep));
+    RC(launch(c, s, k_el_stress, 128, c->ne, d, rep));
+    RC(launch(c, s, k_el_forces, 128, c->ne, d, rep));
+  }
+  return NN_OK;
+}
+
+// DFSPHSolver.substep (SPH/main.py:1546-1555); non_pressure_advect fused.
+static int enq_substep(nn_ctx* c, cudaStream_t s) {
+  if (!c->any_fluid) return NN_OK;
+  Dev d = make_dev(c, c->cur);
+  RC(launch(c, s, k_density_factor, c->block, c->n, d, 1, 1));
+  if (c->any_div) RC(enq_divergence(c, s));
+  RC(launch(c, s, k_clear_acc, 256, c->n, d));
+  RC(enq_nonpressure(c, s, 1));
+  return enq_pressure(c, s);
+}
+
+// SPHBase.step (SPH/main.py:915-937)
+static int enq_step(nn_ctx* c, cudaStream_t s) {
+  RC(launch1(c, s, k_step_reset, make_dev(c, c->cur)));
+  RC(enq_search(c, s));
+  Dev d = make_dev(c, c->cur);
+  RC(launch1(c, s, k_step_dt, d, 1));
+  RC(launch(c, s, k_boundary_volume, c->block, c->n, d, 1));
+  RC(launch(c, s, k_clear_acc, 256, c->n, d));
+  RC(enq_substep(c, s));
+  RC(enq_elastic(c, s));
+  RC(launch(c, s, k_advect_boundary, 256, c->n, d, 1, 1));
+  return launch1(c, s, k_step_end, d);
+}
+
+static int enq_sync_out(nn_ctx* c, cudaStream_t s, uint32_t mask) {
+  Dev d = make_dev(c, c->cur);
+  RC(launch(c, s, k_sync_out, 256, c->n, d, mask));
+  if (c->ne > 0 && (c->state.stress || c->state.rotations)) RC(launch(c, s, k_sync_out_elastic, 256, c->ne, d));
+  return NN_OK;
+}
+
+static cudaStream_t run_stream(nn_ctx* c) { return c->stream ? c->stream : c->side ? c->side : nullptr; }
+
+static void drop_graphs(nn_ctx* c) {
+  for (int p = 0; p < 2; ++p)
+    if (c->exec[p]) { cudaGraphExecDestroy(c->exec[p]); c->exec[p] = nullptr; }
+}
+
+static int capture_step(nn_ctx* c, cudaStream_t s, int parity) {
+  const int saved = c->cur;
+  c->cur = parity;
+  c->in_capture = true;
+  c->capture_nodes = 0;
+  CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  int rc = enq_step(c, s);
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture(s, &g);
+  c->in_capture = false;
+  c->cur = saved;
+  if (rc != NN_OK) { if (g) cudaGraphDestroy(g); return rc; }
+  if (e != cudaSuccess) return fail(c, NN_ERR_CUDA, "step capture: %s", cudaGetErrorString(e));
+  e = cudaGraphInstantiate(&c->exec[parity], g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return fail(c, NN_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+  c->fixed_nodes_per_step = c->capture_nodes;
+  return NN_OK;
+}
+
+// ---- scene setup ----------------------------------------------------------------------
+static float host_kernel_w(float rn, float h, float k_w, float k2_w) {
+  float q = rn / h;
+  float res = 0.f;
+  if (q <= 1.f) {
+    if (q <= 0.5f) {
+      float q2 = q * q;
+      float q3 = q2 * q;
+      res = k_w * (6.f * q3 - 6.f * q2 + 1.f);
+    } else {
+      float t = 1.f - q;
+      res = k2_w * (t * t * t);
+    }
+  }
+  return res;
+}
+
+static SceneDev make_scene(const nn_scene_desc& sd, int64_t cell_base, int el_mult) {
+  const nn_scene_params& p = sd.params;
+  SceneDev s{};
+  s.flags = p.flags;
+  s.start = sd.start;
+  s.n = sd.n;
+  s.n_fluid = sd.n_fluid;
+  s.cell_base = cell_base;
+  const double h = p.support_radius;
+  int g[3];
+  for (int k = 0; k < 3; ++k) {
+    s.origin[k] = (float)(p.domain_start[k] - 2.0 * h);
+    double ext = (p.domain_end[k] - p.domain_start[k]) + 4.0 * h;
+    g[k] = (int)std::min(65535.0, std::max(1.0, std::ceil(ext / h) + 1.0));
+  }
+  s.gx = g[0]; s.gy = g[1]; s.gz = g[2];
+  int mb = 0;
+  while ((1 << mb) < std::max(g[1], g[2])) ++mb;
+  s.mbits = mb;
+  s.cell = (float)h;
+  s.h = (float)h;
+  const double k = 8.0 / kPi / (h * h * h);
+  s.k_w = (float)k;
+  s.k2_w = (float)(k * 2.0);
+  s.k_grad = (float)(6.0 * (8.0 / kPi) / (h * h * h));
+  s.W0 = host_kernel_w(0.f, s.h, s.k_w, s.k2_w);
+  s.rho0 = (float)p.density0;
+  s.inv_rho0 = (float)(1.0 / p.density0);
+  for (int q = 0; q < 3; ++q) s.g[q] = (float)p.gravity[q];
+  s.eps = (float)p.eps;
+  s.sigma = (float)p.surface_tension;
+  const double dia = 2.0 * p.particle_radius;
+  s.dia2 = (float)(dia * dia);
+  s.w_dia = host_kernel_w(std::sqrt((float)dia * (float)dia), s.h, s.k_w, s.k2_w);
+  s.visc = (float)p.viscosity;
+  s.visc_b = (float)p.boundary_viscosity;
+  s.c01h2 = (float)(0.01 * h * h);
+  for (int q = 0; q < 3; ++q) {
+    s.xmin[q] = (float)(p.domain_start[q] + p.padding);
+    s.xmax[q] = (float)(p.domain_end[q] - p.padding);
+  }
+  s.cf = (float)p.collision_coeff;
+  s.sticky = (float)p.sticky_coeff;
+  s.eta_v_fac = p.max_error_v * 0.01 * p.density0;
+  s.eta_p = p.max_error * 0.01 * p.density0;
+  s.max_iter_v = std::min(std::max(p.max_iterations_v, 0), 100000);
+  s.max_iter = std::min(std::max(p.max_iterations, 0), 100000);
+  s.visco_max_iter = std::min(std::max(p.visco_max_iter, 0), 100000);
+  s.nn_method = p.nonnewton_method;
+  s.visco_tol = p.visco_max_error;
+  s.nn_n = (float)p.power_index;
+  s.nn_K = (float)p.consistency_index;
+  s.nn_mu0 = (float)p.viscosity0;
+  s.nn_muinf = (float)p.viscosity_inf;
+  s.nn_gc = (float)p.critical_strain_rate;
+  s.nn_muc = (float)p.mu_c;
+  s.nn_tauy = (float)p.yield_stress;
+  s.mu_newton = (float)(p.viscosity * p.density0);
+  s.mu_b = (float)(p.visco_boundary * p.density0);
+  double E = p.youngs_modulus, nu = p.poisson_ratio;
+  if (p.flags & NN_F_QUIRKS) { E = 25e4; nu = 0.33; }  // SPH/main.py:1188-1189
+  const double f = E / ((1.0 + nu) * (1.0 - 2.0 * nu));
+  s.el_cd = (float)(f * (1.0 - nu));
+  s.el_co = (float)(f * nu);
+  s.el_cs = (float)(f * 0.5 * (1.0 - 2.0 * nu));
+  s.el_mult = el_mult;
+  s.cfl_factor = (float)p.cfl_factor;
+  s.cfl_min_dt = (float)p.cfl_min_dt;
+  s.cfl_max_dt = (float)p.cfl_max_dt;
+  s.diameter = (float)dia;
+  return s;
+}
+
+static int ensure_cells(nn_ctx* c, int64_t cells) {
+  if (cells <= c->max_cells && c->cell_count) return NN_OK;
+  cudaFree(c->cell_count);
+  cudaFree(c->tile_sums);
+  c->cell_count = nullptr;
+  c->tile_sums = nullptr;
+  c->max_cells = std::max<int64_t>(cells, c->max_cells);
+  CK(dalloc(&c->cell_count, (size_t)c->max_cells + 1));
+  CK(dalloc(&c->tile_sums, (size_t)(c->max_cells + 1) / SCAN_TILE + 2));
+  return NN_OK;
+}
+
+static void free_elastic(nn_ctx* c) {
+  cudaFree(c->el_id); cudaFree(c->el_slot); cudaFree(c->el_nb); cudaFree(c->el_cnt);
+  cudaFree(c->el_x0); cudaFree(c->el_R); cudaFree(c->el_S);
+  c->el_id = c->el_slot = c->el_nb = c->el_cnt = nullptr;
+  c->el_x0 = nullptr;
+  c->el_R = c->el_S = nullptr;
+  c->el_stride = 0;
+}
+
+extern "C" {
+
+int nn_abi_version(void) { return NNSPH_ABI_VERSION; }
+
+const char* nn_last_error(const nn_ctx* c) { return c ? c->err.c_str() : g_err; }
+
+int nn_ctx_create(int32_t max_particles, int32_t max_scenes, int32_t max_neighbors, int64_t max_cells, nn_ctx** out) {
+  nn_ctx* c = nullptr;
+  if (!out || max_particles <= 0 || max_scenes <= 0 || max_neighbors <= 0 || max_neighbors > 1024 || max_cells < 0)
+    return fail(nullptr, NN_ERR_INVALID_ARG, "nn_ctx_create: invalid capacities");
+  *out = nullptr;
+  c = new nn_ctx();
+  c->cap = max_particles;
+  c->max_scenes = max_scenes;
+  c->max_nb = max_neighbors;
+  c->el_cap = max_neighbors;
+  auto bail = [&](int code) { nn_ctx_destroy(c); return code; };
+  cudaError_t e = cudaGetDevice(&c->dev_id);
+  if (e != cudaSuccess) return bail(fail(nullptr, NN_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(e)));
+  cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->dev_id);
+  const size_t N = (size_t)max_particles;
+#define AL(p, cnt)                                                                                   \
+  do {                                                                                               \
+    cudaError_t _e = dalloc(&(p), (cnt));                                                            \
+    if (_e != cudaSuccess) return bail(fail(nullptr, NN_ERR_OOM, "cudaMalloc %s: %s", #p, cudaGetErrorString(_e))); \
+  } while (0)
+  for (int k = 0; k < 2; ++k) {
+    AL(c->set[k].pos, N); AL(c->set[k].vel, N); AL(c->set[k].mass, N); AL(c->set[k].dens, N);
+    AL(c->set[k].flags, N); AL(c->set[k].id, N);
+  }
+  AL(c->d_n, 4); AL(c->d_sc, (size_t)max_scenes); AL(c->d_dyn, (size_t)max_scenes);
+  AL(c->d_acc, (size_t)max_scenes * ACC_COUNT * NN_STRIPES);
+  AL(c->d_scene_of_id, N); AL(c->d_src_flag, 1); AL(c->acc4, N);
+  AL(c->alpha, N); AL(c->rho_adv, N); AL(c->kappa, N); AL(c->srn, N); AL(c->mu, N);
+  AL(c->slot_of_id, N); AL(c->key, N); AL(c->rank, N); AL(c->src, N);
+  AL(c->nbr, N * (size_t)max_neighbors); AL(c->nbr_cnt, N);
+  AL(c->cg_x, N); AL(c->cg_r, N); AL(c->cg_z, N); AL(c->cg_p, N); AL(c->cg_Ap, N); AL(c->cg_b, N); AL(c->cg_aux, N);
+  AL(c->cg_pinv, 6 * N);
+  AL(c->e_of_id, N);
+  AL(c->d_any, 1); AL(c->d_body, 4);
+#undef AL
+  if (cudaMallocHost((void**)&c->h_any, sizeof(int32_t)) != cudaSuccess)
+    return bail(fail(nullptr, NN_ERR_OOM, "cudaMallocHost failed"));
+  cudaMemset(c->d_acc, 0, (size_t)max_scenes * ACC_COUNT * NN_STRIPES * sizeof(double));
+  cudaMemset(c->d_body, 0, 4 * sizeof(int32_t));
+  cudaMemset(c->d_n, 0, 4 * sizeof(int32_t));
+  cudaMemset(c->nbr_cnt, 0, N * sizeof(int32_t));
+  if (cudaStreamCreateWithFlags(&c->side, cudaStreamDefault) != cudaSuccess)
+    return bail(fail(nullptr, NN_ERR_CUDA, "cudaStreamCreate failed"));
+  if (max_cells > 0) {
+    int rc = ensure_cells(c, max_cells);
+    if (rc != NN_OK) return bail(rc);
+  }
+  e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return bail(fail(nullptr, NN_ERR_CUDA, "setup: %s", cudaGetErrorString(e)));
+  *out = c;
+  return NN_OK;
+}
+
+int nn_ctx_destroy(nn_ctx* c) {
+  if (!c) return NN_OK;
+  drop_graphs(c);
+  for (int k = 0; k < 2; ++k) {
+    cudaFree(c->set[k].pos); cudaFree(c->set[k].vel); cudaFree(c->set[k].mass); cudaFree(c->set[k].dens);
+    cudaFree(c->set[k].flags); cudaFree(c->set[k].id);
+  }
+  void* bufs[] = {c->d_n, c->d_sc, c->d_dyn, c->d_acc, c->d_scene_of_id, c->d_src_flag, c->acc4, c->alpha,
+                  c->rho_adv, c->kappa, c->srn, c->mu, c->slot_of_id, c->key, c->rank, c->src, c->nbr,
+                  c->nbr_cnt, c->cg_x, c->cg_r, c->cg_z, c->cg_p, c->cg_Ap, c->cg_b, c->cg_aux, c->cg_pinv,
+                  c->e_of_id, c->d_any, c->d_body, c->cell_count, c->tile_sums};
+  for (void* b : bufs) cudaFree(b);
+  free_elastic(c);
+  if (c->h_any) cudaFreeHost(c->h_any);
+  if (c->side) cudaStreamDestroy(c->side);
+  delete c;
+  return NN_OK;
+}
+
+int nn_ctx_set_stream(nn_ctx* c, void* stream) {
+  if (!c) return fail(nullptr, NN_ERR_INVALID_ARG, "null context");
+  if ((cudaStream_t)stream != c->stream) drop_graphs(c);
+  c->stream = (cudaStream_t)stream;
+  return NN_OK;
+}
+
+int nn_set_block_size(nn_ctx* c, int32_t threads) {
+  if (!c) return fail(nullptr, NN_ERR_INVALID_ARG, "null context");
+  if (threads == 0) threads = 256;
+  if (threads < 32 || threads > 1024 || (threads % 32)) return fail(c, NN_ERR_INVALID_ARG, "block size %d", threads);
+  if (threads != c->block) drop_graphs(c);
+  c->block = threads;
+  c->occ.clear();
+  return NN_OK;
+}
+
+int64_t nn_launch_count(const nn_ctx* cc) {
+  nn_ctx* c = const_cast<nn_ctx*>(cc);
+  if (!c) return -1;
+  int32_t body[4] = {0, 0, 0, 0};
+  cudaStreamSynchronize(run_stream(c));
+  cudaMemcpy(body, c->d_body, sizeof(body), cudaMemcpyDeviceToHost);
+  return c->launches + c->graph_replays * c->fixed_nodes_per_step + (int64_t)body[0] * c->body_nodes[0] +
+         (int64_t)body[1] * c->body_nodes[1] + (int64_t)body[2] * c->body_nodes[2];
+}
+
+int nn_bind_state(nn_ctx* c, const nn_state* st) {
+  if (!c || !st) return fail(c, NN_ERR_INVALID_ARG, "nn_bind_state: null argument");
+  if (st->size != sizeof(nn_state)) return fail(c, NN_ERR_INVALID_ARG, "nn_state size %u != %zu", st->size, sizeof(nn_state));
+  if (st->n < 0 || st->n > c->cap) return fail(c, NN_ERR_CAPACITY, "state has %d particles, capacity %d", st->n, c->cap);
+  if (st->n > 0 && (!st->x || !st->x_0 || !st->v || !st->acceleration || !st->volume || !st->m || !st->density ||
+                    !st->dfsph_factor || !st->density_adv || !st->material || !st->is_dynamic || !st->phase_id))
+    return fail(c, NN_ERR_INVALID_ARG, "nn_bind_state: required field is NULL");
+  c->state = *st;
+  c->bound = true;
+  c->searched = false;
+  drop_graphs(c);
+  return NN_OK;
+}
+
+int nn_set_scenes(nn_ctx* c, int32_t nscenes, const nn_scene_desc* scenes) {
+  if (!c || (nscenes > 0 && !scenes) || nscenes < 0) return fail(c, NN_ERR_INVALID_ARG, "nn_set_scenes: bad arguments");
+  if (!c->bound) return fail(c, NN_ERR_STATE, "nn_set_scenes: bind the state first");
+  if (nscenes > c->max_scenes) return fail(c, NN_ERR_CAPACITY, "%d scenes > capacity %d", nscenes, c->max_scenes);
+  const int n = c->state.n;
+  std::vector<int32_t> scene_of_id(n, -1);
+  for (int k = 0; k < nscenes; ++k) {
+    const nn_scene_desc& sd = scenes[k];
+    if (sd.size != sizeof(nn_scene_desc) || sd.params.size != sizeof(nn_scene_params))
+      return fail(c, NN_ERR_INVALID_ARG, "scene %d: struct size mismatch", k);
+    if (sd.start < 0 || sd.n < 0 || sd.start + sd.n > n || sd.n_fluid < 0 || sd.n_fluid > sd.n)
+      return fail(c, NN_ERR_INVALID_ARG, "scene %d: range [%d, %d) outside the state", k, sd.start, sd.start + sd.n);
+    if (!(sd.params.support_radius > 0) || !(sd.params.dt > 0) || !(sd.params.density0 > 0))
+      return fail(c, NN_ERR_INVALID_ARG, "scene %d: support_radius, dt and density0 must be positive", k);
+    for (int i = sd.start; i < sd.start + sd.n; ++i) {
+      if (scene_of_id[i] != -1) return fail(c, NN_ERR_INVALID_ARG, "scene %d overlaps another scene", k);
+      scene_of_id[i] = k;
+    }
+  }
+  for (int i = 0; i < n; ++i)
+    if (scene_of_id[i] < 0) return fail(c, NN_ERR_INVALID_ARG, "particle %d belongs to no scene", i);
+  // host copies of the class fields to lay out the elastic particles
+  std::vector<int32_t> mat(n), ph(n);
+  if (n > 0) {
+    CK(cudaMemcpy(mat.data(), c->state.material, n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(ph.data(), c->state.phase_id, n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+  }
+  std::vector<SceneDev> sdev;
+  std::vector<SceneDyn> sdyn(nscenes);
+  std::vector<int32_t> el_id;
+  int64_t cells = 0;
+  c->any_fluid = c->any_div = c->any_nonnewton = c->any_implicit = c->any_cfl = false;
+  c->el_mult_max = 0;
+  for (int k = 0; k < nscenes; ++k) {
+    const nn_scene_desc& sd = scenes[k];
+    const bool q = (sd.params.flags & NN_F_QUIRKS) != 0;
+    std::vector<int> phases;
+    for (int i = sd.start; i < sd.start + sd.n; ++i)
+      if (mat[i] == NN_SOLID && ph[i] >= NN_PHASE_ELASTIC_BASE) phases.push_back(ph[i]);
+    std::sort(phases.begin(), phases.end());
+    phases.erase(std::unique(phases.begin(), phases.end()), phases.end());
+    int el_mult = 0;
+    if ((sd.params.flags & NN_F_ELASTICITY) && !phases.empty()) el_mult = q ? (int)phases.size() : 1;
+    if (el_mult > 0)
+      for (int i = sd.start; i < sd.start + sd.n; ++i)
+        if (q || (mat[i] == NN_SOLID && ph[i] >= NN_PHASE_ELASTIC_BASE)) el_id.push_back(i);
+    SceneDev s = make_scene(sd, cells, el_mult);
+    cells += (int64_t)s.gx * ((int64_t)1 << (2 * s.mbits));
+    sdev.push_back(s);
+    SceneDyn y{};
+    y.dt = (float)sd.params.dt;
+    y.inv_dt = (float)(1.0 / (double)y.dt);
+    y.inv_dt2 = (float)(1.0 / ((double)y.dt * (double)y.dt));
+    sdyn[k] = y;
+    c->any_fluid |= sd.n_fluid > 0;
+    c->any_div |= sd.n_fluid > 0 && (sd.params.flags & NN_F_DIVERGENCE);
+    c->any_nonnewton |= (sd.params.flags & NN_F_NONNEWTON) != 0;
+    c->any_implicit |= sd.n_fluid > 0 && (sd.params.flags & NN_F_IMPLICIT_VISCOSITY) && !q;
+    c->any_cfl |= (sd.params.flags & NN_F_CFL) != 0;
+    c->el_mult_max = std::max(c->el_mult_max, el_mult);
+  }
+  if (cells >= (int64_t)0x7fffffff) return fail(c, NN_ERR_CAPACITY, "%lld grid cells exceed the 32-bit key space", (long long)cells);
+  RC(ensure_cells(c, cells));
+  drop_graphs(c);
+  c->scenes.assign(scenes, scenes + nscenes);
+  c->sdev = sdev;
+  c->n = n;
+  c->ncells = (int)cells;
+  c->ne = (int)el_id.size();
+  free_elastic(c);
+  std::vector<int32_t> e_of_id(c->cap, -1);
+  for (size_t e = 0; e < el_id.size(); ++e) e_of_id[el_id[e]] = (int32_t)e;
+  if (c->ne > 0) {
+    c->el_stride = c->ne;
+    const size_t E = (size_t)c->ne;
+    if (dalloc(&c->el_id, E) != cudaSuccess || dalloc(&c->el_slot, E) != cudaSuccess ||
+        dalloc(&c->el_nb, E * c->el_cap) != cudaSuccess || dalloc(&c->el_cnt, E) != cudaSuccess ||
+        dalloc(&c->el_x0, E) != cudaSuccess || dalloc(&c->el_R, 9 * E) != cudaSuccess ||
+        dalloc(&c->el_S, 6 * E) != cudaSuccess)
+      return fail(c, NN_ERR_OOM, "elastic buffers");
+    CK(cudaMemcpy(c->el_id, el_id.data(), E * sizeof(int32_t), cudaMemcpyHostToDevice));
+    CK(cudaMemset(c->el_cnt, 0, E * sizeof(int32_t)));
+  }
+  CK(cudaMemcpy(c->e_of_id, e_of_id.data(), c->cap * sizeof(int32_t), cudaMemcpyHostToDevice));
+  if (n > 0) CK(cudaMemcpy(c->d_scene_of_id, scene_of_id.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice));
+  if (nscenes > 0) {
+    CK(cudaMemcpy(c->d_sc, sdev.data(), nscenes * sizeof(SceneDev), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->d_dyn, sdyn.data(), nscenes * sizeof(SceneDyn), cudaMemcpyHostToDevice));
+  }
+  int32_t hn[4] = {n, nscenes, (int)cells, c->ne};
+  CK(cudaMemcpy(c->d_n, hn, sizeof(hn), cudaMemcpyHostToDevice));
+  CK(cudaMemset(c->d_acc, 0, (size_t)c->max_scenes * ACC_COUNT * NN_STRIPES * sizeof(double)));
+  c->searched = false;
+  return NN_OK;
+}
+
+static int check_ready(nn_ctx* c) {
+  if (!c) return fail(nullptr, NN_ERR_INVALID_ARG, "null context");
+  if (!c->bound || c->scenes.empty()) return fail(c, NN_ERR_STATE, "bind a state and set scenes first");
+  return NN_OK;
+}
+
+int nn_initialize(nn_ctx* c) {
+  RC(check_ready(c));
+  cudaStream_t s = run_stream(c);
+  // Elasticity constructors run before solver.initialize() (SPH/main.py:1889-1895, 1915)
+  CK(cudaMemsetAsync(c->d_src_flag, 1, sizeof(int32_t), s));
+  RC(enq_search(c, s));
+  Dev d = make_dev(c, c->cur);
+  RC(launch1(c, s, k_step_dt, d, 0));
+  if (c->ne > 0) RC(launch(c, s, k_el_init, 256, c->n, d));
+  RC(launch(c, s, k_boundary_volume, c->block, c->n, d, 0));
+  RC(launch(c, s, k_boundary_volume, c->block, c->n, d, 1));
+  RC(enq_sync_out(c, s, SM_VOL));
+  CK(cudaStreamSynchronize(s));
+  return NN_OK;
+}
+
+int nn_step(nn_ctx* c, int32_t nsteps, uint32_t flags) {
+  RC(check_ready(c));
+  if (nsteps < 0) return fail(c, NN_ERR_INVALID_ARG, "nsteps < 0");
+  cudaStream_t s = run_stream(c);
+  if (!s) return fail(c, NN_ERR_STATE, "no stream");
+  const bool host = (flags & NN_STEP_HOST_LOOP) != 0;
+  for (int k = 0; k < nsteps; ++k) {
+    CK(cudaMemsetAsync(c->d_src_flag, k == 0 ? 1 : 0, sizeof(int32_t), s));
+    if (host) {
+      RC(enq_step(c, s));
+    } else {
+      const int parity = c->cur;
+      if (!c->exec[parity]) RC(capture_step(c, s, parity));
+      CK(cudaGraphLaunch(c->exec[parity], s));
+      c->cur = 1 - parity;
+      c->graph_replays++;
+      c->searched = true;
+    }
+  }
+  if (flags & NN_STEP_SYNC_STATE) RC(enq_sync_out(c, s, SM_ALL));
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(c, NN_ERR_CUDA, "nn_step: %s", cudaGetErrorString(e));
+  return NN_OK;
+}
+
+int nn_run_pass(nn_ctx* c, int32_t pass) {
+  RC(check_ready(c));
+  if (pass < 0 || pass >= NN_PASS_COUNT) return fail(c, NN_ERR_INVALID_ARG, "unknown pass %d", pass);
+  cudaStream_t s = run_stream(c);
+  if (pass == NN_PASS_SEARCH) {
+    CK(cudaMemsetAsync(c->d_src_flag, 1, sizeof(int32_t), s));
+    RC(launch1(c, s, k_step_reset, make_dev(c, c->cur)));
+    RC(enq_search(c, s));
+    CK(cudaStreamSynchronize(s));
+    return NN_OK;
+  }
+  if (!c->searched) return fail(c, NN_ERR_STATE, "run the neighbour search first");
+  Dev d = make_dev(c, c->cur);
+  RC(launch(c, s, k_sync_in, 256, c->n, d, (uint32_t)SM_ALL));
+  RC(launch1(c, s, k_step_dt, d, 0));
+  switch (pass) {
+    case NN_PASS_STATIC_BOUNDARY_VOLUME: RC(launch(c, s, k_boundary_volume, c->block, c->n, d, 0)); break;
+    case NN_PASS_MOVING_BOUNDARY_VOLUME: RC(launch(c, s, k_boundary_volume, c->block, c->n, d, 1)); break;
+    case NN_PASS_CLEAR_ACCELERATIONS: RC(launch(c, s, k_clear_acc, 256, c->n, d)); break;
+    case NN_PASS_DENSITIES: RC(launch(c, s, k_density_factor, c->block, c->n, d, 1, 0)); break;
+    case NN_PASS_DFSPH_FACTOR: RC(launch(c, s, k_density_factor, c->block, c->n, d, 0, 1)); break;
+    case NN_PASS_DIVERGENCE_SOLVE: if (c->any_div) RC(enq_divergence(c, s)); break;
+    case NN_PASS_NON_PRESSURE_FORCES: if (c->any_fluid) RC(enq_nonpressure(c, s, 0)); break;
+    case NN_PASS_NON_PRESSURE_ADVECT: RC(launch(c, s, k_np_advect, 256, c->n, d)); break;
+    case NN_PASS_PRESSURE_SOLVE: if (c->any_fluid) RC(enq_pressure(c, s)); break;
+    case NN_PASS_ELASTICITY: RC(enq_elastic(c, s)); break;
+    case NN_PASS_ADVECT: RC(launch(c, s, k_advect_boundary, 256, c->n, d, 1, 0)); break;
+    case NN_PASS_ENFORCE_BOUNDARY: RC(launch(c, s, k_advect_boundary, 256, c->n, d, 0, 1)); break;
+    case NN_PASS_SUBSTEP: RC(enq_substep(c, s)); break;
+    default: break;
+  }
+  RC(enq_sync_out(c, s, SM_ALL));
+  CK(cudaStreamSynchronize(s));
+  return NN_OK;
+}
+
+int nn_time_kernel(nn_ctx* c, int32_t kernel, int32_t reps, float* ms_out) {
+  RC(check_ready(c));
+  if (!ms_out || reps <= 0 || kernel < 0 || kernel >= NN_K_COUNT) return fail(c, NN_ERR_INVALID_ARG, "nn_time_kernel: bad arguments");
+  if (!c->searched) return fail(c, NN_ERR_STATE, "run a step first");
+  cudaStream_t s = run_stream(c);
+  Dev d = make_dev(c, c->cur);
+  RC(launch1(c, s, k_force_active, d));
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  auto one = [&]() -> int {
+    const int B = c->block;
+    switch (kernel) {
+      case NN_K_PRESSURE_UPDATE: return launch(c, s, k_pressure_update, B, c->n, d);
+      case NN_K_DENSITY_ADV: return launch(c, s, k_density_adv, B, c->n, d, 1);
+      case NN_K_DIVERGENCE_UPDATE: return launch(c, s, k_divergence_update, B, c->n, d);
+      case NN_K_DENSITY_CHANGE: return launch(c, s, k_density_change, B, c->n, d, 1);
+      case NN_K_DENSITY_FACTOR: return launch(c, s, k_density_factor, B, c->n, d, 1, 1);
+      case NN_K_BUILD_LISTS: return launch(c, s, k_build_lists, B, c->n, d);
+      case NN_K_CG_MATVEC: return launch(c, s, k_cg_matvec, B, c->n, d);
+      default: return launch(c, s, k_nonpressure, B, c->n, d, 0);
+    }
+  };
+  RC(one());  // warm-up
+  CK(cudaEventRecord(e0, s));
+  for (int r = 0; r < reps; ++r) RC(one());
+  CK(cudaEventRecord(e1, s));
+  CK(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  // leave the accumulators clean for the next step
+  CK(cudaMemsetAsync(c->d_acc, 0, (size_t)c->max_scenes * ACC_COUNT * NN_STRIPES * sizeof(double), s));
+  CK(cudaStreamSynchronize(s));
+  *ms_out = ms / reps;
+  return NN_OK;
+}
+
+int nn_get_neighbors(nn_ctx* c, int32_t* num, int32_t* lists, int32_t width) {
+  RC(check_ready(c));
+  if (!num || !lists || width <= 0) return fail(c, NN_ERR_INVALID_ARG, "nn_get_neighbors: bad arguments");
+  if (!c->searched) return fail(c, NN_ERR_STATE, "run the neighbour search first");
+  cudaStream_t s = run_stream(c);
+  RC(launch(c, s, k_export_neighbors, 256, c->n, make_dev(c, c->cur), num, lists, width));
+  CK(cudaStreamSynchronize(s));
+  return NN_OK;
+}
+
+int nn_get_stats(nn_ctx* c, int32_t scene, nn_stats* out) {
+  RC(check_ready(c));
+  if (!out || scene < 0 || scene >= (int)c->scenes.size()) return fail(c, NN_ERR_INVALID_ARG, "bad scene index");
+  cudaStream_t s = run_stream(c);
+  SceneDyn y;
+  CK(cudaMemcpyAsync(&y, c->d_dyn + scene, sizeof(y), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  std::memset(out, 0, sizeof(*out));
+  out->size = sizeof(*out);
+  out->status = y.status;
+  out->iterations_v = y.it_v;
+  out->iterations = y.it_p;
+  out->cg_iterations = y.it_cg;
+  out->max_neighbors_seen = y.max_nb;
+  out->avg_density_err_v = y.avg_v;
+  out->avg_density_err = y.avg_p;
+  out->cg_residual = y.cg_rel;
+  out->dt = y.dt;
+  unsigned bits = y.max_density_bits;
+  float md;
+  std::memcpy(&md, &bits, sizeof(md));
+  out->max_density = md;
+  out->steps = y.steps;
+  return NN_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,306 @@
+// ns.cuh — cell-linked neighbour search: Z-order counting sort of particles into
+// cells of edge h, deterministic in-cell order (by particle id), gather of the state
+// into the new slot order, and per-slot neighbour lists from the 9 contiguous
+// cell rows of the 27-cell stencil.
+//
+// Replaces NeighborhoodSearchSparse.update_grid / store_neighbors
+// (SPH/main.py:815-847): same pair set (p_i != p_j and |x_i - x_j| < h on absolute
+// f32 positions, SPH/main.py:845), no per-cell cap (the reference stores at most 50
+// particles per cell, SPH/main.py:778) and a checked neighbour cap.
+#pragma once
+#include "dev.cuh"
+
+#define GRID_STRIDE(i, n) for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < (n); i += gridDim.x * blockDim.x)
+
+// Grid-stride loop whose trip count is uniform across a warp (for warp collectives):
+// `valid` is false on the lanes past the end.
+#define FOR_SLOTS_WARP(i, valid, n)                                                        \
+  for (int _base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31; _base < (n);             \
+       _base += gridDim.x * blockDim.x)                                                     \
+    for (int i = _base + (threadIdx.x & 31), _once = 1; _once; _once = 0)                   \
+      for (bool valid = i < (n); _once; _once = 0)
+
+// Cell key of a position in scene s: Morton(cy, cz) * gx + cx + cell_base.
+__device__ __forceinline__ uint32_t cell_key(const SceneDev& s, float x, float y, float z, int* cx_out, int* cy_out,
+                                             int* cz_out) {
+  int cx = (int)floorf((x - s.origin[0]) / s.cell);
+  int cy = (int)floorf((y - s.origin[1]) / s.cell);
+  int cz = (int)floorf((z - s.origin[2]) / s.cell);
+  cx = min(max(cx, 0), s.gx - 1);
+  cy = min(max(cy, 0), s.gy - 1);
+  cz = min(max(cz, 0), s.gz - 1);
+  if (cx_out) { *cx_out = cx; *cy_out = cy; *cz_out = cz; }
+  return (uint32_t)(s.cell_base + (int64_t)morton2((uint32_t)cy, (uint32_t)cz) * s.gx + cx);
+}
+
+__global__ void k_zero_cells(Dev d) {
+  const int nc = d.d_n[2];
+  GRID_STRIDE(i, nc + 1) d.cell_count[i] = 0u;
+}
+
+// Keys and in-cell ranks of every source particle (truth id order or previous slots).
+__global__ void k_keys(Dev d) {
+  const int n = d.d_n[0];
+  const bool truth = *d.src_from_truth != 0;
+  GRID_STRIDE(s, n) {
+    float x, y, z;
+    int sc;
+    if (truth) {
+      x = d.t.x[3 * s]; y = d.t.x[3 * s + 1]; z = d.t.x[3 * s + 2];
+      sc = d.scene_of_id[s];
+    } else {
+      float4 p = d.wo.pos[s];
+      x = p.x; y = p.y; z = p.z;
+      sc = slot_scene(d.wo.flags[s]);
+    }
+    uint32_t k = cell_key(d.sc[sc], x, y, z, nullptr, nullptr, nullptr);
+    d.key[s] = k;
+    d.rank[s] = atomicAdd(&d.cell_count[k], 1u);
+  }
+}
+
+// Exclusive scan of cell_count[0 .. cells] in place (three phases over tiles).
+#define SCAN_TILE 4096
+#define SCAN_THREADS 1024
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* sh, uint32_t* total) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  uint32_t x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) sh[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    uint32_t w = (lane < (int)(blockDim.x >> 5)) ? sh[lane] : 0u;
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    sh[lane] = w;
+  }
+  __syncthreads();
+  uint32_t base = wid > 0 ? sh[wid - 1] : 0u;
+  uint32_t incl = base + x;
+  if (total) *total = sh[(blockDim.x >> 5) - 1];
+  __syncthreads();
+  return incl - v;
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_tiles(Dev d) {
+  __shared__ uint32_t sh[32];
+  const int len = d.d_n[2] + 1;
+  const int ntiles = (len + SCAN_TILE - 1) / SCAN_TILE;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    uint32_t s = 0;
+    for (int k = threadIdx.x; k < SCAN_TILE; k += blockDim.x) {
+      int i = t * SCAN_TILE + k;
+      if (i < len) s += d.cell_count[i];
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t tot = 0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += sh[w];
+      d.tile_sums[t] = tot;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_sums(Dev d) {
+  __shared__ uint32_t sh[32];
+  const int len = d.d_n[2] + 1;
+  const int ntiles = (len + SCAN_TILE - 1) / SCAN_TILE;
+  uint32_t carry = 0;
+  for (int base = 0; base < ntiles; base += blockDim.x) {
+    int i = base + threadIdx.x;
+    uint32_t v = i < ntiles ? d.tile_sums[i] : 0u;
+    uint32_t tot;
+    uint32_t ex = block_excl_scan(v, sh, &tot);
+    if (i < ntiles) d.tile_sums[i] = ex + carry;
+    carry += tot;
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_apply(Dev d) {
+  __shared__ uint32_t sh[32];
+  const int len = d.d_n[2] + 1;
+  const int ntiles = (len + SCAN_TILE - 1) / SCAN_TILE;
+  constexpr int PER = SCAN_TILE / SCAN_THREADS;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    uint32_t v[PER];
+    uint32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+      int i = t * SCAN_TILE + threadIdx.x * PER + k;
+      v[k] = i < len ? d.cell_count[i] : 0u;
+      s += v[k];
+    }
+    uint32_t ex = block_excl_scan(s, sh, nullptr) + d.tile_sums[t];
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+      int i = t * SCAN_TILE + threadIdx.x * PER + k;
+      if (i < len) d.cell_count[i] = ex;
+      ex += v[k];
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void k_scatter(Dev d) {
+  const int n = d.d_n[0];
+  GRID_STRIDE(s, n) d.src[d.cell_count[d.key[s]] + d.rank[s]] = s;
+}
+
+// In-cell order by particle id, so that the slot order (and every neighbour sum)
+// does not depend on the atomics of k_keys.
+__global__ void k_cell_sort(Dev d) {
+  const int nc = d.d_n[2];
+  const bool truth = *d.src_from_truth != 0;
+  GRID_STRIDE(c, nc) {
+    uint32_t b = d.cell_count[c], e = d.cell_count[c + 1];
+    if (e - b < 2) continue;
+    for (uint32_t i = b + 1; i < e; ++i) {
+      int s = d.src[i];
+      int ids = truth ? s : d.wo.id[s];
+      uint32_t j = i;
+      while (j > b) {
+        int sp = d.src[j - 1];
+        int idp = truth ? sp : d.wo.id[sp];
+        if (idp <= ids) break;
+        d.src[j] = sp;
+        --j;
+      }
+      d.src[j] = s;
+    }
+  }
+}
+
+__device__ __forceinline__ uint32_t class_bits(int material, int dynamic, int phase, const SceneDev& s) {
+  uint32_t c = NN_CLS_VALID;
+  if (material == NN_SOLID) c |= NN_CLS_SOLID;
+  if (dynamic) c |= NN_CLS_DYNAMIC;
+  if (s.el_mult > 0) {
+    if ((s.flags & NN_F_QUIRKS) || (material == NN_SOLID && phase >= NN_PHASE_ELASTIC_BASE)) c |= NN_CLS_ELASTIC;
+  }
+  return c;
+}
+
+// Gather the state into the new slot order (from Truth by id, or from the previous
+// slots), and record max |v| per scene for the CFL step.
+__global__ void k_gather(Dev d) {
+  const int n = d.d_n[0];
+  const bool truth = *d.src_from_truth != 0;
+  FOR_SLOTS_WARP(i, valid, n) {
+    uint32_t fl = 0u;
+    float vm = 0.f;
+    if (valid) {
+      int s = d.src[i];
+      int id;
+      float4 p, v;
+      float m, rho;
+      if (truth) {
+        id = s;
+        int sc = d.scene_of_id[id];
+        p = make_float4(d.t.x[3 * id], d.t.x[3 * id + 1], d.t.x[3 * id + 2], d.t.volume[id]);
+        v = make_float4(d.t.v[3 * id], d.t.v[3 * id + 1], d.t.v[3 * id + 2], 0.f);
+        m = d.t.m[id];
+        rho = d.t.density[id];
+        fl = class_bits(d.t.material[id], d.t.is_dynamic[id], d.t.phase_id[id], d.sc[sc]) |
+             ((uint32_t)sc << NN_SCENE_SHIFT);
+      } else {
+        id = d.wo.id[s];
+        p = d.wo.pos[s];
+        v = d.wo.vel[s];
+        m = d.wo.mass[s];
+        rho = d.wo.dens[s];
+        fl = d.wo.flags[s];
+      }
+      d.w.pos[i] = p;
+      d.w.vel[i] = v;
+      d.w.mass[i] = m;
+      d.w.dens[i] = rho;
+      d.w.flags[i] = fl;
+      d.w.id[i] = id;
+      d.slot_of_id[id] = i;
+      vm = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z);
+    }
+    const bool cfl = valid && (fl & NN_CLS_DYNAMIC) && (d.sc[slot_scene(fl)].flags & NN_F_CFL);
+    warp_max_to(&d.dyn[slot_scene(fl)].vmax_bits, __float_as_uint(vm), cfl);
+  }
+}
+
+// Neighbour lists: for every slot, the 9 (dy, dz) rows of three x-adjacent cells are
+// contiguous slot ranges; candidates are tested with the reference's exact f32
+// expression. Lists hold slot indices, transposed [k][cap] for coalesced reads.
+__global__ void k_build_lists(Dev d) {
+  const int n = d.d_n[0];
+  FOR_SLOTS_WARP(i, valid, n) {
+    int cnt = 0;
+    int scn = 0;
+    if (valid) {
+      const uint32_t fl = d.w.flags[i];
+      scn = slot_scene(fl);
+      const SceneDev& s = d.sc[scn];
+      const float4 pi = d.w.pos[i];
+      int cx, cy, cz;
+      cell_key(s, pi.x, pi.y, pi.z, &cx, &cy, &cz);
+      const int x0 = max(cx - 1, 0), x1 = min(cx + 1, s.gx - 1);
+      const float3 xi = f3(pi);
+      for (int dz = -1; dz <= 1; ++dz) {
+        const int zz = cz + dz;
+        if (zz < 0 || zz >= s.gz) continue;
+        for (int dy = -1; dy <= 1; ++dy) {
+          const int yy = cy + dy;
+          if (yy < 0 || yy >= s.gy) continue;
+          const int64_t row = s.cell_base + (int64_t)morton2((uint32_t)yy, (uint32_t)zz) * s.gx;
+          const uint32_t b = d.cell_count[row + x0], e = d.cell_count[row + x1 + 1];
+          for (uint32_t j = b; j < e; ++j) {
+            if ((int)j == i) continue;
+            const float4 pj = __ldg(&d.w.pos[j]);
+            if (exact_norm(xi - f3(pj)) < s.h) {
+              if (cnt < d.max_nb) d.nbr[(size_t)cnt * d.cap + i] = (int)j;
+              ++cnt;
+            }
+          }
+        }
+      }
+      d.nbr_cnt[i] = min(cnt, d.max_nb);
+      if (cnt > d.max_nb) set_status(&d.dyn[scn], NN_ERR_NEIGHBOR_OVERFLOW);
+    }
+    warp_max_to(&d.dyn[scn].max_nb, cnt, valid);
+  }
+}
+
+// meta.ns.num_neighbors / neighbors in particle-id space, rows sorted by id
+// (materialised on demand for parity checks and the elastic rest state).
+__global__ void k_export_neighbors(Dev d, int32_t* num, int32_t* lists, int width) {
+  const int n = d.d_n[0];
+  GRID_STRIDE(i, n) {
+    const int id = d.w.id[i];
+    const int c = d.nbr_cnt[i];
+    int32_t* row = lists + (size_t)id * width;
+    int w = min(c, width);
+    // insertion sort of the neighbour ids into the output row
+    for (int k = 0; k < w; ++k) {
+      int v = d.w.id[d.nbr[(size_t)k * d.cap + i]];
+      int p = k;
+      while (p > 0 && row[p - 1] > v) { row[p] = row[p - 1]; --p; }
+      row[p] = v;
+    }
+    if (c > width) {  // keep the `width` smallest ids
+      for (int k = width; k < c; ++k) {
+        int v = d.w.id[d.nbr[(size_t)k * d.cap + i]];
+        if (v >= row[width - 1]) continue;
+        int p = width - 1;
+        while (p > 0 && row[p - 1] > v) { row[p] = row[p - 1]; --p; }
+        row[p] = v;
+      }
+    }
+    for (int k = w; k < width; ++k) row[k] = -1;
+    num[id] = c;
+  }
+}

@@ -1,0 +1,1052 @@
+// sph.cuh — the SPH passes of one step on the sorted working set. Each kernel is a
+// grid-stride loop over slots (sizes read from the device, so one captured graph
+// serves any batch composition), walks the slot's neighbour list, and reads per-scene
+// constants from SceneDev. Reductions that decide convergence are FP64.
+#pragma once
+#include "dev.cuh"
+
+#define NB_LOOP(d, i, j)                                   \
+  for (int _k = 0, _c = (d).nbr_cnt[i]; _k < _c; ++_k)     \
+    for (int j = (d).nbr[(size_t)_k * (d).cap + (i)], _o = 1; _o; _o = 0)
+
+// ---------------------------------------------------------------------------
+// compute_static_boundary_volume / compute_moving_boundary_volume (SPH/main.py:1010-1035)
+__global__ void k_boundary_volume(Dev d, int moving) {
+  const int n = d.d_n[0];
+  GRID_STRIDE(i, n) {
+    const uint32_t fl = d.w.flags[i];
+    if (moving ? !cls_dyn_solid(fl) : !cls_static_solid(fl)) continue;
+    const SceneDev& s = d.sc[slot_scene(fl)];
+    const float3 xi = f3(d.w.pos[i]);
+    float delta = s.W0;
+    NB_LOOP(d, i, j) {
+      if (cls_solid(d.w.flags[j])) {
+        float3 r = xi - f3(d.w.pos[j]);
+        delta += kernel_w(sqrtf(dot3(r, r)), s);
+      }
+    }
+    d.w.pos[i].w = 1.f / delta * 3.f;
+  }
+}
+
+// clear_accelerations_kernel (SPH/main.py:945-951)
+__global__ void k_clear_acc(Dev d) {
+  const int n = d.d_n[0];
+  GRID_STRIDE(i, n) {
+    const uint32_t fl = d.w.flags[i];
+    const SceneDev& s = d.sc[slot_scene(fl)];
+    d.acc4[i] = cls_static_solid(fl) ? make_float4(0.f, 0.f, 0.f, 0.f) : make_float4(s.g[0], s.g[1], s.g[2], 0.f);
+  }
+}
+
+// compute_densities (SPH/main.py:975-984) fused with compute_DFSPH_factor
+// (SPH/main.py:1569-1608): both walk the same neighbours with fixed positions.
+__global__ void k_density_factor(Dev d, int do_density, int do_factor) {
+  const int n = d.d_n[0];
+  FOR_SLOTS_WARP(i, valid, n) {
+    const uint32_t fl = valid ? d.w.flags[i] : 0u;
+    const bool work = valid && cls_fluid(fl);
+    const int scn = slot_scene(fl);
+    float rho = 0.f;
+    if (work) {
+      const SceneDev& s = d.sc[scn];
+      const float4 pi = d.w.pos[i];
+      const float3 xi = f3(pi);
+      float den = 0.f, sum_grad = 0.f;
+      float3 gpi = make_float3(0.f, 0.f, 0.f);
+      NB_LOOP(d, i, j) {
+        const float4 pj = d.w.pos[j];
+        const float3 r = xi - f3(pj);
+        const float rn = sqrtf(dot3(r, r));
+        den += pj.w * kernel_w(rn, s);
+        if (do_factor) {
+          const float3 gpj = kernel_grad(r, rn, s) * (-pj.w);
+          if (cls_fluid(d.w.flags[j])) sum_grad += dot3(gpj, gpj);
+          gpi -= gpj;
+        }
+      }
+      if (do_density) {
+        rho = pi.w * s.W0;
+        rho += den;
+        rho = rho * s.rho0;
+        d.w.dens[i] = rho;
+      }
+      if (do_factor) {
+        sum_grad += dot3(gpi, gpi);
+        d.alpha[i] = sum_grad > 1e-6f ? -1.f / sum_grad : 0.f;
+      }
+    }
+    if (do_density) warp_max_to(&d.dyn[scn].max_density_bits, __float_as_uint(rho), work);
+  }
+}
+
+// compute_density_change (SPH/main.py:1610-1645). mode 0: first call of
+// divergence_solve, also applies alpha *= 1/dt (1688); mode 1: solver iteration,
+// accumulates the FP64 density error (1669-1675, 1717-1719).
+__global__ void k_density_change(Dev d, int mode) {
+  const int n = d.d_n[0];
+  FOR_SLOTS_WARP(i, valid, n) {
+    uint32_t fl = valid ? d.w.flags[i] : 0u;
+    const int scn = slot_scene(fl);
+    bool work = valid && cls_fluid(fl) && d.dyn[scn].act_v;
+    double err = 0.0;
+    if (work) {
+      const SceneDev& s = d.sc[scn];
+      const float3 xi = f3(d.w.pos[i]);
+      const float3 vi = f3(d.w.vel[i]);
+      float dd = 0.f;
+      int cnt = 0;
+      NB_LOOP(d, i, j) {
+        const float4 pj = d.w.pos[j];
+        const float3 r = xi - f3(pj);
+        const float rn = sqrtf(dot3(r, r));
+        dd += pj.w * dot3(vi - f3(d.w.vel[j]), kernel_grad(r, rn, s));
+        ++cnt;
+      }
+      dd = fmaxf(dd, 0.f);
+      if (cnt < 20) dd = 0.f;
+      d.rho_adv[i] = dd;
+      float a = d.alpha[i];
+      if (mode == 0) {
+        a = a * d.dyn[scn].inv_dt;
+        d.alpha[i] = a;
+      }
+      d.kappa[i] = dd * a;
+      err = (double)(s.rho0 * dd - 0.f);
+    }
+    if (mode == 1) scene_add(d.acc, ACC_ERR, 0, scn, work, err);
+  }
+}
+
+// divergence_solver_iteration_kernel (SPH/main.py:1721-1760). The pushes onto
+// dynamic solids (1755-1760) are omitted: clear_accelerations (1552) discards them.
+__global__ void k_divergence_update(Dev d) {
+  const int n = d.d_n[0];
+  GRID_STRIDE(i, n) {
+    const uint32_t fl = d.w.flags[i];
+    if (!cls_fluid(fl)) continue;
+    const int scn = slot_scene(fl);
+    if (!d.dyn[scn].act_v) continue;
+    const SceneDev& s = d.sc[scn];
+    const float dt = d.dyn[scn].dt;
+    const float3 xi = f3(d.w.pos[i]);
+    const float k_i = d.kappa[i];
+    float3 dv = make_float3(0.f, 0.f, 0.f);
+    NB_LOOP(d, i, j) {
+      const uint32_t fj = d.w.flags[j];
+      if (cls_fluid(fj)) {
+        const float k_sum = k_i + d.kappa[j];
+        if (fabsf(k_sum) > s.eps) {
+          const float4 pj = d.w.pos[j];
+          const float3 r = xi - f3(pj);
+          const float3 gpj = kernel_grad(r, sqrtf(dot3(r, r)), s) * (-pj.w);
+          dv -= gpj * (dt * k_sum);
+        }
+      } else if (fabsf(k_i) > s.eps) {
+        const float4 pj = d.w.pos[j];
+        const float3 r = xi - f3(pj);
+        const float3 gpj = kernel_grad(r, sqrtf(dot3(r, r)), s) * (-pj.w);
+        dv += gpj * ((-dt * 1.f) * k_i);
+      }
+    }
+    float4 v = d.w.vel[i];
+    v.x += dv.x; v.y += dv.y; v.z += dv.z;
+    d.w.vel[i] = v;
+  }
+}
+
+// multiply_time_step (SPH/main.py:1677-1681): alpha *= dt after the divergence loop.
+__global__ void k_alpha_times_dt(Dev d) {
+  const int n = d.d_n[0];
+  GRID_STRIDE(i, n) {
+    const uint32_t fl = d.w.flags[i];
+    if (!cls_fluid(fl)) continue;
+    const int scn = slot_scene(fl);
+    if (!d.dyn[scn].div_ran) continue;
+    d.alpha[i] = d.alpha[i] * d.dyn[scn].dt;
+  }
+}
+
+// compute_density_adv (SPH/main.py:1647-1667). mode 0: first call of pressure_solve,
+// also alpha *= 1/dt^2 (1771); mode 1: iteration, FP64 error (1793-1797).
+__global__ void k_density_adv(Dev d, int mode) {
+  const int n = d.d_n[0];
+  FOR_SLOTS_WARP(i, valid, n) {
+    uint32_t fl = valid ? d.w.flags[i] : 0u;
+    const int scn = slot_scene(fl);
+    bool work = valid && cls_fluid(fl) && d.dyn[scn].act_p;
+    double err = 0.0;
+    if (work) {
+      const SceneDev& s = d.sc[scn];
+      const float dt = d.dyn[scn].dt;
+      const float3 xi = f3(d.w.pos[i]);
+      const float3 vi = f3(d.w.vel[i]);
+      float delta = 0.f;
+      NB_LOOP(d, i, j) {
+        const float4 pj = d.w.pos[j];
+        const float3 r = xi - f3(pj);
+        const float rn = sqrtf(dot3(r, r));
+        delta += pj.w * dot3(vi - f3(d.w.vel[j]), kernel_grad(r, rn, s));
+      }
+      float da = d.w.dens[i] / s.rho0 + dt * delta;
+      da = fmaxf(da, 1.f);
+      d.rho_adv[i] = da;
+      float a = d.alpha[i];
+      if (mode == 0) {
+        a = a * d.dyn[scn].inv_dt2;
+        d.alpha[i] = a;
+      }
+      d.kappa[i] = (da - 1.f) * a;
+      err = (double)(s.rho0 * da - s.rho0);
+    }
+    if (mode == 1) scene_add(d.acc, ACC_ERR, 0, scn, work, err);
+  }
+}
+
+// pressure_solve_iteration_kernel (SPH/main.py:1799-1841). Fluid slots update v in
+// place per neighbour; dynamic solid slots gather the two-way coupling acceleration
+// from their fluid neighbours (the reference scatters it with atomics, 1835-1841).
+__global__ void k_pressure_update(Dev d) {
+  const int n = d.d_n[0];
+  GRID_STRIDE(i, n) {
+    const uint32_t fl = d.w.flags[i];
+    const bool fluid = cls_fluid(fl);
+    if (!fluid && !cls_dyn_solid(fl)) continue;
+    const int scn = slot_scene(fl);
+    if (!d.dyn[scn].act_p) continue;
+    const SceneDev& s = d.sc[scn];
+    const float dt = d.dyn[scn].dt;
+    const float4 pi = d.w.pos[i];
+    const float3 xi = f3(pi);
+    if (fluid) {
+      const float k_i = d.kappa[i];
+      float4 v4 = d.w.vel[i];
+      float3 vi = f3(v4);
+      NB_LOOP(d, i, j) {
+        const uint32_t fj = d.w.flags[j];
+        if (cls_fluid(fj)) {
+          const float k_sum = k_i + d.kappa[j];
+          if (fabsf(k_sum) > s.eps) {
+            const float4 pj = d.w.pos[j];
+            const float3 r = xi - f3(pj);
+            const float3 gpj = kernel_grad(r, sqrtf(dot3(r, r)), s) * (-pj.w);
+            vi -= gpj * (dt * k_sum);
+          }
+        } else if (fabsf(k_i) > s.eps) {
+          const float4 pj = d.w.pos[j];
+          const float3 r = xi - f3(pj);
+          const float3 gpj = kernel_grad(r, sqrtf(dot3(r, r)), s) * (-pj.w);
+          vi += gpj * ((-dt * 1.f) * k_i);
+        }
+      }
+      d.w.vel[i] = make_float4(vi.x, vi.y, vi.z, v4.w);
+    } else {
+      float3 ai = make_float3(0.f, 0.f, 0.f);
+      NB_LOOP(d, i, j) {
+        const uint32_t fj = d.w.flags[j];
+        if (!cls_fluid(fj)) continue;
+        const float k_j = d.kappa[j];
+        if (!(fabsf(k_j) > s.eps)) continue;
+        const float3 r = f3(d.w.pos[j]) - xi;  // x_fluid - x_solid, as the fluid sees it
+        const float3 gpj = kernel_grad(r, sqrtf(dot3(r, r)), s) * (-pi.w);
+        const float3 vc = gpj * ((-dt * 1.f) * k_j);
+        ai.x += (-vc.x) * 1.f / dt;
+        ai.y += (-vc.y) * 1.f / dt;
+        ai.z += (-vc.z) * 1.f / dt;
+      }
+      float4 a = d.acc4[i];
+      a.x += ai.x; a.y += ai.y; a.z += ai.z;
+      d.acc4[i] = a;
+    }
+  }
+}
+
+// Loop control after each solver iteration: per-scene average error against eta,
+// the reference's iteration counting (SPH/main.py:1695-1703, 1778-1784), and the
+// CUDA graph while-condition (any scene still iterating).
+__global__ void k_solver_check(Dev d, int which /*0 div, 1 pressure*/) {
+  __shared__ int any;
+  if (threadIdx.x == 0) any = 0;
+  __syncthreads();
+  const int ns = d.d_n[1];
+  for (int sc = threadIdx.x; sc < ns; sc += blockDim.x) {
+    SceneDyn& y = d.dyn[sc];
+    const SceneDev& s = d.sc[sc];
+    int* act = which == 0 ? &y.act_v : &y.act_p;
+    if (!*act) continue;
+    double err = acc_sum(d.acc, sc, ACC_ERR);
+    acc_zero(d.acc, sc, ACC_ERR);
+    double avg = err / (double)s.n_fluid;
+    double eta = which == 0 ? (1.0 / (double)y.dt) * s.eta_v_fac : s.eta_p;
+    int* it = which == 0 ? &y.it_v : &y.it_p;
+    int mx = which == 0 ? s.max_iter_v : s.max_iter;
+    if (which == 0) y.avg_v = avg; else y.avg_p = avg;
+    if (avg <= eta) {
+      *act = 0;
+    } else {
+      *it += 1;
+      if (*it >= max(mx, 1)) *act = 0;
+    }
+    if (!(avg == avg)) { set_status(&y, NN_ERR_NAN); *act = 0; }
+    if (*act) any = 1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    *d.any_active = any;
+    atomicAdd(&d.body_count[which], 1);
+#if defined(__CUDA_ARCH__) && (__CUDA_ARCH__ >= 900)
+    if (d.loop_handle) cudaGraphSetConditional((cudaGraphConditionalHandle)d.loop_handle, any ? 1u : 0u);
+#endif
+  }
+}
+
+// Per-scene loop start: which scenes iterate, counters reset, dt-derived constants.
+__global__ void k_solver_begin(Dev d, int which /*0 div, 1 pressure, 2 cg*/) {
+  const int ns = d.d_n[1];
+  int any = 0;
+  for (int sc = threadIdx.x; sc < ns; sc += blockDim.x) {
+    SceneDyn& y = d.dyn[sc];
+    const SceneDev& s = d.sc[sc];
+    int on = s.n_fluid > 0;
+    if (which == 0) { on = on && (s.flags & NN_F_DIVERGENCE); y.act_v = on; y.it_v = 0; y.div_ran = on; }
+    else if (which == 1) { y.act_p = on; y.it_p = 0; }
+    else { y.it_cg = 0; }
+    any |= on;
+  }
+  (void)any;
+}
+
+// Per-step counters reset (before the neighbour search).
+__global__ void k_step_reset(Dev d) {
+  const int ns = d.d_n[1];
+  for (int sc = threadIdx.x; sc < ns; sc += blockDim.x) {
+    SceneDyn& y = d.dyn[sc];
+    y.max_density_bits = 0u;
+    y.max_nb = 0;
+  }
+}
+
+// Time step of the step: the CFL step from max |v| of the gather (extension; the
+// reference keeps dt fixed), and the f32 constants the reference passes to its
+// kernels (1/dt and 1/dt^2 computed in f64 from the f32 dt field, SPH/main.py:1687,1764).
+__global__ void k_step_dt(Dev d, int do_cfl) {
+  const int ns = d.d_n[1];
+  for (int sc = threadIdx.x; sc < ns; sc += blockDim.x) {
+    SceneDyn& y = d.dyn[sc];
+    const SceneDev& s = d.sc[sc];
+    if (do_cfl && (s.flags & NN_F_CFL)) {
+      const float vm = __uint_as_float(y.vmax_bits);
+      double dtn = s.cfl_max_dt;
+      if (vm > 1e-9f) dtn = (double)s.cfl_factor * 0.4 * (double)s.diameter / (double)vm;
+      dtn = fmin(fmax(dtn, (double)s.cfl_min_dt), (double)s.cfl_max_dt);
+      y.dt = (float)dtn;
+    }
+    y.inv_dt = (float)(1.0 / (double)y.dt);
+    y.inv_dt2 = (float)(1.0 / ((double)y.dt * (double)y.dt));
+    y.vmax_bits = 0u;
+    y.it_v = y.it_p = y.it_cg = 0;
+    y.div_ran = 0;
+  }
+}
+
+// non_pressure_advect (SPH/main.py:1843-1848) as a pass of its own.
+__global__ void k_np_advect(Dev d) {
+  const int n = d.d_n[0];
+  GRID_STRIDE(i, n) {
+    const uint32_t fl = d.w.flags[i];
+    if (!cls_fluid(fl) || !(fl & NN_CLS_DYNAMIC)) continue;
+    const float dt = d.dyn[slot_scene(fl)].dt;
+    const float4 a = d.acc4[i];
+    float4 v = d.w.vel[i];
+    v.x += dt * a.x; v.y += dt * a.y; v.z += dt * a.z;
+    d.w.vel[i] = v;
+  }
+}
+
+__global__ void k_force_active(Dev d) {
+  const int ns = d.d_n[1];
+  for (int sc = threadIdx.x; sc < ns; sc += blockDim.x) {
+    SceneDyn& y = d.dyn[sc];
+    const bool on = d.sc[sc].n_fluid > 0;
+    y.act_v = y.act_p = on;
+    y.act_cg = on && scene_implicit(d.sc[sc]);
+  }
+}
+
+__global__ void k_step_end(Dev d) {
+  const int ns = d.d_n[1];
+  for (int sc = threadIdx.x; sc < ns; sc += blockDim.x) d.dyn[sc].steps += 1;
+}
+
+// ---------------------------------------------------------------------------
+// NonNewton viscosity laws (SPH/main.py:404-459); quirk mode keeps the Newtonian
+// branch that the reference's int-vs-Enum dispatch always takes (387-402).
+__device__ __forceinline__ float nn_law(float g, const SceneDev& s) {
+  const int method = (s.flags & NN_F_QUIRKS) ? NN_NEWTONIAN : s.nn_method;
+  switch (method) {
+    case NN_POWER_LAW: return s.nn_K * powf(g, s.nn_n - 1.f);
+    case NN_CROSS: return s.nn_muinf + (s.nn_mu0 - s.nn_muinf) / (1.f + powf(s.nn_K * g, s.nn_n));
+    case NN_CASSON: { float q = sqrtf(s.nn_muc) + sqrtf(s.nn_tauy / g); return q * q; }
+    case NN_CARREAU:
+      if (s.flags & NN_F_CARREAU_TEXTBOOK)
+        return s.nn_muinf + (s.nn_mu0 - s.nn_muinf) * powf(1.f + (s.nn_K * g) * (s.nn_K * g), (s.nn_n - 1.f) / 2.f);
+      return s.nn_muinf + (s.nn_mu0 - s.nn_muinf) / (1.f + powf(s.nn_K * g * g, (1.f - s.nn_n) / 2.f));
+    case NN_BINGHAM:
+      if (g < s.nn_gc) return s.nn_mu0;
+      return s.nn_gc * (s.nn_mu0 - s.nn_muinf) / g + s.nn_muinf;
+    case NN_HERSCHEL_BULKLEY:
+      if (g < s.nn_gc) return s.nn_mu0;
+      return (s.nn_mu0 * s.nn_gc - s.nn_K * powf(s.nn_gc, s.nn_n)) / g + s.nn_K * powf(g, s.nn_n - 1.f);
+    default: return s.nn_mu0;
+  }
+}
+
+// NonNewton.calcStrainRate (SPH/main.py:461-492) + law. Quirk mode: every particle,
+// the accumulator keeps only the last neighbour, norm before scaling. Otherwise: fluid
+// particles, D = (0.5/rho_i) sum_j m_j (v_ji (x) gW + gW (x) v_ji), gamma = |D|_F.
+__global__ void k_strain_rate(Dev d) {
+  const int n = d.d_n[0];
+  GRID_STRIDE(i, n) {
+    const uint32_t fl = d.w.flags[i];
+    const SceneDev& s = d.sc[slot_scene(fl)];
+    if (!(s.flags & NN_F_NONNEWTON)) continue;
+    const bool q = (s.flags & NN_F_QUIRKS) != 0;
+    if (!q && !cls_fluid(fl)) { d.srn[i] = 0.f; d.mu[i] = 0.f; continue; }
+    const float3 xi = f3(d.w.pos[i]);
+    const float3 vi = f3(d.w.vel[i]);
+    float S[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // symmetric: 00 11 22 01 02 12
+    int last_id = -1;  // quirk: the term of the last neighbour in id order survives
+    NB_LOOP(d, i, j) {
+      const float3 r = xi - f3(d.w.pos[j]);
+      const float3 gw = kernel_grad(r, sqrtf(dot3(r, r)), s);
+      const float3 vji = f3(d.w.vel[j]) - vi;
+      const float mj = d.w.mass[j];
+      float t[6] = {(vji.x * gw.x + vji.x * gw.x) * mj, (vji.y * gw.y + vji.y * gw.y) * mj,
+                    (vji.z * gw.z + vji.z * gw.z) * mj, (vji.x * gw.y + vji.y * gw.x) * mj,
+                    (vji.x * gw.z + vji.z * gw.x) * mj, (vji.y * gw.z + vji.z * gw.y) * mj};
+      const int jid = d.w.id[j];
+      const bool take = jid > last_id;
+      if (q && take) last_id = jid;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) S[k] = q ? (take ? t[k] : S[k]) : S[k] + t[k];
+    }
+    const float sc = 0.5f / d.w.dens[i];
+    float nrm2;
+    if (q) {
+      nrm2 = S[0] * S[0] + S[1] * S[1] + S[2] * S[2] + 2.f * (S[3] * S[3] + S[4] * S[4] + S[5] * S[5]);
+    } else {
+      float D[6];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) D[k] = S[k] * sc;
+      nrm2 = D[0] * D[0] + D[1] * D[1] + D[2] * D[2] + 2.f * (D[3] * D[3] + D[4] * D[4] + D[5] * D[5]);
+    }
+    const float g = sqrtf(nrm2);
+    d.srn[i] = g;
+    d.mu[i] = nn_law(g, s);
+  }
+}
+
+// SurfaceTension (SPH/main.py:1387-1414) and ViscosityModel (SPH/main.py:1426-1468)
+// fused in one neighbour pass, then non_pressure_advect (1843-1848) when the explicit
+// model is the last force. Dynamic solids gather the boundary-viscosity reaction
+// from their fluid neighbours (the reference scatters it, 1459-1460).
+__global__ void k_nonpressure(Dev d, int advect) {
+  const int n = d.d_n[0];
+  GRID_STRIDE(i, n) {
+    const uint32_t fl = d.w.flags[i];
+    const bool fluid = cls_fluid(fl);
+    const int scn = slot_scene(fl);
+    const SceneDev& s = d.sc[scn];
+    if (s.n_fluid == 0) continue;
+    const bool implicit_visc = scene_implicit(s);
+    const bool st_on = (s.flags & NN_F_SURFACE_TENSION) != 0;
+    const bool vi_on = !implicit_visc && (s.flags & NN_F_VISCOSITY) != 0;
+    const float4 pi = d.w.pos[i];
+    const float3 xi = f3(pi);
+    const float4 v4 = d.w.vel[i];
+    const float3 vi = f3(v4);
+    if (fluid) {
+      const float mi = d.w.mass[i];
+      float3 st = make_float3(0.f, 0.f, 0.f), vs = make_float3(0.f, 0.f, 0.f);
+      const float rho_i = d.w.dens[i];
+      NB_LOOP(d, i, j) {
+        const uint32_t fj = d.w.flags[j];
+        const float4 pj = d.w.pos[j];
+        const float3 r = xi - f3(pj);
+        const float r2 = dot3(r, r);
+        const float rn = sqrtf(r2);
+        if (cls_fluid(fj)) {
+          const float mj = d.w.mass[j];
+          if (st_on) {
+            const float c = s.sigma / mi * mj;
+            const float w = r2 > s.dia2 ? kernel_w(rn, s) : s.w_dia;
+            st -= (r * c) * w;
+          }
+          if (vi_on) {
+            const float v_xy = dot3(vi - f3(d.w.vel[j]), r);
+            const float sc = 10.f * s.visc * (mj / d.w.dens[j]) * v_xy / (rn * rn + s.c01h2);
+            vs += kernel_grad(r, rn, s) * sc;
+          }
+        } else if (vi_on && s.visc_b != 0.f) {
+          const float v_xy = dot3(vi - f3(d.w.vel[j]), r);
+          const float sc = 10.f * s.visc_b * (s.rho0 * pj.w / rho_i) * v_xy / (rn * rn + s.c01h2);
+          vs += kernel_grad(r, rn, s) * sc;
+        }
+      }
+      float4 a = d.acc4[i];
+      if (st_on) { a.x += st.x; a.y += st.y; a.z += st.z; }
+      if (vi_on) { a.x += vs.x; a.y += vs.y; a.z += vs.z; }
+      d.acc4[i] = a;
+      if (advect && !implicit_visc && (fl & NN_CLS_DYNAMIC)) {
+        const float dt = d.dyn[scn].dt;
+        d.w.vel[i] = make_float4(vi.x + dt * a.x, vi.y + dt * a.y, vi.z + dt * a.z, v4.w);
+      }
+    } else if (cls_dyn_solid(fl) && vi_on && s.visc_b != 0.f) {
+      float3 f = make_float3(0.f, 0.f, 0.f);
+      NB_LOOP(d, i, j) {
+        const uint32_t fj = d.w.flags[j];
+        if (!cls_fluid(fj)) continue;
+        const float3 xj = f3(d.w.pos[j]);
+        const float3 r = xj - xi;  // fluid minus solid, as the fluid computes it
+        const float rn = sqrtf(dot3(r, r));
+        const float v_xy = dot3(f3(d.w.vel[j]) - vi, r);
+        const float sc = 10.f * s.visc_b * (s.rho0 * pi.w / d.w.dens[j]) * v_xy / (rn * rn + s.c01h2);
+        f += kernel_grad(r, rn, s) * sc;
+      }
+      float4 a = d.acc4[i];
+      a.x -= f.x; a.y -= f.y; a.z -= f.z;
+      d.acc4[i] = a;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Implicit viscosity (Weiler, Koschier, Brand, Bender 2018), matrix-free PCG on the
+// mass-weighted SPD system (the reference stubs it, SPH/main.py:1471-1513):
+//   m_i x_i - sum_fluid c_ij K_ij (x_i - x_j) - sum_solid c_ib K_ib (x_i - v_b) = m_i v_i
+//   c_ij = dt * 10 * (mu_i + mu_j)/2 * (m_i/rho_i) (m_j/rho_j),  c_ib = dt*10*mu_b*m_i*rho0*V_b/rho_i^2
+//   K_ij = gradW_ij x_ij^T / (|x_ij|^2 + 0.01 h^2)
+// FP32 vectors, FP64 dot products, 3x3 block-Jacobi preconditioner.
+
+__global__ void k_cg_aux(Dev d) {
+  const int n = d.d_n[0];
+  GRID_STRIDE(i, n) {
+    const uint32_t fl = d.w.flags[i];
+    const SceneDev& s = d.sc[slot_scene(fl)];
+    float mu = (s.flags & NN_F_NONNEWTON) ? d.mu[i] : s.mu_newton;
+    d.cg_aux[i] = make_float4(mu, d.w.mass[i] / d.w.dens[i], 0.f, 0.f);
+  }
+}
+
+__device__ __forceinline__ bool cg_row(const Dev& d, int i, uint32_t fl) {
+  if (!cls_fluid(fl)) return false;
+  return scene_implicit(d.sc[slot_scene(fl)]);
+}
+
+// A p for one row; also the diagonal block (setup) when D != nullptr.
+__device__ __forceinline__ float3 cg_apply(const Dev& d, int i, const float4* vec, float3 vi, const SceneDev& s,
+                                           float dt, float* D, float3* bcorr) {
+  const float4 pi = d.w.pos[i];
+  const float3 xi = f3(pi);
+  const float4 ai = d.cg_aux[i];
+  const float mi = d.w.mass[i];
+  const float rho_i = d.w.dens[i];
+  float3 acc = vi * mi;
+  const float cdt = dt * 10.f;
+  NB_LOOP(d, i, j) {
+    const uint32_t fj = d.w.flags[j];
+    const float4 pj = d.w.pos[j];
+    const float3 r = xi - f3(pj);
+    const float r2 = dot3(r, r);
+    const float rn = sqrtf(r2);
+    const float3 gw = kernel_grad(r, rn, s);
+    const float w = 1.f / (rn * rn + s.c01h2);
+    float c;
+    float3 diff;
+    if (cls_fluid(fj)) {
+      const float4 aj = d.cg_aux[j];
+      c = cdt * 0.5f * (ai.x + aj.x) * ai.y * aj.y;
+      diff = vi - f3(vec[j]);
+    } else {
+      c = cdt * s.mu_b * mi * s.rho0 * pj.w / (rho_i * rho_i);
+      diff = vi;
+      if (bcorr && cls_dyn_solid(fj)) {  // known boundary velocity moves to the rhs
+        const float kv = dot3(r, f3(d.w.vel[j])) * w;
+        *bcorr -= gw * (c * kv);
+      }
+    }
+    acc -= gw * (c * dot3(r, diff) * w);
+    if (D) {
+      const float cw = c * w;
+      D[0] -= cw * gw.x * r.x; D[1] -= cw * gw.y * r.y; D[2] -= cw * gw.z * r.z;
+      D[3] -= cw * gw.x * r.y; D[4] -= cw * gw.x * r.z; D[5] -= cw * gw.y * r.z;
+    }
+  }
+  return acc;
+}
+
+__device__ __forceinline__ float3 sym_apply(const float* P, float3 v) {  // P: 00 11 22 01 02 12
+  return make_float3(P[0] * v.x + P[3] * v.y + P[4] * v.z, P[3] * v.x + P[1] * v.y + P[5] * v.z,
+                     P[4] * v.x + P[5] * v.y + P[2] * v.z);
+}
+
+__global__ void k_cg_setup(Dev d) {
+  const int n = d.d_n[0];
+  FOR_SLOTS_WARP(i, valid, n) {
+    const uint32_t fl = valid ? d.w.flags[i] : 0u;
+    const int scn = slot_scene(fl);
+    const bool work = valid && cg_row(d, i, fl);
+    double rr = 0, bb = 0, rz = 0;
+    if (work) {
+      const SceneDev& s = d.sc[scn];
+      const float dt = d.dyn[scn].dt;
+      const float mi = d.w.mass[i];
+      const float3 vi = f3(d.w.vel[i]);
+      float D[6] = {mi, mi, mi, 0.f, 0.f, 0.f};
+      float3 bc = make_float3(0.f, 0.f, 0.f);
+      const float3 Av = cg_apply(d, i, d.w.vel, vi, s, dt, D, &bc);
+      const float3 b = vi * mi + bc;
+      // symmetric 3x3 inverse in double
+      double a00 = D[0], a11 = D[1], a22 = D[2], a01 = D[3], a02 = D[4], a12 = D[5];
+      double c00 = a11 * a22 - a12 * a12, c01 = a02 * a12 - a01 * a22, c02 = a01 * a12 - a02 * a11;
+      double det = a00 * c00 + a01 * c01 + a02 * c02;
+      double id = 1.0 / det;
+      float P[6] = {(float)(c00 * id), (float)((a00 * a22 - a02 * a02) * id), (float)((a00 * a11 - a01 * a01) * id),
+                    (float)(c01 * id), (float)(c02 * id), (float)((a01 * a02 - a00 * a12) * id)};
+#pragma unroll
+      for (int k = 0; k < 6; ++k) d.cg_pinv[(size_t)k * d.cap + i] = P[k];
+      const float3 r = b - Av;
+      const float3 z = sym_apply(P, r);
+      d.cg_b[i] = make_float4(b.x, b.y, b.z, 0.f);
+      d.cg_x[i] = make_float4(vi.x, vi.y, vi.z, 0.f);
+      d.cg_r[i] = make_float4(r.x, r.y, r.z, 0.f);
+      d.cg_z[i] = make_float4(z.x, z.y, z.z, 0.f);
+      d.cg_p[i] = make_float4(z.x, z.y, z.z, 0.f);
+      rr = (double)r.x * r.x + (double)r.y * r.y + (double)r.z * r.z;
+      bb = (double)b.x * b.x + (double)b.y * b.y + (double)b.z * b.z;
+      rz = (double)r.x * z.x + (double)r.y * z.y + (double)r.z * z.z;
+    }
+    scene_add(d.acc, ACC_RR, 0, scn, work, rr);
+    scene_add(d.acc, ACC_BB, 0, scn, work, bb);
+    scene_add(d.acc, ACC_RZ, 0, scn, work, rz);
+  }
+}
+
+// After setup: relative residual of the initial guess decides whether to iterate.
+__global__ void k_cg_check0(Dev d) {
+  __shared__ int any;
+  if (threadIdx.x == 0) any = 0;
+  __syncthreads();
+  const int ns = d.d_n[1];
+  for (int sc = threadIdx.x; sc < ns; sc += blockDim.x) {
+    SceneDyn& y = d.dyn[sc];
+    const SceneDev& s = d.sc[sc];
+    const bool on = s.n_fluid > 0 && scene_implicit(s);
+    double rr = acc_sum(d.acc, sc, ACC_RR), bb = acc_sum(d.acc, sc, ACC_BB), rz = acc_sum(d.acc, sc, ACC_RZ);
+    acc_zero(d.acc, sc, ACC_RR); acc_zero(d.acc, sc, ACC_BB); acc_zero(d.acc, sc, ACC_RZ);
+    y.it_cg = 0;
+    y.cg_bnorm2 = bb;
+    y.cg_rz = rz;
+    y.cg_rel = bb > 0 ? sqrt(rr / bb) : 0.0;
+    y.act_cg = on && (y.cg_rel > s.visco_tol) && s.visco_max_iter > 0;
+    if (y.act_cg) any = 1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    *d.any_active = any;
+#if defined(__CUDA_ARCH__) && (__CUDA_ARCH__ >= 900)
+    if (d.loop_handle) cudaGraphSetConditional((cudaGraphConditionalHandle)d.loop_handle, any ? 1u : 0u);
+#endif
+  }
+}
+
+__global__ void k_cg_matvec(Dev d) {
+  const int n = d.d_n[0];
+  FOR_SLOTS_WARP(i, valid, n) {
+    const uint32_t fl = valid ? d.w.flags[i] : 0u;
+    const int scn = slot_scene(fl);
+    const bool work = valid && cg_row(d, i, fl) && d.dyn[scn].act_cg;
+    double pap = 0;
+    if (work) {
+      const SceneDev& s = d.sc[scn];
+      const float3 p = f3(d.cg_p[i]);
+      const float3 Ap = cg_apply(d, i, d.cg_p, p, s, d.dyn[scn].dt, nullptr, nullptr);
+      d.cg_Ap[i] = make_float4(Ap.x, Ap.y, Ap.z, 0.f);
+      pap = (double)p.x * Ap.x + (double)p.y * Ap.y + (double)p.z * Ap.z;
+    }
+    scene_add(d.acc, ACC_PAP, 0, scn, work, pap);
+  }
+}
+
+__global__ void k_cg_update(Dev d) {
+  const int n = d.d_n[0];
+  FOR_SLOTS_WARP(i, valid, n) {
+    const uint32_t fl = valid ? d.w.flags[i] : 0u;
+    const int scn = slot_scene(fl);
+    const bool work = valid && cg_row(d, i, fl) && d.dyn[scn].act_cg;
+    double rr = 0, rz = 0;
+    if (work) {
+      const float al = (float)d.dyn[scn].cg_alpha;
+      float3 x = f3(d.cg_x[i]), r = f3(d.cg_r[i]);
+      const float3 p = f3(d.cg_p[i]), Ap = f3(d.cg_Ap[i]);
+      x += p * al;
+      r -= Ap * al;
+      float P[6];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) P[k] = d.cg_pinv[(size_t)k * d.cap + i];
+      const float3 z = sym_apply(P, r);
+      d.cg_x[i] = make_float4(x.x, x.y, x.z, 0.f);
+      d.cg_r[i] = make_float4(r.x, r.y, r.z, 0.f);
+      d.cg_z[i] = make_float4(z.x, z.y, z.z, 0.f);
+      rr = (double)r.x * r.x + (double)r.y * r.y + (double)r.z * r.z;
+      rz = (double)r.x * z.x + (double)r.y * z.y + (double)r.z * z.z;
+    }
+    scene_add(d.acc, ACC_RR, 0, scn, work, rr);
+    scene_add(d.acc, ACC_RZ, 0, scn, work, rz);
+  }
+}
+
+// PCG step length per scene: alpha = (r.z) / (p.Ap).
+__global__ void k_cg_alpha(Dev d) {
+  const int ns = d.d_n[1];
+  for (int sc = threadIdx.x; sc < ns; sc += blockDim.x) {
+    SceneDyn& y = d.dyn[sc];
+    if (!y.act_cg) continue;
+    const double pap = acc_sum(d.acc, sc, ACC_PAP);
+    acc_zero(d.acc, sc, ACC_PAP);
+    y.cg_alpha = pap != 0.0 ? y.cg_rz / pap : 0.0;
+  }
+}
+
+// PCG convergence check per scene (relative residual, FP64) and beta.
+__global__ void k_cg_check(Dev d) {
+  __shared__ int any;
+  if (threadIdx.x == 0) any = 0;
+  __syncthreads();
+  const int ns = d.d_n[1];
+  for (int sc = threadIdx.x; sc < ns; sc += blockDim.x) {
+    SceneDyn& y = d.dyn[sc];
+    const SceneDev& s = d.sc[sc];
+    if (!y.act_cg) continue;
+    const double rr = acc_sum(d.acc, sc, ACC_RR), rz = acc_sum(d.acc, sc, ACC_RZ);
+    acc_zero(d.acc, sc, ACC_RR);
+    acc_zero(d.acc, sc, ACC_RZ);
+    y.it_cg += 1;
+    y.cg_rel = y.cg_bnorm2 > 0 ? sqrt(rr / y.cg_bnorm2) : 0.0;
+    y.cg_beta = y.cg_rz != 0.0 ? rz / y.cg_rz : 0.0;
+    y.cg_rz = rz;
+    if (y.cg_rel <= s.visco_tol || y.it_cg >= s.visco_max_iter || !(y.cg_rel == y.cg_rel)) y.act_cg = 0;
+    if (y.act_cg) any = 1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    *d.any_active = any;
+    atomicAdd(&d.body_count[2], 1);
+#if defined(__CUDA_ARCH__) && (__CUDA_ARCH__ >= 900)
+    if (d.loop_handle) cudaGraphSetConditional((cudaGraphConditionalHandle)d.loop_handle, any ? 1u : 0u);
+#endif
+  }
+}
+
+__global__ void k_cg_pupdate(Dev d) {
+  const int n = d.d_n[0];
+  GRID_STRIDE(i, n) {
+    const uint32_t fl = d.w.flags[i];
+    const int scn = slot_scene(fl);
+    if (!cg_row(d, i, fl) || !d.dyn[scn].act_cg) continue;
+    const float be = (float)d.dyn[scn].cg_beta;
+    const float3 z = f3(d.cg_z[i]), p = f3(d.cg_p[i]);
+    const float3 np = z + p * be;
+    d.cg_p[i] = make_float4(np.x, np.y, np.z, 0.f);
+  }
+}
+
+// a_i += (x_i - v_i)/dt, then non_pressure_advect (SPH/main.py:1843-1848).
+__global__ void k_cg_finish(Dev d, int advect) {
+  const int n = d.d_n[0];
+  GRID_STRIDE(i, n) {
+    const uint32_t fl = d.w.flags[i];
+    if (!cls_fluid(fl)) continue;
+    const int scn = slot_scene(fl);
+    const SceneDev& s = d.sc[scn];
+    if (s.n_fluid == 0) continue;
+    const float dt = d.dyn[scn].dt;
+    float4 a = d.acc4[i];
+    const float4 v4 = d.w.vel[i];
+    if (!scene_implicit(s)) continue;
+    {
+      const float inv_dt = d.dyn[scn].inv_dt;
+      const float3 x = f3(d.cg_x[i]);
+      a.x += (x.x - v4.x) * inv_dt;
+      a.y += (x.y - v4.y) * inv_dt;
+      a.z += (x.z - v4.z) * inv_dt;
+      d.acc4[i] = a;
+    }
+    if (advect && (fl & NN_CLS_DYNAMIC)) d.w.vel[i] = make_float4(v4.x + dt * a.x, v4.y + dt * a.y, v4.z + dt * a.z, v4.w);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Elasticity (Becker et al. 2009), SPH/main.py:1182-1375, on elastic particles
+// ("e-space", id order); current positions through the slot map of the last sort.
+__global__ void k_el_slots(Dev d) {
+  const int ne = d.d_n[3];
+  GRID_STRIDE(e, ne) d.el_slot[e] = d.slot_of_id[d.el_id[e]];
+}
+
+// computeRotations_kernel, SPH/main.py:1249-1274
+__global__ void k_el_rotations(Dev d, int rep) {
+  const int ne = d.d_n[3];
+  GRID_STRIDE(e, ne) {
+    const int i = d.el_slot[e];
+    const uint32_t fl = d.w.flags[i];
+    const SceneDev& s = d.sc[slot_scene(fl)];
+    if (rep >= s.el_mult) continue;
+    const float3 xi = f3(d.w.pos[i]);
+    const float3 x0i = f3(d.el_x0[e]);
+    const float mi = d.w.mass[i];
+    float A[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    const int c = d.el_cnt[e];
+    for (int k = 0; k < c; ++k) {
+      const int je = d.el_nb[(size_t)k * d.el_stride + e];
+      const float3 xji = f3(d.w.pos[d.el_slot[je]]) - xi;
+      const float3 xji0 = f3(d.el_x0[je]) - x0i;
+      const float wgt = mi * kernel_w(sqrtf(dot3(xji0, xji0)), s);
+      A[0] += xji.x * xji0.x * wgt; A[1] += xji.x * xji0.y * wgt; A[2] += xji.x * xji0.z * wgt;
+      A[3] += xji.y * xji0.x * wgt; A[4] += xji.y * xji0.y * wgt; A[5] += xji.y * xji0.z * wgt;
+      A[6] += xji.z * xji0.x * wgt; A[7] += xji.z * xji0.y * wgt; A[8] += xji.z * xji0.z * wgt;
+    }
+    double Ad[3][3], Rd[3][3];
+    for (int k = 0; k < 9; ++k) Ad[k / 3][k % 3] = (double)A[k];
+    closest_rotation(Ad, Rd);
+    for (int k = 0; k < 9; ++k) d.el_R[(size_t)k * d.el_stride + e] = (float)Rd[k / 3][k % 3];
+  }
+}
+
+// computeStress_kernel, SPH/main.py:1285-1323
+__global__ void k_el_stress(Dev d, int rep) {
+  const int ne = d.d_n[3];
+  GRID_STRIDE(e, ne) {
+    const int i = d.el_slot[e];
+    const uint32_t fl = d.w.flags[i];
+    const SceneDev& s = d.sc[slot_scene(fl)];
+    if (rep >= s.el_mult) continue;
+    const float3 xi = f3(d.w.pos[i]);
+    const float3 x0i = f3(d.el_x0[e]);
+    float R[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) R[k] = d.el_R[(size_t)k * d.el_stride + e];
+    float G[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    const int c = d.el_cnt[e];
+    for (int k = 0; k < c; ++k) {
+      const int je = d.el_nb[(size_t)k * d.el_stride + e];
+      const float4 x0j = d.el_x0[je];
+      const float3 xji = f3(d.w.pos[d.el_slot[je]]) - xi;
+      const float3 xji0 = f3(x0j) - x0i;
+      // u_ji = R^T x_ji - x0_ji
+      float3 u = make_float3(R[0] * xji.x + R[3] * xji.y + R[6] * xji.z - xji0.x,
+                             R[1] * xji.x + R[4] * xji.y + R[7] * xji.z - xji0.y,
+                             R[2] * xji.x + R[5] * xji.y + R[8] * xji.z - xji0.z);
+      u = u * x0j.w;
+      const float3 gw = kernel_grad(xji0, sqrtf(dot3(xji0, xji0)), s);
+      G[0] -= u.x * gw.x; G[1] -= u.x * gw.y; G[2] -= u.x * gw.z;
+      G[3] -= u.y * gw.x; G[4] -= u.y * gw.y; G[5] -= u.y * gw.z;
+      G[6] -= u.z * gw.x; G[7] -= u.z * gw.y; G[8] -= u.z * gw.z;
+    }
+    const float e0 = G[0], e1 = G[4], e2 = G[8];
+    const float e3 = 0.5f * (G[1] + G[3]), e4 = 0.5f * (G[2] + G[6]), e5 = 0.5f * (G[5] + G[7]);
+    float S[6];
+    S[0] = s.el_cd * e0 + s.el_co * e1 + s.el_co * e2;
+    S[1] = s.el_co * e0 + s.el_cd * e1 + s.el_co * e2;
+    S[2] = s.el_co * e0 + s.el_co * e1 + s.el_cd * e2;
+    S[3] = s.el_cs * e3;
+    S[4] = s.el_cs * e4;
+    S[5] = s.el_cs * e5;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) d.el_S[(size_t)k * d.el_stride + e] = S[k];
+  }
+}
+
+__device__ __forceinline__ float3 sym6_mul(const float* M, float3 v) {  // symMatTimesVec 1328-1332
+  return make_float3(M[0] * v.x + M[3] * v.y + M[4] * v.z, M[3] * v.x + M[1] * v.y + M[5] * v.z,
+                     M[4] * v.x + M[5] * v.y + M[2] * v.z);
+}
+
+// computeForces_kernel, SPH/main.py:1334-1375
+__global__ void k_el_forces(Dev d, int rep) {
+  const int ne = d.d_n[3];
+  GRID_STRIDE(e, ne) {
+    const int i = d.el_slot[e];
+    const uint32_t fl = d.w.flags[i];
+    const SceneDev& s = d.sc[slot_scene(fl)];
+    if (rep >= s.el_mult) continue;
+    const float4 x0i4 = d.el_x0[e];
+    const float3 x0i = f3(x0i4);
+    const float Vi = x0i4.w;
+    float Ri[9], Si[6];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) Ri[k] = d.el_R[(size_t)k * d.el_stride + e];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) Si[k] = d.el_S[(size_t)k * d.el_stride + e];
+    float3 f = make_float3(0.f, 0.f, 0.f);
+    const int c = d.el_cnt[e];
+    for (int k = 0; k < c; ++k) {
+      const int je = d.el_nb[(size_t)k * d.el_stride + e];
+      const float4 x0j = d.el_x0[je];
+      const float3 xji0 = f3(x0j) - x0i;
+      const float3 gw0 = kernel_grad(xji0, sqrtf(dot3(xji0, xji0)), s);
+      const float3 dji = gw0 * Vi;
+      const float3 dij = gw0 * (-x0j.w);
+      float Sj[6], Rj[9];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) Sj[q] = d.el_S[(size_t)q * d.el_stride + je];
+#pragma unroll
+      for (int q = 0; q < 9; ++q) Rj[q] = d.el_R[(size_t)q * d.el_stride + je];
+      const float3 fij = sym6_mul(Sj, dji) * (-x0j.w);
+      const float3 fji = sym6_mul(Si, dij) * (-Vi);
+      f.x += (Rj[0] * fij.x + Rj[1] * fij.y + Rj[2] * fij.z) - (Ri[0] * fji.x + Ri[1] * fji.y + Ri[2] * fji.z);
+      f.y += (Rj[3] * fij.x + Rj[4] * fij.y + Rj[5] * fij.z) - (Ri[3] * fji.x + Ri[4] * fji.y + Ri[5] * fji.z);
+      f.z += (Rj[6] * fij.x + Rj[7] * fij.y + Rj[8] * fij.z) - (Ri[6] * fji.x + Ri[7] * fji.y + Ri[8] * fji.z);
+    }
+    f = f * 0.5f;
+    const float mi = d.w.mass[i];
+    float4 a = d.acc4[i];
+    a.x += f.x / mi; a.y += f.y / mi; a.z += f.z / mi;
+    d.acc4[i] = a;
+  }
+}
+
+// Elasticity.initValues_kernel (SPH/main.py:1220-1239): rest neighbourhood from the
+// current lists (quirk: all neighbours, at most 50, SPH/main.py:1192; otherwise the
+// elastic neighbours of the same phase) and rest volume m_i / rho_i (mass-based
+// density, compute_density_func SPH/main.py:1170-1179).
+__global__ void k_el_init(Dev d) {
+  const int n = d.d_n[0];
+  GRID_STRIDE(i, n) {
+    const uint32_t fl = d.w.flags[i];
+    if (!(fl & NN_CLS_ELASTIC)) continue;
+    const int id = d.w.id[i];
+    const int e = d.e_of_id[id];
+    if (e < 0) continue;
+    const SceneDev& s = d.sc[slot_scene(fl)];
+    const bool q = (s.flags & NN_F_QUIRKS) != 0;
+    const int cap = q ? min(50, d.el_cap) : d.el_cap;
+    const int ph = d.t.phase_id[id];
+    const float3 xi = f3(d.w.pos[i]);
+    const float mi = d.w.mass[i];
+    float den = mi * s.W0;
+    int c = 0;
+    NB_LOOP(d, i, j) {
+      const int jid = d.w.id[j];
+      const int je = d.e_of_id[jid];
+      const bool member = q ? (je >= 0) : (je >= 0 && d.t.phase_id[jid] == ph);
+      const float3 r = xi - f3(d.w.pos[j]);
+      const float wj = d.w.mass[j] * kernel_w(sqrtf(dot3(r, r)), s);
+      if (q || member) den += wj;
+      if (member) {
+        if (c < cap) d.el_nb[(size_t)c * d.el_stride + e] = je;
+        ++c;
+      }
+    }
+    d.el_cnt[e] = min(c, cap);
+    const float3 x0 = make_float3(d.t.x_0[3 * id], d.t.x_0[3 * id + 1], d.t.x_0[3 * id + 2]);
+    d.el_x0[e] = make_float4(x0.x, x0.y, x0.z, mi / den);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) d.el_R[(size_t)k * d.el_stride + e] = (k % 4 == 0) ? 1.f : 0.f;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) d.el_S[(size_t)k * d.el_stride + e] = 0.f;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// advect (SPH/main.py:1086-1093) + enforce_boundary_3D for FLUID then SOLID
+// (SPH/main.py:1044-1080; each particle is handled by the loop of its material).
+__global__ void k_advect_boundary(Dev d, int do_advect, int do_boundary) {
+  const int n = d.d_n[0];
+  GRID_STRIDE(i, n) {
+    const uint32_t fl = d.w.flags[i];
+    if (!(fl & NN_CLS_DYNAMIC)) continue;
+    const int scn = slot_scene(fl);
+    const SceneDev& s = d.sc[scn];
+    const float dt = d.dyn[scn].dt;
+    float4 p = d.w.pos[i];
+    float4 v = d.w.vel[i];
+    if (do_advect) {
+      if (cls_dyn_solid(fl)) {
+        const float4 a = d.acc4[i];
+        v.x += dt * a.x; v.y += dt * a.y; v.z += dt * a.z;
+      }
+      p.x += dt * v.x; p.y += dt * v.y; p.z += dt * v.z;
+    }
+    if (do_boundary) {
+      float pos[3] = {p.x, p.y, p.z};
+      float nrm[3] = {0.f, 0.f, 0.f};
+      float q[3] = {p.x, p.y, p.z};
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        if (pos[k] > s.xmax[k]) { nrm[k] += 1.f; q[k] = s.xmax[k]; }
+        if (pos[k] <= s.xmin[k]) { nrm[k] += -1.f; q[k] = s.xmin[k]; }
+      }
+      p.x = q[0]; p.y = q[1]; p.z = q[2];
+      const float len = sqrtf(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
+      if (len > 1e-6f) {
+        const float3 nn = make_float3(nrm[0] / len, nrm[1] / len, nrm[2] / len);
+        const float vd = (1.f + s.cf) * (v.x * nn.x + v.y * nn.y + v.z * nn.z);
+        v.x -= nn.x * vd; v.y -= nn.y * vd; v.z -= nn.z * vd;
+        v.x *= s.sticky; v.y *= s.sticky; v.z *= s.sticky;
+      }
+    }
+    if (!(isfinite(p.x) && isfinite(p.y) && isfinite(p.z) && isfinite(v.x) && isfinite(v.y) && isfinite(v.z)))
+      set_status(&d.dyn[scn], NN_ERR_NAN);
+    d.w.pos[i] = p;
+    d.w.vel[i] = v;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Synchronisation with the caller's id-order state (meta.pd).
+__global__ void k_sync_out(Dev d, uint32_t mask) {
+  const int n = d.d_n[0];
+  GRID_STRIDE(i, n) {
+    const int id = d.w.id[i];
+    const float4 p = d.w.pos[i];
+    if (mask & 1u) { d.t.x[3 * id] = p.x; d.t.x[3 * id + 1] = p.y; d.t.x[3 * id + 2] = p.z; }
+    if (mask & 2u) { const float4 v = d.w.vel[i]; d.t.v[3 * id] = v.x; d.t.v[3 * id + 1] = v.y; d.t.v[3 * id + 2] = v.z; }
+    if (mask & 4u) { const float4 a = d.acc4[i]; d.t.a[3 * id] = a.x; d.t.a[3 * id + 1] = a.y; d.t.a[3 * id + 2] = a.z; }
+    if (mask & 8u) d.t.volume[id] = p.w;
+    if (mask & 16u) d.t.density[id] = d.w.dens[i];
+    if (mask & 32u) d.t.dfsph_factor[id] = d.alpha[i];
+    if (mask & 64u) d.t.density_adv[id] = d.rho_adv[i];
+    if ((mask & 128u) && d.t.srn) d.t.srn[id] = d.srn[i];
+    if ((mask & 128u) && d.t.mu) d.t.mu[id] = d.mu[i];
+  }
+}
+
+__global__ void k_sync_out_elastic(Dev d) {
+  const int ne = d.d_n[3];
+  GRID_STRIDE(e, ne) {
+    const int id = d.el_id[e];
+    if (d.t.stress)
+      for (int k = 0; k < 6; ++k) d.t.stress[6 * (size_t)id + k] = d.el_S[(size_t)k * d.el_stride + e];
+    if (d.t.rot)
+      for (int k = 0; k < 9; ++k) d.t.rot[9 * (size_t)id + k] = d.el_R[(size_t)k * d.el_stride + e];
+  }
+}
+
+// Gather the per-pass fields from the caller's state into the current slots.
+__global__ void k_sync_in(Dev d, uint32_t mask) {
+  const int n = d.d_n[0];
+  GRID_STRIDE(i, n) {
+    const int id = d.w.id[i];
+    float4 p = d.w.pos[i];
+    if (mask & 1u) { p.x = d.t.x[3 * id]; p.y = d.t.x[3 * id + 1]; p.z = d.t.x[3 * id + 2]; }
+    if (mask & 8u) p.w = d.t.volume[id];
+    d.w.pos[i] = p;
+    if (mask & 2u) d.w.vel[i] = make_float4(d.t.v[3 * id], d.t.v[3 * id + 1], d.t.v[3 * id + 2], 0.f);
+    if (mask & 4u) d.acc4[i] = make_float4(d.t.a[3 * id], d.t.a[3 * id + 1], d.t.a[3 * id + 2], 0.f);
+    if (mask & 16u) d.w.dens[i] = d.t.density[id];
+    if (mask & 32u) d.alpha[i] = d.t.dfsph_factor[id];
+    if (mask & 64u) d.rho_adv[i] = d.t.density_adv[id];
+    if (mask & 256u) d.w.mass[i] = d.t.m[id];
+  }
+}

@@ -1,0 +1,159 @@
+"""ctypes binding of libnnsph.so (include/nnsph.h) and a thin engine object.
+
+The CUDA library is the only compute path: if `libnnsph.so` is missing or no CUDA
+device is present, constructing an Engine raises. There is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import torch
+
+from . import _abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libnnsph.so")
+
+_lib = None
+
+
+class NNError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{_abi.ERROR_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python __graft_entry__.py build` "
+                              "(or nonnewton_b200.build.build())")
+        L = C.CDLL(LIB_PATH)
+        vp, i32, i64, u32 = C.c_void_p, C.c_int32, C.c_int64, C.c_uint32
+        L.nn_abi_version.restype = C.c_int
+        L.nn_last_error.restype = C.c_char_p
+        L.nn_last_error.argtypes = [vp]
+        L.nn_ctx_create.argtypes = [i32, i32, i32, i64, C.POINTER(vp)]
+        L.nn_ctx_destroy.argtypes = [vp]
+        L.nn_ctx_set_stream.argtypes = [vp, vp]
+        L.nn_bind_state.argtypes = [vp, C.POINTER(_abi.nn_state)]
+        L.nn_set_scenes.argtypes = [vp, i32, C.POINTER(_abi.nn_scene_desc)]
+        L.nn_initialize.argtypes = [vp]
+        L.nn_step.argtypes = [vp, i32, u32]
+        L.nn_run_pass.argtypes = [vp, i32]
+        L.nn_get_neighbors.argtypes = [vp, vp, vp, i32]
+        L.nn_get_stats.argtypes = [vp, i32, C.POINTER(_abi.nn_stats)]
+        L.nn_launch_count.argtypes = [vp]
+        L.nn_launch_count.restype = i64
+        L.nn_set_block_size.argtypes = [vp, i32]
+        L.nn_time_kernel.argtypes = [vp, i32, i32, C.POINTER(C.c_float)]
+        L.nn_time_kernel.restype = C.c_int
+        for name in ("nn_ctx_create", "nn_ctx_destroy", "nn_ctx_set_stream", "nn_bind_state", "nn_set_scenes",
+                     "nn_initialize", "nn_step", "nn_run_pass", "nn_get_neighbors", "nn_get_stats",
+                     "nn_set_block_size"):
+            getattr(L, name).restype = C.c_int
+        if L.nn_abi_version() != 1:
+            raise ImportError("libnnsph.so ABI version mismatch")
+        _lib = L
+    return _lib
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else None
+
+
+class Engine:
+    """One nn_ctx: capacities fixed at creation, state bound from torch tensors."""
+
+    def __init__(self, max_particles: int, max_scenes: int = 1, max_neighbors: int = 64, max_cells: int = 0,
+                 device=None):
+        if not torch.cuda.is_available():
+            raise RuntimeError("nonnewton_b200 needs a CUDA device (the SPH step runs only as sm_100a kernels)")
+        self.device = torch.device(device if device is not None else "cuda")
+        torch.cuda.set_device(self.device)
+        self.L = lib()
+        h = C.c_void_p()
+        self._rc(self.L.nn_ctx_create(int(max_particles), int(max_scenes), int(max_neighbors), int(max_cells),
+                                      C.byref(h)), None)
+        self.h = h
+        self.max_neighbors = max_neighbors
+        self._state = None
+        self._scenes = None
+        self._keep = []
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.L.nn_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _rc(self, rc, h="ctx"):
+        if rc != 0:
+            msg = self.L.nn_last_error(self.h if h == "ctx" else None)
+            raise NNError(rc, msg.decode() if msg else "")
+
+    def set_stream(self, stream: torch.cuda.Stream | None):
+        self._rc(self.L.nn_ctx_set_stream(self.h, C.c_void_p(stream.cuda_stream if stream is not None else 0)))
+
+    def set_block_size(self, threads: int):
+        self._rc(self.L.nn_set_block_size(self.h, int(threads)))
+
+    def bind(self, pd) -> None:
+        st = _abi.nn_state()
+        st.size = C.sizeof(_abi.nn_state)
+        st.n = int(pd.x.shape[0])
+        for name in ("x", "x_0", "v", "acceleration", "volume", "m", "density", "pressure", "dfsph_factor",
+                     "density_adv", "material", "is_dynamic", "phase_id", "strain_rate_norm",
+                     "nonnewton_viscosity", "stress", "rotations"):
+            t = getattr(pd, name, None)
+            if t is not None:
+                assert t.is_cuda and t.is_contiguous(), name
+                setattr(st, name, t.data_ptr())
+        self._state = st
+        self._rc(self.L.nn_bind_state(self.h, C.byref(st)))
+
+    def set_scenes(self, scenes):
+        """scenes: list of (start, n, n_fluid, nn_scene_params)."""
+        arr = (_abi.nn_scene_desc * len(scenes))()
+        for k, (start, n, nf, p) in enumerate(scenes):
+            arr[k].size = C.sizeof(_abi.nn_scene_desc)
+            arr[k].start, arr[k].n, arr[k].n_fluid = int(start), int(n), int(nf)
+            arr[k].params = p
+        self._scenes = arr
+        self._rc(self.L.nn_set_scenes(self.h, len(scenes), arr))
+
+    def initialize(self):
+        self._rc(self.L.nn_initialize(self.h))
+
+    def step(self, nsteps: int = 1, sync: bool = True, host_loop: bool = False):
+        flags = (_abi.NN_STEP_SYNC_STATE if sync else 0) | (_abi.NN_STEP_HOST_LOOP if host_loop else 0)
+        self._rc(self.L.nn_step(self.h, int(nsteps), flags))
+
+    def run_pass(self, p: int):
+        self._rc(self.L.nn_run_pass(self.h, int(p)))
+
+    def neighbors(self, n: int, width: int = 60):
+        num = torch.zeros(n, dtype=torch.int32, device=self.device)
+        lists = torch.full((n, width), -1, dtype=torch.int32, device=self.device)
+        self._rc(self.L.nn_get_neighbors(self.h, _ptr(num), _ptr(lists), int(width)))
+        return num, lists
+
+    def stats(self, scene: int = 0) -> dict:
+        s = _abi.nn_stats()
+        self._rc(self.L.nn_get_stats(self.h, int(scene), C.byref(s)))
+        return s.as_dict()
+
+    def time_kernel(self, kernel: int, reps: int = 20) -> float:
+        ms = C.c_float()
+        self._rc(self.L.nn_time_kernel(self.h, int(kernel), int(reps), C.byref(ms)))
+        return float(ms.value)
+
+    def launch_count(self) -> int:
+        return int(self.L.nn_launch_count(self.h))

@@ -1,0 +1,262 @@
+"""The reference's object API for the SPH step, backed by libnnsph.so.
+
+Mirrors SPH/main.py: the global `meta` (19-23), `ParticleData` (697-723),
+`NeighborhoodSearchSparse` (764-853), `SPHBase` / `DFSPHSolver` (908-1848),
+`initialize()` (1870-1895), `build_solver()` (196-203) and the headless main loop
+(1909-1921). Field names, shapes and dtypes are the reference's; the fields are
+torch CUDA tensors instead of Taichi fields. Every method runs sm_100a kernels
+through the C ABI.
+"""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import torch
+
+from . import _abi
+from .config import Parameter, SimConfig
+from .engine import Engine
+from .scene import ParticleSet, export_ply_particles, load_particles
+
+FLUID, SOLID = _abi.NN_FLUID, _abi.NN_SOLID
+
+
+class Meta:
+    """Global simulation state (`meta`, SPH/main.py:19-23)."""
+
+
+meta = Meta()
+
+
+class ParticleData:
+    """`ParticleData` (SPH/main.py:697-723): SoA particle fields on the GPU."""
+
+    def __init__(self, particle_max_num: int, device="cuda"):
+        n = int(particle_max_num)
+        self.particle_max_num = n
+        self.dim = 3
+        f = dict(dtype=torch.float32, device=device)
+        i = dict(dtype=torch.int32, device=device)
+        self.phase_id = torch.zeros(n, **i)
+        self.x = torch.zeros(n, 3, **f)
+        self.x_0 = torch.zeros(n, 3, **f)
+        self.v = torch.zeros(n, 3, **f)
+        self.acceleration = torch.zeros(n, 3, **f)
+        self.volume = torch.zeros(n, **f)
+        self.m = torch.zeros(n, **f)
+        self.density = torch.zeros(n, **f)
+        self.pressure = torch.zeros(n, **f)
+        self.material = torch.zeros(n, **i)
+        self.color = torch.zeros(n, 3, **f)
+        self.is_dynamic = torch.zeros(n, **i)
+        self.particle_id = torch.arange(n, **i)
+        self.dfsph_factor = torch.zeros(n, **f)
+        self.density_adv = torch.zeros(n, **f)
+        # NonNewton / Elasticity outputs (SPH/main.py:340-342, 1201-1203)
+        self.strain_rate_norm = torch.zeros(n, **f)
+        self.nonnewton_viscosity = torch.zeros(n, **f)
+        self.stress = torch.zeros(n, 6, **f)
+        self.rotations = torch.zeros(n, 9, **f)
+
+
+def initialize_particles(pd: ParticleData, ps: ParticleSet, param: Parameter) -> None:
+    """`initialize_particles` (SPH/main.py:735-758)."""
+    dev = pd.x.device
+    x = torch.from_numpy(np.ascontiguousarray(ps.x, dtype=np.float32)).to(dev)
+    pd.x.copy_(x)
+    pd.x_0.copy_(x)
+    pd.v.zero_()
+    pd.volume.fill_(param.volume0)
+    pd.m.copy_(torch.from_numpy(ps.mass).to(dev))
+    pd.density.fill_(param.density0)
+    pd.pressure.zero_()
+    pd.material.copy_(torch.from_numpy(ps.material).to(dev))
+    pd.is_dynamic.copy_(torch.from_numpy(ps.is_dynamic).to(dev))
+    pd.phase_id.copy_(torch.from_numpy(ps.phase_id).to(dev))
+    pd.color.fill_(1.0)
+    pd.rotations.zero_()
+    pd.rotations[:, [0, 4, 8]] = 1.0
+
+
+class NeighborhoodSearchSparse:
+    """`NeighborhoodSearchSparse` (SPH/main.py:764-853) over the engine's cell-sorted
+    lists. `neighbors` / `num_neighbors` are materialised in particle-id order, each
+    row sorted by id and padded with -1, after every `run_search()`."""
+
+    max_num_neighbors = 60
+
+    def __init__(self, positions, num_particle, support_radius, domain_size, use_sparse_grid=False, engine=None):
+        self.positions = positions
+        self.num_particle = int(num_particle)
+        self.support_radius = support_radius
+        self.domain_size = np.asarray(domain_size)
+        self.grid_size = support_radius
+        self.grid_num = np.ceil(self.domain_size / self.grid_size).astype(int)
+        self.engine = engine
+        self._lists = None
+
+    def run_search(self):
+        self.engine.run_pass(_abi.NN_PASS_SEARCH)
+        self._lists = None
+
+    def _materialise(self):
+        if self._lists is None:
+            self._lists = self.engine.neighbors(self.num_particle, self.max_num_neighbors)
+        return self._lists
+
+    @property
+    def num_neighbors(self):
+        return self._materialise()[0]
+
+    @property
+    def neighbors(self):
+        return self._materialise()[1]
+
+    def get_num_neighbors(self, i):
+        return int(self.num_neighbors[i])
+
+    def get_neighbor(self, i, j):
+        return int(self.neighbors[i, j])
+
+
+class SPHBase:
+    """`SPHBase` (SPH/main.py:908-1093): every method is one or more CUDA passes."""
+
+    def __init__(self):
+        self.gravity = meta.parm.gravity
+        self.density_0 = meta.parm.density0
+        self.dt = meta.parm.dt
+        self.engine: Engine = meta.engine
+        self.host_loop = False
+
+    def step(self):
+        """SPHBase.step (SPH/main.py:915-940) as one CUDA-graph replay."""
+        self.engine.step(1, sync=True, host_loop=self.host_loop)
+        meta.ns._lists = None
+        meta.step_num = getattr(meta, "step_num", 0) + 1
+        if meta.config.get_cfg("exportPly"):
+            torch.cuda.synchronize()
+            export_ply_particles(meta.pd.x.cpu().numpy(), f"results/{meta.step_num - 1}.ply")
+
+    def run(self, nsteps: int):
+        """`nsteps` steps with the particle state kept resident in cell order between
+        steps; meta.pd is written back once at the end."""
+        self.engine.step(int(nsteps), sync=True, host_loop=self.host_loop)
+        meta.ns._lists = None
+        meta.step_num = getattr(meta, "step_num", 0) + int(nsteps)
+
+    def initialize(self):
+        """SPHBase.initialize (SPH/main.py:957-960) and the elastic rest state."""
+        self.engine.initialize()
+        meta.ns._lists = None
+
+    def _pass(self, p):
+        self.engine.run_pass(p)
+
+    def clear_accelerations(self):
+        self._pass(_abi.NN_PASS_CLEAR_ACCELERATIONS)
+
+    def compute_densities(self):
+        self._pass(_abi.NN_PASS_DENSITIES)
+
+    def compute_static_boundary_volume(self):
+        self._pass(_abi.NN_PASS_STATIC_BOUNDARY_VOLUME)
+
+    def compute_moving_boundary_volume(self):
+        self._pass(_abi.NN_PASS_MOVING_BOUNDARY_VOLUME)
+
+    def enforce_boundary_3D(self, positions=None, vel=None, particle_type=None):
+        """Both materials in one pass (the reference calls it for FLUID then SOLID)."""
+        self._pass(_abi.NN_PASS_ENFORCE_BOUNDARY)
+
+    def advect(self):
+        self._pass(_abi.NN_PASS_ADVECT)
+
+    def stats(self) -> dict:
+        return self.engine.stats(0)
+
+
+class DFSPHSolver(SPHBase):
+    """`DFSPHSolver` (SPH/main.py:1519-1848)."""
+
+    def __init__(self):
+        super().__init__()
+        p = meta.parm
+        self.enable_divergence_solver = p.enable_divergence_solver
+        self.m_max_iterations_v = p.max_iterations_v
+        self.m_max_iterations = p.max_iterations
+        self.m_eps = p.m_eps
+        self.max_error_V = p.max_error_v
+        self.max_error = p.max_error
+        self.num_particles = meta.particle_max_num
+        self.use_surfaceTensionModel = p.use_surface_tension
+        self.use_nonNewtonianModel = p.use_nonnewtonian
+        self.use_viscosityModel = p.use_viscosity
+
+    def substep(self):
+        self._pass(_abi.NN_PASS_SUBSTEP)
+
+    def compute_DFSPH_factor(self):
+        self._pass(_abi.NN_PASS_DFSPH_FACTOR)
+
+    def divergence_solve(self):
+        self._pass(_abi.NN_PASS_DIVERGENCE_SOLVE)
+
+    def compute_non_pressure_forces(self):
+        self._pass(_abi.NN_PASS_NON_PRESSURE_FORCES)
+
+    def non_pressure_advect(self):
+        self._pass(_abi.NN_PASS_NON_PRESSURE_ADVECT)
+
+    def pressure_solve(self):
+        self._pass(_abi.NN_PASS_PRESSURE_SOLVE)
+
+    def elasticity_substep(self):
+        self._pass(_abi.NN_PASS_ELASTICITY)
+
+
+def build_solver():
+    """`build_solver` (SPH/main.py:196-203)."""
+    solver_type = meta.config.get_cfg("simulationMethod")
+    if solver_type == 4:
+        return DFSPHSolver()
+    raise NotImplementedError(f"Solver type {solver_type} has not been implemented.")
+
+
+def initialize(config: SimConfig | str | dict | None = None, particles: ParticleSet | None = None,
+               quirks: bool = False, max_neighbors: int = 64, device="cuda"):
+    """`initialize()` (SPH/main.py:1870-1895): parameters, particles, fields, the
+    neighbour search object and the CUDA engine (which also sets up elastic bodies)."""
+    if isinstance(config, str):
+        config = SimConfig(config)
+    elif isinstance(config, dict):
+        config = SimConfig(config=config)
+    if config is not None:
+        meta.config = config
+    meta.parm = Parameter.from_config(meta.config, quirks=quirks)
+    ps = particles if particles is not None else load_particles(meta.config, meta.parm)
+    meta.phase_info = ps.phase_info
+    meta.particle_max_num = ps.n
+    meta.fluid_particle_num = ps.n_fluid
+    meta.pd = ParticleData(ps.n, device=device)
+    initialize_particles(meta.pd, ps, meta.parm)
+    meta.engine = Engine(max(ps.n, 1), 1, max_neighbors, device=device)
+    meta.engine.bind(meta.pd)
+    meta.engine.set_scenes([(0, ps.n, ps.n_fluid, meta.parm.to_c())])
+    meta.ns = NeighborhoodSearchSparse(meta.pd.x, ps.n, meta.parm.support_radius, meta.parm.domain_size,
+                                       use_sparse_grid=True, engine=meta.engine)
+    meta.num_elastic_bodies = len([p for p in ps.phase_info.values() if getattr(p, "solid_type", 0) == 2])
+    meta.step_num = 0
+    return meta
+
+
+def main(scene_path: str):
+    """Headless `main()` (the reference's noGUI branch, SPH/main.py:1909-1921)."""
+    initialize(scene_path)
+    solver = build_solver()
+    solver.initialize()
+    meta.step_num = 0
+    for _ in range(int(meta.config.get_cfg("maxStep", 1))):
+        solver.step()
+    return meta

@@ -1,0 +1,163 @@
+"""CUDA path vs the CPU oracle, through the reference-facing object API and the C ABI.
+
+Tolerances: neighbour lists bit-exact as sorted id sets (pairs within 4 ulp of h are
+excluded); FP32 fields within 1e-4 relative to the field's scale; iteration counts
+equal.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from nonnewton_b200 import _abi
+from nonnewton_b200 import scene as S
+from nonnewton_b200.config import Parameter, SimConfig
+
+from .helpers import gpu_sim, near_cutoff_pairs, oracle_sim, pd_field, rel_err
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+TOL = 1e-4
+
+
+def _scene_9pt():
+    g = json.load(open(os.path.join(GOLD, "neighbor_9pt.json")))
+    conf = {"Configuration": {"domainStart": [0, 0, 0], "domainEnd": [0.1, 0.1, 0.1], "particleRadius": 0.01,
+                              "density0": 1000, "simulationMethod": 4, "gravitation": [0, -9.81, 0],
+                              "timeStepSize": 0.004}, "FluidParticles": [{}]}
+    param = Parameter.from_config(SimConfig(config=conf))
+    ps = S.assemble([S.PhaseInfo(uid=0, material=0, is_dynamic=True, pos=np.array(g["x"]))], param)
+    return S.Scene("9pt", conf, param, ps, 1), g
+
+
+def test_neighbors_9pt_golden(cuda_lib):
+    sc, g = _scene_9pt()
+    m, solver = gpu_sim(sc)
+    m.ns.run_search()
+    num = m.ns.num_neighbors.cpu().numpy()
+    lists = m.ns.neighbors.cpu().numpy()
+    assert num.tolist() == g["num_neighbors"]
+    for i, row in enumerate(g["neighbors"]):
+        assert lists[i, : len(row)].tolist() == row and np.all(lists[i, len(row):] == -1)
+
+
+def test_lattice_kat(cuda_lib):
+    g = json.load(open(os.path.join(GOLD, "lattice_kat.json")))
+    r, n = g["particle_radius"], g["n_side"]
+    idx = np.stack(np.meshgrid(*[np.arange(n)] * 3, indexing="ij"), -1).reshape(-1, 3)
+    x = g["origin"] + idx * 2 * r
+    conf = {"Configuration": {"domainStart": [0, 0, 0], "domainEnd": [1, 1, 1], "particleRadius": r,
+                              "density0": 1000, "simulationMethod": 4, "timeStepSize": 1e-3},
+            "FluidParticles": [{}]}
+    param = Parameter.from_config(SimConfig(config=conf))
+    ps = S.assemble([S.PhaseInfo(uid=0, material=0, is_dynamic=True, pos=x)], param)
+    m, solver = gpu_sim(S.Scene("lat", conf, param, ps, 1))
+    m.ns.run_search()
+    solver.compute_densities()
+    inter = np.array(g["interior_ids"])
+    assert np.all(m.ns.num_neighbors.cpu().numpy()[inter] == 26)
+    rho = pd_field(m, "density")[inter]
+    assert np.abs(rho - g["rho_interior"]).max() / g["rho_interior"] < 1e-5
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_neighbor_lists_bit_exact(cuda_lib, seed):
+    sc = S.dam_break(seed=seed, n_side=(12, 12, 12), box=0.4)
+    m, solver = gpu_sim(sc)
+    m.ns.run_search()
+    o = oracle_sim(sc)
+    o.run_pass(_abi.NN_PASS_SEARCH)
+    on, ol = o.neighbors(60)
+    gn = m.ns.num_neighbors.cpu().numpy()
+    gl = m.ns.neighbors.cpu().numpy()
+    ties = near_cutoff_pairs(sc.particles.x, sc.param.support_radius)
+    bad = np.nonzero((gn != on) | np.any(gl != ol, axis=1))[0]
+    tie_ids = {a for a, b in ties} | {b for a, b in ties}
+    assert set(bad.tolist()) <= tie_ids, f"{len(bad)} rows differ outside cut-off ties"
+
+
+def _init_both(sc, **kw):
+    m, solver = gpu_sim(sc, **kw)
+    solver.initialize()
+    o = oracle_sim(sc)
+    o.initialize()
+    return m, solver, o
+
+
+def _compare(m, o, names, nf=None, tol=TOL):
+    for name in names:
+        g = pd_field(m, name)
+        r = o.get(name)
+        if nf is not None and name in ("density", "dfsph_factor", "density_adv"):
+            g, r = g[:nf], r[:nf]
+        e = rel_err(g, r)
+        assert e < tol, f"{name}: rel err {e:.2e}"
+
+
+def test_passes_one_by_one(cuda_lib):
+    sc = S.dam_break(seed=0, n_side=(10, 10, 10), box=0.4)
+    m, solver, o = _init_both(sc)
+    nf = sc.particles.n_fluid
+    _compare(m, o, ["volume"])
+    rng = np.random.default_rng(0)
+    v = rng.normal(0, 0.2, size=(sc.particles.n, 3)).astype(np.float32)
+    v[nf:] = 0
+    import torch
+    m.pd.v.copy_(torch.from_numpy(v))
+    o.set("v", v)
+    for p, names in [(_abi.NN_PASS_CLEAR_ACCELERATIONS, ["acceleration"]),
+                     (_abi.NN_PASS_DENSITIES, ["density"]),
+                     (_abi.NN_PASS_DFSPH_FACTOR, ["dfsph_factor"]),
+                     (_abi.NN_PASS_DIVERGENCE_SOLVE, ["v", "dfsph_factor", "density_adv"]),
+                     (_abi.NN_PASS_CLEAR_ACCELERATIONS, ["acceleration"]),
+                     (_abi.NN_PASS_NON_PRESSURE_FORCES, ["acceleration"]),
+                     (_abi.NN_PASS_NON_PRESSURE_ADVECT, ["v"]),
+                     (_abi.NN_PASS_PRESSURE_SOLVE, ["v", "dfsph_factor", "density_adv"]),
+                     (_abi.NN_PASS_ADVECT, ["x", "v"]),
+                     (_abi.NN_PASS_ENFORCE_BOUNDARY, ["x", "v"])]:
+        m.engine.run_pass(p)
+        o.run_pass(p)
+        _compare(m, o, names, nf)
+    gs, os_ = m.engine.stats(0), o.stats()
+    assert gs["iterations_v"] == os_["iterations_v"] and gs["iterations"] == os_["iterations"]
+
+
+@pytest.mark.parametrize("quirks", [False, True])
+def test_step_parity(cuda_lib, quirks):
+    sc = S.dam_break(seed=0, n_side=(10, 10, 10), box=0.4, quirks=quirks)
+    m, solver, o = _init_both(sc)
+    nf = sc.particles.n_fluid
+    for k in range(10):
+        solver.step()
+        o.step(1)
+        gs, os_ = m.engine.stats(0), o.stats()
+        assert (gs["iterations_v"], gs["iterations"]) == (os_["iterations_v"], os_["iterations"]), k
+        _compare(m, o, ["x", "v", "density"], nf)
+    assert abs(gs["avg_density_err"] - os_["avg_density_err"]) <= 1e-3 * max(1.0, abs(os_["avg_density_err"]))
+
+
+def test_graph_equals_host_loop(cuda_lib):
+    sc = S.dam_break(seed=2, n_side=(10, 10, 10), box=0.4)
+    outs = []
+    for host in (False, True):
+        m, solver = gpu_sim(sc)
+        solver.host_loop = host
+        solver.initialize()
+        for _ in range(5):
+            solver.step()
+        outs.append((pd_field(m, "x"), pd_field(m, "v")))
+    assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
+
+
+def test_resident_run_equals_steps(cuda_lib):
+    sc = S.dam_break(seed=4, n_side=(10, 10, 10), box=0.4)
+    m1, s1 = gpu_sim(sc)
+    s1.initialize()
+    for _ in range(6):
+        s1.step()
+    x1 = pd_field(m1, "x")
+    m2, s2 = gpu_sim(sc)
+    s2.initialize()
+    s2.run(6)
+    assert np.array_equal(x1, pd_field(m2, "x"))
