@@ -44,6 +44,7 @@ struct nn_ctx {
   int dev_id = 0, sms = 148;
   cudaStream_t stream = nullptr;      // caller stream (0 = legacy default)
   cudaStream_t side = nullptr;        // capture stream for loop bodies
+  cudaStream_t own = nullptr;         // execution stream when the caller sets none
   std::string err;
   int64_t launches = 0;
   int block = 256;
@@ -310,7 +311,7 @@ static int enq_nonpressure(nn_ctx* c, cudaStream_t s, int advect) {
   Dev d = make_dev(c, c->cur);
   const int B = c->block;
   if (c->any_nonnewton) RC(launch(c, s, k_strain_rate, B, c->n, d));
-  RC(launch(c, s, k_nonpressure, B, c->n, d, advect));
+  RC(launch(c, s, k_nonpressure, B, c->n, d));
   if (c->any_implicit) {
     RC(launch(c, s, k_cg_aux, 256, c->n, d));
     RC(launch(c, s, k_cg_setup, B, c->n, d));
@@ -323,8 +324,8 @@ static int enq_nonpressure(nn_ctx* c, cudaStream_t s, int advect) {
                      RC(launch1(c, q, k_cg_check, e));
                      return launch(c, q, k_cg_pupdate, 256, c->n, e);
                    }));
-    RC(launch(c, s, k_cg_finish, 256, c->n, d, advect));
   }
+  if (c->any_implicit || advect) RC(launch(c, s, k_cg_finish, 256, c->n, d, advect));
   return NN_OK;
 }
 
@@ -372,7 +373,7 @@ static int enq_sync_out(nn_ctx* c, cudaStream_t s, uint32_t mask) {
   return NN_OK;
 }
 
-static cudaStream_t run_stream(nn_ctx* c) { return c->stream ? c->stream : c->side ? c->side : nullptr; }
+static cudaStream_t run_stream(nn_ctx* c) { return c->stream ? c->stream : c->own; }
 
 static void drop_graphs(nn_ctx* c) {
   for (int p = 0; p < 2; ++p)
@@ -557,7 +558,8 @@ int nn_ctx_create(int32_t max_particles, int32_t max_scenes, int32_t max_neighbo
   cudaMemset(c->d_body, 0, 4 * sizeof(int32_t));
   cudaMemset(c->d_n, 0, 4 * sizeof(int32_t));
   cudaMemset(c->nbr_cnt, 0, N * sizeof(int32_t));
-  if (cudaStreamCreateWithFlags(&c->side, cudaStreamDefault) != cudaSuccess)
+  if (cudaStreamCreateWithFlags(&c->side, cudaStreamDefault) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->own, cudaStreamDefault) != cudaSuccess)
     return bail(fail(nullptr, NN_ERR_CUDA, "cudaStreamCreate failed"));
   if (max_cells > 0) {
     int rc = ensure_cells(c, max_cells);
@@ -584,6 +586,7 @@ int nn_ctx_destroy(nn_ctx* c) {
   free_elastic(c);
   if (c->h_any) cudaFreeHost(c->h_any);
   if (c->side) cudaStreamDestroy(c->side);
+  if (c->own) cudaStreamDestroy(c->own);
   delete c;
   return NN_OK;
 }
@@ -828,7 +831,7 @@ int nn_time_kernel(nn_ctx* c, int32_t kernel, int32_t reps, float* ms_out) {
       case NN_K_DENSITY_FACTOR: return launch(c, s, k_density_factor, B, c->n, d, 1, 1);
       case NN_K_BUILD_LISTS: return launch(c, s, k_build_lists, B, c->n, d);
       case NN_K_CG_MATVEC: return launch(c, s, k_cg_matvec, B, c->n, d);
-      default: return launch(c, s, k_nonpressure, B, c->n, d, 0);
+      default: return launch(c, s, k_nonpressure, B, c->n, d);
     }
   };
   RC(one());  // warm-up

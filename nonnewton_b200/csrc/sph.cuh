@@ -323,6 +323,8 @@ __global__ void k_step_reset(Dev d) {
     SceneDyn& y = d.dyn[sc];
     y.max_density_bits = 0u;
     y.max_nb = 0;
+    y.it_v = y.it_p = y.it_cg = 0;
+    y.div_ran = 0;
   }
 }
 
@@ -344,8 +346,6 @@ __global__ void k_step_dt(Dev d, int do_cfl) {
     y.inv_dt = (float)(1.0 / (double)y.dt);
     y.inv_dt2 = (float)(1.0 / ((double)y.dt * (double)y.dt));
     y.vmax_bits = 0u;
-    y.it_v = y.it_p = y.it_cg = 0;
-    y.div_ran = 0;
   }
 }
 
@@ -447,10 +447,11 @@ __global__ void k_strain_rate(Dev d) {
 }
 
 // SurfaceTension (SPH/main.py:1387-1414) and ViscosityModel (SPH/main.py:1426-1468)
-// fused in one neighbour pass, then non_pressure_advect (1843-1848) when the explicit
-// model is the last force. Dynamic solids gather the boundary-viscosity reaction
-// from their fluid neighbours (the reference scatters it, 1459-1460).
-__global__ void k_nonpressure(Dev d, int advect) {
+// fused in one neighbour pass. Dynamic solids gather the boundary-viscosity reaction
+// from their fluid neighbours (the reference scatters it, 1459-1460). The velocity
+// update of non_pressure_advect cannot join this pass: the viscosity reads the
+// neighbours' velocities.
+__global__ void k_nonpressure(Dev d) {
   const int n = d.d_n[0];
   GRID_STRIDE(i, n) {
     const uint32_t fl = d.w.flags[i];
@@ -497,10 +498,6 @@ __global__ void k_nonpressure(Dev d, int advect) {
       if (st_on) { a.x += st.x; a.y += st.y; a.z += st.z; }
       if (vi_on) { a.x += vs.x; a.y += vs.y; a.z += vs.z; }
       d.acc4[i] = a;
-      if (advect && !implicit_visc && (fl & NN_CLS_DYNAMIC)) {
-        const float dt = d.dyn[scn].dt;
-        d.w.vel[i] = make_float4(vi.x + dt * a.x, vi.y + dt * a.y, vi.z + dt * a.z, v4.w);
-      }
     } else if (cls_dyn_solid(fl) && vi_on && s.visc_b != 0.f) {
       float3 f = make_float3(0.f, 0.f, 0.f);
       NB_LOOP(d, i, j) {
@@ -761,7 +758,9 @@ __global__ void k_cg_pupdate(Dev d) {
   }
 }
 
-// a_i += (x_i - v_i)/dt, then non_pressure_advect (SPH/main.py:1843-1848).
+// Implicit scenes: a_i += (x_i - v_i)/dt (the viscous acceleration of the CG
+// solution); then, for every scene, non_pressure_advect (SPH/main.py:1843-1848).
+// No neighbour reads, so the velocity update is safe here.
 __global__ void k_cg_finish(Dev d, int advect) {
   const int n = d.d_n[0];
   GRID_STRIDE(i, n) {
@@ -773,8 +772,7 @@ __global__ void k_cg_finish(Dev d, int advect) {
     const float dt = d.dyn[scn].dt;
     float4 a = d.acc4[i];
     const float4 v4 = d.w.vel[i];
-    if (!scene_implicit(s)) continue;
-    {
+    if (scene_implicit(s)) {
       const float inv_dt = d.dyn[scn].inv_dt;
       const float3 x = f3(d.cg_x[i]);
       a.x += (x.x - v4.x) * inv_dt;

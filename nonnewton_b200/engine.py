@@ -71,7 +71,10 @@ class Engine:
                  device=None):
         if not torch.cuda.is_available():
             raise RuntimeError("nonnewton_b200 needs a CUDA device (the SPH step runs only as sm_100a kernels)")
-        self.device = torch.device(device if device is not None else "cuda")
+        dev = torch.device(device if device is not None else "cuda")
+        if dev.index is None:
+            dev = torch.device("cuda", torch.cuda.current_device())
+        self.device = dev
         torch.cuda.set_device(self.device)
         self.L = lib()
         h = C.c_void_p()

@@ -125,16 +125,32 @@ def test_passes_one_by_one(cuda_lib):
 
 @pytest.mark.parametrize("quirks", [False, True])
 def test_step_parity(cuda_lib, quirks):
+    """Each step starts from identical input states (the oracle takes the GPU's x, v)."""
     sc = S.dam_break(seed=0, n_side=(10, 10, 10), box=0.4, quirks=quirks)
     m, solver, o = _init_both(sc)
     nf = sc.particles.n_fluid
-    for k in range(10):
+    for k in range(12):
+        o.set("x", pd_field(m, "x"))
+        o.set("v", pd_field(m, "v"))
         solver.step()
         o.step(1)
         gs, os_ = m.engine.stats(0), o.stats()
         assert (gs["iterations_v"], gs["iterations"]) == (os_["iterations_v"], os_["iterations"]), k
-        _compare(m, o, ["x", "v", "density"], nf)
-    assert abs(gs["avg_density_err"] - os_["avg_density_err"]) <= 1e-3 * max(1.0, abs(os_["avg_density_err"]))
+        _compare(m, o, ["x", "v", "acceleration", "density", "dfsph_factor", "density_adv"], nf)
+        assert abs(gs["avg_density_err"] - os_["avg_density_err"]) <= 1e-4 * sc.param.density0
+
+
+def test_trajectory_parity(cuda_lib):
+    """Free-running 30 steps: summation-order differences compound, so the tolerance is
+    1e-3 of the field scale; the final density error stays within the 0.1 % target."""
+    sc = S.dam_break(seed=1, n_side=(10, 10, 10), box=0.4)
+    m, solver, o = _init_both(sc)
+    nf = sc.particles.n_fluid
+    for _ in range(30):
+        solver.step()
+    o.step(30)
+    _compare(m, o, ["x", "v", "density"], nf, tol=1e-3)
+    assert m.engine.stats(0)["avg_density_err"] <= 0.1 * 0.01 * sc.param.density0 + 1e-9
 
 
 def test_graph_equals_host_loop(cuda_lib):
