@@ -7,8 +7,11 @@
 //
 // Parity status: the reference's Taichi code cannot run in this environment
 // (taichi is not installed), and the reference stores no golden outputs. The
-// oracle is pinned by the known answers derivable from the reference's fixtures
-// (tests/golden/, generated by tests/golden/make_golden.py), not by a live run.
+// neighbour search and the density / boundary-volume / DFSPH-factor passes are
+// pinned by known answers derived from the reference's fixtures (tests/golden/,
+// generated by tests/golden/make_golden.py) and by an independent numpy
+// restatement; for the solver loops, forces and elasticity, parity is unpinned
+// against a live reference run.
 //
 // Templated on Real (float = the reference's ti.f32 default, double = the FP64
 // comparison run). Every neighbour loop walks neighbours in ascending particle id.
