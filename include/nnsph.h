@@ -244,6 +244,29 @@ enum nn_kernel_id {
    full work; it mutates solver scratch and, for the update kernels, velocities. */
 int nn_time_kernel(nn_ctx* ctx, int32_t kernel, int32_t reps, float* ms_out);
 
+/* Neighbour search that allocates no device memory. No counterpart in the
+   reference: it exists for callers that cannot call cudaMalloc themselves or through
+   this library (code that runs where allocation is forbidden or would deadlock, such
+   as inside a host callback, or a host framework that owns every device allocation).
+   Its scratch is a file-scope device array of NN_NOALLOC_SCRATCH_BYTES that every GPU
+   loading the library holds until the process exits. Inputs and outputs are device
+   buffers of the caller: x [n,3] float32; num_neighbors [n] and neighbors [n,width]
+   int32, the same rows as nn_get_neighbors (sorted by particle id, padded with -1,
+   at most NN_NOALLOC_MAX_NEIGHBORS per particle). The grid covers the domain of the
+   scene (positions outside it are clamped into the border cells). Returns
+   NN_ERR_CAPACITY beyond NN_NOALLOC_MAX_PARTICLES particles or
+   NN_ERR_CAPACITY when the domain needs more than NN_NOALLOC_MAX_CELLS cells of edge
+   support_radius. The first call on a device looks up the array's address; make it
+   before any stream capture. All calls share the array: calls that overlap on the
+   GPU race. Work is enqueued on `cuda_stream` (NULL = legacy default stream). */
+#define NN_NOALLOC_MAX_PARTICLES 16384
+#define NN_NOALLOC_MAX_NEIGHBORS 64
+#define NN_NOALLOC_MAX_CELLS     (1 << 18)
+#define NN_NOALLOC_SCRATCH_BYTES (8u << 20)
+int nn_neighbors_noalloc(const float* x, int32_t n, const double* domain_start, const double* domain_end,
+                         double support_radius, int32_t width, int32_t* num_neighbors, int32_t* neighbors,
+                         void* cuda_stream);
+
 /* Autotuned launch shape: threads per block for the neighbour passes. 0 = default. */
 int nn_set_block_size(nn_ctx* ctx, int32_t threads);
 

@@ -14,6 +14,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -887,3 +888,152 @@ int nn_get_stats(nn_ctx* c, int32_t scene, nn_stats* out) {
 }
 
 }  // extern "C"
+
+// ---- neighbour search without device allocation ------------------------------------
+// For callers that cannot call cudaMalloc (for example code running inside a host
+// callback or a framework that owns every device allocation): the scratch of the
+// search lives in one file-scope device array that the library carries. Every GPU
+// that loads libnnsph.so holds NN_NOALLOC_SCRATCH_BYTES of device memory until the
+// process exits. All calls share the array, so calls that overlap on the GPU (on
+// different streams, or from several host threads) race; calls on one stream are
+// ordered. The first call on a device looks up the array's device address; make that
+// first call before any stream capture.
+namespace {
+constexpr size_t kNaAlign = 256;
+constexpr size_t na_round(size_t b) { return (b + kNaAlign - 1) / kNaAlign * kNaAlign; }
+constexpr size_t kNaN = NN_NOALLOC_MAX_PARTICLES;
+constexpr size_t kNaC = NN_NOALLOC_MAX_CELLS;
+constexpr size_t kNaNb = NN_NOALLOC_MAX_NEIGHBORS;
+// layout of the scratch array (byte offsets)
+constexpr size_t kOffN = 0;
+constexpr size_t kOffSc = kOffN + na_round(4 * sizeof(int32_t));
+constexpr size_t kOffDyn = kOffSc + na_round(sizeof(SceneDev));
+constexpr size_t kOffFlag = kOffDyn + na_round(sizeof(SceneDyn));
+constexpr size_t kOffSceneOf = kOffFlag + na_round(sizeof(int32_t));
+constexpr size_t kOffKey = kOffSceneOf + na_round(kNaN * 4);
+constexpr size_t kOffRank = kOffKey + na_round(kNaN * 4);
+constexpr size_t kOffSrc = kOffRank + na_round(kNaN * 4);
+constexpr size_t kOffCells = kOffSrc + na_round(kNaN * 4);
+constexpr size_t kOffTiles = kOffCells + na_round((kNaC + 1) * 4);
+constexpr size_t kOffPos = kOffTiles + na_round(((kNaC + 1) / SCAN_TILE + 2) * 4);
+constexpr size_t kOffFlags = kOffPos + na_round(kNaN * sizeof(float4));
+constexpr size_t kOffId = kOffFlags + na_round(kNaN * 4);
+constexpr size_t kOffNbr = kOffId + na_round(kNaN * 4);
+constexpr size_t kOffCnt = kOffNbr + na_round(kNaN * kNaNb * 4);
+constexpr size_t kNaEnd = kOffCnt + na_round(kNaN * 4);
+static_assert(kNaEnd <= NN_NOALLOC_SCRATCH_BYTES, "no-alloc scratch layout exceeds the array");
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_nn_noalloc_scratch[NN_NOALLOC_SCRATCH_BYTES];
+
+// Sizes, scene constants and cleared per-call state, written by a kernel so the call
+// needs no host-to-device copy.
+__global__ void k_na_setup(Dev d, SceneDev s, int32_t n, int32_t cells) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    int32_t* dn = const_cast<int32_t*>(d.d_n);
+    dn[0] = n; dn[1] = 1; dn[2] = cells; dn[3] = 0;
+    *const_cast<SceneDev*>(d.sc) = s;
+    SceneDyn y{};
+    *d.dyn = y;
+    *const_cast<int32_t*>(d.src_from_truth) = 1;
+  }
+  int32_t* so = const_cast<int32_t*>(d.scene_of_id);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) so[i] = 0;
+}
+
+// Positions only: the slot set of the search (no velocities or masses involved).
+__global__ void k_na_gather(Dev d) {
+  const int n = d.d_n[0];
+  GRID_STRIDE(i, n) {
+    const int s = d.src[i];
+    d.w.pos[i] = make_float4(d.t.x[3 * s], d.t.x[3 * s + 1], d.t.x[3 * s + 2], 0.f);
+    d.w.flags[i] = NN_CLS_VALID;
+    d.w.id[i] = s;
+  }
+}
+
+static std::mutex g_na_mutex;
+static void* g_na_ptr[256] = {nullptr};
+
+extern "C" int nn_neighbors_noalloc(const float* x, int32_t n, const double* domain_start,
+                                    const double* domain_end, double support_radius, int32_t width,
+                                    int32_t* num_neighbors, int32_t* neighbors, void* cuda_stream) {
+  nn_ctx* c = nullptr;  // error messages go to nn_last_error(NULL)
+  if (!x || !domain_start || !domain_end || !num_neighbors || !neighbors || n < 0 || width <= 0 || width > 1024 ||
+      !(support_radius > 0))
+    return fail(c, NN_ERR_INVALID_ARG, "nn_neighbors_noalloc: invalid argument");
+  if (n > NN_NOALLOC_MAX_PARTICLES)
+    return fail(c, NN_ERR_CAPACITY, "nn_neighbors_noalloc: %d particles exceed the maximum of %d", n,
+                NN_NOALLOC_MAX_PARTICLES);
+  nn_scene_desc sd{};
+  sd.size = sizeof(sd);
+  sd.n = n;
+  sd.params.size = sizeof(nn_scene_params);
+  for (int k = 0; k < 3; ++k) {
+    if (!(domain_end[k] > domain_start[k])) return fail(c, NN_ERR_INVALID_ARG, "nn_neighbors_noalloc: empty domain");
+    sd.params.domain_start[k] = domain_start[k];
+    sd.params.domain_end[k] = domain_end[k];
+  }
+  sd.params.support_radius = support_radius;
+  sd.params.density0 = 1000.0;
+  sd.params.dt = 1e-3;
+  const SceneDev s = make_scene(sd, 0, 0);
+  const int64_t cells = (int64_t)s.gx * ((int64_t)1 << (2 * s.mbits));
+  if (cells > NN_NOALLOC_MAX_CELLS)
+    return fail(c, NN_ERR_CAPACITY, "nn_neighbors_noalloc: the domain needs %lld cells of edge h, maximum %d",
+                (long long)cells, NN_NOALLOC_MAX_CELLS);
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev < 0 || dev >= 256) return fail(c, NN_ERR_CUDA, "nn_neighbors_noalloc: cudaGetDevice failed");
+  unsigned char* base = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_na_mutex);
+    if (!g_na_ptr[dev]) {  // once per device, with that device current
+      void* p = nullptr;
+      e = cudaGetSymbolAddress(&p, g_nn_noalloc_scratch);
+      if (e != cudaSuccess || !p)
+        return fail(c, NN_ERR_CUDA, "nn_neighbors_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+      g_na_ptr[dev] = p;
+    }
+    base = static_cast<unsigned char*>(g_na_ptr[dev]);
+  }
+  if (n == 0) return NN_OK;
+  Dev d{};
+  d.d_n = reinterpret_cast<int32_t*>(base + kOffN);
+  d.sc = reinterpret_cast<SceneDev*>(base + kOffSc);
+  d.dyn = reinterpret_cast<SceneDyn*>(base + kOffDyn);
+  d.src_from_truth = reinterpret_cast<int32_t*>(base + kOffFlag);
+  d.scene_of_id = reinterpret_cast<int32_t*>(base + kOffSceneOf);
+  d.key = reinterpret_cast<uint32_t*>(base + kOffKey);
+  d.rank = reinterpret_cast<uint32_t*>(base + kOffRank);
+  d.src = reinterpret_cast<int32_t*>(base + kOffSrc);
+  d.cell_count = reinterpret_cast<uint32_t*>(base + kOffCells);
+  d.tile_sums = reinterpret_cast<uint32_t*>(base + kOffTiles);
+  d.w.pos = reinterpret_cast<float4*>(base + kOffPos);
+  d.w.flags = reinterpret_cast<uint32_t*>(base + kOffFlags);
+  d.w.id = reinterpret_cast<int32_t*>(base + kOffId);
+  d.nbr = reinterpret_cast<int32_t*>(base + kOffNbr);
+  d.nbr_cnt = reinterpret_cast<int32_t*>(base + kOffCnt);
+  d.cap = NN_NOALLOC_MAX_PARTICLES;
+  d.max_nb = NN_NOALLOC_MAX_NEIGHBORS;
+  d.t.x = const_cast<float*>(x);
+  cudaStream_t st = (cudaStream_t)cuda_stream;
+  const int B = 256;
+  const int gN = std::max(1, std::min((n + B - 1) / B, 1024));
+  const int gC = std::max(1, std::min((int)((cells + 1 + B - 1) / B), 1024));
+  const int tiles = (int)((cells + 1 + SCAN_TILE - 1) / SCAN_TILE);
+  k_na_setup<<<gN, B, 0, st>>>(d, s, n, (int32_t)cells);
+  k_zero_cells<<<gC, B, 0, st>>>(d);
+  k_keys<<<gN, B, 0, st>>>(d);
+  k_scan_tiles<<<std::min(tiles, 256), SCAN_THREADS, 0, st>>>(d);
+  k_scan_sums<<<1, SCAN_THREADS, 0, st>>>(d);
+  k_scan_apply<<<std::min(tiles, 256), SCAN_THREADS, 0, st>>>(d);
+  k_scatter<<<gN, B, 0, st>>>(d);
+  k_cell_sort<<<gC, B, 0, st>>>(d);
+  k_na_gather<<<gN, B, 0, st>>>(d);
+  k_build_lists<<<gN, B, 0, st>>>(d);
+  k_export_neighbors<<<gN, B, 0, st>>>(d, num_neighbors, neighbors, width);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(c, NN_ERR_CUDA, "nn_neighbors_noalloc: %s", cudaGetErrorString(e));
+  return NN_OK;
+}
