@@ -108,10 +108,11 @@ class Engine:
     def set_block_size(self, threads: int):
         self._rc(self.L.nn_set_block_size(self.h, int(threads)))
 
-    def bind(self, pd) -> None:
+    def bind(self, pd, n: int | None = None) -> None:
+        """Bind the fields of `pd`; `n` active particles (default: all rows)."""
         st = _abi.nn_state()
         st.size = C.sizeof(_abi.nn_state)
-        st.n = int(pd.x.shape[0])
+        st.n = int(pd.x.shape[0] if n is None else n)
         for name in ("x", "x_0", "v", "acceleration", "volume", "m", "density", "pressure", "dfsph_factor",
                      "density_adv", "material", "is_dynamic", "phase_id", "strain_rate_norm",
                      "nonnewton_viscosity", "stress", "rotations"):
