@@ -207,6 +207,96 @@ def run_reference(args):
                               "d2h_bytes_per_step": 0}}))
 
 
+def run_served(args, world, rank):
+    """The mixed served workload: Poisson arrivals of dam-break requests (fluid count
+    log-uniform in [2k, 128k], box at 50 % fill, Cross law with mu0 ~ U[0.1, 20],
+    n ~ U[0.5, 1], implicit viscosity), K steps each, continuously batched; the plain
+    per-scene loop runs a seeded sample of the same requests one after another."""
+    import torch
+
+    from nonnewton_b200 import scene as S
+    from nonnewton_b200.serve import Request, Server, run_plain
+
+    nreq = args.requests
+    work = S.mixed_workload(n_requests=nreq, seed=1000 + rank, rate=args.rate, steps=args.steps)
+    reqs = [Request(k, sc, args.steps, t) for k, (t, sc) in enumerate(work)]
+    # warm-up: a small served run (captures the step graphs of the server context)
+    srv = Server(capacity=args.capacity, max_scenes=args.max_scenes, chunk=args.chunk)
+    warm = [Request(-1 - k, sc, max(args.warmup, 1), 0.0) for k, (t, sc) in enumerate(work[:4])]
+    srv.run(warm, realtime=False)
+    torch.cuda.synchronize()
+    barrier(world)
+    eng = srv.batch.engine
+    l0 = eng.launch_count()
+    clocks_path = os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else "",
+                               f"clocks_rank{rank}.csv")
+    with ClockSampler(clocks_path) as cs:
+        torch.cuda.nvtx.range_push("timed")
+        res = srv.run(reqs, realtime=True)
+        torch.cuda.nvtx.range_pop()
+    launches = eng.launch_count() - l0
+    wall_max = max_over_ranks(res["wall_s"], world)
+    dev_s = max_over_ranks(res["particle_steps"] / max(res["device_throughput"], 1e-9), world)
+    total_ps = sum_over_ranks(float(res["particle_steps"]), world)
+    # plain per-scene loop on a sample
+    rng = np.random.default_rng(7)
+    sample = [reqs[k] for k in sorted(rng.choice(len(reqs), size=min(args.plain_sample, len(reqs)), replace=False))]
+    plain_reqs = [Request(r.rid, r.scene, r.steps, 0.0) for r in sample]
+    plain = run_plain(plain_reqs)
+    # alone-vs-mix agreement on the sample
+    fin = {r.rid: r for r in res["finished"]}
+    mix_err = max(float(np.abs(fin[p.rid].result_x - p.result_x).max()) for p in plain_reqs)
+    # roofline of the dominant kernel on a full batch
+    first = [r.scene for r in reqs]
+    pack, n = [], 0
+    for sc in first:
+        if n + sc.particles.n > args.capacity or len(pack) >= args.max_scenes:
+            break
+        pack.append(sc)
+        n += sc.particles.n
+    srv.batch.set(pack)
+    srv.batch.step(2, sync=False)
+    kms = {k: eng.time_kernel(KERNEL_IDS[k], reps=10) for k in ("pressure_update", "density_adv", "build_lists",
+                                                                "density_factor", "cg_matvec")}
+    peaks, peak_kind = load_peaks()
+    if rank != 0:
+        return
+    dom = "density_adv"
+    achieved = ALG_BYTES[dom] * n / (kms[dom] / 1e3) / 1e9
+    hbm = peaks["hbm_gbs"]
+    h2d = sum(r.scene.particles.n * (12 + 4 + 4 * 3) for r in reqs)
+    d2h = sum(r.scene.particles.n * 12 for r in reqs)
+    batch_steps = max(res["chunks"], 1)
+    line = {
+        "metric": "particle-steps/s (served, continuous batching)", "value": total_ps / dev_s,
+        "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": res["step_ms_p50"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded numpy scene generator, Poisson arrivals)",
+        "config": {"workload": "served_mixed", "requests": nreq, "steps_per_request": args.steps,
+                   "arrival_rate_per_s": args.rate, "capacity_particles": args.capacity,
+                   "max_scenes": args.max_scenes, "chunk_steps": args.chunk,
+                   "l2": "inputs larger than L2", "parallelism": f"scenes sharded over {world} rank(s)"},
+        "served": {"throughput_wall": total_ps / wall_max, "wall_s": wall_max,
+                   "step_ms_p50": res["step_ms_p50"], "step_ms_p99": res["step_ms_p99"],
+                   "request_s_p50": res["request_s_p50"], "request_s_p99": res["request_s_p99"],
+                   "repacks": res["repacks"], "chunks": res["chunks"],
+                   "max_avg_density_err": res["max_density_err"]},
+        "plain": {"throughput": plain["throughput"], "requests": plain["requests"],
+                  "ratio_served_over_plain": (total_ps / wall_max) / plain["throughput"],
+                  "alone_vs_mix_max_abs_dx": mix_err},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "peak_source": f"{peak_kind} hbm_gbs", "alg_bytes_per_launch":
+                     ALG_BYTES[dom] * n, "traffic": None, "kernel_ms": kms, "particles": n},
+        "gpu_launches": launches,
+        "e2e": {"value": total_ps / wall_max, "unit": "particle-steps/s",
+                "h2d_bytes_per_step": int(h2d / batch_steps), "d2h_bytes_per_step": int(d2h / batch_steps)},
+        "clocks": cs.summary(),
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline([reqs[0].scene], budget_s=args.cpu_budget)
+    print(json.dumps(line))
+
+
 def run_ours(args):
     import torch
 
@@ -214,6 +304,11 @@ def run_ours(args):
     from nonnewton_b200.config import SimConfig
 
     world, rank, local = dist_setup(args)
+    if args.workload == "served":
+        run_served(args, world, rank)
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
     scenes = make_workload(args.workload, seed=rank)
     sc = scenes[0]
     m = sph.initialize(SimConfig(config=sc.config), particles=sc.particles, quirks=sc.param.quirks)
@@ -327,6 +422,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--requests", type=int, default=512)
+    ap.add_argument("--rate", type=float, default=200.0, help="Poisson arrival rate of the served workload (1/s)")
+    ap.add_argument("--capacity", type=int, default=4_000_000, help="resident particles of the server")
+    ap.add_argument("--max-scenes", type=int, default=256)
+    ap.add_argument("--chunk", type=int, default=10, help="steps between admissions")
+    ap.add_argument("--plain-sample", type=int, default=48)
     ap.add_argument("--host-loop", action="store_true",
                     help="drive the solver loops from the host instead of CUDA-graph while-nodes "
                          "(for ncu launch lists: ncu does not profile kernel nodes inside conditional nodes)")

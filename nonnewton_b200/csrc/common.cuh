@@ -23,6 +23,8 @@ struct SceneDev {
   float origin[3];
   float cell;                     // cell edge (= h)
   float h, k_w, k2_w, k_grad, W0; // cubic spline constants
+  float inv_h;
+  float h2_thr;                   // smallest float whose rounded sqrt is >= h
   float rho0, inv_rho0;
   float g[3];
   float eps;
@@ -114,6 +116,62 @@ __device__ __forceinline__ float3 kernel_grad(float3 r, float rn, const SceneDev
   }
   return res;
 }
+
+// The same cubic spline and gradient as kernel_w / kernel_grad, from r^2 and without
+// divisions (1/h precomputed, 1/|r| from rsqrt): used inside the neighbour loops,
+// where it agrees with the reference expressions to a few ulp.
+__device__ __forceinline__ void kwg_r2(float3 r, float r2, const SceneDev& s, float& w, float3& g) {
+  const float inv_rn = r2 > 0.f ? rsqrtf(r2) : 0.f;
+  const float rn = r2 * inv_rn;
+  const float q = rn * s.inv_h;
+  const float t = 1.f - q;
+  const bool in = q <= 1.f;
+  const bool inner = q <= 0.5f;
+  w = in ? (inner ? s.k_w * (6.f * q * q * (q - 1.f) + 1.f) : s.k2_w * (t * t * t)) : 0.f;
+  const float f = inner ? s.k_grad * q * (3.f * q - 2.f) : -s.k_grad * t * t;
+  const float c = (rn > 1e-5f && in) ? f * inv_rn * s.inv_h : 0.f;
+  g = make_float3(r.x * c, r.y * c, r.z * c);
+}
+__device__ __forceinline__ float kw_r2(float r2, const SceneDev& s) {
+  const float rn = r2 > 0.f ? r2 * rsqrtf(r2) : 0.f;
+  const float q = rn * s.inv_h;
+  const float t = 1.f - q;
+  const float w = q <= 0.5f ? s.k_w * (6.f * q * q * (q - 1.f) + 1.f) : s.k2_w * (t * t * t);
+  return q <= 1.f ? w : 0.f;
+}
+__device__ __forceinline__ float3 kgrad_r2(float3 r, float r2, const SceneDev& s) {
+  float w;
+  float3 g;
+  kwg_r2(r, r2, s, w, g);
+  return g;
+}
+
+// Neighbour loop in batches of NB_U list entries: the NB_U list loads, then the NB_U
+// gathers of `load`, are issued before any `use`, so several dependent load chains
+// are in flight per thread (the passes are latency-bound on list -> gather).
+#ifndef NB_U
+#define NB_U 4
+#endif
+template <typename Load, typename Use>
+__device__ __forceinline__ void nb_batches(const int32_t* __restrict__ list, int stride, int c, int self, Load load,
+                                           Use use) {
+  for (int k = 0; k < c; k += NB_U) {
+    int j[NB_U];
+#pragma unroll
+    for (int u = 0; u < NB_U; ++u) j[u] = (k + u < c) ? __ldg(list + (size_t)(k + u) * stride) : self;
+    decltype(load(0)) g[NB_U];
+#pragma unroll
+    for (int u = 0; u < NB_U; ++u) g[u] = load(j[u]);
+#pragma unroll
+    for (int u = 0; u < NB_U; ++u)
+      if (k + u < c) use(j[u], g[u]);
+  }
+}
+
+// Material of a slot is also kept in the sign of pos.w: the volume is stored
+// positive for fluid and negative for solid particles, so neighbour loops need no
+// separate class gather.
+__device__ __forceinline__ bool w_fluid(float w) { return w > 0.f; }
 
 __device__ __forceinline__ int slot_scene(uint32_t fl) { return (int)(fl >> NN_SCENE_SHIFT); }
 __device__ __forceinline__ bool cls_fluid(uint32_t fl) { return (fl & (NN_CLS_VALID | NN_CLS_SOLID)) == NN_CLS_VALID; }

@@ -91,7 +91,15 @@ struct nn_ctx {
   unsigned long long cur_handle = 0;
   int64_t capture_nodes = 0;
   std::map<const void*, int> occ;      // blocks per SM per kernel
+  uint64_t graph_sig = 0;              // features the captured graphs were built for
 };
+
+// The kernels and loops a captured step contains depend only on these features.
+static uint64_t feature_sig(const nn_ctx* c) {
+  return (uint64_t)c->any_fluid | ((uint64_t)c->any_div << 1) | ((uint64_t)c->any_nonnewton << 2) |
+         ((uint64_t)c->any_implicit << 3) | ((uint64_t)std::min(c->el_mult_max, 255) << 8) |
+         ((uint64_t)(c->ne > 0) << 16) | ((uint64_t)c->block << 20);
+}
 
 static thread_local char g_err[512];
 
@@ -167,6 +175,9 @@ static int launch(nn_ctx* c, cudaStream_t s, void (*k)(KArgs...), int block, int
   } else {
     per_sm = it->second;
   }
+  // A captured graph must serve any batch composition up to the capacity, so its
+  // grids are sized by the capacity (kernels grid-stride over the device sizes).
+  if (c->in_capture) work = std::max(work, c->cap);
   int64_t want = ((int64_t)std::max(work, 1) + block - 1) / block;
   int grid = (int)std::min<int64_t>(want, (int64_t)c->sms * per_sm);
   grid = std::max(grid, 1);
@@ -265,16 +276,17 @@ static int enq_search(nn_ctx* c, cudaStream_t s) {
   c->cur = 1 - c->cur;
   Dev d = make_dev(c, c->cur);
   const int B = 256;
-  const int tiles = (c->ncells + 1 + SCAN_TILE - 1) / SCAN_TILE;
-  RC(launch(c, s, k_zero_cells, B, c->ncells + 1, d));
+  const int64_t cells = c->in_capture ? c->max_cells : c->ncells;
+  const int tiles = (int)((cells + 1 + SCAN_TILE - 1) / SCAN_TILE);
+  RC(launch(c, s, k_zero_cells, B, (int)std::min<int64_t>(cells + 1, INT32_MAX), d));
   RC(launch(c, s, k_keys, B, c->n, d));
   RC(launch_g(c, s, k_scan_tiles, std::min(tiles, c->sms * 2), SCAN_THREADS, d));
   RC(launch_g(c, s, k_scan_sums, 1, SCAN_THREADS, d));
   RC(launch_g(c, s, k_scan_apply, std::min(tiles, c->sms * 2), SCAN_THREADS, d));
   RC(launch(c, s, k_scatter, B, c->n, d));
-  RC(launch(c, s, k_cell_sort, B, c->ncells, d));
+  RC(launch(c, s, k_cell_sort, B, (int)std::min<int64_t>(cells, INT32_MAX), d));
   RC(launch(c, s, k_gather, B, c->n, d));
-  RC(launch(c, s, k_build_lists, c->block, c->n, d));
+  RC(launch(c, s, k_build_lists, NS_WARPS * 32, c->n, d));
   c->searched = true;
   return NN_OK;
 }
@@ -394,6 +406,7 @@ static int capture_step(nn_ctx* c, cudaStream_t s, int parity) {
   c->cur = saved;
   if (rc != NN_OK) { if (g) cudaGraphDestroy(g); return rc; }
   if (e != cudaSuccess) return fail(c, NN_ERR_CUDA, "step capture: %s", cudaGetErrorString(e));
+  c->graph_sig = feature_sig(c);
   e = cudaGraphInstantiate(&c->exec[parity], g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) return fail(c, NN_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
@@ -439,6 +452,13 @@ static SceneDev make_scene(const nn_scene_desc& sd, int64_t cell_base, int el_mu
   s.mbits = mb;
   s.cell = (float)h;
   s.h = (float)h;
+  s.inv_h = (float)(1.0 / h);
+  {  // exact squared cut-off: sqrt_rn(r2) < h  <=>  r2 < h2_thr
+    float t = s.h * s.h;
+    while (t > 0.f && std::sqrt(t) >= s.h) t = std::nextafter(t, 0.f);
+    while (std::sqrt(t) < s.h) t = std::nextafter(t, INFINITY);
+    s.h2_thr = t;
+  }
   const double k = 8.0 / kPi / (h * h * h);
   s.k_w = (float)k;
   s.k2_w = (float)(k * 2.0);
@@ -626,10 +646,12 @@ int nn_bind_state(nn_ctx* c, const nn_state* st) {
   if (st->n > 0 && (!st->x || !st->x_0 || !st->v || !st->acceleration || !st->volume || !st->m || !st->density ||
                     !st->dfsph_factor || !st->density_adv || !st->material || !st->is_dynamic || !st->phase_id))
     return fail(c, NN_ERR_INVALID_ARG, "nn_bind_state: required field is NULL");
+  nn_state prev = c->state;
+  prev.n = st->n;
+  if (std::memcmp(&prev, st, sizeof(nn_state)) != 0) drop_graphs(c);
   c->state = *st;
   c->bound = true;
   c->searched = false;
-  drop_graphs(c);
   return NN_OK;
 }
 
@@ -695,8 +717,11 @@ int nn_set_scenes(nn_ctx* c, int32_t nscenes, const nn_scene_desc* scenes) {
     c->el_mult_max = std::max(c->el_mult_max, el_mult);
   }
   if (cells >= (int64_t)0x7fffffff) return fail(c, NN_ERR_CAPACITY, "%lld grid cells exceed the 32-bit key space", (long long)cells);
+  if (cells > c->max_cells) drop_graphs(c);  // the scan grids were sized for the old table
   RC(ensure_cells(c, cells));
-  drop_graphs(c);
+  c->ne = (int)el_id.size();
+  // elastic buffers are reallocated below (their pointers and stride are graph arguments)
+  if (feature_sig(c) != c->graph_sig || c->ne > 0) drop_graphs(c);
   c->scenes.assign(scenes, scenes + nscenes);
   c->sdev = sdev;
   c->n = n;
@@ -830,7 +855,7 @@ int nn_time_kernel(nn_ctx* c, int32_t kernel, int32_t reps, float* ms_out) {
       case NN_K_DIVERGENCE_UPDATE: return launch(c, s, k_divergence_update, B, c->n, d);
       case NN_K_DENSITY_CHANGE: return launch(c, s, k_density_change, B, c->n, d, 1);
       case NN_K_DENSITY_FACTOR: return launch(c, s, k_density_factor, B, c->n, d, 1, 1);
-      case NN_K_BUILD_LISTS: return launch(c, s, k_build_lists, B, c->n, d);
+      case NN_K_BUILD_LISTS: return launch(c, s, k_build_lists, NS_WARPS * 32, c->n, d);
       case NN_K_CG_MATVEC: return launch(c, s, k_cg_matvec, B, c->n, d);
       default: return launch(c, s, k_nonpressure, B, c->n, d);
     }
@@ -1031,7 +1056,7 @@ extern "C" int nn_neighbors_noalloc(const float* x, int32_t n, const double* dom
   k_scatter<<<gN, B, 0, st>>>(d);
   k_cell_sort<<<gC, B, 0, st>>>(d);
   k_na_gather<<<gN, B, 0, st>>>(d);
-  k_build_lists<<<gN, B, 0, st>>>(d);
+  k_build_lists<<<gN, NS_WARPS * 32, 0, st>>>(d);
   k_export_neighbors<<<gN, B, 0, st>>>(d, num_neighbors, neighbors, width);
   e = cudaGetLastError();
   if (e != cudaSuccess) return fail(c, NN_ERR_CUDA, "nn_neighbors_noalloc: %s", cudaGetErrorString(e));

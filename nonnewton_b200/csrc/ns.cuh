@@ -205,7 +205,9 @@ __global__ void k_gather(Dev d) {
       if (truth) {
         id = s;
         int sc = d.scene_of_id[id];
-        p = make_float4(d.t.x[3 * id], d.t.x[3 * id + 1], d.t.x[3 * id + 2], d.t.volume[id]);
+        const float vol = d.t.volume[id];
+        p = make_float4(d.t.x[3 * id], d.t.x[3 * id + 1], d.t.x[3 * id + 2],
+                        d.t.material[id] == NN_SOLID ? -vol : vol);  // signed volume: solid < 0
         v = make_float4(d.t.v[3 * id], d.t.v[3 * id + 1], d.t.v[3 * id + 2], 0.f);
         m = d.t.m[id];
         rho = d.t.density[id];
@@ -236,20 +238,83 @@ __global__ void k_gather(Dev d) {
 // Neighbour lists: for every slot, the 9 (dy, dz) rows of three x-adjacent cells are
 // contiguous slot ranges; candidates are tested with the reference's exact f32
 // expression. Lists hold slot indices, transposed [k][cap] for coalesced reads.
-__global__ void k_build_lists(Dev d) {
+//
+// A warp whose 32 slots lie in one (y, z) row of one scene (the common case, since
+// slots are cell-sorted) stages each candidate row, covering all its lanes' windows,
+// into shared memory with coalesced loads, in chunks of NS_CHUNK; each lane then tests
+// its own 3-cell window from shared memory. Other warps read candidates directly.
+// The in-range test sqrt_rn(r2) < h is evaluated as r2 < h2_thr, where h2_thr is the
+// smallest float whose correctly rounded square root is >= h (exactly equivalent).
+#define NS_WARPS 8
+#define NS_CHUNK 128
+__device__ __forceinline__ float exact_r2(float3 r) {
+  return __fadd_rn(__fadd_rn(__fmul_rn(r.x, r.x), __fmul_rn(r.y, r.y)), __fmul_rn(r.z, r.z));
+}
+
+__global__ void __launch_bounds__(NS_WARPS * 32) k_build_lists(Dev d) {
+  __shared__ float4 stage_all[NS_WARPS][NS_CHUNK];
+  float4* stage = stage_all[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31;
+  const unsigned full = 0xffffffffu;
   const int n = d.d_n[0];
   FOR_SLOTS_WARP(i, valid, n) {
-    int cnt = 0;
-    int scn = 0;
+    int cnt = 0, scn = 0, cx = 0, cy = 0, cz = 0;
+    float4 pi = make_float4(0.f, 0.f, 0.f, 0.f);
     if (valid) {
-      const uint32_t fl = d.w.flags[i];
-      scn = slot_scene(fl);
-      const SceneDev& s = d.sc[scn];
-      const float4 pi = d.w.pos[i];
-      int cx, cy, cz;
-      cell_key(s, pi.x, pi.y, pi.z, &cx, &cy, &cz);
-      const int x0 = max(cx - 1, 0), x1 = min(cx + 1, s.gx - 1);
-      const float3 xi = f3(pi);
+      scn = slot_scene(d.w.flags[i]);
+      pi = d.w.pos[i];
+      cell_key(d.sc[scn], pi.x, pi.y, pi.z, &cx, &cy, &cz);
+    }
+    const SceneDev& s = d.sc[scn];
+    const float3 xi = f3(pi);
+    const float thr = s.h2_thr;
+    const int x0 = max(cx - 1, 0), x1 = min(cx + 1, s.gx - 1);
+    // lane 0 is always valid (the warp's first slot is below n)
+    const int ly = __shfl_sync(full, cy, 0), lz = __shfl_sync(full, cz, 0), ls = __shfl_sync(full, scn, 0);
+    const bool uniform = __all_sync(full, !valid || (cy == ly && cz == lz && scn == ls));
+    auto append = [&](int j) {
+      if (cnt < d.max_nb) d.nbr[(size_t)cnt * d.cap + i] = j;
+      ++cnt;
+    };
+    if (uniform) {
+      // every bound below is warp-uniform: the lanes past the end of the array carry
+      // scene 0, so the scene of lane 0 is used (all valid lanes share it)
+      const SceneDev& su = d.sc[ls];
+      const int wx0 = max(__reduce_min_sync(full, valid ? cx : 0x7fffffff) - 1, 0);
+      const int wx1 = min(__reduce_max_sync(full, valid ? cx : -1) + 1, su.gx - 1);
+      for (int dz = -1; dz <= 1; ++dz) {
+        const int zz = lz + dz;
+        if (zz < 0 || zz >= su.gz) continue;
+        for (int dy = -1; dy <= 1; ++dy) {
+          const int yy = ly + dy;
+          if (yy < 0 || yy >= su.gy) continue;
+          const int64_t row = su.cell_base + (int64_t)morton2((uint32_t)yy, (uint32_t)zz) * su.gx;
+          const uint32_t rb = d.cell_count[row + wx0], re = d.cell_count[row + wx1 + 1];
+          uint32_t b = 0, e = 0;
+          if (valid) { b = d.cell_count[row + x0]; e = d.cell_count[row + x1 + 1]; }
+          for (uint32_t c0 = rb; c0 < re; c0 += NS_CHUNK) {
+            const uint32_t c1 = min(c0 + NS_CHUNK, re);
+            for (uint32_t t = lane; t < c1 - c0; t += 32) stage[t] = __ldg(&d.w.pos[c0 + t]);
+            __syncwarp();
+            const uint32_t lo = max(b, c0), hi = min(e, c1);
+            uint32_t j = lo;
+            for (; j + 4 <= hi; j += 4) {  // four independent tests, appended in order
+              const float r0 = exact_r2(xi - f3(stage[j - c0]));
+              const float r1 = exact_r2(xi - f3(stage[j + 1 - c0]));
+              const float r2 = exact_r2(xi - f3(stage[j + 2 - c0]));
+              const float r3 = exact_r2(xi - f3(stage[j + 3 - c0]));
+              if (r0 < thr && (int)j != i) append((int)j);
+              if (r1 < thr && (int)j + 1 != i) append((int)j + 1);
+              if (r2 < thr && (int)j + 2 != i) append((int)j + 2);
+              if (r3 < thr && (int)j + 3 != i) append((int)j + 3);
+            }
+            for (; j < hi; ++j)
+              if (exact_r2(xi - f3(stage[j - c0])) < thr && (int)j != i) append((int)j);
+            __syncwarp();
+          }
+        }
+      }
+    } else if (valid) {
       for (int dz = -1; dz <= 1; ++dz) {
         const int zz = cz + dz;
         if (zz < 0 || zz >= s.gz) continue;
@@ -260,14 +325,12 @@ __global__ void k_build_lists(Dev d) {
           const uint32_t b = d.cell_count[row + x0], e = d.cell_count[row + x1 + 1];
           for (uint32_t j = b; j < e; ++j) {
             if ((int)j == i) continue;
-            const float4 pj = __ldg(&d.w.pos[j]);
-            if (exact_norm(xi - f3(pj)) < s.h) {
-              if (cnt < d.max_nb) d.nbr[(size_t)cnt * d.cap + i] = (int)j;
-              ++cnt;
-            }
+            if (exact_r2(xi - f3(__ldg(&d.w.pos[j]))) < thr) append((int)j);
           }
         }
       }
+    }
+    if (valid) {
       d.nbr_cnt[i] = min(cnt, d.max_nb);
       if (cnt > d.max_nb) set_status(&d.dyn[scn], NN_ERR_NEIGHBOR_OVERFLOW);
     }

@@ -19,13 +19,15 @@ __global__ void k_boundary_volume(Dev d, int moving) {
     const SceneDev& s = d.sc[slot_scene(fl)];
     const float3 xi = f3(d.w.pos[i]);
     float delta = s.W0;
-    NB_LOOP(d, i, j) {
-      if (cls_solid(d.w.flags[j])) {
-        float3 r = xi - f3(d.w.pos[j]);
-        delta += kernel_w(sqrtf(dot3(r, r)), s);
-      }
-    }
-    d.w.pos[i].w = 1.f / delta * 3.f;
+    // plain loads: this pass writes pos.w of solid slots (the sign never changes)
+    nb_batches(d.nbr + i, d.cap, d.nbr_cnt[i], i, [&](int j) { return d.w.pos[j]; },
+               [&](int, float4 pj) {
+                 if (!w_fluid(pj.w)) {
+                   const float3 r = xi - f3(pj);
+                   delta += kw_r2(dot3(r, r), s);
+                 }
+               });
+    d.w.pos[i].w = -(1.f / delta * 3.f);
   }
 }
 
@@ -54,17 +56,18 @@ __global__ void k_density_factor(Dev d, int do_density, int do_factor) {
       const float3 xi = f3(pi);
       float den = 0.f, sum_grad = 0.f;
       float3 gpi = make_float3(0.f, 0.f, 0.f);
-      NB_LOOP(d, i, j) {
-        const float4 pj = d.w.pos[j];
-        const float3 r = xi - f3(pj);
-        const float rn = sqrtf(dot3(r, r));
-        den += pj.w * kernel_w(rn, s);
-        if (do_factor) {
-          const float3 gpj = kernel_grad(r, rn, s) * (-pj.w);
-          if (cls_fluid(d.w.flags[j])) sum_grad += dot3(gpj, gpj);
-          gpi -= gpj;
-        }
-      }
+      nb_batches(d.nbr + i, d.cap, d.nbr_cnt[i], i, [&](int j) { return __ldg(&d.w.pos[j]); },
+                 [&](int, float4 pj) {
+                   const float3 r = xi - f3(pj);
+                   float w;
+                   float3 g;
+                   kwg_r2(r, dot3(r, r), s, w, g);
+                   const float V = fabsf(pj.w);
+                   den += V * w;
+                   const float3 gpj = g * (-V);
+                   if (w_fluid(pj.w)) sum_grad += dot3(gpj, gpj);
+                   gpi -= gpj;
+                 });
       if (do_density) {
         rho = pi.w * s.W0;
         rho += den;
@@ -83,6 +86,7 @@ __global__ void k_density_factor(Dev d, int do_density, int do_factor) {
 // compute_density_change (SPH/main.py:1610-1645). mode 0: first call of
 // divergence_solve, also applies alpha *= 1/dt (1688); mode 1: solver iteration,
 // accumulates the FP64 density error (1669-1675, 1717-1719).
+struct GPV { float4 p, v; };
 __global__ void k_density_change(Dev d, int mode) {
   const int n = d.d_n[0];
   FOR_SLOTS_WARP(i, valid, n) {
@@ -94,17 +98,15 @@ __global__ void k_density_change(Dev d, int mode) {
       const SceneDev& s = d.sc[scn];
       const float3 xi = f3(d.w.pos[i]);
       const float3 vi = f3(d.w.vel[i]);
+      const int c = d.nbr_cnt[i];
       float dd = 0.f;
-      int cnt = 0;
-      NB_LOOP(d, i, j) {
-        const float4 pj = d.w.pos[j];
-        const float3 r = xi - f3(pj);
-        const float rn = sqrtf(dot3(r, r));
-        dd += pj.w * dot3(vi - f3(d.w.vel[j]), kernel_grad(r, rn, s));
-        ++cnt;
-      }
+      nb_batches(d.nbr + i, d.cap, c, i, [&](int j) { return GPV{__ldg(&d.w.pos[j]), __ldg(&d.w.vel[j])}; },
+                 [&](int, const GPV& g) {
+                   const float3 r = xi - f3(g.p);
+                   dd += fabsf(g.p.w) * dot3(vi - f3(g.v), kgrad_r2(r, dot3(r, r), s));
+                 });
       dd = fmaxf(dd, 0.f);
-      if (cnt < 20) dd = 0.f;
+      if (c < 20) dd = 0.f;
       d.rho_adv[i] = dd;
       float a = d.alpha[i];
       if (mode == 0) {
@@ -120,6 +122,7 @@ __global__ void k_density_change(Dev d, int mode) {
 
 // divergence_solver_iteration_kernel (SPH/main.py:1721-1760). The pushes onto
 // dynamic solids (1755-1760) are omitted: clear_accelerations (1552) discards them.
+struct GPK { float4 p; float k; };
 __global__ void k_divergence_update(Dev d) {
   const int n = d.d_n[0];
   GRID_STRIDE(i, n) {
@@ -132,23 +135,16 @@ __global__ void k_divergence_update(Dev d) {
     const float3 xi = f3(d.w.pos[i]);
     const float k_i = d.kappa[i];
     float3 dv = make_float3(0.f, 0.f, 0.f);
-    NB_LOOP(d, i, j) {
-      const uint32_t fj = d.w.flags[j];
-      if (cls_fluid(fj)) {
-        const float k_sum = k_i + d.kappa[j];
-        if (fabsf(k_sum) > s.eps) {
-          const float4 pj = d.w.pos[j];
-          const float3 r = xi - f3(pj);
-          const float3 gpj = kernel_grad(r, sqrtf(dot3(r, r)), s) * (-pj.w);
-          dv -= gpj * (dt * k_sum);
-        }
-      } else if (fabsf(k_i) > s.eps) {
-        const float4 pj = d.w.pos[j];
-        const float3 r = xi - f3(pj);
-        const float3 gpj = kernel_grad(r, sqrtf(dot3(r, r)), s) * (-pj.w);
-        dv += gpj * ((-dt * 1.f) * k_i);
-      }
-    }
+    nb_batches(d.nbr + i, d.cap, d.nbr_cnt[i], i, [&](int j) { return GPK{__ldg(&d.w.pos[j]), __ldg(&d.kappa[j])}; },
+               [&](int, const GPK& g) {
+                 const float3 r = xi - f3(g.p);
+                 if (w_fluid(g.p.w)) {
+                   const float k_sum = k_i + g.k;
+                   if (fabsf(k_sum) > s.eps) dv -= kgrad_r2(r, dot3(r, r), s) * (-g.p.w) * (dt * k_sum);
+                 } else if (fabsf(k_i) > s.eps) {
+                   dv += kgrad_r2(r, dot3(r, r), s) * g.p.w * ((-dt * 1.f) * k_i);
+                 }
+               });
     float4 v = d.w.vel[i];
     v.x += dv.x; v.y += dv.y; v.z += dv.z;
     d.w.vel[i] = v;
@@ -182,13 +178,13 @@ __global__ void k_density_adv(Dev d, int mode) {
       const float3 xi = f3(d.w.pos[i]);
       const float3 vi = f3(d.w.vel[i]);
       float delta = 0.f;
-      NB_LOOP(d, i, j) {
-        const float4 pj = d.w.pos[j];
-        const float3 r = xi - f3(pj);
-        const float rn = sqrtf(dot3(r, r));
-        delta += pj.w * dot3(vi - f3(d.w.vel[j]), kernel_grad(r, rn, s));
-      }
-      float da = d.w.dens[i] / s.rho0 + dt * delta;
+      nb_batches(d.nbr + i, d.cap, d.nbr_cnt[i], i,
+                 [&](int j) { return GPV{__ldg(&d.w.pos[j]), __ldg(&d.w.vel[j])}; },
+                 [&](int, const GPV& g) {
+                   const float3 r = xi - f3(g.p);
+                   delta += fabsf(g.p.w) * dot3(vi - f3(g.v), kgrad_r2(r, dot3(r, r), s));
+                 });
+      float da = d.w.dens[i] * s.inv_rho0 + dt * delta;
       da = fmaxf(da, 1.f);
       d.rho_adv[i] = da;
       float a = d.alpha[i];
@@ -218,42 +214,31 @@ __global__ void k_pressure_update(Dev d) {
     const float dt = d.dyn[scn].dt;
     const float4 pi = d.w.pos[i];
     const float3 xi = f3(pi);
+    auto load = [&](int j) { return GPK{__ldg(&d.w.pos[j]), __ldg(&d.kappa[j])}; };
     if (fluid) {
       const float k_i = d.kappa[i];
       float4 v4 = d.w.vel[i];
       float3 vi = f3(v4);
-      NB_LOOP(d, i, j) {
-        const uint32_t fj = d.w.flags[j];
-        if (cls_fluid(fj)) {
-          const float k_sum = k_i + d.kappa[j];
-          if (fabsf(k_sum) > s.eps) {
-            const float4 pj = d.w.pos[j];
-            const float3 r = xi - f3(pj);
-            const float3 gpj = kernel_grad(r, sqrtf(dot3(r, r)), s) * (-pj.w);
-            vi -= gpj * (dt * k_sum);
-          }
+      nb_batches(d.nbr + i, d.cap, d.nbr_cnt[i], i, load, [&](int, const GPK& g) {
+        const float3 r = xi - f3(g.p);
+        if (w_fluid(g.p.w)) {
+          const float k_sum = k_i + g.k;
+          if (fabsf(k_sum) > s.eps) vi -= kgrad_r2(r, dot3(r, r), s) * (-g.p.w) * (dt * k_sum);
         } else if (fabsf(k_i) > s.eps) {
-          const float4 pj = d.w.pos[j];
-          const float3 r = xi - f3(pj);
-          const float3 gpj = kernel_grad(r, sqrtf(dot3(r, r)), s) * (-pj.w);
-          vi += gpj * ((-dt * 1.f) * k_i);
+          vi += kgrad_r2(r, dot3(r, r), s) * g.p.w * ((-dt * 1.f) * k_i);
         }
-      }
+      });
       d.w.vel[i] = make_float4(vi.x, vi.y, vi.z, v4.w);
     } else {
+      const float Vi = fabsf(pi.w);
+      const float inv_dt = 1.f / dt;
       float3 ai = make_float3(0.f, 0.f, 0.f);
-      NB_LOOP(d, i, j) {
-        const uint32_t fj = d.w.flags[j];
-        if (!cls_fluid(fj)) continue;
-        const float k_j = d.kappa[j];
-        if (!(fabsf(k_j) > s.eps)) continue;
-        const float3 r = f3(d.w.pos[j]) - xi;  // x_fluid - x_solid, as the fluid sees it
-        const float3 gpj = kernel_grad(r, sqrtf(dot3(r, r)), s) * (-pi.w);
-        const float3 vc = gpj * ((-dt * 1.f) * k_j);
-        ai.x += (-vc.x) * 1.f / dt;
-        ai.y += (-vc.y) * 1.f / dt;
-        ai.z += (-vc.z) * 1.f / dt;
-      }
+      nb_batches(d.nbr + i, d.cap, d.nbr_cnt[i], i, load, [&](int, const GPK& g) {
+        if (!w_fluid(g.p.w) || !(fabsf(g.k) > s.eps)) return;
+        const float3 r = f3(g.p) - xi;  // x_fluid - x_solid, as the fluid computes it
+        const float3 vc = kgrad_r2(r, dot3(r, r), s) * (-Vi) * ((-dt * 1.f) * g.k);
+        ai -= vc * inv_dt;
+      });
       float4 a = d.acc4[i];
       a.x += ai.x; a.y += ai.y; a.z += ai.z;
       d.acc4[i] = a;
@@ -404,6 +389,7 @@ __device__ __forceinline__ float nn_law(float g, const SceneDev& s) {
 // NonNewton.calcStrainRate (SPH/main.py:461-492) + law. Quirk mode: every particle,
 // the accumulator keeps only the last neighbour, norm before scaling. Otherwise: fluid
 // particles, D = (0.5/rho_i) sum_j m_j (v_ji (x) gW + gW (x) v_ji), gamma = |D|_F.
+struct GSR { float4 p, v; float m; int id; };
 __global__ void k_strain_rate(Dev d) {
   const int n = d.d_n[0];
   GRID_STRIDE(i, n) {
@@ -416,20 +402,21 @@ __global__ void k_strain_rate(Dev d) {
     const float3 vi = f3(d.w.vel[i]);
     float S[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // symmetric: 00 11 22 01 02 12
     int last_id = -1;  // quirk: the term of the last neighbour in id order survives
-    NB_LOOP(d, i, j) {
-      const float3 r = xi - f3(d.w.pos[j]);
-      const float3 gw = kernel_grad(r, sqrtf(dot3(r, r)), s);
-      const float3 vji = f3(d.w.vel[j]) - vi;
-      const float mj = d.w.mass[j];
-      float t[6] = {(vji.x * gw.x + vji.x * gw.x) * mj, (vji.y * gw.y + vji.y * gw.y) * mj,
-                    (vji.z * gw.z + vji.z * gw.z) * mj, (vji.x * gw.y + vji.y * gw.x) * mj,
-                    (vji.x * gw.z + vji.z * gw.x) * mj, (vji.y * gw.z + vji.z * gw.y) * mj};
-      const int jid = d.w.id[j];
-      const bool take = jid > last_id;
-      if (q && take) last_id = jid;
+    nb_batches(d.nbr + i, d.cap, d.nbr_cnt[i], i,
+               [&](int j) { return GSR{__ldg(&d.w.pos[j]), __ldg(&d.w.vel[j]), __ldg(&d.w.mass[j]), __ldg(&d.w.id[j])}; },
+               [&](int, const GSR& g) {
+                 const float3 r = xi - f3(g.p);
+                 const float3 gw = kgrad_r2(r, dot3(r, r), s);
+                 const float3 vji = f3(g.v) - vi;
+                 const float mj = g.m;
+                 const float t[6] = {(vji.x * gw.x + vji.x * gw.x) * mj, (vji.y * gw.y + vji.y * gw.y) * mj,
+                                     (vji.z * gw.z + vji.z * gw.z) * mj, (vji.x * gw.y + vji.y * gw.x) * mj,
+                                     (vji.x * gw.z + vji.z * gw.x) * mj, (vji.y * gw.z + vji.z * gw.y) * mj};
+                 const bool take = g.id > last_id;
+                 if (q && take) last_id = g.id;
 #pragma unroll
-      for (int k = 0; k < 6; ++k) S[k] = q ? (take ? t[k] : S[k]) : S[k] + t[k];
-    }
+                 for (int k = 0; k < 6; ++k) S[k] = q ? (take ? t[k] : S[k]) : S[k] + t[k];
+               });
     const float sc = 0.5f / d.w.dens[i];
     float nrm2;
     if (q) {
@@ -451,6 +438,7 @@ __global__ void k_strain_rate(Dev d) {
 // from their fluid neighbours (the reference scatters it, 1459-1460). The velocity
 // update of non_pressure_advect cannot join this pass: the viscosity reads the
 // neighbours' velocities.
+struct GNP { float4 p, v; float m, rho; };
 __global__ void k_nonpressure(Dev d) {
   const int n = d.d_n[0];
   GRID_STRIDE(i, n) {
@@ -464,52 +452,49 @@ __global__ void k_nonpressure(Dev d) {
     const bool vi_on = !implicit_visc && (s.flags & NN_F_VISCOSITY) != 0;
     const float4 pi = d.w.pos[i];
     const float3 xi = f3(pi);
-    const float4 v4 = d.w.vel[i];
-    const float3 vi = f3(v4);
+    const float3 vi = f3(d.w.vel[i]);
+    auto load = [&](int j) {
+      return GNP{__ldg(&d.w.pos[j]), __ldg(&d.w.vel[j]), __ldg(&d.w.mass[j]), __ldg(&d.w.dens[j])};
+    };
     if (fluid) {
+      if (!st_on && !vi_on) continue;
       const float mi = d.w.mass[i];
       float3 st = make_float3(0.f, 0.f, 0.f), vs = make_float3(0.f, 0.f, 0.f);
       const float rho_i = d.w.dens[i];
-      NB_LOOP(d, i, j) {
-        const uint32_t fj = d.w.flags[j];
-        const float4 pj = d.w.pos[j];
-        const float3 r = xi - f3(pj);
+      nb_batches(d.nbr + i, d.cap, d.nbr_cnt[i], i, load, [&](int, const GNP& g) {
+        const float3 r = xi - f3(g.p);
         const float r2 = dot3(r, r);
-        const float rn = sqrtf(r2);
-        if (cls_fluid(fj)) {
-          const float mj = d.w.mass[j];
+        float w;
+        float3 gw;
+        kwg_r2(r, r2, s, w, gw);
+        if (w_fluid(g.p.w)) {
           if (st_on) {
-            const float c = s.sigma / mi * mj;
-            const float w = r2 > s.dia2 ? kernel_w(rn, s) : s.w_dia;
-            st -= (r * c) * w;
+            const float c = s.sigma / mi * g.m;
+            st -= (r * c) * (r2 > s.dia2 ? w : s.w_dia);
           }
           if (vi_on) {
-            const float v_xy = dot3(vi - f3(d.w.vel[j]), r);
-            const float sc = 10.f * s.visc * (mj / d.w.dens[j]) * v_xy / (rn * rn + s.c01h2);
-            vs += kernel_grad(r, rn, s) * sc;
+            const float v_xy = dot3(vi - f3(g.v), r);
+            vs += gw * (10.f * s.visc * (g.m / g.rho) * v_xy / (r2 + s.c01h2));
           }
         } else if (vi_on && s.visc_b != 0.f) {
-          const float v_xy = dot3(vi - f3(d.w.vel[j]), r);
-          const float sc = 10.f * s.visc_b * (s.rho0 * pj.w / rho_i) * v_xy / (rn * rn + s.c01h2);
-          vs += kernel_grad(r, rn, s) * sc;
+          const float v_xy = dot3(vi - f3(g.v), r);
+          vs += gw * (10.f * s.visc_b * (s.rho0 * fabsf(g.p.w) / rho_i) * v_xy / (r2 + s.c01h2));
         }
-      }
+      });
       float4 a = d.acc4[i];
       if (st_on) { a.x += st.x; a.y += st.y; a.z += st.z; }
       if (vi_on) { a.x += vs.x; a.y += vs.y; a.z += vs.z; }
       d.acc4[i] = a;
     } else if (cls_dyn_solid(fl) && vi_on && s.visc_b != 0.f) {
+      const float Vi = fabsf(pi.w);
       float3 f = make_float3(0.f, 0.f, 0.f);
-      NB_LOOP(d, i, j) {
-        const uint32_t fj = d.w.flags[j];
-        if (!cls_fluid(fj)) continue;
-        const float3 xj = f3(d.w.pos[j]);
-        const float3 r = xj - xi;  // fluid minus solid, as the fluid computes it
-        const float rn = sqrtf(dot3(r, r));
-        const float v_xy = dot3(f3(d.w.vel[j]) - vi, r);
-        const float sc = 10.f * s.visc_b * (s.rho0 * pi.w / d.w.dens[j]) * v_xy / (rn * rn + s.c01h2);
-        f += kernel_grad(r, rn, s) * sc;
-      }
+      nb_batches(d.nbr + i, d.cap, d.nbr_cnt[i], i, load, [&](int, const GNP& g) {
+        if (!w_fluid(g.p.w)) return;
+        const float3 r = f3(g.p) - xi;  // fluid minus solid, as the fluid computes it
+        const float r2 = dot3(r, r);
+        const float v_xy = dot3(f3(g.v) - vi, r);
+        f += kgrad_r2(r, r2, s) * (10.f * s.visc_b * (s.rho0 * Vi / g.rho) * v_xy / (r2 + s.c01h2));
+      });
       float4 a = d.acc4[i];
       a.x -= f.x; a.y -= f.y; a.z -= f.z;
       d.acc4[i] = a;
@@ -540,45 +525,50 @@ __device__ __forceinline__ bool cg_row(const Dev& d, int i, uint32_t fl) {
   return scene_implicit(d.sc[slot_scene(fl)]);
 }
 
-// A p for one row; also the diagonal block (setup) when D != nullptr.
-__device__ __forceinline__ float3 cg_apply(const Dev& d, int i, const float4* vec, float3 vi, const SceneDev& s,
-                                           float dt, float* D, float3* bcorr) {
-  const float4 pi = d.w.pos[i];
-  const float3 xi = f3(pi);
+// A p for one row; in the setup also the diagonal block D and the right-hand-side
+// correction of moving boundaries (SETUP: `vec` is the velocity field).
+struct GCG { float4 p, x, a; uint32_t fl; };
+template <bool SETUP>
+__device__ __forceinline__ float3 cg_apply(const Dev& d, int i, const float4* __restrict__ vec, float3 vi,
+                                           const SceneDev& s, float dt, float* D, float3* bcorr) {
+  const float3 xi = f3(d.w.pos[i]);
   const float4 ai = d.cg_aux[i];
   const float mi = d.w.mass[i];
   const float rho_i = d.w.dens[i];
   float3 acc = vi * mi;
   const float cdt = dt * 10.f;
-  NB_LOOP(d, i, j) {
-    const uint32_t fj = d.w.flags[j];
-    const float4 pj = d.w.pos[j];
-    const float3 r = xi - f3(pj);
-    const float r2 = dot3(r, r);
-    const float rn = sqrtf(r2);
-    const float3 gw = kernel_grad(r, rn, s);
-    const float w = 1.f / (rn * rn + s.c01h2);
-    float c;
-    float3 diff;
-    if (cls_fluid(fj)) {
-      const float4 aj = d.cg_aux[j];
-      c = cdt * 0.5f * (ai.x + aj.x) * ai.y * aj.y;
-      diff = vi - f3(vec[j]);
-    } else {
-      c = cdt * s.mu_b * mi * s.rho0 * pj.w / (rho_i * rho_i);
-      diff = vi;
-      if (bcorr && cls_dyn_solid(fj)) {  // known boundary velocity moves to the rhs
-        const float kv = dot3(r, f3(d.w.vel[j])) * w;
-        *bcorr -= gw * (c * kv);
-      }
-    }
-    acc -= gw * (c * dot3(r, diff) * w);
-    if (D) {
-      const float cw = c * w;
-      D[0] -= cw * gw.x * r.x; D[1] -= cw * gw.y * r.y; D[2] -= cw * gw.z * r.z;
-      D[3] -= cw * gw.x * r.y; D[4] -= cw * gw.x * r.z; D[5] -= cw * gw.y * r.z;
-    }
-  }
+  const float cb = cdt * s.mu_b * mi * s.rho0 / (rho_i * rho_i);
+  nb_batches(d.nbr + i, d.cap, d.nbr_cnt[i], i,
+             [&](int j) {
+               GCG g;
+               g.p = __ldg(&d.w.pos[j]);
+               g.x = __ldg(&vec[j]);
+               g.a = __ldg(&d.cg_aux[j]);
+               g.fl = SETUP ? __ldg(&d.w.flags[j]) : 0u;
+               return g;
+             },
+             [&](int, const GCG& g) {
+               const float3 r = xi - f3(g.p);
+               const float r2 = dot3(r, r);
+               const float3 gw = kgrad_r2(r, r2, s);
+               const float w = __fdividef(1.f, r2 + s.c01h2);
+               float c;
+               float3 diff;
+               if (w_fluid(g.p.w)) {
+                 c = cdt * 0.5f * (ai.x + g.a.x) * ai.y * g.a.y;
+                 diff = vi - f3(g.x);
+               } else {
+                 c = cb * fabsf(g.p.w);
+                 diff = vi;
+                 if (SETUP && cls_dyn_solid(g.fl)) *bcorr -= gw * (c * dot3(r, f3(g.x)) * w);
+               }
+               acc -= gw * (c * dot3(r, diff) * w);
+               if (SETUP) {
+                 const float cw = c * w;
+                 D[0] -= cw * gw.x * r.x; D[1] -= cw * gw.y * r.y; D[2] -= cw * gw.z * r.z;
+                 D[3] -= cw * gw.x * r.y; D[4] -= cw * gw.x * r.z; D[5] -= cw * gw.y * r.z;
+               }
+             });
   return acc;
 }
 
@@ -601,7 +591,7 @@ __global__ void k_cg_setup(Dev d) {
       const float3 vi = f3(d.w.vel[i]);
       float D[6] = {mi, mi, mi, 0.f, 0.f, 0.f};
       float3 bc = make_float3(0.f, 0.f, 0.f);
-      const float3 Av = cg_apply(d, i, d.w.vel, vi, s, dt, D, &bc);
+      const float3 Av = cg_apply<true>(d, i, d.w.vel, vi, s, dt, D, &bc);
       const float3 b = vi * mi + bc;
       // symmetric 3x3 inverse in double
       double a00 = D[0], a11 = D[1], a22 = D[2], a01 = D[3], a02 = D[4], a12 = D[5];
@@ -667,7 +657,7 @@ __global__ void k_cg_matvec(Dev d) {
     if (work) {
       const SceneDev& s = d.sc[scn];
       const float3 p = f3(d.cg_p[i]);
-      const float3 Ap = cg_apply(d, i, d.cg_p, p, s, d.dyn[scn].dt, nullptr, nullptr);
+      const float3 Ap = cg_apply<false>(d, i, d.cg_p, p, s, d.dyn[scn].dt, nullptr, nullptr);
       d.cg_Ap[i] = make_float4(Ap.x, Ap.y, Ap.z, 0.f);
       pap = (double)p.x * Ap.x + (double)p.y * Ap.y + (double)p.z * Ap.z;
     }
@@ -1011,7 +1001,7 @@ __global__ void k_sync_out(Dev d, uint32_t mask) {
     if (mask & 1u) { d.t.x[3 * id] = p.x; d.t.x[3 * id + 1] = p.y; d.t.x[3 * id + 2] = p.z; }
     if (mask & 2u) { const float4 v = d.w.vel[i]; d.t.v[3 * id] = v.x; d.t.v[3 * id + 1] = v.y; d.t.v[3 * id + 2] = v.z; }
     if (mask & 4u) { const float4 a = d.acc4[i]; d.t.a[3 * id] = a.x; d.t.a[3 * id + 1] = a.y; d.t.a[3 * id + 2] = a.z; }
-    if (mask & 8u) d.t.volume[id] = p.w;
+    if (mask & 8u) d.t.volume[id] = fabsf(p.w);
     if (mask & 16u) d.t.density[id] = d.w.dens[i];
     if (mask & 32u) d.t.dfsph_factor[id] = d.alpha[i];
     if (mask & 64u) d.t.density_adv[id] = d.rho_adv[i];
@@ -1038,7 +1028,7 @@ __global__ void k_sync_in(Dev d, uint32_t mask) {
     const int id = d.w.id[i];
     float4 p = d.w.pos[i];
     if (mask & 1u) { p.x = d.t.x[3 * id]; p.y = d.t.x[3 * id + 1]; p.z = d.t.x[3 * id + 2]; }
-    if (mask & 8u) p.w = d.t.volume[id];
+    if (mask & 8u) p.w = cls_solid(d.w.flags[i]) ? -d.t.volume[id] : d.t.volume[id];
     d.w.pos[i] = p;
     if (mask & 2u) d.w.vel[i] = make_float4(d.t.v[3 * id], d.t.v[3 * id + 1], d.t.v[3 * id + 2], 0.f);
     if (mask & 4u) d.acc4[i] = make_float4(d.t.a[3 * id], d.t.a[3 * id + 1], d.t.a[3 * id + 2], 0.f);
