@@ -223,6 +223,9 @@ int nn_get_neighbors(nn_ctx* ctx, int32_t* num_neighbors, int32_t* neighbors, in
 /* Statistics of scene `scene` (copies from the device; synchronises the stream). */
 int nn_get_stats(nn_ctx* ctx, int32_t scene, nn_stats* out);
 
+/* Statistics of scenes [first, first + count) in one device-to-host copy. */
+int nn_get_stats_range(nn_ctx* ctx, int32_t first, int32_t count, nn_stats* out);
+
 /* Kernel launches enqueued by this context since creation (for launch accounting). */
 int64_t nn_launch_count(const nn_ctx* ctx);
 

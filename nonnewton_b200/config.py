@@ -110,6 +110,7 @@ class Parameter:
     cfl_min_dt: float = 1e-4
     cfl_max_dt: float = 5e-3
     quirks: bool = False
+    has_elastic: bool = False
     surface_tension: float = 0.01
     extra: dict = field(default_factory=dict)
 
@@ -194,6 +195,7 @@ class Parameter:
             cfl_min_dt=float(g("cflMinTimeStepSize", 1e-4)),
             cfl_max_dt=float(g("cflMaxTimeStepSize", 5e-3)),
             quirks=bool(g("referenceQuirks", quirks)),
+            has_elastic=bool(el),
         )
         if p.simulation_method not in (4, None):
             # build_solver (SPH/main.py:196-203)
@@ -218,7 +220,8 @@ class Parameter:
             f |= _abi.NN_F_QUIRKS
         if self.carreau_textbook:
             f |= _abi.NN_F_CARREAU_TEXTBOOK
-        f |= _abi.NN_F_ELASTICITY
+        if self.has_elastic:
+            f |= _abi.NN_F_ELASTICITY
         return f
 
     def to_c(self) -> _abi.nn_scene_params:

@@ -660,7 +660,7 @@ int nn_set_scenes(nn_ctx* c, int32_t nscenes, const nn_scene_desc* scenes) {
   if (!c->bound) return fail(c, NN_ERR_STATE, "nn_set_scenes: bind the state first");
   if (nscenes > c->max_scenes) return fail(c, NN_ERR_CAPACITY, "%d scenes > capacity %d", nscenes, c->max_scenes);
   const int n = c->state.n;
-  std::vector<int32_t> scene_of_id(n, -1);
+  std::vector<std::pair<int, int>> ranges;  // (start, scene): the scenes must tile [0, n)
   for (int k = 0; k < nscenes; ++k) {
     const nn_scene_desc& sd = scenes[k];
     if (sd.size != sizeof(nn_scene_desc) || sd.params.size != sizeof(nn_scene_params))
@@ -669,16 +669,24 @@ int nn_set_scenes(nn_ctx* c, int32_t nscenes, const nn_scene_desc* scenes) {
       return fail(c, NN_ERR_INVALID_ARG, "scene %d: range [%d, %d) outside the state", k, sd.start, sd.start + sd.n);
     if (!(sd.params.support_radius > 0) || !(sd.params.dt > 0) || !(sd.params.density0 > 0))
       return fail(c, NN_ERR_INVALID_ARG, "scene %d: support_radius, dt and density0 must be positive", k);
-    for (int i = sd.start; i < sd.start + sd.n; ++i) {
-      if (scene_of_id[i] != -1) return fail(c, NN_ERR_INVALID_ARG, "scene %d overlaps another scene", k);
-      scene_of_id[i] = k;
-    }
+    if (sd.n > 0) ranges.push_back({sd.start, k});
   }
-  for (int i = 0; i < n; ++i)
-    if (scene_of_id[i] < 0) return fail(c, NN_ERR_INVALID_ARG, "particle %d belongs to no scene", i);
-  // host copies of the class fields to lay out the elastic particles
-  std::vector<int32_t> mat(n), ph(n);
-  if (n > 0) {
+  std::sort(ranges.begin(), ranges.end());
+  int covered = 0;
+  for (auto& r : ranges) {
+    if (r.first < covered) return fail(c, NN_ERR_INVALID_ARG, "scene %d overlaps another scene", r.second);
+    if (r.first > covered) return fail(c, NN_ERR_INVALID_ARG, "particle %d belongs to no scene", covered);
+    covered = r.first + scenes[r.second].n;
+  }
+  if (covered != n) return fail(c, NN_ERR_INVALID_ARG, "particle %d belongs to no scene", covered);
+  // host copies of the class fields lay out the elastic particles; scenes without the
+  // elasticity flag need none (no transfer for pure-fluid batches)
+  bool want_el = false;
+  for (int k = 0; k < nscenes; ++k) want_el |= (scenes[k].params.flags & NN_F_ELASTICITY) != 0;
+  std::vector<int32_t> mat, ph;
+  if (n > 0 && want_el) {
+    mat.resize(n);
+    ph.resize(n);
     CK(cudaMemcpy(mat.data(), c->state.material, n * sizeof(int32_t), cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(ph.data(), c->state.phase_id, n * sizeof(int32_t), cudaMemcpyDeviceToHost));
   }
@@ -692,8 +700,9 @@ int nn_set_scenes(nn_ctx* c, int32_t nscenes, const nn_scene_desc* scenes) {
     const nn_scene_desc& sd = scenes[k];
     const bool q = (sd.params.flags & NN_F_QUIRKS) != 0;
     std::vector<int> phases;
-    for (int i = sd.start; i < sd.start + sd.n; ++i)
-      if (mat[i] == NN_SOLID && ph[i] >= NN_PHASE_ELASTIC_BASE) phases.push_back(ph[i]);
+    if (sd.params.flags & NN_F_ELASTICITY)
+      for (int i = sd.start; i < sd.start + sd.n; ++i)
+        if (mat[i] == NN_SOLID && ph[i] >= NN_PHASE_ELASTIC_BASE) phases.push_back(ph[i]);
     std::sort(phases.begin(), phases.end());
     phases.erase(std::unique(phases.begin(), phases.end()), phases.end());
     int el_mult = 0;
@@ -728,8 +737,7 @@ int nn_set_scenes(nn_ctx* c, int32_t nscenes, const nn_scene_desc* scenes) {
   c->ncells = (int)cells;
   c->ne = (int)el_id.size();
   free_elastic(c);
-  std::vector<int32_t> e_of_id(c->cap, -1);
-  for (size_t e = 0; e < el_id.size(); ++e) e_of_id[el_id[e]] = (int32_t)e;
+
   if (c->ne > 0) {
     c->el_stride = c->ne;
     const size_t E = (size_t)c->ne;
@@ -741,8 +749,13 @@ int nn_set_scenes(nn_ctx* c, int32_t nscenes, const nn_scene_desc* scenes) {
     CK(cudaMemcpy(c->el_id, el_id.data(), E * sizeof(int32_t), cudaMemcpyHostToDevice));
     CK(cudaMemset(c->el_cnt, 0, E * sizeof(int32_t)));
   }
-  CK(cudaMemcpy(c->e_of_id, e_of_id.data(), c->cap * sizeof(int32_t), cudaMemcpyHostToDevice));
-  if (n > 0) CK(cudaMemcpy(c->d_scene_of_id, scene_of_id.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice));
+  if (c->ne > 0) {
+    std::vector<int32_t> e_of_id(n, -1);
+    for (size_t e = 0; e < el_id.size(); ++e) e_of_id[el_id[e]] = (int32_t)e;
+    CK(cudaMemcpy(c->e_of_id, e_of_id.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice));
+  } else if (n > 0) {
+    CK(cudaMemset(c->e_of_id, 0xff, n * sizeof(int32_t)));  // all -1
+  }
   if (nscenes > 0) {
     CK(cudaMemcpy(c->d_sc, sdev.data(), nscenes * sizeof(SceneDev), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(c->d_dyn, sdyn.data(), nscenes * sizeof(SceneDyn), cudaMemcpyHostToDevice));
@@ -750,6 +763,10 @@ int nn_set_scenes(nn_ctx* c, int32_t nscenes, const nn_scene_desc* scenes) {
   int32_t hn[4] = {n, nscenes, (int)cells, c->ne};
   CK(cudaMemcpy(c->d_n, hn, sizeof(hn), cudaMemcpyHostToDevice));
   CK(cudaMemset(c->d_acc, 0, (size_t)c->max_scenes * ACC_COUNT * NN_STRIPES * sizeof(double)));
+  if (nscenes > 0 && n > 0) {  // scene of every particle id, filled from the scene table on the device
+    k_scene_of_id<<<std::min(nscenes, 65535), 256>>>(make_dev(c, c->cur));
+    CK(cudaGetLastError());
+  }
   c->searched = false;
   return NN_OK;
 }
@@ -886,13 +903,7 @@ int nn_get_neighbors(nn_ctx* c, int32_t* num, int32_t* lists, int32_t width) {
   return NN_OK;
 }
 
-int nn_get_stats(nn_ctx* c, int32_t scene, nn_stats* out) {
-  RC(check_ready(c));
-  if (!out || scene < 0 || scene >= (int)c->scenes.size()) return fail(c, NN_ERR_INVALID_ARG, "bad scene index");
-  cudaStream_t s = run_stream(c);
-  SceneDyn y;
-  CK(cudaMemcpyAsync(&y, c->d_dyn + scene, sizeof(y), cudaMemcpyDeviceToHost, s));
-  CK(cudaStreamSynchronize(s));
+static void fill_stats(const SceneDyn& y, nn_stats* out) {
   std::memset(out, 0, sizeof(*out));
   out->size = sizeof(*out);
   out->status = y.status;
@@ -909,7 +920,25 @@ int nn_get_stats(nn_ctx* c, int32_t scene, nn_stats* out) {
   std::memcpy(&md, &bits, sizeof(md));
   out->max_density = md;
   out->steps = y.steps;
+}
+
+int nn_get_stats_range(nn_ctx* c, int32_t first, int32_t count, nn_stats* out) {
+  RC(check_ready(c));
+  if (!out || first < 0 || count < 0 || first + count > (int)c->scenes.size())
+    return fail(c, NN_ERR_INVALID_ARG, "bad scene range");
+  if (count == 0) return NN_OK;
+  cudaStream_t s = run_stream(c);
+  std::vector<SceneDyn> y(count);
+  CK(cudaMemcpyAsync(y.data(), c->d_dyn + first, count * sizeof(SceneDyn), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  for (int k = 0; k < count; ++k) fill_stats(y[k], out + k);
   return NN_OK;
+}
+
+int nn_get_stats(nn_ctx* c, int32_t scene, nn_stats* out) {
+  RC(check_ready(c));
+  if (!out || scene < 0 || scene >= (int)c->scenes.size()) return fail(c, NN_ERR_INVALID_ARG, "bad scene index");
+  return nn_get_stats_range(c, scene, 1, out);
 }
 
 }  // extern "C"

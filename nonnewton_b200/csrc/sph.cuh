@@ -358,6 +358,16 @@ __global__ void k_force_active(Dev d) {
   }
 }
 
+// Scene index of every particle id, from the scene table (block b walks scenes b, b+grid, ...).
+__global__ void k_scene_of_id(Dev d) {
+  const int ns = d.d_n[1];
+  int32_t* so = const_cast<int32_t*>(d.scene_of_id);
+  for (int sc = blockIdx.x; sc < ns; sc += gridDim.x) {
+    const int b = d.sc[sc].start, n = d.sc[sc].n;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) so[b + i] = sc;
+  }
+}
+
 __global__ void k_step_end(Dev d) {
   const int ns = d.d_n[1];
   for (int sc = threadIdx.x; sc < ns; sc += blockDim.x) d.dyn[sc].steps += 1;

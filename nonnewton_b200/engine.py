@@ -49,6 +49,8 @@ def lib():
         L.nn_launch_count.restype = i64
         L.nn_set_block_size.argtypes = [vp, i32]
         L.nn_time_kernel.argtypes = [vp, i32, i32, C.POINTER(C.c_float)]
+        L.nn_get_stats_range.argtypes = [vp, i32, i32, C.POINTER(_abi.nn_stats)]
+        L.nn_get_stats_range.restype = C.c_int
         L.nn_time_kernel.restype = C.c_int
         for name in ("nn_ctx_create", "nn_ctx_destroy", "nn_ctx_set_stream", "nn_bind_state", "nn_set_scenes",
                      "nn_initialize", "nn_step", "nn_run_pass", "nn_get_neighbors", "nn_get_stats",
@@ -153,6 +155,11 @@ class Engine:
         s = _abi.nn_stats()
         self._rc(self.L.nn_get_stats(self.h, int(scene), C.byref(s)))
         return s.as_dict()
+
+    def stats_range(self, first: int, count: int) -> list[dict]:
+        arr = (_abi.nn_stats * max(count, 1))()
+        self._rc(self.L.nn_get_stats_range(self.h, int(first), int(count), arr))
+        return [arr[k].as_dict() for k in range(count)]
 
     def time_kernel(self, kernel: int, reps: int = 20) -> float:
         ms = C.c_float()

@@ -71,11 +71,19 @@ class Server:
             # retire finished requests
             done = [r for r in self.resident if r.done_steps >= r.steps]
             keep_idx = [k for k, r in enumerate(self.resident) if r.done_steps < r.steps]
-            for k, r in enumerate(self.resident):
-                if r.done_steps >= r.steps:
-                    r.result_x = self.batch.scene_view(k, "x").cpu().numpy()
-                    r.stats = self.batch.stats(k)
-                    r.finished = now()
+            if done:  # one device-to-host copy of all finished results and stats
+                ks = [k for k, r in enumerate(self.resident) if r.done_steps >= r.steps]
+                xs = torch.cat([self.batch.scene_view(k, "x") for k in ks]).cpu().numpy()
+                st = self.batch.engine.stats_range(0, len(self.resident))
+                off = 0
+                tf = now()
+                for k in ks:
+                    r = self.resident[k]
+                    m = r.scene.particles.n
+                    r.result_x = xs[off:off + m]
+                    off += m
+                    r.stats = st[k]
+                    r.finished = tf
                     finished.append(r)
             # admit arrived requests that fit
             t = now()
