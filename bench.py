@@ -311,7 +311,18 @@ def run_ours(args):
         return
     scenes = make_workload(args.workload, seed=rank)
     sc = scenes[0]
-    m = sph.initialize(SimConfig(config=sc.config), particles=sc.particles, quirks=sc.param.quirks)
+    tuning, tune_ms = None, None
+    if args.autotune:
+        from nonnewton_b200.autotune import autotune
+        from nonnewton_b200.batch import Batch
+
+        b = Batch(sc.particles.n, 1)
+        b.set([sc])
+        r = autotune(b, steps=3, warmup=2)
+        tuning, tune_ms = r["best"], {k: round(v, 4) for k, v in r["ms"].items()}
+        b.engine.close()
+        del b
+    m = sph.initialize(SimConfig(config=sc.config), particles=sc.particles, quirks=sc.param.quirks, tuning=tuning)
     solver = sph.build_solver()
     solver.initialize()
     n = sc.particles.n
@@ -392,7 +403,9 @@ def run_ours(args):
                    "l2": ("inputs larger than L2" if n * (48 + 4 * st["max_neighbors_seen"] * 0.75) > 126e6
                           else "inputs smaller than L2; not flushed"),
                    "step_graph": "host-driven loops" if args.host_loop else
-                   "CUDA graph with while-node solver loops"},
+                   "CUDA graph with while-node solver loops",
+                   "tuning": tuning or {"block": 256, "unroll": 4, "cell_factor": 1}},
+        "autotune_ms_per_step": tune_ms,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "peak_source": f"{peak_kind} hbm_gbs",
                      "alg_bytes_per_launch": ab, "traffic": None,
@@ -428,6 +441,7 @@ def main():
     ap.add_argument("--max-scenes", type=int, default=256)
     ap.add_argument("--chunk", type=int, default=10, help="steps between admissions")
     ap.add_argument("--plain-sample", type=int, default=48)
+    ap.add_argument("--autotune", action="store_true", help="pick block size, unroll and cell factor first")
     ap.add_argument("--host-loop", action="store_true",
                     help="drive the solver loops from the host instead of CUDA-graph while-nodes "
                          "(for ncu launch lists: ncu does not profile kernel nodes inside conditional nodes)")

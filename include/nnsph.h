@@ -273,6 +273,12 @@ int nn_neighbors_noalloc(const float* x, int32_t n, const double* domain_start, 
 /* Autotuned launch shape: threads per block for the neighbour passes. 0 = default. */
 int nn_set_block_size(nn_ctx* ctx, int32_t threads);
 
+/* All tuning knobs at once (0 = default): threads per block of the neighbour passes
+   (32..1024), neighbour chains each thread keeps in flight (2, 4 or 8), and the cell
+   factor f (cells of edge h / f searched with a (2f+1)-cell stencil; 1 or 2). A new
+   cell factor takes effect at the next nn_set_scenes, which must follow. */
+int nn_set_tuning(nn_ctx* ctx, int32_t block, int32_t unroll, int32_t cell_factor);
+
 #ifdef __cplusplus
 }
 #endif

@@ -21,7 +21,8 @@ struct SceneDev {
   int64_t cell_base;              // first cell key of the scene
   int32_t gx, gy, gz, mbits;      // grid size; rows (y,z) are Morton-ordered with mbits per axis
   float origin[3];
-  float cell;                     // cell edge (= h)
+  float cell;                     // cell edge (h / nf)
+  int32_t nf;                     // stencil half-width in cells (cell factor)
   float h, k_w, k2_w, k_grad, W0; // cubic spline constants
   float inv_h;
   float h2_thr;                   // smallest float whose rounded sqrt is >= h
@@ -149,16 +150,20 @@ __device__ __forceinline__ float3 kgrad_r2(float3 r, float r2, const SceneDev& s
 // Neighbour loop in batches of NB_U list entries: the NB_U list loads, then the NB_U
 // gathers of `load`, are issued before any `use`, so several dependent load chains
 // are in flight per thread (the passes are latency-bound on list -> gather).
-#ifndef NB_U
-#define NB_U 4
-#endif
-template <typename Load, typename Use>
+template <int NB_U, typename Load, typename Use>
 __device__ __forceinline__ void nb_batches(const int32_t* __restrict__ list, int stride, int c, int self, Load load,
                                            Use use) {
+  // software pipeline: the list entries of batch b+1 are loaded while batch b gathers
+  int jn[NB_U];
+#pragma unroll
+  for (int u = 0; u < NB_U; ++u) jn[u] = (u < c) ? __ldg(list + (size_t)u * stride) : self;
   for (int k = 0; k < c; k += NB_U) {
     int j[NB_U];
 #pragma unroll
-    for (int u = 0; u < NB_U; ++u) j[u] = (k + u < c) ? __ldg(list + (size_t)(k + u) * stride) : self;
+    for (int u = 0; u < NB_U; ++u) j[u] = jn[u];
+#pragma unroll
+    for (int u = 0; u < NB_U; ++u)
+      jn[u] = (k + NB_U + u < c) ? __ldg(list + (size_t)(k + NB_U + u) * stride) : self;
     decltype(load(0)) g[NB_U];
 #pragma unroll
     for (int u = 0; u < NB_U; ++u) g[u] = load(j[u]);

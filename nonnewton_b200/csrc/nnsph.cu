@@ -49,6 +49,8 @@ struct nn_ctx {
   std::string err;
   int64_t launches = 0;
   int block = 256;
+  int unroll = 4;                      // neighbour chains in flight per thread (2, 4, 8)
+  int cell_factor = 1;                 // cells of edge h / cell_factor
   // state binding and scenes
   nn_state state{};
   bool bound = false;
@@ -198,6 +200,9 @@ static int launch1(nn_ctx* c, cudaStream_t s, void (*k)(KArgs...), Args... args)
   return NN_OK;
 }
 
+// The instantiation of a neighbour kernel for the context's neighbour-batch depth.
+#define KU(k) (c->unroll == 8 ? &k<8> : c->unroll == 2 ? &k<2> : &k<4>)
+
 #define RC(x)                 \
   do {                        \
     int _r = (x);             \
@@ -296,11 +301,11 @@ static int enq_divergence(nn_ctx* c, cudaStream_t s) {
   const int B = c->block;
   RC(launch1(c, s, k_solver_begin, d, 0));
   RC(solver_loop(c, s, false,
-                 [&](cudaStream_t q) { return launch(c, q, k_density_change, B, c->n, make_dev(c, c->cur), 0); },
+                 [&](cudaStream_t q) { return launch(c, q, KU(k_density_change), B, c->n, make_dev(c, c->cur), 0); },
                  [&](cudaStream_t q) {
                    Dev e = make_dev(c, c->cur);
-                   RC(launch(c, q, k_divergence_update, B, c->n, e));
-                   RC(launch(c, q, k_density_change, B, c->n, e, 1));
+                   RC(launch(c, q, KU(k_divergence_update), B, c->n, e));
+                   RC(launch(c, q, KU(k_density_change), B, c->n, e, 1));
                    return launch1(c, q, k_solver_check, e, 0);
                  }));
   return launch(c, s, k_alpha_times_dt, 256, c->n, d);
@@ -311,11 +316,11 @@ static int enq_pressure(nn_ctx* c, cudaStream_t s) {
   const int B = c->block;
   RC(launch1(c, s, k_solver_begin, d, 1));
   return solver_loop(c, s, false,
-                     [&](cudaStream_t q) { return launch(c, q, k_density_adv, B, c->n, make_dev(c, c->cur), 0); },
+                     [&](cudaStream_t q) { return launch(c, q, KU(k_density_adv), B, c->n, make_dev(c, c->cur), 0); },
                      [&](cudaStream_t q) {
                        Dev e = make_dev(c, c->cur);
-                       RC(launch(c, q, k_pressure_update, B, c->n, e));
-                       RC(launch(c, q, k_density_adv, B, c->n, e, 1));
+                       RC(launch(c, q, KU(k_pressure_update), B, c->n, e));
+                       RC(launch(c, q, KU(k_density_adv), B, c->n, e, 1));
                        return launch1(c, q, k_solver_check, e, 1);
                      });
 }
@@ -323,15 +328,15 @@ static int enq_pressure(nn_ctx* c, cudaStream_t s) {
 static int enq_nonpressure(nn_ctx* c, cudaStream_t s, int advect) {
   Dev d = make_dev(c, c->cur);
   const int B = c->block;
-  if (c->any_nonnewton) RC(launch(c, s, k_strain_rate, B, c->n, d));
-  RC(launch(c, s, k_nonpressure, B, c->n, d));
+  if (c->any_nonnewton) RC(launch(c, s, KU(k_strain_rate), B, c->n, d));
+  RC(launch(c, s, KU(k_nonpressure), B, c->n, d));
   if (c->any_implicit) {
     RC(launch(c, s, k_cg_aux, 256, c->n, d));
-    RC(launch(c, s, k_cg_setup, B, c->n, d));
+    RC(launch(c, s, KU(k_cg_setup), B, c->n, d));
     RC(solver_loop(c, s, true, [&](cudaStream_t q) { return launch1(c, q, k_cg_check0, make_dev(c, c->cur)); },
                    [&](cudaStream_t q) {
                      Dev e = make_dev(c, c->cur);
-                     RC(launch(c, q, k_cg_matvec, B, c->n, e));
+                     RC(launch(c, q, KU(k_cg_matvec), B, c->n, e));
                      RC(launch1(c, q, k_cg_alpha, e));
                      RC(launch(c, q, k_cg_update, 256, c->n, e));
                      RC(launch1(c, q, k_cg_check, e));
@@ -358,7 +363,7 @@ static int enq_elastic(nn_ctx* c, cudaStream_t s) {
 static int enq_substep(nn_ctx* c, cudaStream_t s) {
   if (!c->any_fluid) return NN_OK;
   Dev d = make_dev(c, c->cur);
-  RC(launch(c, s, k_density_factor, c->block, c->n, d, 1, 1));
+  RC(launch(c, s, KU(k_density_factor), c->block, c->n, d, 1, 1));
   if (c->any_div) RC(enq_divergence(c, s));
   RC(launch(c, s, k_clear_acc, 256, c->n, d));
   RC(enq_nonpressure(c, s, 1));
@@ -371,7 +376,7 @@ static int enq_step(nn_ctx* c, cudaStream_t s) {
   RC(enq_search(c, s));
   Dev d = make_dev(c, c->cur);
   RC(launch1(c, s, k_step_dt, d, 1));
-  RC(launch(c, s, k_boundary_volume, c->block, c->n, d, 1));
+  RC(launch(c, s, KU(k_boundary_volume), c->block, c->n, d, 1));
   RC(launch(c, s, k_clear_acc, 256, c->n, d));
   RC(enq_substep(c, s));
   RC(enq_elastic(c, s));
@@ -431,7 +436,7 @@ static float host_kernel_w(float rn, float h, float k_w, float k2_w) {
   return res;
 }
 
-static SceneDev make_scene(const nn_scene_desc& sd, int64_t cell_base, int el_mult) {
+static SceneDev make_scene(const nn_scene_desc& sd, int64_t cell_base, int el_mult, int cell_factor = 1) {
   const nn_scene_params& p = sd.params;
   SceneDev s{};
   s.flags = p.flags;
@@ -441,16 +446,18 @@ static SceneDev make_scene(const nn_scene_desc& sd, int64_t cell_base, int el_mu
   s.cell_base = cell_base;
   const double h = p.support_radius;
   int g[3];
+  const double cell = h / cell_factor;
   for (int k = 0; k < 3; ++k) {
     s.origin[k] = (float)(p.domain_start[k] - 2.0 * h);
     double ext = (p.domain_end[k] - p.domain_start[k]) + 4.0 * h;
-    g[k] = (int)std::min(65535.0, std::max(1.0, std::ceil(ext / h) + 1.0));
+    g[k] = (int)std::min(65535.0, std::max(1.0, std::ceil(ext / cell) + 1.0));
   }
   s.gx = g[0]; s.gy = g[1]; s.gz = g[2];
   int mb = 0;
   while ((1 << mb) < std::max(g[1], g[2])) ++mb;
   s.mbits = mb;
-  s.cell = (float)h;
+  s.cell = (float)cell;
+  s.nf = cell_factor;
   s.h = (float)h;
   s.inv_h = (float)(1.0 / h);
   {  // exact squared cut-off: sqrt_rn(r2) < h  <=>  r2 < h2_thr
@@ -629,6 +636,23 @@ int nn_set_block_size(nn_ctx* c, int32_t threads) {
   return NN_OK;
 }
 
+int nn_set_tuning(nn_ctx* c, int32_t block, int32_t unroll, int32_t cell_factor) {
+  if (!c) return fail(nullptr, NN_ERR_INVALID_ARG, "null context");
+  if (block == 0) block = 256;
+  if (unroll == 0) unroll = 4;
+  if (cell_factor == 0) cell_factor = 1;
+  if (block < 32 || block > 1024 || (block % 32) || (unroll != 2 && unroll != 4 && unroll != 8) ||
+      (cell_factor != 1 && cell_factor != 2))
+    return fail(c, NN_ERR_INVALID_ARG, "tuning: block %d, unroll %d, cell factor %d", block, unroll, cell_factor);
+  if (block != c->block || unroll != c->unroll || cell_factor != c->cell_factor) drop_graphs(c);
+  if (cell_factor != c->cell_factor) c->scenes.clear();  // cell layout changes: set the scenes again
+  c->block = block;
+  c->unroll = unroll;
+  c->cell_factor = cell_factor;
+  c->occ.clear();
+  return NN_OK;
+}
+
 int64_t nn_launch_count(const nn_ctx* cc) {
   nn_ctx* c = const_cast<nn_ctx*>(cc);
   if (!c) return -1;
@@ -710,7 +734,7 @@ int nn_set_scenes(nn_ctx* c, int32_t nscenes, const nn_scene_desc* scenes) {
     if (el_mult > 0)
       for (int i = sd.start; i < sd.start + sd.n; ++i)
         if (q || (mat[i] == NN_SOLID && ph[i] >= NN_PHASE_ELASTIC_BASE)) el_id.push_back(i);
-    SceneDev s = make_scene(sd, cells, el_mult);
+    SceneDev s = make_scene(sd, cells, el_mult, c->cell_factor);
     cells += (int64_t)s.gx * ((int64_t)1 << (2 * s.mbits));
     sdev.push_back(s);
     SceneDyn y{};
@@ -786,8 +810,8 @@ int nn_initialize(nn_ctx* c) {
   Dev d = make_dev(c, c->cur);
   RC(launch1(c, s, k_step_dt, d, 0));
   if (c->ne > 0) RC(launch(c, s, k_el_init, 256, c->n, d));
-  RC(launch(c, s, k_boundary_volume, c->block, c->n, d, 0));
-  RC(launch(c, s, k_boundary_volume, c->block, c->n, d, 1));
+  RC(launch(c, s, KU(k_boundary_volume), c->block, c->n, d, 0));
+  RC(launch(c, s, KU(k_boundary_volume), c->block, c->n, d, 1));
   RC(enq_sync_out(c, s, SM_VOL));
   CK(cudaStreamSynchronize(s));
   return NN_OK;
@@ -834,11 +858,11 @@ int nn_run_pass(nn_ctx* c, int32_t pass) {
   RC(launch(c, s, k_sync_in, 256, c->n, d, (uint32_t)SM_ALL));
   RC(launch1(c, s, k_step_dt, d, 0));
   switch (pass) {
-    case NN_PASS_STATIC_BOUNDARY_VOLUME: RC(launch(c, s, k_boundary_volume, c->block, c->n, d, 0)); break;
-    case NN_PASS_MOVING_BOUNDARY_VOLUME: RC(launch(c, s, k_boundary_volume, c->block, c->n, d, 1)); break;
+    case NN_PASS_STATIC_BOUNDARY_VOLUME: RC(launch(c, s, KU(k_boundary_volume), c->block, c->n, d, 0)); break;
+    case NN_PASS_MOVING_BOUNDARY_VOLUME: RC(launch(c, s, KU(k_boundary_volume), c->block, c->n, d, 1)); break;
     case NN_PASS_CLEAR_ACCELERATIONS: RC(launch(c, s, k_clear_acc, 256, c->n, d)); break;
-    case NN_PASS_DENSITIES: RC(launch(c, s, k_density_factor, c->block, c->n, d, 1, 0)); break;
-    case NN_PASS_DFSPH_FACTOR: RC(launch(c, s, k_density_factor, c->block, c->n, d, 0, 1)); break;
+    case NN_PASS_DENSITIES: RC(launch(c, s, KU(k_density_factor), c->block, c->n, d, 1, 0)); break;
+    case NN_PASS_DFSPH_FACTOR: RC(launch(c, s, KU(k_density_factor), c->block, c->n, d, 0, 1)); break;
     case NN_PASS_DIVERGENCE_SOLVE: if (c->any_div) RC(enq_divergence(c, s)); break;
     case NN_PASS_NON_PRESSURE_FORCES: if (c->any_fluid) RC(enq_nonpressure(c, s, 0)); break;
     case NN_PASS_NON_PRESSURE_ADVECT: RC(launch(c, s, k_np_advect, 256, c->n, d)); break;
@@ -867,14 +891,14 @@ int nn_time_kernel(nn_ctx* c, int32_t kernel, int32_t reps, float* ms_out) {
   auto one = [&]() -> int {
     const int B = c->block;
     switch (kernel) {
-      case NN_K_PRESSURE_UPDATE: return launch(c, s, k_pressure_update, B, c->n, d);
-      case NN_K_DENSITY_ADV: return launch(c, s, k_density_adv, B, c->n, d, 1);
-      case NN_K_DIVERGENCE_UPDATE: return launch(c, s, k_divergence_update, B, c->n, d);
-      case NN_K_DENSITY_CHANGE: return launch(c, s, k_density_change, B, c->n, d, 1);
-      case NN_K_DENSITY_FACTOR: return launch(c, s, k_density_factor, B, c->n, d, 1, 1);
+      case NN_K_PRESSURE_UPDATE: return launch(c, s, KU(k_pressure_update), B, c->n, d);
+      case NN_K_DENSITY_ADV: return launch(c, s, KU(k_density_adv), B, c->n, d, 1);
+      case NN_K_DIVERGENCE_UPDATE: return launch(c, s, KU(k_divergence_update), B, c->n, d);
+      case NN_K_DENSITY_CHANGE: return launch(c, s, KU(k_density_change), B, c->n, d, 1);
+      case NN_K_DENSITY_FACTOR: return launch(c, s, KU(k_density_factor), B, c->n, d, 1, 1);
       case NN_K_BUILD_LISTS: return launch(c, s, k_build_lists, NS_WARPS * 32, c->n, d);
-      case NN_K_CG_MATVEC: return launch(c, s, k_cg_matvec, B, c->n, d);
-      default: return launch(c, s, k_nonpressure, B, c->n, d);
+      case NN_K_CG_MATVEC: return launch(c, s, KU(k_cg_matvec), B, c->n, d);
+      default: return launch(c, s, KU(k_nonpressure), B, c->n, d);
     }
   };
   RC(one());  // warm-up

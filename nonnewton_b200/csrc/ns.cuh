@@ -268,7 +268,7 @@ __global__ void __launch_bounds__(NS_WARPS * 32) k_build_lists(Dev d) {
     const SceneDev& s = d.sc[scn];
     const float3 xi = f3(pi);
     const float thr = s.h2_thr;
-    const int x0 = max(cx - 1, 0), x1 = min(cx + 1, s.gx - 1);
+    const int x0 = max(cx - s.nf, 0), x1 = min(cx + s.nf, s.gx - 1);
     // lane 0 is always valid (the warp's first slot is below n)
     const int ly = __shfl_sync(full, cy, 0), lz = __shfl_sync(full, cz, 0), ls = __shfl_sync(full, scn, 0);
     const bool uniform = __all_sync(full, !valid || (cy == ly && cz == lz && scn == ls));
@@ -280,12 +280,12 @@ __global__ void __launch_bounds__(NS_WARPS * 32) k_build_lists(Dev d) {
       // every bound below is warp-uniform: the lanes past the end of the array carry
       // scene 0, so the scene of lane 0 is used (all valid lanes share it)
       const SceneDev& su = d.sc[ls];
-      const int wx0 = max(__reduce_min_sync(full, valid ? cx : 0x7fffffff) - 1, 0);
-      const int wx1 = min(__reduce_max_sync(full, valid ? cx : -1) + 1, su.gx - 1);
-      for (int dz = -1; dz <= 1; ++dz) {
+      const int wx0 = max(__reduce_min_sync(full, valid ? cx : 0x7fffffff) - su.nf, 0);
+      const int wx1 = min(__reduce_max_sync(full, valid ? cx : -1) + su.nf, su.gx - 1);
+      for (int dz = -su.nf; dz <= su.nf; ++dz) {
         const int zz = lz + dz;
         if (zz < 0 || zz >= su.gz) continue;
-        for (int dy = -1; dy <= 1; ++dy) {
+        for (int dy = -su.nf; dy <= su.nf; ++dy) {
           const int yy = ly + dy;
           if (yy < 0 || yy >= su.gy) continue;
           const int64_t row = su.cell_base + (int64_t)morton2((uint32_t)yy, (uint32_t)zz) * su.gx;
@@ -315,10 +315,10 @@ __global__ void __launch_bounds__(NS_WARPS * 32) k_build_lists(Dev d) {
         }
       }
     } else if (valid) {
-      for (int dz = -1; dz <= 1; ++dz) {
+      for (int dz = -s.nf; dz <= s.nf; ++dz) {
         const int zz = cz + dz;
         if (zz < 0 || zz >= s.gz) continue;
-        for (int dy = -1; dy <= 1; ++dy) {
+        for (int dy = -s.nf; dy <= s.nf; ++dy) {
           const int yy = cy + dy;
           if (yy < 0 || yy >= s.gy) continue;
           const int64_t row = s.cell_base + (int64_t)morton2((uint32_t)yy, (uint32_t)zz) * s.gx;

@@ -11,6 +11,7 @@
 
 // ---------------------------------------------------------------------------
 // compute_static_boundary_volume / compute_moving_boundary_volume (SPH/main.py:1010-1035)
+template <int U>
 __global__ void k_boundary_volume(Dev d, int moving) {
   const int n = d.d_n[0];
   GRID_STRIDE(i, n) {
@@ -20,7 +21,7 @@ __global__ void k_boundary_volume(Dev d, int moving) {
     const float3 xi = f3(d.w.pos[i]);
     float delta = s.W0;
     // plain loads: this pass writes pos.w of solid slots (the sign never changes)
-    nb_batches(d.nbr + i, d.cap, d.nbr_cnt[i], i, [&](int j) { return d.w.pos[j]; },
+    nb_batches<U>(d.nbr + i, d.cap, d.nbr_cnt[i], i, [&](int j) { return d.w.pos[j]; },
                [&](int, float4 pj) {
                  if (!w_fluid(pj.w)) {
                    const float3 r = xi - f3(pj);
@@ -43,6 +44,7 @@ __global__ void k_clear_acc(Dev d) {
 
 // compute_densities (SPH/main.py:975-984) fused with compute_DFSPH_factor
 // (SPH/main.py:1569-1608): both walk the same neighbours with fixed positions.
+template <int U>
 __global__ void k_density_factor(Dev d, int do_density, int do_factor) {
   const int n = d.d_n[0];
   FOR_SLOTS_WARP(i, valid, n) {
@@ -56,7 +58,7 @@ __global__ void k_density_factor(Dev d, int do_density, int do_factor) {
       const float3 xi = f3(pi);
       float den = 0.f, sum_grad = 0.f;
       float3 gpi = make_float3(0.f, 0.f, 0.f);
-      nb_batches(d.nbr + i, d.cap, d.nbr_cnt[i], i, [&](int j) { return __ldg(&d.w.pos[j]); },
+      nb_batches<U>(d.nbr + i, d.cap, d.nbr_cnt[i], i, [&](int j) { return __ldg(&d.w.pos[j]); },
                  [&](int, float4 pj) {
                    const float3 r = xi - f3(pj);
                    float w;
@@ -87,6 +89,7 @@ __global__ void k_density_factor(Dev d, int do_density, int do_factor) {
 // divergence_solve, also applies alpha *= 1/dt (1688); mode 1: solver iteration,
 // accumulates the FP64 density error (1669-1675, 1717-1719).
 struct GPV { float4 p, v; };
+template <int U>
 __global__ void k_density_change(Dev d, int mode) {
   const int n = d.d_n[0];
   FOR_SLOTS_WARP(i, valid, n) {
@@ -100,7 +103,7 @@ __global__ void k_density_change(Dev d, int mode) {
       const float3 vi = f3(d.w.vel[i]);
       const int c = d.nbr_cnt[i];
       float dd = 0.f;
-      nb_batches(d.nbr + i, d.cap, c, i, [&](int j) { return GPV{__ldg(&d.w.pos[j]), __ldg(&d.w.vel[j])}; },
+      nb_batches<U>(d.nbr + i, d.cap, c, i, [&](int j) { return GPV{__ldg(&d.w.pos[j]), __ldg(&d.w.vel[j])}; },
                  [&](int, const GPV& g) {
                    const float3 r = xi - f3(g.p);
                    dd += fabsf(g.p.w) * dot3(vi - f3(g.v), kgrad_r2(r, dot3(r, r), s));
@@ -123,6 +126,7 @@ __global__ void k_density_change(Dev d, int mode) {
 // divergence_solver_iteration_kernel (SPH/main.py:1721-1760). The pushes onto
 // dynamic solids (1755-1760) are omitted: clear_accelerations (1552) discards them.
 struct GPK { float4 p; float k; };
+template <int U>
 __global__ void k_divergence_update(Dev d) {
   const int n = d.d_n[0];
   GRID_STRIDE(i, n) {
@@ -135,7 +139,7 @@ __global__ void k_divergence_update(Dev d) {
     const float3 xi = f3(d.w.pos[i]);
     const float k_i = d.kappa[i];
     float3 dv = make_float3(0.f, 0.f, 0.f);
-    nb_batches(d.nbr + i, d.cap, d.nbr_cnt[i], i, [&](int j) { return GPK{__ldg(&d.w.pos[j]), __ldg(&d.kappa[j])}; },
+    nb_batches<U>(d.nbr + i, d.cap, d.nbr_cnt[i], i, [&](int j) { return GPK{__ldg(&d.w.pos[j]), __ldg(&d.kappa[j])}; },
                [&](int, const GPK& g) {
                  const float3 r = xi - f3(g.p);
                  if (w_fluid(g.p.w)) {
@@ -165,6 +169,7 @@ __global__ void k_alpha_times_dt(Dev d) {
 
 // compute_density_adv (SPH/main.py:1647-1667). mode 0: first call of pressure_solve,
 // also alpha *= 1/dt^2 (1771); mode 1: iteration, FP64 error (1793-1797).
+template <int U>
 __global__ void k_density_adv(Dev d, int mode) {
   const int n = d.d_n[0];
   FOR_SLOTS_WARP(i, valid, n) {
@@ -178,7 +183,7 @@ __global__ void k_density_adv(Dev d, int mode) {
       const float3 xi = f3(d.w.pos[i]);
       const float3 vi = f3(d.w.vel[i]);
       float delta = 0.f;
-      nb_batches(d.nbr + i, d.cap, d.nbr_cnt[i], i,
+      nb_batches<U>(d.nbr + i, d.cap, d.nbr_cnt[i], i,
                  [&](int j) { return GPV{__ldg(&d.w.pos[j]), __ldg(&d.w.vel[j])}; },
                  [&](int, const GPV& g) {
                    const float3 r = xi - f3(g.p);
@@ -202,6 +207,7 @@ __global__ void k_density_adv(Dev d, int mode) {
 // pressure_solve_iteration_kernel (SPH/main.py:1799-1841). Fluid slots update v in
 // place per neighbour; dynamic solid slots gather the two-way coupling acceleration
 // from their fluid neighbours (the reference scatters it with atomics, 1835-1841).
+template <int U>
 __global__ void k_pressure_update(Dev d) {
   const int n = d.d_n[0];
   GRID_STRIDE(i, n) {
@@ -219,7 +225,7 @@ __global__ void k_pressure_update(Dev d) {
       const float k_i = d.kappa[i];
       float4 v4 = d.w.vel[i];
       float3 vi = f3(v4);
-      nb_batches(d.nbr + i, d.cap, d.nbr_cnt[i], i, load, [&](int, const GPK& g) {
+      nb_batches<U>(d.nbr + i, d.cap, d.nbr_cnt[i], i, load, [&](int, const GPK& g) {
         const float3 r = xi - f3(g.p);
         if (w_fluid(g.p.w)) {
           const float k_sum = k_i + g.k;
@@ -233,7 +239,7 @@ __global__ void k_pressure_update(Dev d) {
       const float Vi = fabsf(pi.w);
       const float inv_dt = 1.f / dt;
       float3 ai = make_float3(0.f, 0.f, 0.f);
-      nb_batches(d.nbr + i, d.cap, d.nbr_cnt[i], i, load, [&](int, const GPK& g) {
+      nb_batches<U>(d.nbr + i, d.cap, d.nbr_cnt[i], i, load, [&](int, const GPK& g) {
         if (!w_fluid(g.p.w) || !(fabsf(g.k) > s.eps)) return;
         const float3 r = f3(g.p) - xi;  // x_fluid - x_solid, as the fluid computes it
         const float3 vc = kgrad_r2(r, dot3(r, r), s) * (-Vi) * ((-dt * 1.f) * g.k);
@@ -400,6 +406,7 @@ __device__ __forceinline__ float nn_law(float g, const SceneDev& s) {
 // the accumulator keeps only the last neighbour, norm before scaling. Otherwise: fluid
 // particles, D = (0.5/rho_i) sum_j m_j (v_ji (x) gW + gW (x) v_ji), gamma = |D|_F.
 struct GSR { float4 p, v; float m; int id; };
+template <int U>
 __global__ void k_strain_rate(Dev d) {
   const int n = d.d_n[0];
   GRID_STRIDE(i, n) {
@@ -412,7 +419,7 @@ __global__ void k_strain_rate(Dev d) {
     const float3 vi = f3(d.w.vel[i]);
     float S[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // symmetric: 00 11 22 01 02 12
     int last_id = -1;  // quirk: the term of the last neighbour in id order survives
-    nb_batches(d.nbr + i, d.cap, d.nbr_cnt[i], i,
+    nb_batches<U>(d.nbr + i, d.cap, d.nbr_cnt[i], i,
                [&](int j) { return GSR{__ldg(&d.w.pos[j]), __ldg(&d.w.vel[j]), __ldg(&d.w.mass[j]), __ldg(&d.w.id[j])}; },
                [&](int, const GSR& g) {
                  const float3 r = xi - f3(g.p);
@@ -449,6 +456,7 @@ __global__ void k_strain_rate(Dev d) {
 // update of non_pressure_advect cannot join this pass: the viscosity reads the
 // neighbours' velocities.
 struct GNP { float4 p, v; float m, rho; };
+template <int U>
 __global__ void k_nonpressure(Dev d) {
   const int n = d.d_n[0];
   GRID_STRIDE(i, n) {
@@ -471,7 +479,7 @@ __global__ void k_nonpressure(Dev d) {
       const float mi = d.w.mass[i];
       float3 st = make_float3(0.f, 0.f, 0.f), vs = make_float3(0.f, 0.f, 0.f);
       const float rho_i = d.w.dens[i];
-      nb_batches(d.nbr + i, d.cap, d.nbr_cnt[i], i, load, [&](int, const GNP& g) {
+      nb_batches<U>(d.nbr + i, d.cap, d.nbr_cnt[i], i, load, [&](int, const GNP& g) {
         const float3 r = xi - f3(g.p);
         const float r2 = dot3(r, r);
         float w;
@@ -498,7 +506,7 @@ __global__ void k_nonpressure(Dev d) {
     } else if (cls_dyn_solid(fl) && vi_on && s.visc_b != 0.f) {
       const float Vi = fabsf(pi.w);
       float3 f = make_float3(0.f, 0.f, 0.f);
-      nb_batches(d.nbr + i, d.cap, d.nbr_cnt[i], i, load, [&](int, const GNP& g) {
+      nb_batches<U>(d.nbr + i, d.cap, d.nbr_cnt[i], i, load, [&](int, const GNP& g) {
         if (!w_fluid(g.p.w)) return;
         const float3 r = f3(g.p) - xi;  // fluid minus solid, as the fluid computes it
         const float r2 = dot3(r, r);
@@ -538,7 +546,7 @@ __device__ __forceinline__ bool cg_row(const Dev& d, int i, uint32_t fl) {
 // A p for one row; in the setup also the diagonal block D and the right-hand-side
 // correction of moving boundaries (SETUP: `vec` is the velocity field).
 struct GCG { float4 p, x, a; uint32_t fl; };
-template <bool SETUP>
+template <int U, bool SETUP>
 __device__ __forceinline__ float3 cg_apply(const Dev& d, int i, const float4* __restrict__ vec, float3 vi,
                                            const SceneDev& s, float dt, float* D, float3* bcorr) {
   const float3 xi = f3(d.w.pos[i]);
@@ -548,7 +556,7 @@ __device__ __forceinline__ float3 cg_apply(const Dev& d, int i, const float4* __
   float3 acc = vi * mi;
   const float cdt = dt * 10.f;
   const float cb = cdt * s.mu_b * mi * s.rho0 / (rho_i * rho_i);
-  nb_batches(d.nbr + i, d.cap, d.nbr_cnt[i], i,
+  nb_batches<U>(d.nbr + i, d.cap, d.nbr_cnt[i], i,
              [&](int j) {
                GCG g;
                g.p = __ldg(&d.w.pos[j]);
@@ -587,6 +595,7 @@ __device__ __forceinline__ float3 sym_apply(const float* P, float3 v) {  // P: 0
                      P[4] * v.x + P[5] * v.y + P[2] * v.z);
 }
 
+template <int U>
 __global__ void k_cg_setup(Dev d) {
   const int n = d.d_n[0];
   FOR_SLOTS_WARP(i, valid, n) {
@@ -601,7 +610,7 @@ __global__ void k_cg_setup(Dev d) {
       const float3 vi = f3(d.w.vel[i]);
       float D[6] = {mi, mi, mi, 0.f, 0.f, 0.f};
       float3 bc = make_float3(0.f, 0.f, 0.f);
-      const float3 Av = cg_apply<true>(d, i, d.w.vel, vi, s, dt, D, &bc);
+      const float3 Av = cg_apply<U, true>(d, i, d.w.vel, vi, s, dt, D, &bc);
       const float3 b = vi * mi + bc;
       // symmetric 3x3 inverse in double
       double a00 = D[0], a11 = D[1], a22 = D[2], a01 = D[3], a02 = D[4], a12 = D[5];
@@ -657,6 +666,7 @@ __global__ void k_cg_check0(Dev d) {
   }
 }
 
+template <int U>
 __global__ void k_cg_matvec(Dev d) {
   const int n = d.d_n[0];
   FOR_SLOTS_WARP(i, valid, n) {
@@ -667,7 +677,7 @@ __global__ void k_cg_matvec(Dev d) {
     if (work) {
       const SceneDev& s = d.sc[scn];
       const float3 p = f3(d.cg_p[i]);
-      const float3 Ap = cg_apply<false>(d, i, d.cg_p, p, s, d.dyn[scn].dt, nullptr, nullptr);
+      const float3 Ap = cg_apply<U, false>(d, i, d.cg_p, p, s, d.dyn[scn].dt, nullptr, nullptr);
       d.cg_Ap[i] = make_float4(Ap.x, Ap.y, Ap.z, 0.f);
       pap = (double)p.x * Ap.x + (double)p.y * Ap.y + (double)p.z * Ap.z;
     }

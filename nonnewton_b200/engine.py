@@ -110,6 +110,13 @@ class Engine:
     def set_block_size(self, threads: int):
         self._rc(self.L.nn_set_block_size(self.h, int(threads)))
 
+    def set_tuning(self, block: int = 0, unroll: int = 0, cell_factor: int = 0):
+        """Launch shape of the neighbour passes; a new cell factor needs set_scenes again."""
+        f = self.L.nn_set_tuning
+        f.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]
+        f.restype = C.c_int
+        self._rc(f(self.h, int(block), int(unroll), int(cell_factor)))
+
     def bind(self, pd, n: int | None = None) -> None:
         """Bind the fields of `pd`; `n` active particles (default: all rows)."""
         st = _abi.nn_state()

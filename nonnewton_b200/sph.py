@@ -225,7 +225,7 @@ def build_solver():
 
 
 def initialize(config: SimConfig | str | dict | None = None, particles: ParticleSet | None = None,
-               quirks: bool = False, max_neighbors: int = 64, device="cuda"):
+               quirks: bool = False, max_neighbors: int = 64, device="cuda", tuning: dict | None = None):
     """`initialize()` (SPH/main.py:1870-1895): parameters, particles, fields, the
     neighbour search object and the CUDA engine (which also sets up elastic bodies)."""
     if isinstance(config, str):
@@ -242,6 +242,8 @@ def initialize(config: SimConfig | str | dict | None = None, particles: Particle
     meta.pd = ParticleData(ps.n, device=device)
     initialize_particles(meta.pd, ps, meta.parm)
     meta.engine = Engine(max(ps.n, 1), 1, max_neighbors, device=device)
+    if tuning:
+        meta.engine.set_tuning(tuning.get("block", 0), tuning.get("unroll", 0), tuning.get("cell_factor", 0))
     meta.engine.bind(meta.pd)
     meta.engine.set_scenes([(0, ps.n, ps.n_fluid, meta.parm.to_c())])
     meta.ns = NeighborhoodSearchSparse(meta.pd.x, ps.n, meta.parm.support_radius, meta.parm.domain_size,

@@ -177,3 +177,27 @@ def test_resident_run_equals_steps(cuda_lib):
     s2.initialize()
     s2.run(6)
     assert np.array_equal(x1, pd_field(m2, "x"))
+
+
+@pytest.mark.parametrize("tuning", [dict(block=128, unroll=8, cell_factor=2), dict(block=512, unroll=2, cell_factor=1),
+                                    dict(block=64, unroll=4, cell_factor=2)])
+def test_tuning_invariance(cuda_lib, tuning):
+    """Launch shape and cell size change neither the neighbour sets nor (beyond
+    summation-order rounding) the trajectory."""
+    from nonnewton_b200 import sph
+    from nonnewton_b200.config import SimConfig
+
+    sc = S.dam_break(seed=9, n_side=(10, 10, 10), box=0.4)
+    out = []
+    for tn in (None, tuning):
+        m = sph.initialize(SimConfig(config=sc.config), particles=sc.particles, tuning=tn)
+        solver = sph.build_solver()
+        m.ns.run_search()
+        num, lists = m.ns.num_neighbors.cpu().numpy(), m.ns.neighbors.cpu().numpy()
+        solver.initialize()
+        for _ in range(5):
+            solver.step()
+        out.append((num, lists, pd_field(m, "x"), pd_field(m, "v")))
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+    assert np.abs(out[0][2] - out[1][2]).max() < 1e-6
+    assert rel_err(out[1][3], out[0][3]) < 1e-4
