@@ -202,6 +202,7 @@ static int launch1(nn_ctx* c, cudaStream_t s, void (*k)(KArgs...), Args... args)
 
 // The instantiation of a neighbour kernel for the context's neighbour-batch depth.
 #define KU(k) (c->unroll == 8 ? &k<8> : c->unroll == 2 ? &k<2> : &k<4>)
+#define KU2(k, B) (c->unroll == 8 ? &k<8, B> : c->unroll == 2 ? &k<2, B> : &k<4, B>)
 
 #define RC(x)                 \
   do {                        \
@@ -296,27 +297,36 @@ static int enq_search(nn_ctx* c, cudaStream_t s) {
   return NN_OK;
 }
 
-static int enq_divergence(nn_ctx* c, cudaStream_t s) {
+// DFSPHSolver.divergence_solve (SPH/main.py:1683-1713). In the fused step the first
+// density change and alpha *= 1/dt were done by k_density_factor<CHANGE> and the
+// closing alpha *= dt is folded into the pressure solve's first pass (fused = true).
+static int enq_divergence(nn_ctx* c, cudaStream_t s, bool fused) {
   Dev d = make_dev(c, c->cur);
   const int B = c->block;
-  RC(launch1(c, s, k_solver_begin, d, 0));
+  if (!fused) RC(launch1(c, s, k_solver_begin, d, 0));
   RC(solver_loop(c, s, false,
-                 [&](cudaStream_t q) { return launch(c, q, KU(k_density_change), B, c->n, make_dev(c, c->cur), 0); },
+                 [&](cudaStream_t q) {
+                   return fused ? NN_OK : launch(c, q, KU(k_density_change), B, c->n, make_dev(c, c->cur), 0);
+                 },
                  [&](cudaStream_t q) {
                    Dev e = make_dev(c, c->cur);
                    RC(launch(c, q, KU(k_divergence_update), B, c->n, e));
                    RC(launch(c, q, KU(k_density_change), B, c->n, e, 1));
                    return launch1(c, q, k_solver_check, e, 0);
                  }));
-  return launch(c, s, k_alpha_times_dt, 256, c->n, d);
+  return fused ? NN_OK : launch(c, s, k_alpha_times_dt, 256, c->n, d);
 }
 
-static int enq_pressure(nn_ctx* c, cudaStream_t s) {
+// DFSPHSolver.pressure_solve (SPH/main.py:1762-1791); init_mode 2 also folds the
+// divergence solve's alpha *= dt.
+static int enq_pressure(nn_ctx* c, cudaStream_t s, int init_mode) {
   Dev d = make_dev(c, c->cur);
   const int B = c->block;
   RC(launch1(c, s, k_solver_begin, d, 1));
   return solver_loop(c, s, false,
-                     [&](cudaStream_t q) { return launch(c, q, KU(k_density_adv), B, c->n, make_dev(c, c->cur), 0); },
+                     [&](cudaStream_t q) {
+                       return launch(c, q, KU(k_density_adv), B, c->n, make_dev(c, c->cur), init_mode);
+                     },
                      [&](cudaStream_t q) {
                        Dev e = make_dev(c, c->cur);
                        RC(launch(c, q, KU(k_pressure_update), B, c->n, e));
@@ -325,13 +335,14 @@ static int enq_pressure(nn_ctx* c, cudaStream_t s) {
                      });
 }
 
-static int enq_nonpressure(nn_ctx* c, cudaStream_t s, int advect) {
+// compute_non_pressure_forces (SPH/main.py:1557-1567), with the substep's
+// clear_accelerations when `clear`, then the implicit viscosity and, when `advect`,
+// non_pressure_advect.
+static int enq_nonpressure(nn_ctx* c, cudaStream_t s, int advect, int clear) {
   Dev d = make_dev(c, c->cur);
   const int B = c->block;
-  if (c->any_nonnewton) RC(launch(c, s, KU(k_strain_rate), B, c->n, d));
-  RC(launch(c, s, KU(k_nonpressure), B, c->n, d));
+  RC(launch(c, s, KU(k_forces), B, c->n, d, clear));
   if (c->any_implicit) {
-    RC(launch(c, s, k_cg_aux, 256, c->n, d));
     RC(launch(c, s, KU(k_cg_setup), B, c->n, d));
     RC(solver_loop(c, s, true, [&](cudaStream_t q) { return launch1(c, q, k_cg_check0, make_dev(c, c->cur)); },
                    [&](cudaStream_t q) {
@@ -359,15 +370,19 @@ static int enq_elastic(nn_ctx* c, cudaStream_t s) {
   return NN_OK;
 }
 
-// DFSPHSolver.substep (SPH/main.py:1546-1555); non_pressure_advect fused.
+// DFSPHSolver.substep (SPH/main.py:1546-1555) with the fused passes.
 static int enq_substep(nn_ctx* c, cudaStream_t s) {
   if (!c->any_fluid) return NN_OK;
   Dev d = make_dev(c, c->cur);
-  RC(launch(c, s, KU(k_density_factor), c->block, c->n, d, 1, 1));
-  if (c->any_div) RC(enq_divergence(c, s));
-  RC(launch(c, s, k_clear_acc, 256, c->n, d));
-  RC(enq_nonpressure(c, s, 1));
-  return enq_pressure(c, s);
+  if (c->any_div) {
+    RC(launch1(c, s, k_solver_begin, d, 0));
+    RC(launch(c, s, KU2(k_density_factor, true), c->block, c->n, d, 1, 1));
+    RC(enq_divergence(c, s, true));
+  } else {
+    RC(launch(c, s, KU2(k_density_factor, false), c->block, c->n, d, 1, 1));
+  }
+  RC(enq_nonpressure(c, s, 1, 1));
+  return enq_pressure(c, s, 2);
 }
 
 // SPHBase.step (SPH/main.py:915-937)
@@ -861,12 +876,12 @@ int nn_run_pass(nn_ctx* c, int32_t pass) {
     case NN_PASS_STATIC_BOUNDARY_VOLUME: RC(launch(c, s, KU(k_boundary_volume), c->block, c->n, d, 0)); break;
     case NN_PASS_MOVING_BOUNDARY_VOLUME: RC(launch(c, s, KU(k_boundary_volume), c->block, c->n, d, 1)); break;
     case NN_PASS_CLEAR_ACCELERATIONS: RC(launch(c, s, k_clear_acc, 256, c->n, d)); break;
-    case NN_PASS_DENSITIES: RC(launch(c, s, KU(k_density_factor), c->block, c->n, d, 1, 0)); break;
-    case NN_PASS_DFSPH_FACTOR: RC(launch(c, s, KU(k_density_factor), c->block, c->n, d, 0, 1)); break;
-    case NN_PASS_DIVERGENCE_SOLVE: if (c->any_div) RC(enq_divergence(c, s)); break;
-    case NN_PASS_NON_PRESSURE_FORCES: if (c->any_fluid) RC(enq_nonpressure(c, s, 0)); break;
+    case NN_PASS_DENSITIES: RC(launch(c, s, KU2(k_density_factor, false), c->block, c->n, d, 1, 0)); break;
+    case NN_PASS_DFSPH_FACTOR: RC(launch(c, s, KU2(k_density_factor, false), c->block, c->n, d, 0, 1)); break;
+    case NN_PASS_DIVERGENCE_SOLVE: if (c->any_div) RC(enq_divergence(c, s, false)); break;
+    case NN_PASS_NON_PRESSURE_FORCES: if (c->any_fluid) RC(enq_nonpressure(c, s, 0, 0)); break;
     case NN_PASS_NON_PRESSURE_ADVECT: RC(launch(c, s, k_np_advect, 256, c->n, d)); break;
-    case NN_PASS_PRESSURE_SOLVE: if (c->any_fluid) RC(enq_pressure(c, s)); break;
+    case NN_PASS_PRESSURE_SOLVE: if (c->any_fluid) RC(enq_pressure(c, s, 0)); break;
     case NN_PASS_ELASTICITY: RC(enq_elastic(c, s)); break;
     case NN_PASS_ADVECT: RC(launch(c, s, k_advect_boundary, 256, c->n, d, 1, 0)); break;
     case NN_PASS_ENFORCE_BOUNDARY: RC(launch(c, s, k_advect_boundary, 256, c->n, d, 0, 1)); break;
@@ -895,10 +910,10 @@ int nn_time_kernel(nn_ctx* c, int32_t kernel, int32_t reps, float* ms_out) {
       case NN_K_DENSITY_ADV: return launch(c, s, KU(k_density_adv), B, c->n, d, 1);
       case NN_K_DIVERGENCE_UPDATE: return launch(c, s, KU(k_divergence_update), B, c->n, d);
       case NN_K_DENSITY_CHANGE: return launch(c, s, KU(k_density_change), B, c->n, d, 1);
-      case NN_K_DENSITY_FACTOR: return launch(c, s, KU(k_density_factor), B, c->n, d, 1, 1);
+      case NN_K_DENSITY_FACTOR: return launch(c, s, KU2(k_density_factor, false), B, c->n, d, 1, 1);
       case NN_K_BUILD_LISTS: return launch(c, s, k_build_lists, NS_WARPS * 32, c->n, d);
       case NN_K_CG_MATVEC: return launch(c, s, KU(k_cg_matvec), B, c->n, d);
-      default: return launch(c, s, KU(k_nonpressure), B, c->n, d);
+      default: return launch(c, s, KU(k_forces), B, c->n, d, 0);
     }
   };
   RC(one());  // warm-up

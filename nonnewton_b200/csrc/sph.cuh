@@ -9,6 +9,8 @@
   for (int _k = 0, _c = (d).nbr_cnt[i]; _k < _c; ++_k)     \
     for (int j = (d).nbr[(size_t)_k * (d).cap + (i)], _o = 1; _o; _o = 0)
 
+struct GPV { float4 p, v; };
+
 // ---------------------------------------------------------------------------
 // compute_static_boundary_volume / compute_moving_boundary_volume (SPH/main.py:1010-1035)
 template <int U>
@@ -44,7 +46,11 @@ __global__ void k_clear_acc(Dev d) {
 
 // compute_densities (SPH/main.py:975-984) fused with compute_DFSPH_factor
 // (SPH/main.py:1569-1608): both walk the same neighbours with fixed positions.
-template <int U>
+// compute_densities (SPH/main.py:975-984), compute_DFSPH_factor (SPH/main.py:1569-1608)
+// and, with CHANGE, the divergence solve's first compute_density_change and
+// alpha *= 1/dt (SPH/main.py:1686-1688): all read the same neighbours at the same
+// positions and velocities, and each only needs the particle's own factor.
+template <int U, bool CHANGE>
 __global__ void k_density_factor(Dev d, int do_density, int do_factor) {
   const int n = d.d_n[0];
   FOR_SLOTS_WARP(i, valid, n) {
@@ -56,20 +62,29 @@ __global__ void k_density_factor(Dev d, int do_density, int do_factor) {
       const SceneDev& s = d.sc[scn];
       const float4 pi = d.w.pos[i];
       const float3 xi = f3(pi);
-      float den = 0.f, sum_grad = 0.f;
+      const float3 vi = f3(d.w.vel[i]);
+      const int c = d.nbr_cnt[i];
+      float den = 0.f, sum_grad = 0.f, dd = 0.f;
       float3 gpi = make_float3(0.f, 0.f, 0.f);
-      nb_batches<U>(d.nbr + i, d.cap, d.nbr_cnt[i], i, [&](int j) { return __ldg(&d.w.pos[j]); },
-                 [&](int, float4 pj) {
-                   const float3 r = xi - f3(pj);
-                   float w;
-                   float3 g;
-                   kwg_r2(r, dot3(r, r), s, w, g);
-                   const float V = fabsf(pj.w);
-                   den += V * w;
-                   const float3 gpj = g * (-V);
-                   if (w_fluid(pj.w)) sum_grad += dot3(gpj, gpj);
-                   gpi -= gpj;
-                 });
+      auto body = [&](float4 pj, float4 vj) {
+        const float3 r = xi - f3(pj);
+        float w;
+        float3 g;
+        kwg_r2(r, dot3(r, r), s, w, g);
+        const float V = fabsf(pj.w);
+        den += V * w;
+        const float3 gpj = g * (-V);
+        if (w_fluid(pj.w)) sum_grad += dot3(gpj, gpj);
+        gpi -= gpj;
+        if (CHANGE) dd += V * dot3(vi - f3(vj), g);
+      };
+      if constexpr (CHANGE) {
+        nb_batches<U>(d.nbr + i, d.cap, c, i, [&](int j) { return GPV{__ldg(&d.w.pos[j]), __ldg(&d.w.vel[j])}; },
+                      [&](int, const GPV& g) { body(g.p, g.v); });
+      } else {
+        nb_batches<U>(d.nbr + i, d.cap, c, i, [&](int j) { return __ldg(&d.w.pos[j]); },
+                      [&](int, float4 pj) { body(pj, pj); });
+      }
       if (do_density) {
         rho = pi.w * s.W0;
         rho += den;
@@ -78,7 +93,15 @@ __global__ void k_density_factor(Dev d, int do_density, int do_factor) {
       }
       if (do_factor) {
         sum_grad += dot3(gpi, gpi);
-        d.alpha[i] = sum_grad > 1e-6f ? -1.f / sum_grad : 0.f;
+        float alpha = sum_grad > 1e-6f ? -1.f / sum_grad : 0.f;
+        if (CHANGE && d.dyn[scn].act_v) {
+          dd = fmaxf(dd, 0.f);
+          if (c < 20) dd = 0.f;
+          d.rho_adv[i] = dd;
+          alpha = alpha * d.dyn[scn].inv_dt;
+          d.kappa[i] = dd * alpha;
+        }
+        d.alpha[i] = alpha;
       }
     }
     if (do_density) warp_max_to(&d.dyn[scn].max_density_bits, __float_as_uint(rho), work);
@@ -88,7 +111,6 @@ __global__ void k_density_factor(Dev d, int do_density, int do_factor) {
 // compute_density_change (SPH/main.py:1610-1645). mode 0: first call of
 // divergence_solve, also applies alpha *= 1/dt (1688); mode 1: solver iteration,
 // accumulates the FP64 density error (1669-1675, 1717-1719).
-struct GPV { float4 p, v; };
 template <int U>
 __global__ void k_density_change(Dev d, int mode) {
   const int n = d.d_n[0];
@@ -193,7 +215,9 @@ __global__ void k_density_adv(Dev d, int mode) {
       da = fmaxf(da, 1.f);
       d.rho_adv[i] = da;
       float a = d.alpha[i];
-      if (mode == 0) {
+      if (mode != 1) {
+        // mode 2 also applies the divergence solve's closing alpha *= dt (1713)
+        if (mode == 2 && d.dyn[scn].div_ran) a = a * d.dyn[scn].dt;
         a = a * d.dyn[scn].inv_dt2;
         d.alpha[i] = a;
       }
@@ -402,121 +426,108 @@ __device__ __forceinline__ float nn_law(float g, const SceneDev& s) {
   }
 }
 
-// NonNewton.calcStrainRate (SPH/main.py:461-492) + law. Quirk mode: every particle,
-// the accumulator keeps only the last neighbour, norm before scaling. Otherwise: fluid
-// particles, D = (0.5/rho_i) sum_j m_j (v_ji (x) gW + gW (x) v_ji), gamma = |D|_F.
-struct GSR { float4 p, v; float m; int id; };
-template <int U>
-__global__ void k_strain_rate(Dev d) {
-  const int n = d.d_n[0];
-  GRID_STRIDE(i, n) {
-    const uint32_t fl = d.w.flags[i];
-    const SceneDev& s = d.sc[slot_scene(fl)];
-    if (!(s.flags & NN_F_NONNEWTON)) continue;
-    const bool q = (s.flags & NN_F_QUIRKS) != 0;
-    if (!q && !cls_fluid(fl)) { d.srn[i] = 0.f; d.mu[i] = 0.f; continue; }
-    const float3 xi = f3(d.w.pos[i]);
-    const float3 vi = f3(d.w.vel[i]);
-    float S[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // symmetric: 00 11 22 01 02 12
-    int last_id = -1;  // quirk: the term of the last neighbour in id order survives
-    nb_batches<U>(d.nbr + i, d.cap, d.nbr_cnt[i], i,
-               [&](int j) { return GSR{__ldg(&d.w.pos[j]), __ldg(&d.w.vel[j]), __ldg(&d.w.mass[j]), __ldg(&d.w.id[j])}; },
-               [&](int, const GSR& g) {
-                 const float3 r = xi - f3(g.p);
-                 const float3 gw = kgrad_r2(r, dot3(r, r), s);
-                 const float3 vji = f3(g.v) - vi;
-                 const float mj = g.m;
-                 const float t[6] = {(vji.x * gw.x + vji.x * gw.x) * mj, (vji.y * gw.y + vji.y * gw.y) * mj,
-                                     (vji.z * gw.z + vji.z * gw.z) * mj, (vji.x * gw.y + vji.y * gw.x) * mj,
-                                     (vji.x * gw.z + vji.z * gw.x) * mj, (vji.y * gw.z + vji.z * gw.y) * mj};
-                 const bool take = g.id > last_id;
-                 if (q && take) last_id = g.id;
-#pragma unroll
-                 for (int k = 0; k < 6; ++k) S[k] = q ? (take ? t[k] : S[k]) : S[k] + t[k];
-               });
-    const float sc = 0.5f / d.w.dens[i];
-    float nrm2;
-    if (q) {
-      nrm2 = S[0] * S[0] + S[1] * S[1] + S[2] * S[2] + 2.f * (S[3] * S[3] + S[4] * S[4] + S[5] * S[5]);
-    } else {
-      float D[6];
-#pragma unroll
-      for (int k = 0; k < 6; ++k) D[k] = S[k] * sc;
-      nrm2 = D[0] * D[0] + D[1] * D[1] + D[2] * D[2] + 2.f * (D[3] * D[3] + D[4] * D[4] + D[5] * D[5]);
-    }
-    const float g = sqrtf(nrm2);
-    d.srn[i] = g;
-    d.mu[i] = nn_law(g, s);
-  }
-}
 
-// SurfaceTension (SPH/main.py:1387-1414) and ViscosityModel (SPH/main.py:1426-1468)
-// fused in one neighbour pass. Dynamic solids gather the boundary-viscosity reaction
-// from their fluid neighbours (the reference scatters it, 1459-1460). The velocity
-// update of non_pressure_advect cannot join this pass: the viscosity reads the
-// neighbours' velocities.
-struct GNP { float4 p, v; float m, rho; };
+
+// compute_non_pressure_forces (SPH/main.py:1557-1567) in one neighbour pass:
+// [clear_accelerations (1552)] + SurfaceTension (1387-1414) + NonNewton strain rate
+// and law (461-492, 404-459) + ViscosityModel (1426-1468), and the per-particle
+// coefficients (mu_i, m_i / rho_i) of the implicit viscosity. Dynamic solids gather
+// the boundary-viscosity reaction from their fluid neighbours (the reference scatters
+// it, 1459-1460). The velocity update of non_pressure_advect cannot join this pass:
+// the viscosity reads the neighbours' velocities.
+struct GF { float4 p, v; float m, rho; int id; };
 template <int U>
-__global__ void k_nonpressure(Dev d) {
+__global__ void k_forces(Dev d, int clear) {
   const int n = d.d_n[0];
   GRID_STRIDE(i, n) {
     const uint32_t fl = d.w.flags[i];
     const bool fluid = cls_fluid(fl);
     const int scn = slot_scene(fl);
     const SceneDev& s = d.sc[scn];
-    if (s.n_fluid == 0) continue;
-    const bool implicit_visc = scene_implicit(s);
-    const bool st_on = (s.flags & NN_F_SURFACE_TENSION) != 0;
-    const bool vi_on = !implicit_visc && (s.flags & NN_F_VISCOSITY) != 0;
+    if (s.n_fluid == 0) continue;  // the reference runs the substep only with fluid
+    const bool implicit = scene_implicit(s);
+    const bool quirks = (s.flags & NN_F_QUIRKS) != 0;
+    const bool st_on = fluid && (s.flags & NN_F_SURFACE_TENSION);
+    const bool vi_on = fluid && !implicit && (s.flags & NN_F_VISCOSITY);
+    const bool vb_on = cls_dyn_solid(fl) && !implicit && (s.flags & NN_F_VISCOSITY) && s.visc_b != 0.f;
+    const bool nn_on = (s.flags & NN_F_NONNEWTON) != 0;
+    const bool sr_on = nn_on && (fluid || quirks);
     const float4 pi = d.w.pos[i];
     const float3 xi = f3(pi);
     const float3 vi = f3(d.w.vel[i]);
-    auto load = [&](int j) {
-      return GNP{__ldg(&d.w.pos[j]), __ldg(&d.w.vel[j]), __ldg(&d.w.mass[j]), __ldg(&d.w.dens[j])};
-    };
-    if (fluid) {
-      if (!st_on && !vi_on) continue;
+    float4 a;
+    if (clear) a = cls_static_solid(fl) ? make_float4(0.f, 0.f, 0.f, 0.f) : make_float4(s.g[0], s.g[1], s.g[2], 0.f);
+    else a = d.acc4[i];
+    float3 st = make_float3(0.f, 0.f, 0.f), vs = make_float3(0.f, 0.f, 0.f), rf = make_float3(0.f, 0.f, 0.f);
+    float S[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // strain-rate sum: 00 11 22 01 02 12
+    int last_id = -1;                             // quirk: the last neighbour in id order survives
+    if (st_on || vi_on || vb_on || sr_on) {
       const float mi = d.w.mass[i];
-      float3 st = make_float3(0.f, 0.f, 0.f), vs = make_float3(0.f, 0.f, 0.f);
       const float rho_i = d.w.dens[i];
-      nb_batches<U>(d.nbr + i, d.cap, d.nbr_cnt[i], i, load, [&](int, const GNP& g) {
-        const float3 r = xi - f3(g.p);
-        const float r2 = dot3(r, r);
-        float w;
-        float3 gw;
-        kwg_r2(r, r2, s, w, gw);
-        if (w_fluid(g.p.w)) {
-          if (st_on) {
-            const float c = s.sigma / mi * g.m;
-            st -= (r * c) * (r2 > s.dia2 ? w : s.w_dia);
-          }
-          if (vi_on) {
-            const float v_xy = dot3(vi - f3(g.v), r);
-            vs += gw * (10.f * s.visc * (g.m / g.rho) * v_xy / (r2 + s.c01h2));
-          }
-        } else if (vi_on && s.visc_b != 0.f) {
-          const float v_xy = dot3(vi - f3(g.v), r);
-          vs += gw * (10.f * s.visc_b * (s.rho0 * fabsf(g.p.w) / rho_i) * v_xy / (r2 + s.c01h2));
-        }
-      });
-      float4 a = d.acc4[i];
-      if (st_on) { a.x += st.x; a.y += st.y; a.z += st.z; }
-      if (vi_on) { a.x += vs.x; a.y += vs.y; a.z += vs.z; }
-      d.acc4[i] = a;
-    } else if (cls_dyn_solid(fl) && vi_on && s.visc_b != 0.f) {
       const float Vi = fabsf(pi.w);
-      float3 f = make_float3(0.f, 0.f, 0.f);
-      nb_batches<U>(d.nbr + i, d.cap, d.nbr_cnt[i], i, load, [&](int, const GNP& g) {
-        if (!w_fluid(g.p.w)) return;
-        const float3 r = f3(g.p) - xi;  // fluid minus solid, as the fluid computes it
-        const float r2 = dot3(r, r);
-        const float v_xy = dot3(f3(g.v) - vi, r);
-        f += kgrad_r2(r, r2, s) * (10.f * s.visc_b * (s.rho0 * Vi / g.rho) * v_xy / (r2 + s.c01h2));
-      });
-      float4 a = d.acc4[i];
-      a.x -= f.x; a.y -= f.y; a.z -= f.z;
-      d.acc4[i] = a;
+      nb_batches<U>(d.nbr + i, d.cap, d.nbr_cnt[i], i,
+                    [&](int j) {
+                      return GF{__ldg(&d.w.pos[j]), __ldg(&d.w.vel[j]), __ldg(&d.w.mass[j]), __ldg(&d.w.dens[j]),
+                                __ldg(&d.w.id[j])};
+                    },
+                    [&](int, const GF& g) {
+                      const float3 r = xi - f3(g.p);
+                      const float r2 = dot3(r, r);
+                      float w;
+                      float3 gw;
+                      kwg_r2(r, r2, s, w, gw);
+                      const bool jf = w_fluid(g.p.w);
+                      if (jf && st_on) st -= (r * (s.sigma / mi * g.m)) * (r2 > s.dia2 ? w : s.w_dia);
+                      if (vi_on) {
+                        const float v_xy = dot3(vi - f3(g.v), r);
+                        if (jf) vs += gw * (10.f * s.visc * (g.m / g.rho) * v_xy / (r2 + s.c01h2));
+                        else if (s.visc_b != 0.f)
+                          vs += gw * (10.f * s.visc_b * (s.rho0 * fabsf(g.p.w) / rho_i) * v_xy / (r2 + s.c01h2));
+                      }
+                      if (vb_on && jf) {  // reaction on a dynamic solid: the fluid's term with i <-> j
+                        const float3 rr = -r;
+                        const float v_xy = dot3(f3(g.v) - vi, rr);
+                        rf += (-gw) * (10.f * s.visc_b * (s.rho0 * Vi / g.rho) * v_xy / (r2 + s.c01h2));
+                      }
+                      if (sr_on) {
+                        const float3 vji = f3(g.v) - vi;
+                        const float t[6] = {(vji.x * gw.x + vji.x * gw.x) * g.m, (vji.y * gw.y + vji.y * gw.y) * g.m,
+                                            (vji.z * gw.z + vji.z * gw.z) * g.m, (vji.x * gw.y + vji.y * gw.x) * g.m,
+                                            (vji.x * gw.z + vji.z * gw.x) * g.m, (vji.y * gw.z + vji.z * gw.y) * g.m};
+                        const bool take = g.id > last_id;
+                        if (quirks && take) last_id = g.id;
+#pragma unroll
+                        for (int k = 0; k < 6; ++k) S[k] = quirks ? (take ? t[k] : S[k]) : S[k] + t[k];
+                      }
+                    });
     }
+    if (st_on) { a.x += st.x; a.y += st.y; a.z += st.z; }
+    if (vi_on) { a.x += vs.x; a.y += vs.y; a.z += vs.z; }
+    if (vb_on) { a.x -= rf.x; a.y -= rf.y; a.z -= rf.z; }
+    d.acc4[i] = a;
+    float mu = s.mu_newton;
+    if (nn_on) {
+      float g = 0.f;
+      if (sr_on) {
+        float nrm2;
+        if (quirks) {
+          nrm2 = S[0] * S[0] + S[1] * S[1] + S[2] * S[2] + 2.f * (S[3] * S[3] + S[4] * S[4] + S[5] * S[5]);
+        } else {
+          const float sc = 0.5f / d.w.dens[i];
+          float D[6];
+#pragma unroll
+          for (int k = 0; k < 6; ++k) D[k] = S[k] * sc;
+          nrm2 = D[0] * D[0] + D[1] * D[1] + D[2] * D[2] + 2.f * (D[3] * D[3] + D[4] * D[4] + D[5] * D[5]);
+        }
+        g = sqrtf(nrm2);
+        mu = nn_law(g, s);
+      } else {
+        mu = 0.f;
+      }
+      d.srn[i] = g;
+      d.mu[i] = mu;
+    }
+    if (implicit && fluid) d.cg_aux[i] = make_float4(mu, d.w.mass[i] / d.w.dens[i], 0.f, 0.f);
   }
 }
 
@@ -528,15 +539,6 @@ __global__ void k_nonpressure(Dev d) {
 //   K_ij = gradW_ij x_ij^T / (|x_ij|^2 + 0.01 h^2)
 // FP32 vectors, FP64 dot products, 3x3 block-Jacobi preconditioner.
 
-__global__ void k_cg_aux(Dev d) {
-  const int n = d.d_n[0];
-  GRID_STRIDE(i, n) {
-    const uint32_t fl = d.w.flags[i];
-    const SceneDev& s = d.sc[slot_scene(fl)];
-    float mu = (s.flags & NN_F_NONNEWTON) ? d.mu[i] : s.mu_newton;
-    d.cg_aux[i] = make_float4(mu, d.w.mass[i] / d.w.dens[i], 0.f, 0.f);
-  }
-}
 
 __device__ __forceinline__ bool cg_row(const Dev& d, int i, uint32_t fl) {
   if (!cls_fluid(fl)) return false;
