@@ -819,12 +819,21 @@ static int check_ready(nn_ctx* c) {
 int nn_initialize(nn_ctx* c) {
   RC(check_ready(c));
   cudaStream_t s = run_stream(c);
-  // Elasticity constructors run before solver.initialize() (SPH/main.py:1889-1895, 1915)
+  // Elasticity constructors run before solver.initialize() (SPH/main.py:1889-1895, 1915).
+  // Their rest neighbourhoods come from a search over the rest positions x_0 (equal to
+  // x at t = 0, as in the reference; after a checkpoint restore they differ).
+  if (c->ne > 0) {
+    CK(cudaMemsetAsync(c->d_src_flag, 0, sizeof(int32_t), s));
+    RC(launch1(c, s, k_set_int, c->d_src_flag, 2));
+    RC(enq_search(c, s));
+    Dev dr = make_dev(c, c->cur);
+    RC(launch1(c, s, k_step_dt, dr, 0));
+    RC(launch(c, s, k_el_init, 256, c->n, dr));
+  }
   CK(cudaMemsetAsync(c->d_src_flag, 1, sizeof(int32_t), s));
   RC(enq_search(c, s));
   Dev d = make_dev(c, c->cur);
   RC(launch1(c, s, k_step_dt, d, 0));
-  if (c->ne > 0) RC(launch(c, s, k_el_init, 256, c->n, d));
   RC(launch(c, s, KU(k_boundary_volume), c->block, c->n, d, 0));
   RC(launch(c, s, KU(k_boundary_volume), c->block, c->n, d, 1));
   RC(enq_sync_out(c, s, SM_VOL));

@@ -41,12 +41,14 @@ __global__ void k_zero_cells(Dev d) {
 // Keys and in-cell ranks of every source particle (truth id order or previous slots).
 __global__ void k_keys(Dev d) {
   const int n = d.d_n[0];
-  const bool truth = *d.src_from_truth != 0;
+  const int mode = *d.src_from_truth;  // 0 previous slots, 1 caller state, 2 caller rest positions
+  const bool truth = mode != 0;
+  const float* __restrict__ X = mode == 2 ? d.t.x_0 : d.t.x;
   GRID_STRIDE(s, n) {
     float x, y, z;
     int sc;
     if (truth) {
-      x = d.t.x[3 * s]; y = d.t.x[3 * s + 1]; z = d.t.x[3 * s + 2];
+      x = X[3 * s]; y = X[3 * s + 1]; z = X[3 * s + 2];
       sc = d.scene_of_id[s];
     } else {
       float4 p = d.wo.pos[s];
@@ -193,7 +195,9 @@ __device__ __forceinline__ uint32_t class_bits(int material, int dynamic, int ph
 // slots), and record max |v| per scene for the CFL step.
 __global__ void k_gather(Dev d) {
   const int n = d.d_n[0];
-  const bool truth = *d.src_from_truth != 0;
+  const int mode = *d.src_from_truth;
+  const bool truth = mode != 0;
+  const float* __restrict__ X = mode == 2 ? d.t.x_0 : d.t.x;
   FOR_SLOTS_WARP(i, valid, n) {
     uint32_t fl = 0u;
     float vm = 0.f;
@@ -206,7 +210,7 @@ __global__ void k_gather(Dev d) {
         id = s;
         int sc = d.scene_of_id[id];
         const float vol = d.t.volume[id];
-        p = make_float4(d.t.x[3 * id], d.t.x[3 * id + 1], d.t.x[3 * id + 2],
+        p = make_float4(X[3 * id], X[3 * id + 1], X[3 * id + 2],
                         d.t.material[id] == NN_SOLID ? -vol : vol);  // signed volume: solid < 0
         v = make_float4(d.t.v[3 * id], d.t.v[3 * id + 1], d.t.v[3 * id + 2], 0.f);
         m = d.t.m[id];

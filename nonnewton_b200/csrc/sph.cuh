@@ -398,6 +398,10 @@ __global__ void k_scene_of_id(Dev d) {
   }
 }
 
+__global__ void k_set_int(int32_t* p, int32_t v) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *const_cast<int32_t*>(p) = v;
+}
+
 __global__ void k_step_end(Dev d) {
   const int ns = d.d_n[1];
   for (int sc = threadIdx.x; sc < ns; sc += blockDim.x) d.dyn[sc].steps += 1;

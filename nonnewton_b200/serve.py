@@ -36,6 +36,7 @@ class Request:
     step_ms: list = field(default_factory=list)
     result_x: np.ndarray | None = None
     stats: dict | None = None
+    failed: int = 0          # NN_ERR_* status that evicted the request, 0 if it completed
 
 
 def footprint_bytes(n_particles: int, max_neighbors: int = 64) -> int:
@@ -131,6 +132,13 @@ class Server:
                 r.done_steps += k
                 r.step_ms.extend([ms] * k)
                 total_ps += r.scene.particles.n * k
+            # failure detection: a scene whose device status word is set (non-finite
+            # state, neighbour overflow) is evicted at once; the others go on
+            st = self.batch.engine.stats_range(0, len(self.resident))
+            for r, y in zip(self.resident, st):
+                if y["status"] != 0:
+                    r.failed = y["status"]
+                    r.done_steps = r.steps
         wall = now()
         lat = np.concatenate([np.asarray(r.step_ms) for r in finished]) if finished else np.zeros(1)
         return {
@@ -142,7 +150,9 @@ class Server:
             "step_ms_p99": float(np.percentile(lat, 99)),
             "request_s_p50": float(np.percentile([r.finished - r.arrival for r in finished], 50)),
             "request_s_p99": float(np.percentile([r.finished - r.arrival for r in finished], 99)),
-            "max_density_err": max((r.stats or {}).get("avg_density_err", 0.0) for r in finished),
+            "max_density_err": max(((r.stats or {}).get("avg_density_err", 0.0) for r in finished if not r.failed),
+                                   default=0.0),
+            "failed": [r.rid for r in finished if r.failed],
             "device_throughput": total_ps / (self.device_ms / 1e3) if self.device_ms > 0 else 0.0,
             "repacks": self.repacks,
             "chunks": self.chunks,

@@ -1,0 +1,54 @@
+"""Multi-GPU form of the batched/served step: whole scenes are sharded across ranks
+(one process per GPU); scenes never interact, so there is no collective on the data
+path. Ranks only combine their metrics (particle-steps summed, times max-reduced)
+once, after the run.
+
+A single scene is not split across GPUs (replicas only): a spatial split would need
+a halo exchange before every neighbour pass.
+"""
+from __future__ import annotations
+
+import heapq
+
+
+def request_cost(req) -> float:
+    """Work of a request: particles x steps."""
+    return float(req.scene.particles.n) * float(req.steps)
+
+
+def shard_requests(requests, world: int) -> list[list[int]]:
+    """Longest-processing-time-first assignment of requests to `world` ranks by
+    particle-steps (deterministic: ties broken by request id). Returns, per rank, the
+    indices into `requests`, in arrival order."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    order = sorted(range(len(requests)), key=lambda k: (-request_cost(requests[k]), requests[k].rid))
+    heap = [(0.0, r) for r in range(world)]
+    heapq.heapify(heap)
+    out = [[] for _ in range(world)]
+    for k in order:
+        load, r = heapq.heappop(heap)
+        out[r].append(k)
+        heapq.heappush(heap, (load + request_cost(requests[k]), r))
+    for r in range(world):
+        out[r].sort(key=lambda k: (requests[k].arrival, requests[k].rid))
+    return out
+
+
+def combine_metrics(local: dict, world: int) -> dict:
+    """Sum particle-steps and requests, max-reduce wall and device times over ranks
+    (torch.distributed, any backend)."""
+    if world <= 1:
+        return dict(local)
+    import torch
+    import torch.distributed as dist
+
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    s = torch.tensor([local["particle_steps"], local["requests"]], dtype=torch.float64, device=dev)
+    m = torch.tensor([local["wall_s"], local.get("device_s", 0.0)], dtype=torch.float64, device=dev)
+    dist.all_reduce(s, op=dist.ReduceOp.SUM)
+    dist.all_reduce(m, op=dist.ReduceOp.MAX)
+    out = dict(local)
+    out.update(particle_steps=float(s[0]), requests=int(s[1]), wall_s=float(m[0]), device_s=float(m[1]))
+    out["throughput"] = out["particle_steps"] / out["wall_s"] if out["wall_s"] > 0 else 0.0
+    return out

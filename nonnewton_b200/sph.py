@@ -262,3 +262,39 @@ def main(scene_path: str):
     for _ in range(int(meta.config.get_cfg("maxStep", 1))):
         solver.step()
     return meta
+
+
+# ---------------------------------------------------------------- checkpoint / resume
+CHECKPOINT_FIELDS = ("x", "x_0", "v", "acceleration", "volume", "m", "density", "pressure", "dfsph_factor",
+                     "density_adv", "material", "is_dynamic", "phase_id", "strain_rate_norm",
+                     "nonnewton_viscosity", "stress", "rotations")
+
+
+def save_checkpoint(path: str) -> None:
+    """Full particle state, step counter and scene configuration (the reference only
+    exports positions to PLY, SPH/main.py:939-940). Resuming runs the same kernels in
+    the same order, so the continuation is bit-identical."""
+    torch.cuda.synchronize()
+    torch.save({"fields": {k: getattr(meta.pd, k).detach().cpu() for k in CHECKPOINT_FIELDS},
+                "step_num": getattr(meta, "step_num", 0), "config": meta.config.config,
+                "quirks": bool(meta.parm.quirks), "n_fluid": int(meta.fluid_particle_num)}, path)
+
+
+def load_checkpoint(path: str, max_neighbors: int = 64, device="cuda", tuning: dict | None = None):
+    """Rebuild `meta` from a checkpoint and re-initialise the solver state that is not
+    part of the fields (neighbour lists, boundary volumes, elastic rest neighbourhoods
+    from x_0). Returns (meta, solver)."""
+    from .scene import ParticleSet
+
+    ck = torch.load(path, weights_only=False)
+    f = ck["fields"]
+    ps = ParticleSet(x=f["x"].numpy(), material=f["material"].numpy(), is_dynamic=f["is_dynamic"].numpy(),
+                     phase_id=f["phase_id"].numpy(), mass=f["m"].numpy(), n_fluid=ck["n_fluid"])
+    initialize(SimConfig(config=ck["config"]), particles=ps, quirks=ck["quirks"], max_neighbors=max_neighbors,
+               device=device, tuning=tuning)
+    for k in CHECKPOINT_FIELDS:
+        getattr(meta.pd, k).copy_(f[k].to(meta.pd.x.device))
+    solver = build_solver()
+    solver.initialize()
+    meta.step_num = ck["step_num"]
+    return meta, solver

@@ -1,0 +1,111 @@
+"""The C ABI without a GPU: libnnsph.so loads, exports every function the header
+declares, and the ctypes mirror of the structs matches the C layout."""
+import ctypes as C
+import os
+import re
+import subprocess
+import tempfile
+
+import pytest
+
+from nonnewton_b200 import _abi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "nnsph.h")
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from nonnewton_b200 import build as B
+
+    B.build()
+    return C.CDLL(B.OUT)
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?[\w\s\*]+?\b(nn_\w+)\s*\(", src, flags=re.M)))
+
+
+def test_exports_every_declared_function(lib):
+    names = declared_functions()
+    assert len(names) >= 18
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_abi_version(lib):
+    lib.nn_abi_version.restype = C.c_int
+    assert lib.nn_abi_version() == 1
+
+
+def test_struct_layout_matches_header():
+    code = r'''
+#include <stdio.h>
+#include <stddef.h>
+#include "nnsph.h"
+int main(void) {
+  printf("%zu %zu %zu %zu\n", sizeof(nn_scene_params), sizeof(nn_scene_desc), sizeof(nn_state), sizeof(nn_stats));
+  printf("%zu %zu %zu %zu\n", offsetof(nn_scene_params, max_iterations_v), offsetof(nn_scene_params, cfl_max_dt),
+         offsetof(nn_state, rotations), offsetof(nn_stats, steps));
+  return 0;
+}'''
+    with tempfile.TemporaryDirectory() as d:
+        src = os.path.join(d, "t.c")
+        open(src, "w").write(code)
+        exe = os.path.join(d, "t")
+        subprocess.run(["gcc", "-I", os.path.dirname(HEADER), src, "-o", exe], check=True)
+        out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()
+    sizes = list(map(int, out[:4]))
+    offs = list(map(int, out[4:]))
+    assert sizes == [C.sizeof(_abi.nn_scene_params), C.sizeof(_abi.nn_scene_desc), C.sizeof(_abi.nn_state),
+                     C.sizeof(_abi.nn_stats)]
+    assert offs == [_abi.nn_scene_params.max_iterations_v.offset, _abi.nn_scene_params.cfl_max_dt.offset,
+                    _abi.nn_state.rotations.offset, _abi.nn_stats.steps.offset]
+
+
+def test_invalid_arguments_are_rejected_without_a_context(lib):
+    """Argument checks happen before any device call."""
+    lib.nn_ctx_create.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int64, C.POINTER(C.c_void_p)]
+    lib.nn_ctx_create.restype = C.c_int
+    h = C.c_void_p()
+    assert lib.nn_ctx_create(0, 1, 64, 0, C.byref(h)) == _abi.NN_ERR_INVALID_ARG
+    assert lib.nn_ctx_create(100, 1, 5000, 0, C.byref(h)) == _abi.NN_ERR_INVALID_ARG
+    lib.nn_last_error.restype = C.c_char_p
+    lib.nn_last_error.argtypes = [C.c_void_p]
+    assert b"invalid" in lib.nn_last_error(None)
+    lib.nn_neighbors_noalloc.restype = C.c_int
+    lo = (C.c_double * 3)(0, 0, 0)
+    hi = (C.c_double * 3)(1, 1, 1)
+    assert lib.nn_neighbors_noalloc(None, C.c_int32(10), lo, hi, C.c_double(0.04), C.c_int32(8), None, None,
+                                    None) == _abi.NN_ERR_INVALID_ARG
+
+
+def test_config_parses_reference_scenes():
+    """The reference's scene JSON schema and defaults (SPH/main.py:594-621)."""
+    from nonnewton_b200.config import Parameter, SimConfig
+
+    cfg = SimConfig(config={"Configuration": {"particleRadius": 0.01, "simulationMethod": 4,
+                                              "timeStepSize": 0.004},
+                            "FluidParticles": [{"nonNewtonMethod": 2, "viscosityMethod": 13,
+                                                "viscoMaxError": 0.001, "viscosityBoundary": 0.1}]})
+    p = Parameter.from_config(cfg)
+    assert abs(p.support_radius - 0.04) < 1e-15 and abs(p.volume0 - 0.8 * 0.02 ** 3) < 1e-18
+    assert p.density0 == 1000.0 and list(p.gravity) == [0.0, -9.8, 0.0] and p.max_error == 0.05
+    assert p.use_surface_tension and p.use_viscosity and not p.use_nonnewtonian
+    assert p.implicit_viscosity and p.visco_max_error == 0.001 and p.visco_boundary == 0.1
+    assert p.flags() & _abi.NN_F_IMPLICIT_VISCOSITY and not p.flags() & _abi.NN_F_ELASTICITY
+    with pytest.raises(NotImplementedError):
+        Parameter.from_config(SimConfig(config={"Configuration": {"simulationMethod": 0}}))
+
+
+def test_ply_roundtrip(tmp_path):
+    import numpy as np
+
+    from nonnewton_b200.scene import export_ply_particles, read_ply_particles
+
+    x = np.random.default_rng(0).normal(size=(100, 3)).astype(np.float32)
+    f = tmp_path / "p.ply"
+    export_ply_particles(x, str(f))
+    assert np.array_equal(read_ply_particles(str(f)), x)
