@@ -312,6 +312,9 @@ def run_ours(args):
     scenes = make_workload(args.workload, seed=rank)
     sc = scenes[0]
     tuning, tune_ms = None, None
+    if args.tuning:
+        b_, u_, f_ = (int(t) for t in args.tuning.split(","))
+        tuning = {"block": b_, "unroll": u_, "cell_factor": f_}
     if args.autotune:
         from nonnewton_b200.autotune import autotune
         from nonnewton_b200.batch import Batch
@@ -442,6 +445,7 @@ def main():
     ap.add_argument("--chunk", type=int, default=10, help="steps between admissions")
     ap.add_argument("--plain-sample", type=int, default=48)
     ap.add_argument("--autotune", action="store_true", help="pick block size, unroll and cell factor first")
+    ap.add_argument("--tuning", default=None, help="block,unroll,cell_factor (e.g. 128,2,1)")
     ap.add_argument("--host-loop", action="store_true",
                     help="drive the solver loops from the host instead of CUDA-graph while-nodes "
                          "(for ncu launch lists: ncu does not profile kernel nodes inside conditional nodes)")

@@ -62,6 +62,7 @@ extern "C" {
 #define NN_F_CFL               (1u << 6) /* CFL time step (extension: the reference has none) */
 #define NN_F_QUIRKS            (1u << 7) /* reproduce the reference's documented quirks */
 #define NN_F_CARREAU_TEXTBOOK  (1u << 8) /* (1+(K g)^2)^((n-1)/2) instead of SPH/main.py:431-437 */
+#define NN_F_RIGID             (1u << 9) /* RigidBodySolver shape matching, SPH/main.py:1099-1158 */
 
 /* non-Newtonian laws, SPH/main.py:347-355 */
 #define NN_NEWTONIAN        0
@@ -112,6 +113,9 @@ typedef struct nn_scene_params {
   double youngs_modulus, poisson_ratio;
   /* CFL (extension) */
   double cfl_factor, cfl_min_dt, cfl_max_dt;
+  /* rigid bodies: RigidBodySolver.substep runs coupling_interval times per step */
+  int32_t coupling_interval;      /* couplingInterval (SPH/main.py:616, 930) */
+  int32_t pad2;
 } nn_scene_params;
 
 /* One scene of a segmented particle array. */
@@ -182,6 +186,7 @@ enum nn_pass {
   NN_PASS_ADVECT,                     /* SPHBase.advect, 1086-1093 */
   NN_PASS_ENFORCE_BOUNDARY,           /* SPHBase.enforce_boundary_3D (FLUID then SOLID), 936-937 */
   NN_PASS_SUBSTEP,                    /* DFSPHSolver.substep, 1546-1555 */
+  NN_PASS_RIGID,                      /* RigidBodySolver.substep (all bodies), 1108-1111 */
   NN_PASS_COUNT
 };
 

@@ -41,6 +41,7 @@ NN_F_DIVERGENCE = 1 << 5
 NN_F_CFL = 1 << 6
 NN_F_QUIRKS = 1 << 7
 NN_F_CARREAU_TEXTBOOK = 1 << 8
+NN_F_RIGID = 1 << 9
 
 NN_NEWTONIAN = 0
 NN_POWER_LAW = 1
@@ -54,7 +55,7 @@ NN_HERSCHEL_BULKLEY = 6
  NN_PASS_CLEAR_ACCELERATIONS, NN_PASS_DENSITIES, NN_PASS_DFSPH_FACTOR,
  NN_PASS_DIVERGENCE_SOLVE, NN_PASS_NON_PRESSURE_FORCES, NN_PASS_NON_PRESSURE_ADVECT,
  NN_PASS_PRESSURE_SOLVE, NN_PASS_ELASTICITY, NN_PASS_ADVECT, NN_PASS_ENFORCE_BOUNDARY,
- NN_PASS_SUBSTEP, NN_PASS_COUNT) = range(15)
+ NN_PASS_SUBSTEP, NN_PASS_RIGID, NN_PASS_COUNT) = range(16)
 
 (NN_K_PRESSURE_UPDATE, NN_K_DENSITY_ADV, NN_K_DIVERGENCE_UPDATE, NN_K_DENSITY_CHANGE, NN_K_DENSITY_FACTOR,
  NN_K_BUILD_LISTS, NN_K_CG_MATVEC, NN_K_NONPRESSURE, NN_K_COUNT) = range(9)
@@ -104,6 +105,8 @@ class nn_scene_params(C.Structure):
         ("cfl_factor", C.c_double),
         ("cfl_min_dt", C.c_double),
         ("cfl_max_dt", C.c_double),
+        ("coupling_interval", C.c_int32),
+        ("pad2", C.c_int32),
     ]
 
 

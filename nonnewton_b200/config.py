@@ -111,6 +111,7 @@ class Parameter:
     cfl_max_dt: float = 5e-3
     quirks: bool = False
     has_elastic: bool = False
+    has_rigid: bool = False
     surface_tension: float = 0.01
     extra: dict = field(default_factory=dict)
 
@@ -196,6 +197,7 @@ class Parameter:
             cfl_max_dt=float(g("cflMaxTimeStepSize", 5e-3)),
             quirks=bool(g("referenceQuirks", quirks)),
             has_elastic=bool(el),
+            has_rigid=any(s_.get("solidType") == "RIGID" for s_ in solids),
         )
         if p.simulation_method not in (4, None):
             # build_solver (SPH/main.py:196-203)
@@ -222,6 +224,8 @@ class Parameter:
             f |= _abi.NN_F_CARREAU_TEXTBOOK
         if self.has_elastic:
             f |= _abi.NN_F_ELASTICITY
+        if self.has_rigid:
+            f |= _abi.NN_F_RIGID
         return f
 
     def to_c(self) -> _abi.nn_scene_params:
@@ -243,6 +247,7 @@ class Parameter:
             visco_max_error=self.visco_max_error, visco_boundary=self.visco_boundary,
             youngs_modulus=self.youngs_modulus, poisson_ratio=self.poisson_ratio,
             cfl_factor=self.cfl_factor, cfl_min_dt=self.cfl_min_dt, cfl_max_dt=self.cfl_max_dt,
+            coupling_interval=self.coupling_interval,
         )
 
 

@@ -42,6 +42,8 @@ struct SceneDev {
   float el_cd, el_co, el_cs;      // isotropic C of Becker 2009 (SPH/main.py:1276-1283)
   int32_t el_mult;                // elastic substeps per step (quirk: one per elastic phase)
   float cfl_factor, cfl_min_dt, cfl_max_dt, diameter;
+  float V0, padding;              // volume0 and padding (rigid-body mass, ground clamp)
+  int32_t n_rigid, coupling;      // rigid bodies of the scene, substeps per step
 };
 
 // Mutable per-scene state on the device.
@@ -153,17 +155,27 @@ __device__ __forceinline__ float3 kgrad_r2(float3 r, float r2, const SceneDev& s
 template <int NB_U, typename Load, typename Use>
 __device__ __forceinline__ void nb_batches(const int32_t* __restrict__ list, int stride, int c, int self, Load load,
                                            Use use) {
-  // software pipeline: the list entries of batch b+1 are loaded while batch b gathers
-  int jn[NB_U];
+  // software pipeline: list entries are loaded PD batches (8 entries) ahead of the
+  // gathers, so the DRAM latency of the list stream overlaps several batches
+  constexpr int PD = NB_U >= 8 ? 1 : 8 / NB_U;
+  int q[PD][NB_U];
 #pragma unroll
-  for (int u = 0; u < NB_U; ++u) jn[u] = (u < c) ? __ldg(list + (size_t)u * stride) : self;
+  for (int p = 0; p < PD; ++p)
+#pragma unroll
+    for (int u = 0; u < NB_U; ++u) q[p][u] = (p * NB_U + u < c) ? __ldg(list + (size_t)(p * NB_U + u) * stride) : self;
   for (int k = 0; k < c; k += NB_U) {
     int j[NB_U];
 #pragma unroll
-    for (int u = 0; u < NB_U; ++u) j[u] = jn[u];
+    for (int u = 0; u < NB_U; ++u) j[u] = q[0][u];
 #pragma unroll
-    for (int u = 0; u < NB_U; ++u)
-      jn[u] = (k + NB_U + u < c) ? __ldg(list + (size_t)(k + NB_U + u) * stride) : self;
+    for (int p = 0; p + 1 < PD; ++p)
+#pragma unroll
+      for (int u = 0; u < NB_U; ++u) q[p][u] = q[p + 1][u];
+#pragma unroll
+    for (int u = 0; u < NB_U; ++u) {
+      const int kk = k + PD * NB_U + u;
+      q[PD - 1][u] = (kk < c) ? __ldg(list + (size_t)kk * stride) : self;
+    }
     decltype(load(0)) g[NB_U];
 #pragma unroll
     for (int u = 0; u < NB_U; ++u) g[u] = load(j[u]);

@@ -64,6 +64,14 @@ struct Dev {
   int32_t el_stride;           // Ne capacity
   float* el_R;                 // [9][Ne]
   float* el_S;                 // [6][Ne]
+  // rigid bodies ("r-space")
+  int32_t n_rb;
+  const int32_t* rb_of_id;     // [cap] body index or -1
+  const int32_t* rb_round;     // [n_rb] position of the body among its scene's bodies
+  double* rb_acc;              // [n_rb][13] reductions
+  double* rb_rest;             // [n_rb][3] rest centre of mass
+  double* rb_cm;               // [n_rb][3] current centre of mass
+  double* rb_R;                // [n_rb][9] rotation
   // loop control
   int32_t* any_active;         // host-visible flag of the last check
   unsigned long long loop_handle; // cudaGraphConditionalHandle (0 when not in a graph)

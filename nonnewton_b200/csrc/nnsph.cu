@@ -81,6 +81,9 @@ struct nn_ctx {
   int32_t *el_id = nullptr, *el_slot = nullptr, *e_of_id = nullptr, *el_nb = nullptr, *el_cnt = nullptr;
   float4* el_x0 = nullptr;
   float *el_R = nullptr, *el_S = nullptr;
+  int n_rb = 0, rb_rounds = 0, coupling_max = 1;
+  int32_t *rb_of_id = nullptr, *rb_round = nullptr;
+  double *rb_acc = nullptr, *rb_rest = nullptr, *rb_cm = nullptr, *rb_R = nullptr;
   int32_t* d_any = nullptr;
   int32_t* h_any = nullptr;            // pinned
   int32_t* d_body = nullptr;
@@ -157,6 +160,8 @@ static Dev make_dev(nn_ctx* c, int cur) {
   d.el_id = c->el_id; d.el_slot = c->el_slot; d.e_of_id = c->e_of_id; d.el_x0 = c->el_x0;
   d.el_nb = c->el_nb; d.el_cnt = c->el_cnt; d.el_cap = c->el_cap; d.el_stride = c->el_stride;
   d.el_R = c->el_R; d.el_S = c->el_S;
+  d.n_rb = c->n_rb; d.rb_of_id = c->rb_of_id; d.rb_round = c->rb_round; d.rb_acc = c->rb_acc;
+  d.rb_rest = c->rb_rest; d.rb_cm = c->rb_cm; d.rb_R = c->rb_R;
   d.any_active = c->d_any;
   d.loop_handle = c->cur_handle;
   d.body_count = c->d_body;
@@ -370,6 +375,22 @@ static int enq_elastic(nn_ctx* c, cudaStream_t s) {
   return NN_OK;
 }
 
+// for rb in meta.rbs: coupling_interval x RigidBodySolver.substep (SPH/main.py:929-931)
+static int enq_rigid(nn_ctx* c, cudaStream_t s) {
+  if (c->n_rb == 0) return NN_OK;
+  Dev d = make_dev(c, c->cur);
+  for (int rep = 0; rep < c->coupling_max; ++rep)
+    for (int r = 0; r < c->rb_rounds; ++r) {
+      RC(launch(c, s, k_rigid_ground, 256, c->n, d, r, rep));
+      RC(launch(c, s, k_rigid_com, 256, c->n, d, r, 0));
+      RC(launch1(c, s, k_rigid_cm, d, r, 0));
+      RC(launch(c, s, k_rigid_A, 256, c->n, d, r));
+      RC(launch1(c, s, k_rigid_R, d, r));
+      RC(launch(c, s, k_rigid_apply, 256, c->n, d, r));
+    }
+  return NN_OK;
+}
+
 // DFSPHSolver.substep (SPH/main.py:1546-1555) with the fused passes.
 static int enq_substep(nn_ctx* c, cudaStream_t s) {
   if (!c->any_fluid) return NN_OK;
@@ -395,6 +416,7 @@ static int enq_step(nn_ctx* c, cudaStream_t s) {
   RC(launch(c, s, k_clear_acc, 256, c->n, d));
   RC(enq_substep(c, s));
   RC(enq_elastic(c, s));
+  RC(enq_rigid(c, s));
   RC(launch(c, s, k_advect_boundary, 256, c->n, d, 1, 1));
   return launch1(c, s, k_step_end, d);
 }
@@ -530,6 +552,9 @@ static SceneDev make_scene(const nn_scene_desc& sd, int64_t cell_base, int el_mu
   s.cfl_min_dt = (float)p.cfl_min_dt;
   s.cfl_max_dt = (float)p.cfl_max_dt;
   s.diameter = (float)dia;
+  s.V0 = (float)p.volume0;
+  s.padding = (float)p.padding;
+  s.coupling = std::max(p.coupling_interval, 1);
   return s;
 }
 
@@ -627,6 +652,8 @@ int nn_ctx_destroy(nn_ctx* c) {
                   c->e_of_id, c->d_any, c->d_body, c->cell_count, c->tile_sums};
   for (void* b : bufs) cudaFree(b);
   free_elastic(c);
+  cudaFree(c->rb_of_id); cudaFree(c->rb_round); cudaFree(c->rb_acc); cudaFree(c->rb_rest); cudaFree(c->rb_cm);
+  cudaFree(c->rb_R);
   if (c->h_any) cudaFreeHost(c->h_any);
   if (c->side) cudaStreamDestroy(c->side);
   if (c->own) cudaStreamDestroy(c->own);
@@ -721,7 +748,7 @@ int nn_set_scenes(nn_ctx* c, int32_t nscenes, const nn_scene_desc* scenes) {
   // host copies of the class fields lay out the elastic particles; scenes without the
   // elasticity flag need none (no transfer for pure-fluid batches)
   bool want_el = false;
-  for (int k = 0; k < nscenes; ++k) want_el |= (scenes[k].params.flags & NN_F_ELASTICITY) != 0;
+  for (int k = 0; k < nscenes; ++k) want_el |= (scenes[k].params.flags & (NN_F_ELASTICITY | NN_F_RIGID)) != 0;
   std::vector<int32_t> mat, ph;
   if (n > 0 && want_el) {
     mat.resize(n);
@@ -732,6 +759,8 @@ int nn_set_scenes(nn_ctx* c, int32_t nscenes, const nn_scene_desc* scenes) {
   std::vector<SceneDev> sdev;
   std::vector<SceneDyn> sdyn(nscenes);
   std::vector<int32_t> el_id;
+  struct RB { int scene, phase, round; };
+  std::vector<RB> rb_list;
   int64_t cells = 0;
   c->any_fluid = c->any_div = c->any_nonnewton = c->any_implicit = c->any_cfl = false;
   c->el_mult_max = 0;
@@ -750,6 +779,16 @@ int nn_set_scenes(nn_ctx* c, int32_t nscenes, const nn_scene_desc* scenes) {
       for (int i = sd.start; i < sd.start + sd.n; ++i)
         if (q || (mat[i] == NN_SOLID && ph[i] >= NN_PHASE_ELASTIC_BASE)) el_id.push_back(i);
     SceneDev s = make_scene(sd, cells, el_mult, c->cell_factor);
+    // rigid bodies of the scene (RIGID phases: dynamic solids with phase ids 2000..2999)
+    if (sd.params.flags & NN_F_RIGID) {
+      std::vector<int> rp;
+      for (int i = sd.start; i < sd.start + sd.n; ++i)
+        if (mat[i] == NN_SOLID && ph[i] >= NN_PHASE_RIGID_BASE && ph[i] < NN_PHASE_ELASTIC_BASE) rp.push_back(ph[i]);
+      std::sort(rp.begin(), rp.end());
+      rp.erase(std::unique(rp.begin(), rp.end()), rp.end());
+      s.n_rigid = (int)rp.size();
+      for (int r = 0; r < (int)rp.size(); ++r) rb_list.push_back({k, rp[r], r});
+    }
     cells += (int64_t)s.gx * ((int64_t)1 << (2 * s.mbits));
     sdev.push_back(s);
     SceneDyn y{};
@@ -802,6 +841,34 @@ int nn_set_scenes(nn_ctx* c, int32_t nscenes, const nn_scene_desc* scenes) {
   int32_t hn[4] = {n, nscenes, (int)cells, c->ne};
   CK(cudaMemcpy(c->d_n, hn, sizeof(hn), cudaMemcpyHostToDevice));
   CK(cudaMemset(c->d_acc, 0, (size_t)c->max_scenes * ACC_COUNT * NN_STRIPES * sizeof(double)));
+  // rigid bodies ("r-space")
+  cudaFree(c->rb_of_id); cudaFree(c->rb_round); cudaFree(c->rb_acc); cudaFree(c->rb_rest); cudaFree(c->rb_cm);
+  cudaFree(c->rb_R);
+  c->rb_of_id = c->rb_round = nullptr;
+  c->rb_acc = c->rb_rest = c->rb_cm = c->rb_R = nullptr;
+  c->n_rb = (int)rb_list.size();
+  c->rb_rounds = 0;
+  c->coupling_max = 1;
+  if (c->n_rb > 0) {
+    std::vector<int32_t> rb_of(n, -1), rounds(c->n_rb);
+    for (int b = 0; b < c->n_rb; ++b) {
+      const nn_scene_desc& sd = scenes[rb_list[b].scene];
+      for (int i = sd.start; i < sd.start + sd.n; ++i)
+        if (mat[i] == NN_SOLID && ph[i] == rb_list[b].phase) rb_of[i] = b;
+      rounds[b] = rb_list[b].round;
+      c->rb_rounds = std::max(c->rb_rounds, rb_list[b].round + 1);
+      c->coupling_max = std::max(c->coupling_max, std::max(sd.params.coupling_interval, 1));
+    }
+    const size_t B = (size_t)c->n_rb;
+    if (dalloc(&c->rb_of_id, (size_t)n) != cudaSuccess || dalloc(&c->rb_round, B) != cudaSuccess ||
+        dalloc(&c->rb_acc, B * 13) != cudaSuccess || dalloc(&c->rb_rest, B * 3) != cudaSuccess ||
+        dalloc(&c->rb_cm, B * 3) != cudaSuccess || dalloc(&c->rb_R, B * 9) != cudaSuccess)
+      return fail(c, NN_ERR_OOM, "rigid-body buffers");
+    CK(cudaMemcpy(c->rb_of_id, rb_of.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->rb_round, rounds.data(), B * sizeof(int32_t), cudaMemcpyHostToDevice));
+    CK(cudaMemset(c->rb_acc, 0, B * 13 * sizeof(double)));
+    drop_graphs(c);  // body buffers and counts are graph arguments
+  }
   if (nscenes > 0 && n > 0) {  // scene of every particle id, filled from the scene table on the device
     k_scene_of_id<<<std::min(nscenes, 65535), 256>>>(make_dev(c, c->cur));
     CK(cudaGetLastError());
@@ -834,6 +901,11 @@ int nn_initialize(nn_ctx* c) {
   RC(enq_search(c, s));
   Dev d = make_dev(c, c->cur);
   RC(launch1(c, s, k_step_dt, d, 0));
+  // RigidBodySolver.__init__: rest centre of mass of every body (SPH/main.py:1101-1106)
+  for (int r = 0; r < c->rb_rounds; ++r) {
+    RC(launch(c, s, k_rigid_com, 256, c->n, d, r, 1));
+    RC(launch1(c, s, k_rigid_cm, d, r, 1));
+  }
   RC(launch(c, s, KU(k_boundary_volume), c->block, c->n, d, 0));
   RC(launch(c, s, KU(k_boundary_volume), c->block, c->n, d, 1));
   RC(enq_sync_out(c, s, SM_VOL));
@@ -895,6 +967,7 @@ int nn_run_pass(nn_ctx* c, int32_t pass) {
     case NN_PASS_ADVECT: RC(launch(c, s, k_advect_boundary, 256, c->n, d, 1, 0)); break;
     case NN_PASS_ENFORCE_BOUNDARY: RC(launch(c, s, k_advect_boundary, 256, c->n, d, 0, 1)); break;
     case NN_PASS_SUBSTEP: RC(enq_substep(c, s)); break;
+    case NN_PASS_RIGID: RC(enq_rigid(c, s)); break;
     default: break;
   }
   RC(enq_sync_out(c, s, SM_ALL));

@@ -5,6 +5,13 @@
 #pragma once
 #include "dev.cuh"
 
+// Register cap of the solver-loop passes (occupancy vs. spills; set at build time).
+#ifdef NN_PASS_MAXREG
+#define NN_PASS_REGS __maxnreg__(NN_PASS_MAXREG)
+#else
+#define NN_PASS_REGS
+#endif
+
 #define NB_LOOP(d, i, j)                                   \
   for (int _k = 0, _c = (d).nbr_cnt[i]; _k < _c; ++_k)     \
     for (int j = (d).nbr[(size_t)_k * (d).cap + (i)], _o = 1; _o; _o = 0)
@@ -112,7 +119,7 @@ __global__ void k_density_factor(Dev d, int do_density, int do_factor) {
 // divergence_solve, also applies alpha *= 1/dt (1688); mode 1: solver iteration,
 // accumulates the FP64 density error (1669-1675, 1717-1719).
 template <int U>
-__global__ void k_density_change(Dev d, int mode) {
+__global__ void NN_PASS_REGS k_density_change(Dev d, int mode) {
   const int n = d.d_n[0];
   FOR_SLOTS_WARP(i, valid, n) {
     uint32_t fl = valid ? d.w.flags[i] : 0u;
@@ -149,7 +156,7 @@ __global__ void k_density_change(Dev d, int mode) {
 // dynamic solids (1755-1760) are omitted: clear_accelerations (1552) discards them.
 struct GPK { float4 p; float k; };
 template <int U>
-__global__ void k_divergence_update(Dev d) {
+__global__ void NN_PASS_REGS k_divergence_update(Dev d) {
   const int n = d.d_n[0];
   GRID_STRIDE(i, n) {
     const uint32_t fl = d.w.flags[i];
@@ -192,7 +199,7 @@ __global__ void k_alpha_times_dt(Dev d) {
 // compute_density_adv (SPH/main.py:1647-1667). mode 0: first call of pressure_solve,
 // also alpha *= 1/dt^2 (1771); mode 1: iteration, FP64 error (1793-1797).
 template <int U>
-__global__ void k_density_adv(Dev d, int mode) {
+__global__ void NN_PASS_REGS k_density_adv(Dev d, int mode) {
   const int n = d.d_n[0];
   FOR_SLOTS_WARP(i, valid, n) {
     uint32_t fl = valid ? d.w.flags[i] : 0u;
@@ -232,7 +239,7 @@ __global__ void k_density_adv(Dev d, int mode) {
 // place per neighbour; dynamic solid slots gather the two-way coupling acceleration
 // from their fluid neighbours (the reference scatters it with atomics, 1835-1841).
 template <int U>
-__global__ void k_pressure_update(Dev d) {
+__global__ void NN_PASS_REGS k_pressure_update(Dev d) {
   const int n = d.d_n[0];
   GRID_STRIDE(i, n) {
     const uint32_t fl = d.w.flags[i];
@@ -1062,5 +1069,144 @@ __global__ void k_sync_in(Dev d, uint32_t mask) {
     if (mask & 32u) d.alpha[i] = d.t.dfsph_factor[id];
     if (mask & 64u) d.rho_adv[i] = d.t.density_adv[id];
     if (mask & 256u) d.w.mass[i] = d.t.m[id];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Rigid bodies: RigidBodySolver.substep (SPH/main.py:1108-1158), shape matching per
+// body. Bodies are numbered per context ("r-space"); round r processes the r-th body
+// of every scene, so each scene's bodies run in the reference's order.
+#define RB_ACC 13  // per body: sum m x (3), sum m (1), sum m p (x) q (9)
+
+// FP64 sums of `nv` values per body over a warp: body-uniform warps reduce with
+// shuffles and one lane issues the atomics; mixed warps use per-lane atomics.
+template <int NV>
+__device__ __forceinline__ void body_add(double* acc, int body, const double (&v)[NV]) {
+  const unsigned full = 0xffffffffu;
+  const unsigned vb = __ballot_sync(full, body >= 0);
+  if (vb == 0) return;
+  const int leader = __ffs(vb) - 1;
+  const int b0 = __shfl_sync(full, body, leader);
+  const bool uniform = __all_sync(full, body < 0 || body == b0);
+  if (uniform) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+      double x = body >= 0 ? v[k] : 0.0;
+      for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(full, x, o);
+      if ((int)(threadIdx.x & 31) == leader) atomicAdd(&acc[(size_t)b0 * RB_ACC + k], x);
+    }
+  } else if (body >= 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) atomicAdd(&acc[(size_t)body * RB_ACC + k], v[k]);
+  }
+}
+
+__device__ __forceinline__ int rigid_body_of_slot(const Dev& d, int i, int round) {
+  const int b = d.rb_of_id[d.w.id[i]];
+  return (b >= 0 && d.rb_round[b] == round) ? b : -1;
+}
+
+// ground_collision (SPH/main.py:1113-1118): every solid particle of a scene with
+// rigid bodies is lifted to y >= padding (once per body substep, like the reference).
+__global__ void k_rigid_ground(Dev d, int round, int rep) {
+  const int n = d.d_n[0];
+  GRID_STRIDE(i, n) {
+    const uint32_t fl = d.w.flags[i];
+    if (!cls_solid(fl)) continue;
+    const SceneDev& s = d.sc[slot_scene(fl)];
+    if (!(s.flags & NN_F_RIGID) || round >= s.n_rigid || rep >= s.coupling) continue;
+    float4 p = d.w.pos[i];
+    if (p.y < s.padding) { p.y = s.padding; d.w.pos[i] = p; }
+  }
+}
+
+// compute_com (SPH/main.py:1120-1130) over the current (rest = 0) or rest positions.
+__global__ void k_rigid_com(Dev d, int round, int rest) {
+  const int n = d.d_n[0];
+  FOR_SLOTS_WARP(i, valid, n) {
+    int b = valid ? rigid_body_of_slot(d, i, round) : -1;
+    double v[4] = {0, 0, 0, 0};
+    if (b >= 0) {
+      const SceneDev& s = d.sc[slot_scene(d.w.flags[i])];
+      const double m = (double)(s.V0 * d.w.dens[i]);
+      float3 x;
+      if (rest) {
+        const int id = d.w.id[i];
+        x = make_float3(d.t.x_0[3 * id], d.t.x_0[3 * id + 1], d.t.x_0[3 * id + 2]);
+      } else {
+        x = f3(d.w.pos[i]);
+      }
+      v[0] = m * x.x; v[1] = m * x.y; v[2] = m * x.z; v[3] = m;
+    }
+    body_add<4>(d.rb_acc, b, v);
+  }
+}
+
+// Per body: centre of mass (into rb_rest for the rest state, rb_cm otherwise).
+__global__ void k_rigid_cm(Dev d, int round, int rest) {
+  for (int b = threadIdx.x; b < d.n_rb; b += blockDim.x) {
+    if (d.rb_round[b] != round) continue;
+    double* a = &d.rb_acc[(size_t)b * RB_ACC];
+    double* out = rest ? &d.rb_rest[3 * b] : &d.rb_cm[3 * b];
+    for (int k = 0; k < 3; ++k) out[k] = a[3] > 0 ? a[k] / a[3] : 0.0;
+    for (int k = 0; k < RB_ACC; ++k) a[k] = 0.0;
+  }
+}
+
+// A = sum m (x - cm) (x) (x0 - rest_cm) (SPH/main.py:1141-1146).
+__global__ void k_rigid_A(Dev d, int round) {
+  const int n = d.d_n[0];
+  FOR_SLOTS_WARP(i, valid, n) {
+    int b = valid ? rigid_body_of_slot(d, i, round) : -1;
+    double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (b >= 0) {
+      const SceneDev& s = d.sc[slot_scene(d.w.flags[i])];
+      const double m = (double)(s.V0 * d.w.dens[i]);
+      const int id = d.w.id[i];
+      const float4 x = d.w.pos[i];
+      const double p[3] = {(double)x.x - d.rb_cm[3 * b], (double)x.y - d.rb_cm[3 * b + 1],
+                           (double)x.z - d.rb_cm[3 * b + 2]};
+      const double q[3] = {(double)d.t.x_0[3 * id] - d.rb_rest[3 * b], (double)d.t.x_0[3 * id + 1] - d.rb_rest[3 * b + 1],
+                           (double)d.t.x_0[3 * id + 2] - d.rb_rest[3 * b + 2]};
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) v[3 * r + c] = m * p[r] * q[c];
+    }
+    double* acc = d.rb_acc + 4;  // the A block of each body's accumulator
+    body_add<9>(acc, b, v);
+  }
+}
+
+// R = polar(A) (SPH/main.py:1148-1151), identity if every entry is below 1e-6.
+__global__ void k_rigid_R(Dev d, int round) {
+  for (int b = threadIdx.x; b < d.n_rb; b += blockDim.x) {
+    if (d.rb_round[b] != round) continue;
+    double* a = &d.rb_acc[(size_t)b * RB_ACC + 4];
+    double A[3][3], R[3][3];
+    for (int k = 0; k < 9; ++k) A[k / 3][k % 3] = a[k];
+    closest_rotation(A, R);
+    bool small = true;
+    for (int k = 0; k < 9; ++k) small = small && fabs(R[k / 3][k % 3]) < 1e-6;
+    for (int k = 0; k < 9; ++k) d.rb_R[9 * b + k] = small ? ((k % 4 == 0) ? 1.0 : 0.0) : R[k / 3][k % 3];
+    for (int k = 0; k < RB_ACC; ++k) d.rb_acc[(size_t)b * RB_ACC + k] = 0.0;
+  }
+}
+
+// x = cm + R (x0 - rest_cm) (SPH/main.py:1153-1157).
+__global__ void k_rigid_apply(Dev d, int round) {
+  const int n = d.d_n[0];
+  GRID_STRIDE(i, n) {
+    const int b = rigid_body_of_slot(d, i, round);
+    if (b < 0) continue;
+    const int id = d.w.id[i];
+    const double q[3] = {(double)d.t.x_0[3 * id] - d.rb_rest[3 * b], (double)d.t.x_0[3 * id + 1] - d.rb_rest[3 * b + 1],
+                         (double)d.t.x_0[3 * id + 2] - d.rb_rest[3 * b + 2]};
+    const double* R = &d.rb_R[9 * b];
+    float4 p = d.w.pos[i];
+    p.x = (float)(d.rb_cm[3 * b] + R[0] * q[0] + R[1] * q[1] + R[2] * q[2]);
+    p.y = (float)(d.rb_cm[3 * b + 1] + R[3] * q[0] + R[4] * q[1] + R[5] * q[2]);
+    p.z = (float)(d.rb_cm[3 * b + 2] + R[6] * q[0] + R[7] * q[1] + R[8] * q[2]);
+    d.w.pos[i] = p;
   }
 }

@@ -6,8 +6,8 @@
   trimesh: rotation about the point-cloud centroid, then translation; the tank is a
   lattice of spacing 2r filling the padded domain up to `height`.
 - `load_particles` (SPH/main.py:628-691): phases ordered fluid -> static solid ->
-  elastic solid, with the reference's phase_id bases 0 / 1000 / 3000. Rigid phases
-  (2000..) are rejected: rigid coupling is outside this path.
+  rigid solid -> elastic solid, with the reference's phase_id bases 0 / 1000 / 2000 /
+  3000.
 - Generators for the benchmark scenes (dam break, shear-thinning drop, fluid +
   elastic, the 2.4M-particle roofline scene, the mixed served workload), all seeded.
 """
@@ -149,7 +149,7 @@ def assemble(phases: list[PhaseInfo], param: Parameter, mass_density_default: fl
     """`initialize_particles` (SPH/main.py:735-758). Mass is volume0 * 1000
     (SPH/main.py:743) unless the phase sets its own density0 (extension)."""
     order = sorted(phases, key=lambda ph: (0 if ph.material == FLUID else
-                                           (1 if ph.solid_type == STATIC else 3)))
+                                           (1 if ph.solid_type == STATIC else (2 if ph.solid_type == RIGID else 3))))
     start = 0
     xs, mats, dyns, pids, masses = [], [], [], [], []
     info = {}
@@ -192,12 +192,14 @@ def load_particles(cfg: SimConfig, param: Parameter, root: str | None = None) ->
     for k, c in enumerate(cfg.get_cfg_list("FluidTanks", [])):
         phases.append(PhaseInfo(uid=c.get("id", base + k), material=FLUID, is_dynamic=True, cfg=c,
                                 pos=_pos(c, fill_tank(param, c["height"]))))
-    cnt_s = cnt_e = 0
+    cnt_s = cnt_e = cnt_r = 0
     for c in cfg.get_solid_cfg():
         st = c.get("solidType", "STATIC")
         if st == "RIGID":
-            raise NotImplementedError("RIGID solids (RigidBodySolver) are outside this SPH path")
-        if st == "ELASTIC":
+            phases.append(PhaseInfo(uid=c.get("id", cnt_r) + 2000, material=SOLID, is_dynamic=True, cfg=c,
+                                    pos=_pos(c), solid_type=RIGID))
+            cnt_r += 1
+        elif st == "ELASTIC":
             phases.append(PhaseInfo(uid=c.get("id", cnt_e) + 3000, material=SOLID, is_dynamic=True, cfg=c,
                                     pos=_pos(c), solid_type=ELASTIC, density0=c.get("density0")))
             cnt_e += 1
@@ -426,3 +428,27 @@ SCENES = {
     "fluid_elastic": fluid_elastic,
     "roofline_2m": roofline_scene,
 }
+
+
+def rigid_drop(seed=0, n_fluid=(10, 5, 10), n_body=(4, 4, 4), box=0.4, r=0.01, coupling=1, quirks=False,
+               steps=100) -> Scene:
+    """A rigid cube (RIGID phase, shape matching with two-way pressure coupling,
+    SPH/main.py:1099-1158) dropped into a shallow fluid layer in a boundary box."""
+    h = 4 * r
+    sp = 2 * r
+    rng = np.random.default_rng(seed)
+    conf = {"Configuration": _base_config(r, [0, 0, 0], [box + 2 * h] * 3, 1e-3, couplingInterval=coupling),
+            "FluidParticles": [{}],
+            "SolidParticles": [{"solidType": "STATIC"}, {"solidType": "RIGID"}]}
+
+    def phases(param):
+        fl = block([h + sp] * 3, n_fluid, sp, 1e-4, rng)
+        bd = box_shell([h] * 3, [box + h] * 3, sp)
+        side = (n_body[0] - 1) * sp
+        top = h + sp + n_fluid[1] * sp + 3 * sp
+        rb = block([h + box / 2 - side / 2, top, h + box / 2 - side / 2], n_body, sp)
+        return [PhaseInfo(uid=0, material=FLUID, is_dynamic=True, pos=fl),
+                PhaseInfo(uid=1000, material=SOLID, is_dynamic=False, pos=bd, solid_type=STATIC),
+                PhaseInfo(uid=2000, material=SOLID, is_dynamic=True, pos=rb, solid_type=RIGID)]
+
+    return _make("rigid_drop", conf, phases, steps, quirks)

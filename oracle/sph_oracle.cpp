@@ -1023,6 +1023,80 @@ class Sim : public SimBase {
     }
   }
 
+  // ---- Rigid bodies: RigidBodySolver, SPH/main.py:1099-1158 ---------------------
+  std::vector<int> rigid_phases;
+  std::vector<V3<double>> rigid_rest_cm;
+  bool is_rigid(int i) const {
+    return material[i] == NN_SOLID && is_dynamic[i] && phase_id[i] >= NN_PHASE_RIGID_BASE &&
+           phase_id[i] < NN_PHASE_ELASTIC_BASE;
+  }
+  // compute_com, SPH/main.py:1120-1130 (mass = volume0 * density; FP64 accumulation)
+  V3<double> rigid_com(int ph, bool rest) const {
+    double sm = 0, c[3] = {0, 0, 0};
+    const double V0 = double(R(p.volume0));
+    for (int i = 0; i < n; ++i) {
+      if (!(material[i] == NN_SOLID && is_dynamic[i] && phase_id[i] == ph)) continue;
+      const double mass = double(R(V0) * density[i]);
+      const V3<R>& xi = rest ? x0[i] : x[i];
+      for (int d = 0; d < 3; ++d) c[d] += mass * double(xi[d]);
+      sm += mass;
+    }
+    return V3<double>(c[0] / sm, c[1] / sm, c[2] / sm);
+  }
+  // RigidBodySolver.__init__ / compute_rigid_rest_cm, SPH/main.py:1101-1106, 1132-1134
+  void rigid_init() {
+    rigid_phases.clear();
+    rigid_rest_cm.clear();
+    if (!has(NN_F_RIGID)) return;
+    for (int i = 0; i < n; ++i)
+      if (is_rigid(i)) rigid_phases.push_back(phase_id[i]);
+    std::sort(rigid_phases.begin(), rigid_phases.end());
+    rigid_phases.erase(std::unique(rigid_phases.begin(), rigid_phases.end()), rigid_phases.end());
+    for (int ph : rigid_phases) rigid_rest_cm.push_back(rigid_com(ph, true));
+  }
+  // RigidBodySolver.substep: ground_collision + solve_constraints, SPH/main.py:1108-1158
+  void rigid_substep() {
+    const R pad = R(p.padding);
+    const double V0 = double(R(p.volume0));
+    for (size_t b = 0; b < rigid_phases.size(); ++b) {
+      const int ph = rigid_phases[b];
+      for (int i = 0; i < n; ++i)  // ground_collision, 1113-1118: every solid particle
+        if (material[i] == NN_SOLID && x[i][1] < pad) x[i][1] = pad;
+      const V3<double> cm = rigid_com(ph, false);
+      const V3<double>& rc = rigid_rest_cm[b];
+      double A[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+      for (int i = 0; i < n; ++i) {
+        if (!(material[i] == NN_SOLID && is_dynamic[i] && phase_id[i] == ph)) continue;
+        const double mass = double(R(V0) * density[i]);
+        double q[3], pp[3];
+        for (int d = 0; d < 3; ++d) { q[d] = double(x0[i][d]) - rc[d]; pp[d] = double(x[i][d]) - cm[d]; }
+        for (int r = 0; r < 3; ++r)
+          for (int c = 0; c < 3; ++c) A[r][c] += mass * pp[r] * q[c];
+      }
+      double Rm[3][3];
+      closest_rotation(A, Rm);
+      bool small = true;
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) small = small && std::fabs(Rm[r][c]) < 1e-6;
+      if (small)
+        for (int r = 0; r < 3; ++r)
+          for (int c = 0; c < 3; ++c) Rm[r][c] = r == c ? 1.0 : 0.0;
+      for (int i = 0; i < n; ++i) {
+        if (!(material[i] == NN_SOLID && is_dynamic[i] && phase_id[i] == ph)) continue;
+        double q[3];
+        for (int d = 0; d < 3; ++d) q[d] = double(x0[i][d]) - rc[d];
+        for (int d = 0; d < 3; ++d) {
+          const double goal = cm[d] + Rm[d][0] * q[0] + Rm[d][1] * q[1] + Rm[d][2] * q[2];
+          x[i][d] = R(goal);
+        }
+      }
+    }
+  }
+  void rigid_step() {
+    const int reps = std::max(p.coupling_interval, 1);
+    for (int k = 0; k < reps; ++k) rigid_substep();
+  }
+
   // DFSPHSolver.substep, SPH/main.py:1546-1555
   void substep() {
     compute_densities();
@@ -1044,6 +1118,7 @@ class Sim : public SimBase {
     clear_accelerations();
     if (n_fluid > 0) substep();
     elasticity_substep();
+    rigid_step();  // for rb in meta.rbs: coupling_interval x rb.substep() (SPH/main.py:929-931)
     advect();
     enforce_boundary(NN_FLUID);
     enforce_boundary(NN_SOLID);
@@ -1055,6 +1130,7 @@ class Sim : public SimBase {
   int initialize() override {
     // initialize() builds Elasticity objects before solver.initialize() (1889-1895, 1915)
     elastic_init();
+    rigid_init();
     run_search();
     boundary_volume(false);
     boundary_volume(true);
@@ -1083,6 +1159,7 @@ class Sim : public SimBase {
       case NN_PASS_ADVECT: advect(); return 0;
       case NN_PASS_ENFORCE_BOUNDARY: enforce_boundary(NN_FLUID); enforce_boundary(NN_SOLID); return 0;
       case NN_PASS_SUBSTEP: if (n_fluid > 0) substep(); return 0;
+      case NN_PASS_RIGID: rigid_step(); return 0;
       default: return NN_ERR_INVALID_ARG;
     }
   }

@@ -176,3 +176,21 @@ def test_elastic_rest_state(oracle_lib):
     assert np.allclose(R, np.eye(3), atol=1e-9)
     assert np.abs(o.get("stress")).max() < 1e-6
     assert np.abs(o.get("acceleration")).max() < 1e-6
+
+
+def test_rigid_body_stays_rigid(oracle_lib):
+    """RigidBodySolver shape matching (SPH/main.py:1136-1158): after the step's
+    projection the body's pairwise distances equal the rest ones; it falls."""
+    sc = S.rigid_drop(seed=0)
+    o = oracle_lib.OracleSim(sc.particles, sc.param, "f64")
+    o.initialize()
+    rb = np.nonzero(sc.particles.phase_id == 2000)[0]
+    x0 = o.get("x")[rb]
+    for _ in range(5):
+        o.step(1)
+        o.run_pass(_abi.NN_PASS_RIGID)  # project once more, after the advect of the step
+        x = o.get("x")[rb]
+        d0 = np.linalg.norm(x0[:, None] - x0[None], axis=-1)
+        d1 = np.linalg.norm(x[:, None] - x[None], axis=-1)
+        assert np.abs(d1 - d0).max() < 1e-9
+    assert x[:, 1].mean() < x0[:, 1].mean()
