@@ -37,8 +37,14 @@ ALG_BYTES = {
     "divergence_update": 16 + 16 + 4 + 4 + 16,
     "density_change": 16 + 16 + 4 + 4 + 4 + 4,
     "density_factor": 16 + 4 + 4 + 4,
-    "cg_matvec": 16 + 16 + 16 + 4 + 4 + 16,       # pos4, p, aux, mass, flags -> Ap
+    "cg_matvec": 16 + 16 + 8 + 4 + 4 + 16,        # pos4, p, aux2, mass, flags -> Ap
+    "nonpressure": 4 + 16 + 16 + 4 + 4 + 16 + 4 + 4 + 8,  # flags, pos4, vel4, mass, dens -> acc4, srn, mu, aux2
+    "build_lists": 16 + 4 + 4,                    # pos4, flags -> count; + 4 B per list entry (added live)
 }
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch on the
+# 2.4M-particle dam break, from `ncu --set full` captures of the current kernels
+# (profiles/k_build_lists_roofline_2m.md, k_density_adv_roofline_2m.md, k_forces_roofline_2m.md).
+NCU_TRAFFIC_2M = {"build_lists": 493_405_696, "density_adv": 380_488_448, "nonpressure": 430_376_960}
 KERNEL_IDS = {"pressure_update": 0, "density_adv": 1, "divergence_update": 2, "density_change": 3,
               "density_factor": 4, "build_lists": 5, "cg_matvec": 6, "nonpressure": 7}
 
@@ -218,8 +224,8 @@ def run_served(args, world, rank):
     from nonnewton_b200.serve import Request, Server, run_plain
 
     nreq = args.requests
-    work = S.mixed_workload(n_requests=nreq, seed=1000 + rank, rate=args.rate, steps=args.steps)
-    reqs = [Request(k, sc, args.steps, t) for k, (t, sc) in enumerate(work)]
+    work = S.mixed_workload(n_requests=nreq, seed=1000 + rank, rate=args.rate, steps=args.request_steps)
+    reqs = [Request(k, sc, args.request_steps, t) for k, (t, sc) in enumerate(work)]
     # warm-up: a small served run (captures the step graphs of the server context)
     srv = Server(capacity=args.capacity, max_scenes=args.max_scenes, chunk=args.chunk)
     warm = [Request(-1 - k, sc, max(args.warmup, 1), 0.0) for k, (t, sc) in enumerate(work[:4])]
@@ -272,7 +278,7 @@ def run_served(args, world, rank):
         "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": res["step_ms_p50"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded numpy scene generator, Poisson arrivals)",
-        "config": {"workload": "served_mixed", "requests": nreq, "steps_per_request": args.steps,
+        "config": {"workload": "served_mixed", "requests": nreq, "steps_per_request": args.request_steps,
                    "arrival_rate_per_s": args.rate, "capacity_particles": args.capacity,
                    "max_scenes": args.max_scenes, "chunk_steps": args.chunk,
                    "l2": "inputs larger than L2", "parallelism": f"scenes sharded over {world} rank(s)"},
@@ -361,11 +367,20 @@ def run_ours(args):
     value = total_ps / (ms_max / 1e3)
     # ---- roofline of the dominant kernel: timed live on the current slots
     implicit = bool(sc.param.implicit_viscosity)
-    dom = "pressure_update"
     kms = {}
     for k in ("pressure_update", "density_adv", "build_lists", "density_factor", "divergence_update",
-              "density_change") + (("cg_matvec",) if implicit else ()):
+              "density_change", "nonpressure") + (("cg_matvec",) if implicit else ()):
         kms[k] = eng.time_kernel(KERNEL_IDS[k], reps=10)
+    # launches per step of each timed kernel at the iteration counts of the last step;
+    # the dominant kernel is the one with the largest time per step
+    it_v, it_p = st["iterations_v"] + 1, st["iterations"] + 1
+    per_step = {"build_lists": 1, "density_factor": 1, "nonpressure": 1, "density_adv": it_p + 1,
+                "pressure_update": it_p, "divergence_update": it_v, "density_change": it_v,
+                "cg_matvec": st["cg_iterations"]}
+    dom = max(kms, key=lambda k: kms[k] * per_step[k])
+    num_nb, _ = eng.neighbors(n, 1)
+    entries = int(num_nb.sum().item())
+    del num_nb
     # ---- end to end through the public API: pinned host state in, positions out
     pd = m.pd
     h_x = torch.empty_like(pd.x, device="cpu").pin_memory()
@@ -392,8 +407,9 @@ def run_ours(args):
         if world > 1:
             torch.distributed.destroy_process_group()
         return
-    ab = ALG_BYTES[dom] * n
+    ab = ALG_BYTES[dom] * n + (4 * entries if dom == "build_lists" else 0)
     achieved = ab / (kms[dom] / 1e3) / 1e9
+    traffic = NCU_TRAFFIC_2M.get(dom) if sc.name == "roofline_2m" else None
     hbm = peaks["hbm_gbs"]
     bytes_step = step_bytes(st["iterations_v"] + 1, st["iterations"] + 1, st["cg_iterations"], 0.0, implicit)
     line = {
@@ -407,12 +423,13 @@ def run_ours(args):
                           else "inputs smaller than L2; not flushed"),
                    "step_graph": "host-driven loops" if args.host_loop else
                    "CUDA graph with while-node solver loops",
-                   "tuning": tuning or {"block": 256, "unroll": 4, "cell_factor": 1}},
+                   "tuning": tuning or {"block": 128, "unroll": 2, "cell_factor": 1}},
         "autotune_ms_per_step": tune_ms,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "peak_source": f"{peak_kind} hbm_gbs",
-                     "alg_bytes_per_launch": ab, "traffic": None,
-                     "kernel_ms": kms},
+                     "alg_bytes_per_launch": ab, "traffic": traffic,
+                     "traffic_source": "ncu dram bytes of one launch, same kernel and workload" if traffic else None,
+                     "kernel_ms": kms, "launches_per_step": per_step, "list_entries": entries},
         "step_alg_bytes_per_particle": bytes_step,
         "step_roofline_frac": bytes_step * total_ps / (ms_max / 1e3) / 1e9 / hbm,
         "solver": {k: st[k] for k in ("iterations_v", "iterations", "cg_iterations", "avg_density_err",
@@ -432,13 +449,14 @@ def run_ours(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=200, help="timed steps (200 keep nvidia-smi sampling the clocks during the timed region)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--workload", default="roofline_2m")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--requests", type=int, default=512)
+    ap.add_argument("--request-steps", type=int, default=100, help="steps of each served request")
     ap.add_argument("--rate", type=float, default=200.0, help="Poisson arrival rate of the served workload (1/s)")
     ap.add_argument("--capacity", type=int, default=4_000_000, help="resident particles of the server")
     ap.add_argument("--max-scenes", type=int, default=256)

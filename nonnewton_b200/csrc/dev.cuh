@@ -4,8 +4,8 @@
 
 // Sorted working set: particles in cell order ("slots").
 struct WorkSet {
-  float4* pos;      // x, y, z, volume
-  float4* vel;      // v (w unused)
+  float4* pos;      // x, y, z, volume (negative for solids)
+  float4* vel;      // v, w = mass (a copy of `mass`, so neighbour loops get it with v)
   float* mass;
   float* dens;
   uint32_t* flags;  // class bits | scene << NN_SCENE_SHIFT
@@ -51,7 +51,7 @@ struct Dev {
   float* mu;
   // implicit viscosity CG (slot order)
   float4* cg_x; float4* cg_r; float4* cg_z; float4* cg_p; float4* cg_Ap; float4* cg_b;
-  float4* cg_aux;              // mu_i, m_i / rho_i
+  float2* cg_aux;              // fluid: mu_i, m_i / rho_i; solid: 0, 1 if dynamic
   float* cg_pinv;              // [6][cap] symmetric inverse of the diagonal block
   // elasticity (e-space: elastic particles in id order)
   int32_t* el_id;              // [Ne] particle id

@@ -39,6 +39,12 @@ cudaError_t dalloc(T** p, size_t count) {
 
 }  // namespace
 
+// Default launch shape of the neighbour passes: the autotuner's pick for the
+// 2.4M-particle dam break on B200 (128 threads, 2 neighbour chains per thread was
+// the fastest of block {128, 256, 512} x chains {2, 4, 8} x cell factor {1, 2}).
+#define NN_DEFAULT_BLOCK 128
+#define NN_DEFAULT_UNROLL 2
+
 struct nn_ctx {
   int cap = 0, max_scenes = 0, max_nb = 0;
   int64_t max_cells = 0;
@@ -48,8 +54,8 @@ struct nn_ctx {
   cudaStream_t own = nullptr;         // execution stream when the caller sets none
   std::string err;
   int64_t launches = 0;
-  int block = 256;
-  int unroll = 4;                      // neighbour chains in flight per thread (2, 4, 8)
+  int block = NN_DEFAULT_BLOCK;
+  int unroll = NN_DEFAULT_UNROLL;      // neighbour chains in flight per thread (2, 4, 8)
   int cell_factor = 1;                 // cells of edge h / cell_factor
   // state binding and scenes
   nn_state state{};
@@ -58,6 +64,7 @@ struct nn_ctx {
   std::vector<SceneDev> sdev;
   int n = 0, ncells = 0, ne = 0;
   bool any_fluid = false, any_div = false, any_nonnewton = false, any_implicit = false, any_cfl = false;
+  int forces_feat = 0;                 // FF_* terms of the force pass any scene needs
   int el_mult_max = 0;
   // device buffers
   WorkSet set[2]{};
@@ -74,8 +81,8 @@ struct nn_ctx {
   int32_t* slot_of_id = nullptr;
   uint32_t *key = nullptr, *rank = nullptr, *cell_count = nullptr, *tile_sums = nullptr;
   int32_t *src = nullptr, *nbr = nullptr, *nbr_cnt = nullptr;
-  float4 *cg_x = nullptr, *cg_r = nullptr, *cg_z = nullptr, *cg_p = nullptr, *cg_Ap = nullptr, *cg_b = nullptr,
-         *cg_aux = nullptr;
+  float4 *cg_x = nullptr, *cg_r = nullptr, *cg_z = nullptr, *cg_p = nullptr, *cg_Ap = nullptr, *cg_b = nullptr;
+  float2* cg_aux = nullptr;
   float* cg_pinv = nullptr;
   int el_cap = 64, el_stride = 0;
   int32_t *el_id = nullptr, *el_slot = nullptr, *e_of_id = nullptr, *el_nb = nullptr, *el_cnt = nullptr;
@@ -103,7 +110,8 @@ struct nn_ctx {
 static uint64_t feature_sig(const nn_ctx* c) {
   return (uint64_t)c->any_fluid | ((uint64_t)c->any_div << 1) | ((uint64_t)c->any_nonnewton << 2) |
          ((uint64_t)c->any_implicit << 3) | ((uint64_t)std::min(c->el_mult_max, 255) << 8) |
-         ((uint64_t)(c->ne > 0) << 16) | ((uint64_t)c->block << 20);
+         ((uint64_t)(c->ne > 0) << 16) | ((uint64_t)c->block << 20) |
+         ((uint64_t)c->forces_feat << 40);
 }
 
 static thread_local char g_err[512];
@@ -208,6 +216,18 @@ static int launch1(nn_ctx* c, cudaStream_t s, void (*k)(KArgs...), Args... args)
 // The instantiation of a neighbour kernel for the context's neighbour-batch depth.
 #define KU(k) (c->unroll == 8 ? &k<8> : c->unroll == 2 ? &k<2> : &k<4>)
 #define KU2(k, B) (c->unroll == 8 ? &k<8, B> : c->unroll == 2 ? &k<2, B> : &k<4, B>)
+
+// The force pass instance for the batch's terms (c->forces_feat) and batch depth.
+template <int U, int... F>
+static void (*forces_pick(int feat, std::integer_sequence<int, F...>))(Dev, int) {
+  static void (*const tbl[])(Dev, int) = {&k_forces<U, F>...};
+  return tbl[feat];
+}
+static void (*forces_kernel(const nn_ctx* c))(Dev, int) {
+  using All = std::make_integer_sequence<int, 16>;
+  const int f = c->forces_feat & 15;
+  return c->unroll == 8 ? forces_pick<8>(f, All{}) : c->unroll == 2 ? forces_pick<2>(f, All{}) : forces_pick<4>(f, All{});
+}
 
 #define RC(x)                 \
   do {                        \
@@ -346,7 +366,7 @@ static int enq_pressure(nn_ctx* c, cudaStream_t s, int init_mode) {
 static int enq_nonpressure(nn_ctx* c, cudaStream_t s, int advect, int clear) {
   Dev d = make_dev(c, c->cur);
   const int B = c->block;
-  RC(launch(c, s, KU(k_forces), B, c->n, d, clear));
+  RC(launch(c, s, forces_kernel(c), B, c->n, d, clear));
   if (c->any_implicit) {
     RC(launch(c, s, KU(k_cg_setup), B, c->n, d));
     RC(solver_loop(c, s, true, [&](cudaStream_t q) { return launch1(c, q, k_cg_check0, make_dev(c, c->cur)); },
@@ -670,7 +690,7 @@ int nn_ctx_set_stream(nn_ctx* c, void* stream) {
 
 int nn_set_block_size(nn_ctx* c, int32_t threads) {
   if (!c) return fail(nullptr, NN_ERR_INVALID_ARG, "null context");
-  if (threads == 0) threads = 256;
+  if (threads == 0) threads = NN_DEFAULT_BLOCK;
   if (threads < 32 || threads > 1024 || (threads % 32)) return fail(c, NN_ERR_INVALID_ARG, "block size %d", threads);
   if (threads != c->block) drop_graphs(c);
   c->block = threads;
@@ -680,8 +700,8 @@ int nn_set_block_size(nn_ctx* c, int32_t threads) {
 
 int nn_set_tuning(nn_ctx* c, int32_t block, int32_t unroll, int32_t cell_factor) {
   if (!c) return fail(nullptr, NN_ERR_INVALID_ARG, "null context");
-  if (block == 0) block = 256;
-  if (unroll == 0) unroll = 4;
+  if (block == 0) block = NN_DEFAULT_BLOCK;
+  if (unroll == 0) unroll = NN_DEFAULT_UNROLL;
   if (cell_factor == 0) cell_factor = 1;
   if (block < 32 || block > 1024 || (block % 32) || (unroll != 2 && unroll != 4 && unroll != 8) ||
       (cell_factor != 1 && cell_factor != 2))
@@ -763,6 +783,7 @@ int nn_set_scenes(nn_ctx* c, int32_t nscenes, const nn_scene_desc* scenes) {
   std::vector<RB> rb_list;
   int64_t cells = 0;
   c->any_fluid = c->any_div = c->any_nonnewton = c->any_implicit = c->any_cfl = false;
+  c->forces_feat = 0;
   c->el_mult_max = 0;
   for (int k = 0; k < nscenes; ++k) {
     const nn_scene_desc& sd = scenes[k];
@@ -802,6 +823,13 @@ int nn_set_scenes(nn_ctx* c, int32_t nscenes, const nn_scene_desc* scenes) {
     c->any_implicit |= sd.n_fluid > 0 && (sd.params.flags & NN_F_IMPLICIT_VISCOSITY) && !q;
     c->any_cfl |= (sd.params.flags & NN_F_CFL) != 0;
     c->el_mult_max = std::max(c->el_mult_max, el_mult);
+    if (sd.n_fluid > 0) {  // terms the force pass must compile in (the union over scenes)
+      const bool implicit = (sd.params.flags & NN_F_IMPLICIT_VISCOSITY) && !q;
+      if (sd.params.flags & NN_F_SURFACE_TENSION) c->forces_feat |= FF_ST;
+      if ((sd.params.flags & NN_F_VISCOSITY) && !implicit) c->forces_feat |= FF_VI;
+      if (sd.params.flags & NN_F_NONNEWTON) c->forces_feat |= FF_SR;
+      if (q) c->forces_feat |= FF_Q;
+    }
   }
   if (cells >= (int64_t)0x7fffffff) return fail(c, NN_ERR_CAPACITY, "%lld grid cells exceed the 32-bit key space", (long long)cells);
   if (cells > c->max_cells) drop_graphs(c);  // the scan grids were sized for the old table
@@ -995,7 +1023,7 @@ int nn_time_kernel(nn_ctx* c, int32_t kernel, int32_t reps, float* ms_out) {
       case NN_K_DENSITY_FACTOR: return launch(c, s, KU2(k_density_factor, false), B, c->n, d, 1, 1);
       case NN_K_BUILD_LISTS: return launch(c, s, k_build_lists, NS_WARPS * 32, c->n, d);
       case NN_K_CG_MATVEC: return launch(c, s, KU(k_cg_matvec), B, c->n, d);
-      default: return launch(c, s, KU(k_forces), B, c->n, d, 0);
+      default: return launch(c, s, forces_kernel(c), B, c->n, d, 0);
     }
   };
   RC(one());  // warm-up

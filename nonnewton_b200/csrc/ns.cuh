@@ -212,8 +212,8 @@ __global__ void k_gather(Dev d) {
         const float vol = d.t.volume[id];
         p = make_float4(X[3 * id], X[3 * id + 1], X[3 * id + 2],
                         d.t.material[id] == NN_SOLID ? -vol : vol);  // signed volume: solid < 0
-        v = make_float4(d.t.v[3 * id], d.t.v[3 * id + 1], d.t.v[3 * id + 2], 0.f);
         m = d.t.m[id];
+        v = make_float4(d.t.v[3 * id], d.t.v[3 * id + 1], d.t.v[3 * id + 2], m);  // vel.w carries the mass
         rho = d.t.density[id];
         fl = class_bits(d.t.material[id], d.t.is_dynamic[id], d.t.phase_id[id], d.sc[sc]) |
              ((uint32_t)sc << NN_SCENE_SHIFT);
@@ -301,19 +301,28 @@ __global__ void __launch_bounds__(NS_WARPS * 32) k_build_lists(Dev d) {
             for (uint32_t t = lane; t < c1 - c0; t += 32) stage[t] = __ldg(&d.w.pos[c0 + t]);
             __syncwarp();
             const uint32_t lo = max(b, c0), hi = min(e, c1);
-            uint32_t j = lo;
-            for (; j + 4 <= hi; j += 4) {  // four independent tests, appended in order
-              const float r0 = exact_r2(xi - f3(stage[j - c0]));
-              const float r1 = exact_r2(xi - f3(stage[j + 1 - c0]));
-              const float r2 = exact_r2(xi - f3(stage[j + 2 - c0]));
-              const float r3 = exact_r2(xi - f3(stage[j + 3 - c0]));
-              if (r0 < thr && (int)j != i) append((int)j);
-              if (r1 < thr && (int)j + 1 != i) append((int)j + 1);
-              if (r2 < thr && (int)j + 2 != i) append((int)j + 2);
-              if (r3 < thr && (int)j + 3 != i) append((int)j + 3);
+            // tests first, into a hit mask per group of 32 candidates (no stores in the
+            // test loop, where every store site would run whenever any lane hits), then
+            // the hits appended in ascending slot order
+            for (uint32_t g0 = lo; g0 < hi; g0 += 32) {
+              const uint32_t len = min(32u, hi - g0);
+              const float4* st = stage + (g0 - c0);
+              uint32_t m = 0u, k = 0u;
+              for (; k + 4 <= len; k += 4) {  // four independent tests
+                const uint32_t h0 = exact_r2(xi - f3(st[k])) < thr;
+                const uint32_t h1 = exact_r2(xi - f3(st[k + 1])) < thr;
+                const uint32_t h2 = exact_r2(xi - f3(st[k + 2])) < thr;
+                const uint32_t h3 = exact_r2(xi - f3(st[k + 3])) < thr;
+                m |= (h0 | (h1 << 1) | (h2 << 2) | (h3 << 3)) << k;
+              }
+              for (; k < len; ++k) m |= (uint32_t)(exact_r2(xi - f3(st[k])) < thr) << k;
+              const uint32_t self = (uint32_t)i - g0;
+              if (self < len) m &= ~(1u << self);
+              while (m) {
+                append((int)(g0 + __ffs(m) - 1));
+                m &= m - 1u;
+              }
             }
-            for (; j < hi; ++j)
-              if (exact_r2(xi - f3(stage[j - c0])) < thr && (int)j != i) append((int)j);
             __syncwarp();
           }
         }

@@ -446,8 +446,14 @@ __device__ __forceinline__ float nn_law(float g, const SceneDev& s) {
 // the boundary-viscosity reaction from their fluid neighbours (the reference scatters
 // it, 1459-1460). The velocity update of non_pressure_advect cannot join this pass:
 // the viscosity reads the neighbours' velocities.
-struct GF { float4 p, v; float m, rho; int id; };
-template <int U>
+struct GF { float4 p, v; float rho; int id; };  // v.w = mass
+// Terms compiled into an instance of the force pass (the host picks the instance
+// that covers every scene of the batch; the scene flags still gate each term).
+#define FF_ST 1  // surface tension
+#define FF_VI 2  // explicit viscosity (fluid and boundary) and its reaction on dynamic solids
+#define FF_SR 4  // strain rate and viscosity law
+#define FF_Q 8   // reference quirk mode
+template <int U, int FF>
 __global__ void k_forces(Dev d, int clear) {
   const int n = d.d_n[0];
   GRID_STRIDE(i, n) {
@@ -457,11 +463,12 @@ __global__ void k_forces(Dev d, int clear) {
     const SceneDev& s = d.sc[scn];
     if (s.n_fluid == 0) continue;  // the reference runs the substep only with fluid
     const bool implicit = scene_implicit(s);
-    const bool quirks = (s.flags & NN_F_QUIRKS) != 0;
-    const bool st_on = fluid && (s.flags & NN_F_SURFACE_TENSION);
-    const bool vi_on = fluid && !implicit && (s.flags & NN_F_VISCOSITY);
-    const bool vb_on = cls_dyn_solid(fl) && !implicit && (s.flags & NN_F_VISCOSITY) && s.visc_b != 0.f;
-    const bool nn_on = (s.flags & NN_F_NONNEWTON) != 0;
+    const bool quirks = (FF & FF_Q) && (s.flags & NN_F_QUIRKS);
+    const bool st_on = (FF & FF_ST) && fluid && (s.flags & NN_F_SURFACE_TENSION);
+    const bool vi_on = (FF & FF_VI) && fluid && !implicit && (s.flags & NN_F_VISCOSITY);
+    const bool vb_on =
+        (FF & FF_VI) && cls_dyn_solid(fl) && !implicit && (s.flags & NN_F_VISCOSITY) && s.visc_b != 0.f;
+    const bool nn_on = (FF & FF_SR) && (s.flags & NN_F_NONNEWTON);
     const bool sr_on = nn_on && (fluid || quirks);
     const float4 pi = d.w.pos[i];
     const float3 xi = f3(pi);
@@ -476,10 +483,11 @@ __global__ void k_forces(Dev d, int clear) {
       const float mi = d.w.mass[i];
       const float rho_i = d.w.dens[i];
       const float Vi = fabsf(pi.w);
+      const bool need_rho = vi_on || vb_on;  // density and id only where a term reads them
       nb_batches<U>(d.nbr + i, d.cap, d.nbr_cnt[i], i,
                     [&](int j) {
-                      return GF{__ldg(&d.w.pos[j]), __ldg(&d.w.vel[j]), __ldg(&d.w.mass[j]), __ldg(&d.w.dens[j]),
-                                __ldg(&d.w.id[j])};
+                      return GF{__ldg(&d.w.pos[j]), __ldg(&d.w.vel[j]), need_rho ? __ldg(&d.w.dens[j]) : 1.f,
+                                quirks ? __ldg(&d.w.id[j]) : 0};
                     },
                     [&](int, const GF& g) {
                       const float3 r = xi - f3(g.p);
@@ -488,10 +496,11 @@ __global__ void k_forces(Dev d, int clear) {
                       float3 gw;
                       kwg_r2(r, r2, s, w, gw);
                       const bool jf = w_fluid(g.p.w);
-                      if (jf && st_on) st -= (r * (s.sigma / mi * g.m)) * (r2 > s.dia2 ? w : s.w_dia);
+                      const float mj = g.v.w;
+                      if (jf && st_on) st -= (r * (s.sigma / mi * mj)) * (r2 > s.dia2 ? w : s.w_dia);
                       if (vi_on) {
                         const float v_xy = dot3(vi - f3(g.v), r);
-                        if (jf) vs += gw * (10.f * s.visc * (g.m / g.rho) * v_xy / (r2 + s.c01h2));
+                        if (jf) vs += gw * (10.f * s.visc * (mj / g.rho) * v_xy / (r2 + s.c01h2));
                         else if (s.visc_b != 0.f)
                           vs += gw * (10.f * s.visc_b * (s.rho0 * fabsf(g.p.w) / rho_i) * v_xy / (r2 + s.c01h2));
                       }
@@ -502,9 +511,9 @@ __global__ void k_forces(Dev d, int clear) {
                       }
                       if (sr_on) {
                         const float3 vji = f3(g.v) - vi;
-                        const float t[6] = {(vji.x * gw.x + vji.x * gw.x) * g.m, (vji.y * gw.y + vji.y * gw.y) * g.m,
-                                            (vji.z * gw.z + vji.z * gw.z) * g.m, (vji.x * gw.y + vji.y * gw.x) * g.m,
-                                            (vji.x * gw.z + vji.z * gw.x) * g.m, (vji.y * gw.z + vji.z * gw.y) * g.m};
+                        const float t[6] = {(vji.x * gw.x + vji.x * gw.x) * mj, (vji.y * gw.y + vji.y * gw.y) * mj,
+                                            (vji.z * gw.z + vji.z * gw.z) * mj, (vji.x * gw.y + vji.y * gw.x) * mj,
+                                            (vji.x * gw.z + vji.z * gw.x) * mj, (vji.y * gw.z + vji.z * gw.y) * mj};
                         const bool take = g.id > last_id;
                         if (quirks && take) last_id = g.id;
 #pragma unroll
@@ -538,7 +547,10 @@ __global__ void k_forces(Dev d, int clear) {
       d.srn[i] = g;
       d.mu[i] = mu;
     }
-    if (implicit && fluid) d.cg_aux[i] = make_float4(mu, d.w.mass[i] / d.w.dens[i], 0.f, 0.f);
+    // CG coefficients: (mu, m / rho) of a fluid slot; (0, 1) marks a dynamic solid
+    if (implicit)
+      d.cg_aux[i] = fluid ? make_float2(mu, d.w.mass[i] / d.w.dens[i])
+                          : make_float2(0.f, cls_dyn_solid(fl) ? 1.f : 0.f);
   }
 }
 
@@ -558,12 +570,12 @@ __device__ __forceinline__ bool cg_row(const Dev& d, int i, uint32_t fl) {
 
 // A p for one row; in the setup also the diagonal block D and the right-hand-side
 // correction of moving boundaries (SETUP: `vec` is the velocity field).
-struct GCG { float4 p, x, a; uint32_t fl; };
+struct GCG { float4 p, x; float2 a; };
 template <int U, bool SETUP>
 __device__ __forceinline__ float3 cg_apply(const Dev& d, int i, const float4* __restrict__ vec, float3 vi,
                                            const SceneDev& s, float dt, float* D, float3* bcorr) {
   const float3 xi = f3(d.w.pos[i]);
-  const float4 ai = d.cg_aux[i];
+  const float2 ai = d.cg_aux[i];
   const float mi = d.w.mass[i];
   const float rho_i = d.w.dens[i];
   float3 acc = vi * mi;
@@ -575,7 +587,6 @@ __device__ __forceinline__ float3 cg_apply(const Dev& d, int i, const float4* __
                g.p = __ldg(&d.w.pos[j]);
                g.x = __ldg(&vec[j]);
                g.a = __ldg(&d.cg_aux[j]);
-               g.fl = SETUP ? __ldg(&d.w.flags[j]) : 0u;
                return g;
              },
              [&](int, const GCG& g) {
@@ -591,7 +602,7 @@ __device__ __forceinline__ float3 cg_apply(const Dev& d, int i, const float4* __
                } else {
                  c = cb * fabsf(g.p.w);
                  diff = vi;
-                 if (SETUP && cls_dyn_solid(g.fl)) *bcorr -= gw * (c * dot3(r, f3(g.x)) * w);
+                 if (SETUP && g.a.y > 0.f) *bcorr -= gw * (c * dot3(r, f3(g.x)) * w);  // dynamic solid
                }
                acc -= gw * (c * dot3(r, diff) * w);
                if (SETUP) {
@@ -1063,12 +1074,14 @@ __global__ void k_sync_in(Dev d, uint32_t mask) {
     if (mask & 1u) { p.x = d.t.x[3 * id]; p.y = d.t.x[3 * id + 1]; p.z = d.t.x[3 * id + 2]; }
     if (mask & 8u) p.w = cls_solid(d.w.flags[i]) ? -d.t.volume[id] : d.t.volume[id];
     d.w.pos[i] = p;
-    if (mask & 2u) d.w.vel[i] = make_float4(d.t.v[3 * id], d.t.v[3 * id + 1], d.t.v[3 * id + 2], 0.f);
+    float m = d.w.mass[i];  // vel.w carries the mass
+    if (mask & 256u) { m = d.t.m[id]; d.w.mass[i] = m; }
+    if (mask & 2u) d.w.vel[i] = make_float4(d.t.v[3 * id], d.t.v[3 * id + 1], d.t.v[3 * id + 2], m);
+    else if (mask & 256u) d.w.vel[i].w = m;
     if (mask & 4u) d.acc4[i] = make_float4(d.t.a[3 * id], d.t.a[3 * id + 1], d.t.a[3 * id + 2], 0.f);
     if (mask & 16u) d.w.dens[i] = d.t.density[id];
     if (mask & 32u) d.alpha[i] = d.t.dfsph_factor[id];
     if (mask & 64u) d.rho_adv[i] = d.t.density_adv[id];
-    if (mask & 256u) d.w.mass[i] = d.t.m[id];
   }
 }
 
