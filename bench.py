@@ -191,23 +191,54 @@ def cpu_baseline(scenes, budget_s=20.0, threads=None):
 
 
 def run_reference(args):
-    world, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    """The reference arm: the oracle (FP32 restatement of the reference step, the
+    reference's own Taichi code being unavailable) on all host cores, on the same
+    workload. Each timed step is one full SPH step of the scene; the run stops after K
+    steps or when --cpu-budget seconds of timed steps are used up, whichever comes
+    first (the line states how many ran), so that it ends within a few minutes."""
+    rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    scenes = make_workload(args.workload)
-    budget = max(3.0, 60.0 / max(args.steps + args.warmup, 1))
-    vals = []
-    cb = None
-    for _ in range(args.warmup):
-        cpu_baseline(scenes, budget_s=budget / 4)
-    for _ in range(args.steps):
-        cb = cpu_baseline(scenes, budget_s=budget)
-        vals.append(cb["value"])
-    v = statistics.median(vals) if vals else 0.0
-    cb["value"] = v
+    from oracle import oracle as O
+
+    if args.workload == "served":
+        # the reference has no batching: its form of the served workload is the plain
+        # per-request loop, over the requests in arrival order
+        from nonnewton_b200 import scene as S
+
+        work = S.mixed_workload(n_requests=args.requests, seed=1000, rate=args.rate, steps=args.request_steps)
+        scenes, name = [sc for _, sc in work], "served_mixed"
+    else:
+        scenes = make_workload(args.workload)
+        name = scenes[0].name
+    O.build()
+    O.set_threads(os.cpu_count())
+    times, psteps = [], 0
+    t_all = time.perf_counter()
+    for sc in scenes:
+        o = O.OracleSim(sc.particles, sc.param, "f32")
+        o.initialize()
+        for _ in range(min(args.warmup, 1)):
+            o.step(1)
+        for _ in range(args.request_steps if args.workload == "served" else args.steps):
+            if len(times) >= args.steps or time.perf_counter() - t_all >= args.cpu_budget:
+                break
+            t0 = time.perf_counter()
+            o.step(1)
+            times.append(time.perf_counter() - t0)
+            psteps += sc.particles.n
+        if len(times) >= args.steps or time.perf_counter() - t_all >= args.cpu_budget:
+            break
+    v = psteps / sum(times)
+    n = scenes[0].particles.n
+    cb = {"value": v, "unit": "particle-steps/s", "cores": O.get_threads(), "kind": "port",
+          "sample": f"{len(times)} of {args.steps} requested steps of {name} ({psteps} particle-steps), one full "
+                    f"SPH step each, FP32 oracle, OpenMP {O.get_threads()} threads"}
     print(json.dumps({"impl": "reference", "metric": "particle-steps/s", "value": v, "unit": "particle-steps/s",
-                      "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
-                      "dtype": "f32", "data": "synthetic", "config": {"workload": args.workload},
+                      "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "samples": len(times),
+                      "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
+                      "dtype": "f32", "data": "synthetic (seeded numpy scene generator)",
+                      "config": {"workload": name, "particles": n, "fluid": scenes[0].particles.n_fluid},
                       "cpu_baseline": cb,
                       "e2e": {"value": v, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
                               "d2h_bytes_per_step": 0}}))
