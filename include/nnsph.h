@@ -284,6 +284,68 @@ int nn_set_block_size(nn_ctx* ctx, int32_t threads);
    cell factor takes effect at the next nn_set_scenes, which must follow. */
 int nn_set_tuning(nn_ctx* ctx, int32_t block, int32_t unroll, int32_t cell_factor);
 
+/* ---- Surface reconstruction (SPH/surf_recon/srtool.py, SRTool) ------------------
+   The particle-to-mesh step after the simulation: fluid field on a vertex grid (an
+   isotropic poly6 splat and the anisotropic Yu-Turk splat), one value-weighted
+   Gaussian smoothing pass, dual contouring (one vertex per crossing cube from a
+   clamped QEF around the mass point, two triangles per crossing edge), optional
+   per-vertex normals. Replaces SRTool.dual_contouring (srtool.py:1264-1304) and
+   export_mesh's data (1802-1838); the Python mirror is nonnewton_b200/surface.py.
+
+   Vertex (x, y, z) of the grid lies at origin + (x, y, z) * voxel_size; linear index
+   x + dims[0] * (y + dims[1] * z). Taichi's sparse fields are emulated: a block of
+   NN_SR_BLOCK^3 vertices is active once any of its vertices is written, and the
+   smoothing and contouring passes visit every vertex of the active blocks (what a
+   struct-for over the reference's pointer/dense hierarchy visits). */
+#define NN_SR_BLOCK 32
+typedef struct nn_sr_params {
+  int32_t size;                 /* sizeof(nn_sr_params) */
+  int32_t dims[3];              /* vertices per axis */
+  double origin[3];             /* bounding_box_extent[0] */
+  double voxel_size;            /* SRTool(voxel_size) */
+  double particle_radius;       /* SRTool(particle_radius): splat volume 4/3 pi r^3 */
+  double smooth_radius;         /* dual_contouring(smooth_radius) */
+  double isolevel;              /* dual_contouring(isolevel) */
+  int32_t use_smooth_field;     /* dual_contouring(use_smooth_fluid_field) */
+  int32_t smooth_iterations;    /* smooth_sdf(iteration), 1 in the reference */
+  int32_t smooth_cells;         /* smooth_sdf(radius), 1 in the reference */
+  int32_t record_normals;       /* SRTool(record_normals) */
+} nn_sr_params;
+
+typedef struct nn_sr_ctx nn_sr_ctx;
+
+/* Capacities: particles, vertex grid cells, mesh vertices and triangle indices
+   (SRTool(max_num_particles, max_num_vertices, max_num_indices)). */
+int nn_sr_create(int32_t max_particles, int64_t max_cells, int32_t max_vertices, int32_t max_indices,
+                 nn_sr_ctx** out);
+int nn_sr_destroy(nn_sr_ctx* ctx);
+const char* nn_sr_last_error(const nn_sr_ctx* ctx);
+
+/* SRTool.dual_contouring for `n` particles at device positions pos [n,3] f32, enqueued
+   on `cuda_stream`; the mesh stays in the context. NN_ERR_CAPACITY when the grid,
+   the mesh or a voxel's particle list (NN_SR_MAX_PER_VOXEL, the reference's 64) is
+   too small; NN_ERR_INVALID_ARG for particles outside the grid. Synchronises the
+   stream once (to read the mesh sizes). */
+#define NN_SR_MAX_PER_VOXEL 64
+int nn_sr_dual_contouring(nn_sr_ctx* ctx, const nn_sr_params* params, const float* pos, int32_t n,
+                          void* cuda_stream);
+
+/* The mesh of the last call: counts, and copies into caller device buffers when
+   non-NULL: vertices [num_vertices,3] f32, indices [num_indices] i32 (triangles),
+   normals [num_vertices,3] f32 (when record_normals was set). Vertices are numbered
+   by the linear index of their cube, triangles ordered by cube and then by edge
+   (x, y, z edges of the cube's first corner). */
+int nn_sr_get_mesh(nn_sr_ctx* ctx, int32_t* num_vertices, int32_t* num_indices, float* vertices,
+                   int32_t* indices, float* normals, void* cuda_stream);
+
+/* Stage outputs for parity checks (device buffers, each optional): the field [cells]
+   f32, the active-block flags [blocks] u8 (blocks of NN_SR_BLOCK^3 in x-fastest
+   order), the anisotropic kernels G [n,9] and centres x_bar [n,3] f32, and the
+   smoothing's standard deviation (host double). `stage` 0 = after the splats,
+   1 = after smoothing (the field the contouring reads). */
+int nn_sr_get_stage(nn_sr_ctx* ctx, int32_t stage, float* field, uint8_t* active_blocks, float* G, float* xbar,
+                    double* sd, void* cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -173,3 +173,41 @@ def make_params(**kw) -> nn_scene_params:
         else:
             setattr(p, k, v)
     return p
+
+
+NN_SR_BLOCK = 32
+NN_SR_MAX_PER_VOXEL = 64
+
+
+class nn_sr_params(C.Structure):
+    """Mirror of nn_sr_params (surface reconstruction)."""
+    _fields_ = [
+        ("size", C.c_int32),
+        ("dims", C.c_int32 * 3),
+        ("origin", C.c_double * 3),
+        ("voxel_size", C.c_double),
+        ("particle_radius", C.c_double),
+        ("smooth_radius", C.c_double),
+        ("isolevel", C.c_double),
+        ("use_smooth_field", C.c_int32),
+        ("smooth_iterations", C.c_int32),
+        ("smooth_cells", C.c_int32),
+        ("record_normals", C.c_int32),
+    ]
+
+
+def make_sr_params(dims, origin, voxel_size, particle_radius, smooth_radius, isolevel, use_smooth_field=True,
+                   smooth_iterations=1, smooth_cells=1, record_normals=False) -> nn_sr_params:
+    p = nn_sr_params()
+    p.size = C.sizeof(nn_sr_params)
+    p.dims[:] = [int(t) for t in dims]
+    p.origin[:] = [float(t) for t in origin]
+    p.voxel_size = float(voxel_size)
+    p.particle_radius = float(particle_radius)
+    p.smooth_radius = float(smooth_radius)
+    p.isolevel = float(isolevel)
+    p.use_smooth_field = int(bool(use_smooth_field))
+    p.smooth_iterations = int(smooth_iterations)
+    p.smooth_cells = int(smooth_cells)
+    p.record_normals = int(bool(record_normals))
+    return p

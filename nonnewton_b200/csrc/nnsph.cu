@@ -1240,3 +1240,6 @@ extern "C" int nn_neighbors_noalloc(const float* x, int32_t n, const double* dom
   if (e != cudaSuccess) return fail(c, NN_ERR_CUDA, "nn_neighbors_noalloc: %s", cudaGetErrorString(e));
   return NN_OK;
 }
+
+// Surface reconstruction (SRTool): kernels and its C ABI.
+#include "surf.cuh"

@@ -49,6 +49,8 @@ int main(void) {
   printf("%zu %zu %zu %zu\n", sizeof(nn_scene_params), sizeof(nn_scene_desc), sizeof(nn_state), sizeof(nn_stats));
   printf("%zu %zu %zu %zu\n", offsetof(nn_scene_params, max_iterations_v), offsetof(nn_scene_params, cfl_max_dt),
          offsetof(nn_state, rotations), offsetof(nn_stats, steps));
+  printf("%zu %zu %zu\n", sizeof(nn_sr_params), offsetof(nn_sr_params, isolevel),
+         offsetof(nn_sr_params, record_normals));
   return 0;
 }'''
     with tempfile.TemporaryDirectory() as d:
@@ -58,7 +60,9 @@ int main(void) {
         subprocess.run(["gcc", "-I", os.path.dirname(HEADER), src, "-o", exe], check=True)
         out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()
     sizes = list(map(int, out[:4]))
-    offs = list(map(int, out[4:]))
+    offs = list(map(int, out[4:8]))
+    assert list(map(int, out[8:])) == [C.sizeof(_abi.nn_sr_params), _abi.nn_sr_params.isolevel.offset,
+                                       _abi.nn_sr_params.record_normals.offset]
     assert sizes == [C.sizeof(_abi.nn_scene_params), C.sizeof(_abi.nn_scene_desc), C.sizeof(_abi.nn_state),
                      C.sizeof(_abi.nn_stats)]
     assert offs == [_abi.nn_scene_params.max_iterations_v.offset, _abi.nn_scene_params.cfl_max_dt.offset,
@@ -80,6 +84,10 @@ def test_invalid_arguments_are_rejected_without_a_context(lib):
     hi = (C.c_double * 3)(1, 1, 1)
     assert lib.nn_neighbors_noalloc(None, C.c_int32(10), lo, hi, C.c_double(0.04), C.c_int32(8), None, None,
                                     None) == _abi.NN_ERR_INVALID_ARG
+    lib.nn_sr_create.argtypes = [C.c_int32, C.c_int64, C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]
+    lib.nn_sr_create.restype = C.c_int
+    assert lib.nn_sr_create(0, 1000, 10, 10, C.byref(h)) == _abi.NN_ERR_INVALID_ARG
+    assert lib.nn_sr_create(10, 0, 10, 10, C.byref(h)) == _abi.NN_ERR_INVALID_ARG
 
 
 def test_config_parses_reference_scenes():

@@ -1,0 +1,118 @@
+"""CUDA surface reconstruction (nn_sr_*, nonnewton_b200.surface.SRTool) against the CPU
+oracle, stage by stage, on the same inputs:
+
+  - anisotropic kernels G, x_bar: 1e-4 / 1e-6 of each array's scale;
+  - splat field from the CUDA G, x_bar: 1e-5 of the field's scale, identical active blocks;
+  - smoothing of the CUDA splat field: 1e-5 of the field's scale (sd 1e-6 relative);
+  - contouring of the CUDA smoothed field: the same triangles, index for index, and
+    vertices within 1e-6 m;
+and end to end: a closed, consistently wound mesh of the same size."""
+import numpy as np
+import pytest
+import torch
+
+from .surf_cases import ball, block, closed_oriented, default_params
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def surf():
+    from oracle import surf as S
+
+    S.build()
+    return S
+
+
+def _tool(**kw):
+    from nonnewton_b200.surface import SRTool
+
+    kw.setdefault("record_normals", True)
+    return SRTool([[0, 0, 0], [1, 1, 1]], voxel_size=0.01, particle_radius=0.02, max_num_vertices=200000,
+                  max_num_indices=2000000, max_num_particles=100000, **kw)
+
+
+def _scale_err(g, r):
+    g, r = np.asarray(g, np.float64), np.asarray(r, np.float64)
+    return float(np.abs(g - r).max() / max(np.abs(r).max(), 1e-30))
+
+
+@pytest.mark.parametrize("case", ["ball", "block"])
+def test_surface_stages_match_oracle(cuda_lib, surf, case):
+    pos = ball(seed=10) if case == "ball" else block(seed=11)
+    n = len(pos)
+    sr = _tool()
+    sr.dual_contouring(isolevel=0.0, smooth_radius=0.06, num_particles=n, pos=torch.from_numpy(pos).cuda())
+    prm = sr.last_params
+    s0, s1 = sr.stage(0, n), sr.stage(1, n)
+    # anisotropic kernels
+    G, xb = surf.prepass(prm, pos)
+    assert _scale_err(s0["G"].cpu().numpy(), G) < 1e-4
+    assert _scale_err(s0["xbar"].cpu().numpy(), xb) < 1e-6
+    # splats from the CUDA kernels
+    f_or, act_or = surf.splat(prm, pos, s0["G"].cpu().numpy(), s0["xbar"].cpu().numpy())
+    assert np.array_equal(s0["active"].cpu().numpy(), act_or)
+    assert _scale_err(s0["field"].cpu().numpy(), f_or) < 1e-5
+    # smoothing of the CUDA splat field
+    f_sm, sd = surf.smooth(prm, s0["field"].cpu().numpy(), act_or)
+    assert abs(s1["sd"] - sd) <= 1e-6 * abs(sd)
+    assert _scale_err(s1["field"].cpu().numpy(), f_sm) < 1e-5
+    # contouring of the CUDA smoothed field
+    o = surf.contour(prm, s1["field"].cpu().numpy(), act_or)
+    assert sr.num_vertices[None] == len(o["vertices"]) > 0
+    assert sr.num_indices[None] == len(o["indices"])
+    assert np.array_equal(sr.mesh_index.cpu().numpy(), o["indices"])
+    assert np.abs(sr.mesh_vertex.cpu().numpy() - o["vertices"]).max() < 1e-6
+    assert np.abs(sr.mesh_normal.cpu().numpy() - o["normals"]).max() < 1e-4
+
+
+def test_surface_end_to_end_closed_mesh(cuda_lib, surf):
+    pos = ball(seed=12)
+    sr = _tool()
+    sr.dual_contouring(isolevel=0.0, smooth_radius=0.06, num_particles=len(pos), pos=torch.from_numpy(pos).cuda())
+    f = sr.mesh_index.cpu().numpy().reshape(-1, 3)
+    nv = sr.num_vertices[None]
+    assert closed_oriented(f, nv) and len(f) == 2 * nv - 4
+    o = surf.dual_contouring(default_params(), pos)
+    assert abs(nv - len(o["vertices"])) <= max(2, nv // 1000)
+    # the same bits on a second run (fixed-point splats)
+    v1 = sr.mesh_vertex.clone()
+    sr.dual_contouring(isolevel=0.0, smooth_radius=0.06, num_particles=len(pos), pos=torch.from_numpy(pos).cuda())
+    assert torch.equal(v1, sr.mesh_vertex)
+
+
+def test_surface_export_ply(cuda_lib, tmp_path):
+    pos = block(seed=13)
+    sr = _tool()
+    sr.dual_contouring(isolevel=0.0, smooth_radius=0.06, num_particles=len(pos), pos=pos)
+    path = str(tmp_path / "mesh.ply")
+    sr.export_mesh(path, output_normal=True)
+    raw = open(path, "rb").read()
+    head, body = raw.split(b"end_header\n", 1)
+    nv, nf = sr.num_vertices[None], sr.num_indices[None] // 3
+    assert f"element vertex {nv}".encode() in head and f"element face {nf}".encode() in head
+    assert len(body) == nv * 24 + nf * 13
+    v = np.frombuffer(body[: nv * 24], "<f4").reshape(nv, 6)
+    assert np.array_equal(v[:, :3], sr.mesh_vertex.cpu().numpy())
+
+
+def test_surface_errors(cuda_lib):
+    from nonnewton_b200 import _abi
+    from nonnewton_b200.engine import NNError
+    from nonnewton_b200.surface import SRTool
+
+    pos = ball(seed=14)
+    bad = pos.copy()
+    bad[3] = [-0.5, 0.5, 0.5]
+    sr = _tool()
+    with pytest.raises(NNError) as e:
+        sr.dual_contouring(isolevel=0.0, smooth_radius=0.06, num_particles=len(bad), pos=bad)
+    assert e.value.code == _abi.NN_ERR_INVALID_ARG
+    small = SRTool([[0, 0, 0], [1, 1, 1]], voxel_size=0.01, particle_radius=0.02, max_num_vertices=100,
+                   max_num_indices=600, max_num_particles=10000)
+    with pytest.raises(NNError) as e:
+        small.dual_contouring(isolevel=0.0, smooth_radius=0.06, num_particles=len(pos), pos=pos)
+    assert e.value.code == _abi.NN_ERR_CAPACITY
+    # the context stays usable after an error
+    sr.dual_contouring(isolevel=0.0, smooth_radius=0.06, num_particles=len(pos), pos=pos)
+    assert sr.num_vertices[None] > 0

@@ -1,0 +1,74 @@
+"""The CPU oracle of the surface reconstruction (SRTool, SPH/surf_recon/srtool.py)
+on known shapes: closed, consistently oriented meshes around particle balls and an
+analytic sphere, the reference's quirks (particle 0 skipped, no surface without
+negative field values). No GPU."""
+import numpy as np
+import pytest
+
+from .surf_cases import ball, block, closed_oriented, default_params
+
+
+@pytest.fixture(scope="module")
+def surf():
+    from oracle import surf as S
+
+    S.build()
+    return S
+
+
+def test_oracle_ball_is_a_closed_sphere(surf):
+    pos = ball(seed=0)
+    o = surf.dual_contouring(default_params(), pos)
+    v, f = o["vertices"], o["indices"].reshape(-1, 3)
+    assert len(v) > 1000
+    assert closed_oriented(f, len(v))
+    assert len(f) == 2 * len(v) - 4  # Euler characteristic 2
+    r = np.linalg.norm(v - 0.5, axis=1)
+    assert 0.10 < r.min() and r.max() < 0.16
+    assert np.isfinite(o["sd"]) and o["sd"] > 0
+
+
+def test_oracle_block_is_closed(surf):
+    o = surf.dual_contouring(default_params(), block(seed=1))
+    f = o["indices"].reshape(-1, 3)
+    assert len(f) > 0 and closed_oriented(f, len(o["vertices"]))
+
+
+def test_oracle_contour_of_an_analytic_sphere(surf):
+    """Dual contouring of a signed distance field (negative inside): every vertex lies
+    within a voxel of the sphere and the mesh is closed with consistent winding."""
+    prm = default_params(dims=(48, 48, 48))
+    vs = prm.voxel_size
+    idx = np.stack(np.meshgrid(*[np.arange(48)] * 3, indexing="ij"), -1)  # x, y, z
+    c, R = np.array([0.24, 0.23, 0.25]), 0.13
+    sdf = np.linalg.norm(idx * vs - c, axis=-1) - R
+    o = surf.contour(prm, np.transpose(sdf, (2, 1, 0)), np.ones(8, np.uint8))
+    v, f = o["vertices"], o["indices"].reshape(-1, 3)
+    assert closed_oriented(f, len(v))
+    assert np.abs(np.linalg.norm(v - c, axis=1) - R).max() < vs
+
+
+def test_oracle_particle_zero_is_skipped(surf):
+    """pre_process_data starts at particle 1 (srtool.py:1013): G and x_bar of particle 0
+    stay 0, every other particle gets a symmetric positive definite G."""
+    G, xb = surf.prepass(default_params(), ball(seed=2))
+    assert np.all(G[0] == 0) and np.all(xb[0] == 0)
+    M = G[1:].reshape(-1, 3, 3).astype(np.float64)
+    assert np.allclose(M, np.transpose(M, (0, 2, 1)), rtol=1e-5, atol=1e-3)
+    assert np.all(np.linalg.eigvalsh(M) > 0)
+
+
+def test_oracle_isotropic_field_alone_gives_no_surface(surf):
+    """Without the anisotropic splat the field has no negative value, the smoothing's
+    standard deviation is 0/0 and the field turns NaN, so no cube crosses the level,
+    which is what the reference computes (density_field_stats, srtool.py:1436-1456)."""
+    o = surf.dual_contouring(default_params(use_smooth_field=False), ball(seed=3))
+    assert np.isnan(o["sd"])
+    assert len(o["vertices"]) == 0 and len(o["indices"]) == 0
+
+
+def test_oracle_rejects_particles_outside_the_grid(surf):
+    pos = ball(seed=4)
+    pos[5] = [-1.0, 0.5, 0.5]
+    with pytest.raises(RuntimeError):
+        surf.dual_contouring(default_params(), pos)
