@@ -16,6 +16,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -199,6 +200,9 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    if args.workload == "surface":
+        run_reference_surface(args)
+        return
     from oracle import oracle as O
 
     if args.workload == "served":
@@ -334,6 +338,150 @@ def run_served(args, world, rank):
     print(json.dumps(line))
 
 
+def surface_setup(seed=0):
+    """The surface workload: the fluid of the shear-thinning drop (125,000 particles at
+    0.02 m) with the reference example's settings (SPH/surf_recon/example.py: voxel
+    0.01 m, particle radius 0.02 m, smoothing radius 0.06 m, level 0)."""
+    from nonnewton_b200 import scene as S
+
+    sc = S.shear_thinning_drop(seed=seed)
+    nf = sc.particles.n_fluid
+    pos = np.ascontiguousarray(sc.particles.x[:nf], np.float32)
+    p = sc.param
+    return pos, [list(p.domain_start), list(p.domain_end)]
+
+
+def surface_sample(pos):
+    """A bounded CPU sample of the surface workload: a 12 x 12 x 12 corner of the block."""
+    lo = pos.min(0)
+    return pos[np.all(pos < lo + 12 * 0.02 - 1e-3, axis=1)]
+
+
+def surface_params(bbox, record_normals=False):
+    from nonnewton_b200 import _abi
+
+    vs, sr_ = 0.01, 0.06
+    rng = int(math.ceil(4 * sr_ / vs)) + 1
+    dims = [int(math.ceil((bbox[1][k] - bbox[0][k]) / vs)) + (rng - rng // 2 + 1) + 3 for k in range(3)]
+    return _abi.make_sr_params(dims, bbox[0], vs, 0.02, sr_, 0.0, record_normals=record_normals)
+
+
+def run_reference_surface(args):
+    """The reference arm of the surface workload: the C++ oracle of SRTool on a bounded
+    sample of the same block, one reconstruction per step, within --cpu-budget seconds."""
+    from oracle import surf as OS
+
+    pos, bbox = surface_setup()
+    sub = surface_sample(pos)
+    prm = surface_params(bbox)
+    times = []
+    t_all = time.perf_counter()
+    while len(times) < args.steps and time.perf_counter() - t_all < args.cpu_budget:
+        t0 = time.perf_counter()
+        OS.dual_contouring(prm, sub)
+        times.append(time.perf_counter() - t0)
+    v = len(sub) * len(times) / sum(times)
+    cb = {"value": v, "unit": "particles/s", "cores": 1, "kind": "port",
+          "sample": f"{len(times)} of {args.steps} requested reconstructions of {len(sub)} particles (a corner of "
+                    f"the surface_drop block), single-threaded C++ oracle"}
+    print(json.dumps({"impl": "reference", "metric": "particles/s (surface reconstruction)", "value": v,
+                      "unit": "particles/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                      "samples": len(times), "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
+                      "dtype": "f32", "data": "synthetic (seeded numpy scene generator)",
+                      "config": {"workload": "surface_drop", "particles": int(len(sub))}, "cpu_baseline": cb,
+                      "e2e": {"value": v, "unit": "particles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
+# Algorithmic bytes per grid vertex of one reconstruction: each dense per-vertex array
+# written once and read once (fixed-point field 8 + 8, splat copy 4, field 4 + 4,
+# smoothing output 4 + 4, crossing flags 4 + 4, index counts 4 + 4, voxel counts 4 + 4)
+SR_BYTES_PER_CELL = 60
+SR_LAUNCHES = 24  # kernels one SRTool.dual_contouring call launches (three 3-kernel scans included)
+
+
+def run_surface(args, world, rank):
+    """SRTool.dual_contouring on the surface workload; one step is one reconstruction.
+    `value` = particles / s with the positions resident; `e2e` copies the positions in
+    from pinned host memory and the mesh out, each step."""
+    import torch
+
+    from nonnewton_b200.surface import SRTool
+
+    pos, bbox = surface_setup(seed=rank)
+    nf = len(pos)
+    kw = dict(isolevel=0.0, smooth_radius=0.06, num_particles=nf)
+    sr = SRTool(bbox, voxel_size=0.01, particle_radius=0.02, max_num_vertices=4_000_000, max_num_indices=24_000_000,
+                max_num_particles=nf)
+    d_pos = torch.from_numpy(pos).cuda()
+    stream = torch.cuda.current_stream()
+    for _ in range(max(args.warmup, 1)):
+        sr.dual_contouring(pos=d_pos, **kw)
+    torch.cuda.synchronize()
+    barrier(world)
+    times = []
+    clocks_path = os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else "",
+                               f"clocks_rank{rank}.csv")
+    with ClockSampler(clocks_path) as cs:
+        for _ in range(args.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            sr.dual_contouring(pos=d_pos, **kw)
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+    torch.cuda.synchronize()
+    barrier(world)
+    ms = max_over_ranks(sum(times), world)
+    value = sum_over_ranks(float(nf) * args.steps, world) / (ms / 1e3)
+    nv, ni = sr.num_vertices[None], sr.num_indices[None]
+    # end to end: host positions in, mesh out
+    h_pos = torch.from_numpy(pos).pin_memory()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        d_pos.copy_(h_pos, non_blocking=True)
+        sr.dual_contouring(pos=d_pos, **kw)
+        hv = sr.mesh_vertex.to("cpu", non_blocking=True)
+        hi = sr.mesh_index.to("cpu", non_blocking=True)
+    e1.record(stream)
+    e1.synchronize()
+    del hv, hi
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), world)
+    if rank != 0:
+        return
+    dims = list(sr.last_params.dims)
+    cells = dims[0] * dims[1] * dims[2]
+    peaks, peak_kind = load_peaks()
+    ab = cells * SR_BYTES_PER_CELL + nf * (12 + 36 + 12)
+    achieved = ab / (ms / args.steps / 1e3) / 1e9
+    line = {
+        "metric": "particles/s (surface reconstruction)", "value": value, "unit": "particles/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded numpy scene generator)",
+        "config": {"workload": "surface_drop", "particles": nf, "grid": dims, "voxel_size": 0.01,
+                   "smooth_radius": 0.06, "particle_radius": 0.02, "l2": "grid larger than L2",
+                   "mesh": {"vertices": nv, "triangles": ni // 3}},
+        "roofline": {"bound": "hbm", "kernel": "whole call", "achieved": achieved, "peak": peaks["hbm_gbs"],
+                     "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "peak_source": f"{peak_kind} hbm_gbs",
+                     "alg_bytes_per_launch": ab, "traffic": None},
+        "gpu_launches": SR_LAUNCHES * args.steps,
+        "e2e": {"value": nf * args.steps / (e2e_ms / 1e3), "unit": "particles/s", "h2d_bytes_per_step": nf * 12,
+                "d2h_bytes_per_step": nv * 12 + ni * 4},
+        "clocks": cs.summary(),
+    }
+    if not args.no_cpu_baseline:
+        from oracle import surf as OS
+
+        sub = surface_sample(pos)
+        t0 = time.perf_counter()
+        OS.dual_contouring(surface_params(bbox), sub)
+        el = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": len(sub) / el, "unit": "particles/s", "cores": 1, "kind": "port",
+                                "sample": f"{len(sub)} particles (a corner of the same block), one reconstruction, "
+                                          f"single-threaded C++ oracle"}
+    print(json.dumps(line))
+
+
 def run_ours(args):
     import torch
 
@@ -341,6 +489,11 @@ def run_ours(args):
     from nonnewton_b200.config import SimConfig
 
     world, rank, local = dist_setup(args)
+    if args.workload == "surface":
+        run_surface(args, world, rank)
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
     if args.workload == "served":
         run_served(args, world, rank)
         if world > 1:

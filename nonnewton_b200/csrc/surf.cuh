@@ -81,6 +81,7 @@ struct SrDev {
   float* nrm;               // [max_v,3]
   int32_t max_v, max_i;
   float iso, sr, volume, acoeff;
+  float q1_thr, q05_thr;     // largest f32 whose rounded square root is <= 1, <= 0.5
   int range, off, smooth_cells, record_normals;
 };
 
@@ -241,44 +242,40 @@ __global__ void k_sr_aniso_pre(SrDev s) {
     int cx, cy, cz;
     s.g.voxel_of(px, py, pz, cx, cy, cz);
     const float rr = 2.f * s.sr;  // isoweight radius
-    double tw = 0.0, xw[3] = {0.0, 0.0, 0.0};
+    // one pass over the neighbourhood: weights, and the first and second moments of
+    // the offsets d_j = x_j - x_i, from which x_w = x_i + <d> and
+    // C = sum w (x_j - x_w)(x_j - x_w)^T / sum w = <d d^T> - <d><d>^T (srtool.py:1021-1061)
+    double tw = 0.0, m1[3] = {0.0, 0.0, 0.0}, m2[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    int nnb = 0;
     // a margin of one voxel on the pruning distance keeps every pair with w > 0
     sr_range_rows(s, cx, cy, cz, px, py, pz, rr + s.g.vs, [&](int j) {
       const float dn = sr_dist(px, py, pz, s.pos + 3 * j);
       if (dn < rr) {
         const float q = dn / rr;
         const double w = 1.0 - (double)(q * q * q);  // isoweight, srtool.py:993-999
+        const double d[3] = {(double)s.pos[3 * j] - px, (double)s.pos[3 * j + 1] - py, (double)s.pos[3 * j + 2] - pz};
         tw += w;
-        xw[0] += w * s.pos[3 * j]; xw[1] += w * s.pos[3 * j + 1]; xw[2] += w * s.pos[3 * j + 2];
+        m1[0] += w * d[0]; m1[1] += w * d[1]; m1[2] += w * d[2];
+        if (w > 0) {
+          ++nnb;
+          m2[0] += w * d[0] * d[0]; m2[1] += w * d[1] * d[1]; m2[2] += w * d[2] * d[2];
+          m2[3] += w * d[0] * d[1]; m2[4] += w * d[0] * d[2]; m2[5] += w * d[1] * d[2];
+        }
       }
     });
-    if (tw != 0.0) { xw[0] /= tw; xw[1] /= tw; xw[2] /= tw; }
+    double db[3] = {0.0, 0.0, 0.0}, C[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    if (tw != 0.0) {
+      db[0] = m1[0] / tw; db[1] = m1[1] / tw; db[2] = m1[2] / tw;
+      C[0][0] = m2[0] / tw - db[0] * db[0]; C[1][1] = m2[1] / tw - db[1] * db[1]; C[2][2] = m2[2] / tw - db[2] * db[2];
+      C[0][1] = C[1][0] = m2[3] / tw - db[0] * db[1];
+      C[0][2] = C[2][0] = m2[4] / tw - db[0] * db[2];
+      C[1][2] = C[2][1] = m2[5] / tw - db[1] * db[2];
+    }
+    const double xw[3] = {tw != 0.0 ? px + db[0] : 0.0, tw != 0.0 ? py + db[1] : 0.0, tw != 0.0 ? pz + db[2] : 0.0};
     const double lam_ = 0.9;  // akLambda
     s.xbar[3 * i] = (float)((1 - lam_) * px + lam_ * xw[0]);
     s.xbar[3 * i + 1] = (float)((1 - lam_) * py + lam_ * xw[1]);
     s.xbar[3 * i + 2] = (float)((1 - lam_) * pz + lam_ * xw[2]);
-    double C[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-    int nnb = 0;
-    sr_range_rows(s, cx, cy, cz, px, py, pz, rr + s.g.vs, [&](int j) {
-      const float dn = sr_dist(px, py, pz, s.pos + 3 * j);
-      if (dn < rr) {
-        const float q = dn / rr;
-        const double w = 1.0 - (double)(q * q * q);
-        if (w > 0) {
-          ++nnb;
-          const double d[3] = {s.pos[3 * j] - xw[0], s.pos[3 * j + 1] - xw[1], s.pos[3 * j + 2] - xw[2]};
-#pragma unroll
-          for (int a = 0; a < 3; ++a)
-#pragma unroll
-            for (int b = 0; b < 3; ++b) C[a][b] += w * d[a] * d[b];
-        }
-      }
-    });
-    if (tw != 0.0)
-#pragma unroll
-      for (int a = 0; a < 3; ++a)
-#pragma unroll
-        for (int b = 0; b < 3; ++b) C[a][b] /= tw;
     double lam[3], V[3][3];
     sr_sym_eig(C, lam, V);
     double sg[3] = {lam[0], lam[1], lam[2]};
@@ -359,32 +356,45 @@ __global__ void k_sr_aniso_splat(SrDev s) {
     }
     if (empty) continue;
     const float k1 = (float)(48.0 / SR_PI * det), k2 = (float)(16.0 / SR_PI * det);
-    const int nx = w1[0] - w0[0] + 1, ny = w1[1] - w0[1] + 1, nz = w1[2] - w0[2] + 1;
-    const int64_t nv = (int64_t)nx * ny * nz;
-    for (int64_t t = lane; t < nv; t += 32) {
-      const int x = w0[0] + (int)(t % nx), y = w0[1] + (int)((t / nx) % ny), z = w0[2] + (int)(t / ((int64_t)nx * ny));
-      // q = |G (x_bar - vertex)| in f32 with unfused operations: the kernel as written
-      // jumps at q = 0.5, so q must round the same way in every f32 evaluation
+    // each lane owns (x, y) columns of the box and walks z; the x and y terms of
+    // G d are per column and the sums keep the order ((G0 d0 + G1 d1) + G2 d2)
+    const int nxw = w1[0] - w0[0] + 1, ncol = nxw * (w1[1] - w0[1] + 1);
+    const int64_t plane = (int64_t)g.nx * g.ny;
+    for (int col = lane; col < ncol; col += 32) {
+      const int x = w0[0] + col % nxw, y = w0[1] + col / nxw;
+      const int mxy = ((x - 1 >= lo[0] && x - 1 <= hi[0]) + (x >= lo[0] && x <= hi[0])) *
+                      ((y - 1 >= lo[1] && y - 1 <= hi[1]) + (y >= lo[1] && y <= hi[1]));
+      if (mxy == 0) continue;
       const float d0 = __fsub_rn(xb[0], __fadd_rn(__fmul_rn((float)x, g.vs), g.ox));
       const float d1 = __fsub_rn(xb[1], __fadd_rn(__fmul_rn((float)y, g.vs), g.oy));
-      const float d2 = __fsub_rn(xb[2], __fadd_rn(__fmul_rn((float)z, g.vs), g.oz));
-      const float q0 = __fadd_rn(__fadd_rn(__fmul_rn(Gm[0], d0), __fmul_rn(Gm[1], d1)), __fmul_rn(Gm[2], d2));
-      const float q1 = __fadd_rn(__fadd_rn(__fmul_rn(Gm[3], d0), __fmul_rn(Gm[4], d1)), __fmul_rn(Gm[5], d2));
-      const float q2 = __fadd_rn(__fadd_rn(__fmul_rn(Gm[6], d0), __fmul_rn(Gm[7], d1)), __fmul_rn(Gm[8], d2));
-      const float q = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(q0, q0), __fmul_rn(q1, q1)), __fmul_rn(q2, q2)));
-      float res;  // cubic_spline_kernel as written (srtool.py:1114-1124)
-      if (q > 0.f && q <= 0.5f) res = k1 * (q * q * q - q * q) + 1.f;
-      else if (q > 0.5f && q <= 1.f) res = k2 * (1.f - q) * (1.f - q) * (1.f - q);
-      else continue;
-      // vertex (x, y, z) belongs to the voxels x - 1 and x of the box, per axis
-      const int m = ((x - 1 >= lo[0] && x - 1 <= hi[0]) + (x >= lo[0] && x <= hi[0])) *
-                    ((y - 1 >= lo[1] && y - 1 <= hi[1]) + (y >= lo[1] && y <= hi[1])) *
-                    ((z - 1 >= lo[2] && z - 1 <= hi[2]) + (z >= lo[2] && z <= hi[2]));
-      if (m == 0) continue;
-      const double c = (double)(s.volume * res);
-      if (!isfinite(c)) { sr_fail(s, NN_ERR_NAN); continue; }
-      const long long u = llrint(fmin(fmax(c, -1e8), 1e8) * SR_FIX);
-      atomicAdd(&s.fix[g.idx(x, y, z)], (unsigned long long)(u * m));
+      const float a0 = __fadd_rn(__fmul_rn(Gm[0], d0), __fmul_rn(Gm[1], d1));
+      const float a1 = __fadd_rn(__fmul_rn(Gm[3], d0), __fmul_rn(Gm[4], d1));
+      const float a2 = __fadd_rn(__fmul_rn(Gm[6], d0), __fmul_rn(Gm[7], d1));
+      const int64_t base = g.idx(x, y, 0);
+      for (int z = w0[2]; z <= w1[2]; ++z) {
+        // q = |G (x_bar - vertex)| in f32 with unfused operations: the kernel as written
+        // jumps at q = 0.5, so q must round the same way in every f32 evaluation
+        const float d2 = __fsub_rn(xb[2], __fadd_rn(__fmul_rn((float)z, g.vs), g.oz));
+        const float q0 = __fadd_rn(a0, __fmul_rn(Gm[2], d2));
+        const float q1 = __fadd_rn(a1, __fmul_rn(Gm[5], d2));
+        const float q2 = __fadd_rn(a2, __fmul_rn(Gm[8], d2));
+        const float q2s = __fadd_rn(__fadd_rn(__fmul_rn(q0, q0), __fmul_rn(q1, q1)), __fmul_rn(q2, q2));
+        // outside the support: rn(sqrt(q2s)) > 1 exactly when q2s > q1_thr
+        if (!(q2s <= s.q1_thr) || !(q2s > 0.f)) continue;
+        // the branch of cubic_spline_kernel (srtool.py:1114-1124) is decided exactly
+        // (rn(sqrt(q2s)) <= 0.5 exactly when q2s <= q05_thr); its value, continuous
+        // within a branch, takes q from the hardware reciprocal square root
+        const float q = q2s * rsqrtf(q2s);
+        const float res = q2s <= s.q05_thr ? k1 * (q * q * q - q * q) + 1.f : k2 * (1.f - q) * (1.f - q) * (1.f - q);
+        // vertex (x, y, z) belongs to the voxels x - 1 and x of the box, per axis; the
+        // multiplicity is 1, 2, 4 or 8, a power of two, so scaling by it is exact
+        const int m = mxy * ((z - 1 >= lo[2] && z - 1 <= hi[2]) + (z >= lo[2] && z <= hi[2]));
+        if (m == 0) continue;
+        const float c = s.volume * res;
+        if (!isfinite(c)) { sr_fail(s, NN_ERR_NAN); continue; }
+        const long long u = __float2ll_rn(fminf(fmaxf(c, -1e8f), 1e8f) * (4294967296.f * (float)m));
+        atomicAdd(&s.fix[base + z * plane], (unsigned long long)u);
+      }
     }
   }
 }
@@ -773,6 +783,16 @@ int nn_sr_dual_contouring(nn_sr_ctx* c, const nn_sr_params* p, const float* pos,
   s.range = (int)std::ceil(4.0 * (double)s.sr / (double)s.g.vs) + 1;  // srtool.py:1137
   s.off = s.range / 2;
   s.smooth_cells = p->smooth_cells;
+  {  // exact branch tests without the square root: rn(sqrt(t)) <= 1 (0.5)  <=>  t <= q1_thr (q05_thr)
+    float t = 1.f;
+    while (std::sqrt(std::nextafter(t, INFINITY)) <= 1.f) t = std::nextafter(t, INFINITY);
+    while (std::sqrt(t) > 1.f) t = std::nextafter(t, 0.f);
+    s.q1_thr = t;
+    t = 0.25f;
+    while (std::sqrt(std::nextafter(t, INFINITY)) <= 0.5f) t = std::nextafter(t, INFINITY);
+    while (std::sqrt(t) > 0.5f) t = std::nextafter(t, 0.f);
+    s.q05_thr = t;
+  }
   s.record_normals = p->record_normals;
   const int B = 256;
   const int grid_n = std::max(1, std::min((n + B - 1) / B, c->sms * 8));
