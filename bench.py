@@ -396,7 +396,7 @@ def run_reference_surface(args):
 # written once and read once (fixed-point field 8 + 8, splat copy 4, field 4 + 4,
 # smoothing output 4 + 4, crossing flags 4 + 4, index counts 4 + 4, voxel counts 4 + 4)
 SR_BYTES_PER_CELL = 60
-SR_LAUNCHES = 24  # kernels one SRTool.dual_contouring call launches (three 3-kernel scans included)
+SR_LAUNCHES = 26  # kernels one SRTool.dual_contouring call launches (three 3-kernel scans included)
 
 
 def run_surface(args, world, rank):

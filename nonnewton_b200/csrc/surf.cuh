@@ -66,6 +66,7 @@ struct SrDev {
   uint32_t* vkey;           // [n]
   uint32_t* vrank;          // [n]
   int32_t* vsrc;            // [n] particles in voxel order
+  float4* spos;             // [n] their positions, in the same order
   unsigned long long* fix;  // [cells] fixed-point field
   float* splat;             // [cells] field after the splats
   float* field;             // [cells] field after smoothing
@@ -76,6 +77,7 @@ struct SrDev {
   double* stats;            // sum, count, var, sd
   uint32_t* vflag;          // [cells+1] crossing-cube flags, then vertex ids
   uint32_t* tcount;         // [cells+1] index counts, then offsets
+  uint32_t* cube_of;        // [max_v] cube (linear index) of each vertex id
   float* vert;              // [max_v,3]
   int32_t* tri;             // [max_i]
   float* nrm;               // [max_v,3]
@@ -128,6 +130,17 @@ __global__ void k_sr_voxel_sort(SrDev s, int64_t cells) {
       while (j > b && s.vsrc[j - 1] > v) { s.vsrc[j] = s.vsrc[j - 1]; --j; }
       s.vsrc[j] = v;
     }
+  }
+}
+
+// Positions in voxel order; only the first vcount[cells] entries of vsrc are filled
+// (particles outside the grid are not binned, and the call then fails).
+__global__ void k_sr_sorted_pos(SrDev s, int64_t cells) {
+  const int nb = (int)min((int64_t)s.vcount[cells], (int64_t)s.n);
+  GRID_STRIDE(k, nb) {
+    const int i = s.vsrc[k];
+    if (i < 0 || i >= s.n) continue;
+    s.spos[k] = make_float4(s.pos[3 * i], s.pos[3 * i + 1], s.pos[3 * i + 2], 0.f);
   }
 }
 
@@ -202,29 +215,25 @@ __device__ void sr_sym_eig(const double S0[3][3], double lam[3], double V[3][3])
 }
 
 // Visits the particles within the smoothing range of voxel (cx, cy, cz) whose voxel
-// can hold a point closer than `reach`, row by row: the voxels of one (y, z) row are
-// one contiguous stretch of vsrc.
+// can hold a point closer than `reach`, row by row (the voxels of one (y, z) row are
+// one contiguous stretch of the voxel-sorted arrays, whose index k is passed to f);
+// lane `lane` of `lanes` takes every lanes-th row.
 template <typename F>
 __device__ __forceinline__ void sr_range_rows(const SrDev& s, int cx, int cy, int cz, float px, float py, float pz,
-                                              float reach, F f) {
+                                              float reach, int lane, int lanes, F f) {
   const SrGrid& g = s.g;
   const int lo = -s.off, hi = s.range - 1 - s.off;
   const float r2 = reach * reach;
-  for (int dz = lo; dz <= hi; ++dz) {
-    const int z = cz + dz;
-    if (z < 0 || z >= g.nz) continue;
+  const int x0 = max(cx + lo, 0), x1 = min(cx + hi, g.nx - 1);
+  if (x0 > x1) return;
+  for (int r = lane; r < s.range * s.range; r += lanes) {
+    const int z = cz + lo + r / s.range, y = cy + lo + r % s.range;
+    if (z < 0 || z >= g.nz || y < 0 || y >= g.ny) continue;
     const float zc = fmaxf(fmaxf(g.oz + z * g.vs - pz, pz - (g.oz + (z + 1) * g.vs)), 0.f);
-    if (zc * zc > r2) continue;
-    for (int dy = lo; dy <= hi; ++dy) {
-      const int y = cy + dy;
-      if (y < 0 || y >= g.ny) continue;
-      const float yc = fmaxf(fmaxf(g.oy + y * g.vs - py, py - (g.oy + (y + 1) * g.vs)), 0.f);
-      if (yc * yc + zc * zc > r2) continue;
-      const int x0 = max(cx + lo, 0), x1 = min(cx + hi, g.nx - 1);
-      if (x0 > x1) continue;
-      const uint32_t b = s.vcount[g.idx(x0, y, z)], e = s.vcount[g.idx(x1, y, z) + 1];
-      for (uint32_t k = b; k < e; ++k) f(s.vsrc[k]);
-    }
+    const float yc = fmaxf(fmaxf(g.oy + y * g.vs - py, py - (g.oy + (y + 1) * g.vs)), 0.f);
+    if (yc * yc + zc * zc > r2) continue;
+    const uint32_t b = s.vcount[g.idx(x0, y, z)], e = s.vcount[g.idx(x1, y, z) + 1];
+    for (uint32_t k = b; k < e; ++k) f(k);
   }
 }
 
@@ -235,8 +244,12 @@ __device__ __forceinline__ float sr_dist(float px, float py, float pz, const flo
   return __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz)));
 }
 
+// One warp per particle: lanes split the rows of the range and the moments are
+// reduced across the warp with shuffles.
 __global__ void k_sr_aniso_pre(SrDev s) {
-  GRID_STRIDE(i, s.n) {
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < s.n; i += warps) {
     if (i == 0) continue;  // the reference's loop starts at 1 (srtool.py:1013)
     const float px = s.pos[3 * i], py = s.pos[3 * i + 1], pz = s.pos[3 * i + 2];
     int cx, cy, cz;
@@ -248,12 +261,14 @@ __global__ void k_sr_aniso_pre(SrDev s) {
     double tw = 0.0, m1[3] = {0.0, 0.0, 0.0}, m2[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     int nnb = 0;
     // a margin of one voxel on the pruning distance keeps every pair with w > 0
-    sr_range_rows(s, cx, cy, cz, px, py, pz, rr + s.g.vs, [&](int j) {
-      const float dn = sr_dist(px, py, pz, s.pos + 3 * j);
+    sr_range_rows(s, cx, cy, cz, px, py, pz, rr + s.g.vs, lane, 32, [&](uint32_t k) {
+      const float4 pj = s.spos[k];
+      const float pjv[3] = {pj.x, pj.y, pj.z};
+      const float dn = sr_dist(px, py, pz, pjv);
       if (dn < rr) {
         const float q = dn / rr;
         const double w = 1.0 - (double)(q * q * q);  // isoweight, srtool.py:993-999
-        const double d[3] = {(double)s.pos[3 * j] - px, (double)s.pos[3 * j + 1] - py, (double)s.pos[3 * j + 2] - pz};
+        const double d[3] = {(double)pj.x - px, (double)pj.y - py, (double)pj.z - pz};
         tw += w;
         m1[0] += w * d[0]; m1[1] += w * d[1]; m1[2] += w * d[2];
         if (w > 0) {
@@ -263,6 +278,16 @@ __global__ void k_sr_aniso_pre(SrDev s) {
         }
       }
     });
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      tw += __shfl_xor_sync(0xffffffffu, tw, o);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) m1[k] += __shfl_xor_sync(0xffffffffu, m1[k], o);
+#pragma unroll
+      for (int k = 0; k < 6; ++k) m2[k] += __shfl_xor_sync(0xffffffffu, m2[k], o);
+      nnb += __shfl_xor_sync(0xffffffffu, nnb, o);
+    }
+    if (lane != 0) continue;
     double db[3] = {0.0, 0.0, 0.0}, C[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
     if (tw != 0.0) {
       db[0] = m1[0] / tw; db[1] = m1[1] / tw; db[2] = m1[2] / tw;
@@ -524,12 +549,20 @@ __device__ void sr_normal_at(const SrDev& s, const double p[3], double n[3]) {
   else n[0] = n[1] = n[2] = 0.0;
 }
 
+// The crossing cubes in vertex-id order, so that the QEF kernel runs on dense work.
+__global__ void k_sr_dc_list(SrDev s, int64_t cells) {
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < cells; c += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t id = s.vflag[c];
+    if (s.vflag[c + 1] != id && (int64_t)id < s.max_v) s.cube_of[id] = (uint32_t)c;
+  }
+}
+
 // One point per crossing cube: the mass point of the edge crossings plus the clamped
 // QEF solution, kept only if it stays in its cube (srtool.py:1536-1596)
 __global__ void k_sr_dc_point(SrDev s, int64_t cells) {
-  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < cells; c += (int64_t)gridDim.x * blockDim.x) {
-    if (s.vflag[c + 1] == s.vflag[c]) continue;  // not a crossing cube (exclusive scan)
-    const uint32_t id = s.vflag[c];
+  const int64_t nv = min((int64_t)s.vflag[cells], (int64_t)s.max_v);
+  for (int64_t id = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; id < nv; id += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = s.cube_of[id];
     const int x = (int)(c % s.g.nx), y = (int)((c / s.g.nx) % s.g.ny), z = (int)(c / ((int64_t)s.g.nx * s.g.ny));
     const int ci = sr_cube_mask(s, x, y, z);
     double P[12][3];
@@ -570,8 +603,7 @@ __global__ void k_sr_dc_point(SrDev s, int64_t cells) {
     int qx, qy, qz;
     s.g.voxel_of((float)(res[0] + mean[0]), (float)(res[1] + mean[1]), (float)(res[2] + mean[2]), qx, qy, qz);
     const bool keep = qx == x && qy == y && qz == z;
-    if ((int64_t)id >= s.max_v) { sr_fail(s, NN_ERR_CAPACITY); continue; }
-    for (int k = 0; k < 3; ++k) s.vert[3 * (int64_t)id + k] = (float)(keep ? res[k] + mean[k] : mean[k]);
+    for (int k = 0; k < 3; ++k) s.vert[3 * id + k] = (float)(keep ? res[k] + mean[k] : mean[k]);
   }
 }
 
@@ -647,8 +679,9 @@ struct nn_sr_ctx {
   int32_t* d_n = nullptr;  // scan sizes ([2] = last index of the current scan)
   int32_t* status = nullptr;
   uint32_t *vcount = nullptr, *vkey = nullptr, *vrank = nullptr, *vflag = nullptr, *tcount = nullptr,
-           *tile_sums = nullptr;
+           *tile_sums = nullptr, *cube_of = nullptr;
   int32_t *vsrc = nullptr, *tri = nullptr;
+  float4* spos = nullptr;
   unsigned long long* fix = nullptr;
   float *splat = nullptr, *fa = nullptr, *fb = nullptr, *G = nullptr, *xbar = nullptr, *vert = nullptr, *nrm = nullptr;
   uint8_t* active = nullptr;
@@ -679,7 +712,8 @@ static int sr_fail_host(nn_sr_ctx* c, int code, const char* fmt, ...) {
 
 static void sr_free(nn_sr_ctx* c) {
   void* bufs[] = {c->d_n, c->status, c->vcount, c->vkey, c->vrank, c->vflag, c->tcount, c->tile_sums, c->vsrc,
-                  c->tri, c->fix, c->splat, c->fa, c->fb, c->G, c->xbar, c->vert, c->nrm, c->active, c->stats};
+                  c->tri, c->fix, c->splat, c->fa, c->fb, c->G, c->xbar, c->vert, c->nrm, c->active, c->stats,
+                  c->cube_of, c->spos};
   for (void* b : bufs) cudaFree(b);
 }
 
@@ -724,9 +758,10 @@ int nn_sr_create(int32_t max_particles, int64_t max_cells, int32_t max_vertices,
   };
   al(&c->d_n, 4); al(&c->status, 1); al(&c->stats, 4);
   al(&c->vcount, CL); al(&c->vflag, CL); al(&c->tcount, CL); al(&c->tile_sums, tiles);
-  al(&c->vkey, N); al(&c->vrank, N); al(&c->vsrc, N); al(&c->G, 9 * N); al(&c->xbar, 3 * N);
+  al(&c->vkey, N); al(&c->vrank, N); al(&c->vsrc, N); al(&c->spos, N); al(&c->G, 9 * N); al(&c->xbar, 3 * N);
   al(&c->fix, CL); al(&c->splat, CL); al(&c->fa, CL); al(&c->fb, CL); al(&c->active, blocks);
   al(&c->vert, 3 * (size_t)max_vertices); al(&c->nrm, 3 * (size_t)max_vertices); al(&c->tri, (size_t)max_indices);
+  al(&c->cube_of, (size_t)max_vertices);
   if (e != cudaSuccess) {
     sr_free(c);
     delete c;
@@ -771,10 +806,11 @@ int nn_sr_dual_contouring(nn_sr_ctx* c, const nn_sr_params* p, const float* pos,
   s.g.vs = (float)p->voxel_size;
   s.g.dox = s.g.ox; s.g.doy = s.g.oy; s.g.doz = s.g.oz; s.g.dvs = s.g.vs;
   s.n = n; s.pos = pos; s.status = c->status;
-  s.vcount = c->vcount; s.vkey = c->vkey; s.vrank = c->vrank; s.vsrc = c->vsrc;
+  s.vcount = c->vcount; s.vkey = c->vkey; s.vrank = c->vrank; s.vsrc = c->vsrc; s.spos = c->spos;
   s.fix = c->fix; s.splat = c->splat; s.field = c->fa; s.tmp = c->fb; s.active = c->active;
   s.G = c->G; s.xbar = c->xbar; s.stats = c->stats; s.vflag = c->vflag; s.tcount = c->tcount;
   s.vert = c->vert; s.tri = c->tri; s.nrm = c->nrm; s.max_v = c->max_v; s.max_i = c->max_i;
+  s.cube_of = c->cube_of;
   s.iso = (float)p->isolevel;
   s.sr = (float)p->smooth_radius;
   const double r = p->particle_radius;
@@ -810,12 +846,13 @@ int nn_sr_dual_contouring(nn_sr_ctx* c, const nn_sr_params* p, const float* pos,
     RC(sr_scan(c, c->vcount, cells + 1, st));
     k_sr_scatter<<<grid_n, B, 0, st>>>(s);
     k_sr_voxel_sort<<<grid_c, B, 0, st>>>(s, cells);
+    k_sr_sorted_pos<<<grid_n, B, 0, st>>>(s, cells);
     // 2. isotropic splat
     k_sr_iso<<<grid_n, B, 0, st>>>(s);
     if (p->use_smooth_field) {
-      // 3-4. anisotropic kernels and splat (one warp per particle)
-      k_sr_aniso_pre<<<grid_n, B, 0, st>>>(s);
+      // 3-4. anisotropic kernels and splat (one warp per particle each)
       const int grid_w = (int)std::max<int64_t>(1, std::min<int64_t>(((int64_t)n * 32 + B - 1) / B, c->sms * 16));
+      k_sr_aniso_pre<<<grid_w, B, 0, st>>>(s);
       k_sr_aniso_splat<<<grid_w, B, 0, st>>>(s);
     }
   }
@@ -833,7 +870,8 @@ int nn_sr_dual_contouring(nn_sr_ctx* c, const nn_sr_params* p, const float* pos,
   SRCK(cudaMemsetAsync(c->vflag, 0, (cells + 1) * sizeof(uint32_t), st));
   k_sr_dc_flag<<<grid_c, B, 0, st>>>(s, cells);
   RC(sr_scan(c, c->vflag, cells + 1, st));
-  k_sr_dc_point<<<grid_c, B, 0, st>>>(s, cells);
+  k_sr_dc_list<<<grid_c, B, 0, st>>>(s, cells);
+  k_sr_dc_point<<<c->sms * 4, 128, 0, st>>>(s, cells);
   SRCK(cudaMemsetAsync(c->tcount, 0, (cells + 1) * sizeof(uint32_t), st));
   k_sr_tris<<<grid_c, B, 0, st>>>(s, cells, 0);
   RC(sr_scan(c, c->tcount, cells + 1, st));
