@@ -11,6 +11,9 @@ each step and the positions read back after it. Inputs are synthetic (seeded num
 generators with the shapes of the benchmark scenes). `--impl reference` times the
 CPU restatement of the reference step (the reference itself is Python + Taichi, which
 is not installed) on all host cores over a bounded sample of the same workload.
+
+`--workload surface` times the surface reconstruction instead (SRTool.dual_contouring
+on a 125,000-particle fluid block; one step is one reconstruction, in particles/s).
 """
 from __future__ import annotations
 
