@@ -637,6 +637,8 @@ def run_ours(args):
     bytes_step = step_bytes(st["iterations_v"] + 1, st["iterations"] + 1, st["cg_iterations"], 0.0, implicit)
     line = {
         "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
+        # the same rate counting only dynamic particles (fluid and moving solids)
+        "value_dynamic": value * float(np.count_nonzero(sc.particles.is_dynamic)) / n,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded numpy scene generator)",
