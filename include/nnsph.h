@@ -315,28 +315,34 @@ typedef struct nn_sr_params {
 typedef struct nn_sr_ctx nn_sr_ctx;
 
 /* Capacities: particles, vertex grid cells, mesh vertices and triangle indices
-   (SRTool(max_num_particles, max_num_vertices, max_num_indices)). */
+   (SRTool(max_num_particles, max_num_vertices, max_num_indices)); options
+   NN_SR_VELOCITY (SRTool(record_velocity=True)) adds the vertex velocity field. */
+#define NN_SR_VELOCITY 1
 int nn_sr_create(int32_t max_particles, int64_t max_cells, int32_t max_vertices, int32_t max_indices,
-                 nn_sr_ctx** out);
+                 int32_t options, nn_sr_ctx** out);
 int nn_sr_destroy(nn_sr_ctx* ctx);
 const char* nn_sr_last_error(const nn_sr_ctx* ctx);
 
-/* SRTool.dual_contouring for `n` particles at device positions pos [n,3] f32, enqueued
-   on `cuda_stream`; the mesh stays in the context. NN_ERR_CAPACITY when the grid,
+/* SRTool.dual_contouring for `n` particles at device positions pos [n,3] f32 (and,
+   with velocities vel [n,3] f32 on a context created with NN_SR_VELOCITY, the
+   velocity splat of srtool.py:1159-1190 and the mesh velocities of
+   process_velocity, 1351-1381; vel NULL records none), enqueued on `cuda_stream`;
+   the mesh stays in the context. NN_ERR_CAPACITY when the grid,
    the mesh or a voxel's particle list (NN_SR_MAX_PER_VOXEL, the reference's 64) is
    too small; NN_ERR_INVALID_ARG for particles outside the grid. Synchronises the
    stream once (to read the mesh sizes). */
 #define NN_SR_MAX_PER_VOXEL 64
-int nn_sr_dual_contouring(nn_sr_ctx* ctx, const nn_sr_params* params, const float* pos, int32_t n,
-                          void* cuda_stream);
+int nn_sr_dual_contouring(nn_sr_ctx* ctx, const nn_sr_params* params, const float* pos, const float* vel,
+                          int32_t n, void* cuda_stream);
 
 /* The mesh of the last call: counts, and copies into caller device buffers when
    non-NULL: vertices [num_vertices,3] f32, indices [num_indices] i32 (triangles),
-   normals [num_vertices,3] f32 (when record_normals was set). Vertices are numbered
+   normals [num_vertices,3] f32 (when record_normals was set), velocities
+   [num_vertices,3] f32 (when velocities were given). Vertices are numbered
    by the linear index of their cube, triangles ordered by cube and then by edge
    (x, y, z edges of the cube's first corner). */
 int nn_sr_get_mesh(nn_sr_ctx* ctx, int32_t* num_vertices, int32_t* num_indices, float* vertices,
-                   int32_t* indices, float* normals, void* cuda_stream);
+                   int32_t* indices, float* normals, float* velocities, void* cuda_stream);
 
 /* Stage outputs for parity checks (device buffers, each optional): the field [cells]
    f32, the active-block flags [blocks] u8 (blocks of NN_SR_BLOCK^3 in x-fastest

@@ -176,6 +176,7 @@ def make_params(**kw) -> nn_scene_params:
 
 
 NN_SR_BLOCK = 32
+NN_SR_VELOCITY = 1
 NN_SR_MAX_PER_VOXEL = 64
 
 

@@ -81,6 +81,9 @@ struct SrDev {
   float* vert;              // [max_v,3]
   int32_t* tri;             // [max_i]
   float* nrm;               // [max_v,3]
+  const float* vel;         // [n,3] particle velocities, or null (no velocity recording)
+  unsigned long long* vfix; // [3][cells] fixed-point vertex velocities
+  float* mvel;              // [max_v,3] mesh-vertex velocities
   int32_t max_v, max_i;
   float iso, sr, volume, acoeff;
   float q1_thr, q05_thr;     // largest f32 whose rounded square root is <= 1, <= 0.5
@@ -424,6 +427,89 @@ __global__ void k_sr_aniso_splat(SrDev s) {
   }
 }
 
+// Velocity splat (generate_smooth_fluid_field_with_velocity_impl, srtool.py:1159-1190):
+// every vertex of every voxel in the smoothing range, once per adjacent voxel, gets
+// v_i * poly6(x_i - vertex, r_s) * voxel_size^3. One warp per particle; lanes own
+// (x, y) columns of the poly6 support's box and walk z.
+__global__ void k_sr_vel_splat(SrDev s) {
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  const float h = s.sr, h2 = h * h, h9 = h2 * h2 * h2 * h2 * h;
+  const float coeff = s.g.vs * s.g.vs * s.g.vs;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < s.n; i += warps) {
+    const SrGrid& g = s.g;
+    const float px = s.pos[3 * i], py = s.pos[3 * i + 1], pz = s.pos[3 * i + 2];
+    int cx, cy, cz;
+    g.voxel_of(px, py, pz, cx, cy, cz);
+    const int lo[3] = {cx - s.off, cy - s.off, cz - s.off};
+    const int hi[3] = {lo[0] + s.range - 1, lo[1] + s.range - 1, lo[2] + s.range - 1};
+    if (hi[0] + 1 >= g.nx || hi[1] + 1 >= g.ny || hi[2] + 1 >= g.nz) continue;  // flagged by the field splat
+    const float p[3] = {px, py, pz};
+    const float org[3] = {g.ox, g.oy, g.oz};
+    int w0[3], w1[3];
+    bool empty = false;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {  // the poly6 support |x_i - vertex| <= r_s, one vertex of margin
+      w0[a] = max(max(lo[a], 0), (int)floorf((p[a] - h - org[a]) / g.vs) - 1);
+      w1[a] = min(hi[a] + 1, (int)ceilf((p[a] + h - org[a]) / g.vs) + 1);
+      empty |= w0[a] > w1[a];
+    }
+    if (empty) continue;
+    const float v[3] = {s.vel[3 * i], s.vel[3 * i + 1], s.vel[3 * i + 2]};
+    const int nxw = w1[0] - w0[0] + 1, ncol = nxw * (w1[1] - w0[1] + 1);
+    const int64_t plane = (int64_t)g.nx * g.ny, cells = plane * g.nz;
+    for (int col = lane; col < ncol; col += 32) {
+      const int x = w0[0] + col % nxw, y = w0[1] + col / nxw;
+      const int mxy = ((x - 1 >= lo[0] && x - 1 <= hi[0]) + (x >= lo[0] && x <= hi[0])) *
+                      ((y - 1 >= lo[1] && y - 1 <= hi[1]) + (y >= lo[1] && y <= hi[1]));
+      if (mxy == 0) continue;
+      const float rx = px - (x * g.vs + g.ox), ry = py - (y * g.vs + g.oy);
+      const int64_t base = g.idx(x, y, 0);
+      for (int z = w0[2]; z <= w1[2]; ++z) {
+        const float rz = pz - (z * g.vs + g.oz);
+        const float r2 = rx * rx + ry * ry + rz * rz;
+        if (!(sqrtf(r2) <= h)) continue;  // poly6_weight, srtool.py:1212-1227
+        const float t = h2 - r2;
+        const float w = s.acoeff * (t * t * t) / h9 * coeff;
+        const int m = mxy * ((z - 1 >= lo[2] && z - 1 <= hi[2]) + (z >= lo[2] && z <= hi[2]));
+        if (m == 0) continue;
+        const int64_t c = base + z * plane;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          const float cv = v[k] * w;
+          if (!isfinite(cv)) { sr_fail(s, NN_ERR_NAN); continue; }
+          const long long u = __float2ll_rn(fminf(fmaxf(cv, -1e8f), 1e8f) * (4294967296.f * (float)m));
+          atomicAdd(&s.vfix[k * cells + c], (unsigned long long)u);
+        }
+      }
+    }
+  }
+}
+
+// process_velocity (srtool.py:1351-1381): trilinear blend of the 8 vertex velocities
+// around each mesh vertex
+__global__ void k_sr_mesh_velocity(SrDev s, int nv) {
+  const int64_t plane = (int64_t)s.g.nx * s.g.ny, cells = plane * s.g.nz;
+  GRID_STRIDE(i, min(nv, s.max_v)) {
+    const double p[3] = {s.vert[3 * i], s.vert[3 * i + 1], s.vert[3 * i + 2]};
+    int x0, y0, z0;
+    s.g.voxel_of((float)p[0], (float)p[1], (float)p[2], x0, y0, z0);
+    const double xd = (p[0] - (x0 * s.g.dvs + s.g.dox)) / s.g.dvs, yd = (p[1] - (y0 * s.g.dvs + s.g.doy)) / s.g.dvs,
+                 zd = (p[2] - (z0 * s.g.dvs + s.g.doz)) / s.g.dvs;
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (int a = 0; a < 2; ++a)
+      for (int b = 0; b < 2; ++b)
+        for (int e = 0; e < 2; ++e) {
+          const int x = x0 + a, y = y0 + b, z = z0 + e;
+          if (!s.g.in(x, y, z)) continue;
+          const double wgt = (a ? xd : 1 - xd) * (b ? yd : 1 - yd) * (e ? zd : 1 - zd);
+          const int64_t c = s.g.idx(x, y, z);
+          for (int k = 0; k < 3; ++k) acc[k] += wgt * ((double)(long long)s.vfix[k * cells + c] / SR_FIX);
+        }
+    for (int k = 0; k < 3; ++k) s.mvel[3 * i + k] = (float)acc[k];
+  }
+}
+
 __global__ void k_sr_fix_to_field(SrDev s, int64_t cells) {
   for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < cells; c += (int64_t)gridDim.x * blockDim.x) {
     const float v = (float)((double)(long long)s.fix[c] / SR_FIX);
@@ -682,6 +768,8 @@ struct nn_sr_ctx {
            *tile_sums = nullptr, *cube_of = nullptr;
   int32_t *vsrc = nullptr, *tri = nullptr;
   float4* spos = nullptr;
+  unsigned long long* vfix = nullptr;  // [3][cells], with NN_SR_VELOCITY only
+  float* mvel = nullptr;
   unsigned long long* fix = nullptr;
   float *splat = nullptr, *fa = nullptr, *fb = nullptr, *G = nullptr, *xbar = nullptr, *vert = nullptr, *nrm = nullptr;
   uint8_t* active = nullptr;
@@ -713,7 +801,7 @@ static int sr_fail_host(nn_sr_ctx* c, int code, const char* fmt, ...) {
 static void sr_free(nn_sr_ctx* c) {
   void* bufs[] = {c->d_n, c->status, c->vcount, c->vkey, c->vrank, c->vflag, c->tcount, c->tile_sums, c->vsrc,
                   c->tri, c->fix, c->splat, c->fa, c->fb, c->G, c->xbar, c->vert, c->nrm, c->active, c->stats,
-                  c->cube_of, c->spos};
+                  c->cube_of, c->spos, c->vfix, c->mvel};
   for (void* b : bufs) cudaFree(b);
 }
 
@@ -736,11 +824,11 @@ static int sr_scan(nn_sr_ctx* c, uint32_t* a, int64_t len, cudaStream_t st) {
 extern "C" {
 
 int nn_sr_create(int32_t max_particles, int64_t max_cells, int32_t max_vertices, int32_t max_indices,
-                 nn_sr_ctx** out) {
+                 int32_t options, nn_sr_ctx** out) {
   if (!out) return NN_ERR_INVALID_ARG;
   *out = nullptr;
   if (max_particles <= 0 || max_cells <= 0 || max_cells >= (int64_t)INT32_MAX - SCAN_TILE || max_vertices <= 0 ||
-      max_indices <= 0)
+      max_indices <= 0 || (options & ~NN_SR_VELOCITY))
     return NN_ERR_INVALID_ARG;
   nn_sr_ctx* c = new nn_sr_ctx();
   cudaGetDevice(&c->dev_id);
@@ -761,7 +849,8 @@ int nn_sr_create(int32_t max_particles, int64_t max_cells, int32_t max_vertices,
   al(&c->vkey, N); al(&c->vrank, N); al(&c->vsrc, N); al(&c->spos, N); al(&c->G, 9 * N); al(&c->xbar, 3 * N);
   al(&c->fix, CL); al(&c->splat, CL); al(&c->fa, CL); al(&c->fb, CL); al(&c->active, blocks);
   al(&c->vert, 3 * (size_t)max_vertices); al(&c->nrm, 3 * (size_t)max_vertices); al(&c->tri, (size_t)max_indices);
-  al(&c->cube_of, (size_t)max_vertices);
+  al(&c->cube_of, (size_t)max_vertices); al(&c->mvel, 3 * (size_t)max_vertices);
+  if (options & NN_SR_VELOCITY) al(&c->vfix, 3 * CL);
   if (e != cudaSuccess) {
     sr_free(c);
     delete c;
@@ -781,13 +870,16 @@ int nn_sr_destroy(nn_sr_ctx* c) {
 
 const char* nn_sr_last_error(const nn_sr_ctx* c) { return c ? c->err.c_str() : "null context"; }
 
-int nn_sr_dual_contouring(nn_sr_ctx* c, const nn_sr_params* p, const float* pos, int32_t n, void* stream) {
+int nn_sr_dual_contouring(nn_sr_ctx* c, const nn_sr_params* p, const float* pos, const float* vel, int32_t n,
+                          void* stream) {
   if (!c) return NN_ERR_INVALID_ARG;
   c->have = false;
   if (!p || p->size != (int32_t)sizeof(nn_sr_params) || (!pos && n > 0) || n < 0)
     return sr_fail_host(c, NN_ERR_INVALID_ARG, "nn_sr_dual_contouring: invalid argument");
   if (n > c->max_particles)
     return sr_fail_host(c, NN_ERR_CAPACITY, "%d particles exceed the context's %d", n, c->max_particles);
+  if (vel && !c->vfix)
+    return sr_fail_host(c, NN_ERR_STATE, "velocities given to a context created without NN_SR_VELOCITY");
   if (!(p->voxel_size > 0) || !(p->smooth_radius > 0) || !(p->particle_radius > 0) || p->dims[0] <= 0 ||
       p->dims[1] <= 0 || p->dims[2] <= 0 || p->smooth_iterations < 0 || p->smooth_cells < 0)
     return sr_fail_host(c, NN_ERR_INVALID_ARG, "nn_sr_dual_contouring: bad parameters");
@@ -811,6 +903,7 @@ int nn_sr_dual_contouring(nn_sr_ctx* c, const nn_sr_params* p, const float* pos,
   s.G = c->G; s.xbar = c->xbar; s.stats = c->stats; s.vflag = c->vflag; s.tcount = c->tcount;
   s.vert = c->vert; s.tri = c->tri; s.nrm = c->nrm; s.max_v = c->max_v; s.max_i = c->max_i;
   s.cube_of = c->cube_of;
+  s.vel = vel; s.vfix = c->vfix; s.mvel = c->mvel;
   s.iso = (float)p->isolevel;
   s.sr = (float)p->smooth_radius;
   const double r = p->particle_radius;
@@ -837,6 +930,7 @@ int nn_sr_dual_contouring(nn_sr_ctx* c, const nn_sr_params* p, const float* pos,
   SRCK(cudaMemsetAsync(c->stats, 0, 4 * sizeof(double), st));
   SRCK(cudaMemsetAsync(c->vcount, 0, (cells + 1) * sizeof(uint32_t), st));
   SRCK(cudaMemsetAsync(c->fix, 0, cells * sizeof(unsigned long long), st));
+  if (vel) SRCK(cudaMemsetAsync(c->vfix, 0, 3 * cells * sizeof(unsigned long long), st));
   SRCK(cudaMemsetAsync(c->active, 0, blocks, st));
   SRCK(cudaMemsetAsync(c->G, 0, 9 * (size_t)std::max(n, 1) * sizeof(float), st));
   SRCK(cudaMemsetAsync(c->xbar, 0, 3 * (size_t)std::max(n, 1) * sizeof(float), st));
@@ -854,6 +948,7 @@ int nn_sr_dual_contouring(nn_sr_ctx* c, const nn_sr_params* p, const float* pos,
       const int grid_w = (int)std::max<int64_t>(1, std::min<int64_t>(((int64_t)n * 32 + B - 1) / B, c->sms * 16));
       k_sr_aniso_pre<<<grid_w, B, 0, st>>>(s);
       k_sr_aniso_splat<<<grid_w, B, 0, st>>>(s);
+      if (vel) k_sr_vel_splat<<<grid_w, B, 0, st>>>(s);
     }
   }
   k_sr_fix_to_field<<<grid_c, B, 0, st>>>(s, cells);
@@ -899,6 +994,10 @@ int nn_sr_dual_contouring(nn_sr_ctx* c, const nn_sr_params* p, const float* pos,
     k_sr_normals<<<std::max(1, std::min((c->nv + B - 1) / B, c->sms * 8)), B, 0, st>>>(s, c->nv);
     SRCK(cudaGetLastError());
   }
+  if (vel && c->nv > 0) {  // process_velocity (srtool.py:1298-1300); a zero field without the smooth splat
+    k_sr_mesh_velocity<<<std::max(1, std::min((c->nv + B - 1) / B, c->sms * 8)), B, 0, st>>>(s, c->nv);
+    SRCK(cudaGetLastError());
+  }
   c->last = s;
   c->cells = cells;
   c->n = n;
@@ -907,7 +1006,7 @@ int nn_sr_dual_contouring(nn_sr_ctx* c, const nn_sr_params* p, const float* pos,
 }
 
 int nn_sr_get_mesh(nn_sr_ctx* c, int32_t* num_vertices, int32_t* num_indices, float* vertices, int32_t* indices,
-                   float* normals, void* stream) {
+                   float* normals, float* velocities, void* stream) {
   if (!c) return NN_ERR_INVALID_ARG;
   if (!c->have) return sr_fail_host(c, NN_ERR_STATE, "no mesh: run nn_sr_dual_contouring first");
   cudaStream_t st = (cudaStream_t)stream;
@@ -920,6 +1019,10 @@ int nn_sr_get_mesh(nn_sr_ctx* c, int32_t* num_vertices, int32_t* num_indices, fl
   if (normals && c->nv) {
     if (!c->last.record_normals) return sr_fail_host(c, NN_ERR_STATE, "normals were not recorded");
     SRCK(cudaMemcpyAsync(normals, c->nrm, 3 * (size_t)c->nv * sizeof(float), cudaMemcpyDeviceToDevice, st));
+  }
+  if (velocities && c->nv) {
+    if (!c->last.vel) return sr_fail_host(c, NN_ERR_STATE, "velocities were not recorded");
+    SRCK(cudaMemcpyAsync(velocities, c->mvel, 3 * (size_t)c->nv * sizeof(float), cudaMemcpyDeviceToDevice, st));
   }
   return NN_OK;
 }

@@ -3,7 +3,7 @@
 
 Same constructor arguments, `dual_contouring(...)` call and mesh attributes
 (`mesh_vertex`, `mesh_index`, `num_vertices[None]`, `num_indices[None]`,
-`mesh_normal`) as the reference, so `SPH/surf_recon/example.py` works unchanged apart
+`mesh_normal`, `mesh_velocity`) as the reference, so `SPH/surf_recon/example.py` works unchanged apart
 from the import:
 
     sr = SRTool([[0, 0, 0], [1, 1, 1]], voxel_size=0.01, particle_radius=0.02,
@@ -11,9 +11,9 @@ from the import:
     sr.dual_contouring(isolevel=0, smooth_radius=0.06, num_particles=n, pos=positions)
     sr.export_mesh("out.ply")
 
-`pos` is a [n, 3] array (torch on the GPU, or numpy). The mesh stays on the GPU as
-torch tensors. Only the dual-contouring path exists: the reference's marching cubes
-(srtool.py:1765-1800) and velocity recording are not built.
+`pos` (and `velocity`, with `record_velocity=True`) is a [n, 3] array (torch on the
+GPU, or numpy). The mesh stays on the GPU as torch tensors. Only the dual-contouring
+path exists: the reference's marching cubes (srtool.py:1765-1800) is not built.
 """
 from __future__ import annotations
 
@@ -44,12 +44,12 @@ def _sr_lib():
     L = lib()
     if not getattr(L, "_sr_bound", False):
         vp, i32, i64 = C.c_void_p, C.c_int32, C.c_int64
-        L.nn_sr_create.argtypes = [i32, i64, i32, i32, C.POINTER(vp)]
+        L.nn_sr_create.argtypes = [i32, i64, i32, i32, i32, C.POINTER(vp)]
         L.nn_sr_destroy.argtypes = [vp]
         L.nn_sr_last_error.argtypes = [vp]
         L.nn_sr_last_error.restype = C.c_char_p
-        L.nn_sr_dual_contouring.argtypes = [vp, C.POINTER(_abi.nn_sr_params), vp, i32, vp]
-        L.nn_sr_get_mesh.argtypes = [vp, C.POINTER(i32), C.POINTER(i32), vp, vp, vp, vp]
+        L.nn_sr_dual_contouring.argtypes = [vp, C.POINTER(_abi.nn_sr_params), vp, vp, i32, vp]
+        L.nn_sr_get_mesh.argtypes = [vp, C.POINTER(i32), C.POINTER(i32), vp, vp, vp, vp, vp]
         L.nn_sr_get_stage.argtypes = [vp, i32, vp, vp, vp, vp, C.POINTER(C.c_double), vp]
         for f in ("nn_sr_create", "nn_sr_destroy", "nn_sr_dual_contouring", "nn_sr_get_mesh", "nn_sr_get_stage"):
             getattr(L, f).restype = C.c_int
@@ -61,14 +61,12 @@ class SRTool:
     def __init__(self, bounding_box_extent, voxel_size=0.01, particle_radius=0.01, record_normals=False,
                  record_velocity=False, max_num_vertices=8000000, max_num_indices=100000000,
                  max_num_particles=9000000, hash_level_dimensions=None, device="cuda"):
-        if record_velocity:
-            raise NotImplementedError("SRTool(record_velocity=True) is not built")
         self.bounding_box_extent = [[float(v) for v in bounding_box_extent[0]],
                                     [float(v) for v in bounding_box_extent[1]]]
         self.voxel_size = float(voxel_size)
         self.radius = float(particle_radius)
         self.record_normals = bool(record_normals)
-        self.record_velocity = False
+        self.record_velocity = bool(record_velocity)
         self.max_num_vertices = int(max_num_vertices)
         self.max_num_indices = int(max_num_indices)
         self.max_num_particles = int(max_num_particles)
@@ -80,6 +78,7 @@ class SRTool:
         self.mesh_vertex = torch.zeros((0, 3), dtype=torch.float32, device=self.device)
         self.mesh_index = torch.zeros(0, dtype=torch.int32, device=self.device)
         self.mesh_normal = torch.zeros((0, 3), dtype=torch.float32, device=self.device)
+        self.mesh_velocity = torch.zeros((0, 3), dtype=torch.float32, device=self.device)
         self._h = None
         self._cells = 0
         self.last_params = None
@@ -100,7 +99,7 @@ class SRTool:
         self.close()
         h = C.c_void_p()
         rc = _sr_lib().nn_sr_create(self.max_num_particles, int(cells), self.max_num_vertices, self.max_num_indices,
-                                    C.byref(h))
+                                    _abi.NN_SR_VELOCITY if self.record_velocity else 0, C.byref(h))
         if rc != 0:
             raise NNError(rc, "nn_sr_create failed")
         self._h, self._cells = h, int(cells)
@@ -128,32 +127,42 @@ class SRTool:
     def dual_contouring(self, isolevel, smooth_radius, num_particles, pos, velocity=None,
                         use_smooth_fluid_field=True, record_normals=True):
         """SRTool.dual_contouring (srtool.py:1264-1304). `record_normals` is accepted
-        and, as in the reference, ignored: the constructor's flag decides."""
-        if velocity is not None:
-            raise NotImplementedError("velocity recording is not built")
+        and, as in the reference, ignored: the constructor's flags decide; `velocity`
+        is used when the tool records velocities."""
         n = int(num_particles)
-        if torch.is_tensor(pos):
-            p = pos[:n].to(device=self.device, dtype=torch.float32).contiguous()
-        else:
-            p = torch.as_tensor(np.asarray(pos)[:n], dtype=torch.float32, device=self.device).contiguous()
+
+        def dev(a):
+            if torch.is_tensor(a):
+                return a[:n].to(device=self.device, dtype=torch.float32).contiguous()
+            return torch.as_tensor(np.asarray(a)[:n], dtype=torch.float32, device=self.device).contiguous()
+        p = dev(pos)
+        vel = None
+        if self.record_velocity:
+            if velocity is None:
+                raise ValueError("SRTool(record_velocity=True) needs the particle velocities")
+            vel = dev(velocity)
         dims = self.grid_dims(smooth_radius, use_smooth_fluid_field)
         self._ensure(dims[0] * dims[1] * dims[2])
         prm = _abi.make_sr_params(dims, self.bounding_box_extent[0], self.voxel_size, self.radius, smooth_radius,
                                   isolevel, use_smooth_field=use_smooth_fluid_field,
                                   record_normals=self.record_normals)
         stream = C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
-        self._rc(_sr_lib().nn_sr_dual_contouring(self._h, C.byref(prm), C.c_void_p(p.data_ptr()), n, stream))
+        self._rc(_sr_lib().nn_sr_dual_contouring(self._h, C.byref(prm), C.c_void_p(p.data_ptr()),
+                                                 C.c_void_p(vel.data_ptr()) if vel is not None else None, n, stream))
         nv, ni = C.c_int32(), C.c_int32()
-        self._rc(_sr_lib().nn_sr_get_mesh(self._h, C.byref(nv), C.byref(ni), None, None, None, stream))
+        self._rc(_sr_lib().nn_sr_get_mesh(self._h, C.byref(nv), C.byref(ni), None, None, None, None, stream))
         self.mesh_vertex = torch.empty((nv.value, 3), dtype=torch.float32, device=self.device)
         self.mesh_index = torch.empty(ni.value, dtype=torch.int32, device=self.device)
         self.mesh_normal = torch.empty((nv.value if self.record_normals else 0, 3), dtype=torch.float32,
                                        device=self.device)
+        self.mesh_velocity = torch.empty((nv.value if self.record_velocity else 0, 3), dtype=torch.float32,
+                                         device=self.device)
 
         def ptr(t):
             return C.c_void_p(t.data_ptr()) if t.numel() else None
         self._rc(_sr_lib().nn_sr_get_mesh(self._h, None, None, ptr(self.mesh_vertex), ptr(self.mesh_index),
-                                          ptr(self.mesh_normal) if self.record_normals else None, stream))
+                                          ptr(self.mesh_normal) if self.record_normals else None,
+                                          ptr(self.mesh_velocity) if self.record_velocity else None, stream))
         self.num_vertices = _Scalar(nv.value)
         self.num_indices = _Scalar(ni.value)
         self.last_params = prm
@@ -180,11 +189,11 @@ class SRTool:
 
     def export_mesh(self, file_path: str, output_normal=False, output_velocity=False):
         """Binary little-endian PLY with the vertices, triangles and optionally the
-        normals (export_mesh, srtool.py:1802-1838)."""
+        normals and the velocities (export_mesh, srtool.py:1802-1838)."""
         if not file_path.endswith("ply"):
             raise ValueError("Output file must be in ply format!")
-        if output_velocity:
-            raise NotImplementedError("velocity recording is not built")
+        if output_velocity and len(self.mesh_velocity) != len(self.mesh_vertex):
+            raise RuntimeError("velocities were not recorded: SRTool(record_velocity=True)")
         v = self.mesh_vertex.cpu().numpy().astype("<f4")
         f = self.mesh_index.cpu().numpy().astype("<i4").reshape(-1, 3)
         if output_normal and len(self.mesh_normal) != len(v):
@@ -193,8 +202,15 @@ class SRTool:
                 "property float x", "property float y", "property float z"]
         if output_normal:
             head += ["property float nx", "property float ny", "property float nz"]
+        if output_velocity:
+            head += ["property float vx", "property float vy", "property float vz"]
         head += [f"element face {len(f)}", "property list uchar int vertex_indices", "end_header"]
-        vert = np.concatenate([v, self.mesh_normal.cpu().numpy().astype("<f4")], axis=1) if output_normal else v
+        cols = [v]
+        if output_normal:
+            cols.append(self.mesh_normal.cpu().numpy().astype("<f4"))
+        if output_velocity:
+            cols.append(self.mesh_velocity.cpu().numpy().astype("<f4"))
+        vert = np.concatenate(cols, axis=1)
         face = np.zeros(len(f), dtype=[("n", "u1"), ("i", "<i4", (3,))])
         face["n"] = 3
         face["i"] = f

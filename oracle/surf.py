@@ -121,3 +121,26 @@ def contour(params: _abi.nn_sr_params, field: np.ndarray, active: np.ndarray, ma
     _check(lib().sro_contour(C.byref(params), _p(f), _p(a), _p(v), max_vertices, _p(idx), max_indices, _p(nrm),
                              C.byref(nv), C.byref(ni)))
     return {"vertices": v[: nv.value], "indices": idx[: ni.value], "normals": nrm[: nv.value]}
+
+
+def vel_field(params, pos, vel):
+    pos = np.ascontiguousarray(pos, np.float32)
+    vel = np.ascontiguousarray(vel, np.float32)
+    dims, cells, _ = _shape(params)
+    f = np.zeros(3 * cells, np.float64)
+    L = lib()
+    L.sro_vel_field.argtypes = [C.POINTER(_abi.nn_sr_params), C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]
+    L.sro_vel_field.restype = C.c_int
+    _check(L.sro_vel_field(C.byref(params), _p(pos), _p(vel), pos.shape[0], _p(f)))
+    return f
+
+
+def mesh_velocity(params, vfield, vertices):
+    v = np.ascontiguousarray(vertices, np.float64)
+    out = np.zeros_like(v)
+    L = lib()
+    L.sro_mesh_velocity.argtypes = [C.POINTER(_abi.nn_sr_params), C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]
+    L.sro_mesh_velocity.restype = C.c_int
+    _check(L.sro_mesh_velocity(C.byref(params), _p(np.ascontiguousarray(vfield, np.float64)), _p(v), len(v),
+                               _p(out)))
+    return out

@@ -18,6 +18,8 @@
 //                         process_normal_at 1335-1349, calc_vertex_normal 1306-1321)
 //   dual_contouring_polygen 1707-1763 (get_edge_adjacent_cubes 1612-1705)
 //   process_normal        srtool.py:1383-1410
+//   generate_smooth_fluid_field_with_velocity_impl (velocity part) 1159-1190,
+//   process_velocity      srtool.py:1351-1381
 //
 // Taichi's sparse fields are emulated with one "active" flag per 32^3 block of
 // vertices (the reference's leaf blocks are dense 32^3 under pointer levels): a
@@ -566,6 +568,65 @@ int sro_dual_contouring(const nn_sr_params* prm, const float* pos, int32_t n, do
   if (G_out) std::memcpy(G_out, G.data(), sizeof(float) * 9 * n);
   if (xbar_out) std::memcpy(xbar_out, xbar.data(), sizeof(float) * 3 * n);
   return contour(g, prm->isolevel, prm->record_normals, vertices, max_v, indices, max_i, normals, nv, ni);
+}
+
+// generate_smooth_fluid_field_with_velocity_impl's velocity part (srtool.py:1159-1190):
+// vfield [3][cells] (x-fastest per component) gets, for every vertex of every voxel in
+// the smoothing range (once per adjacent voxel), v_i * poly6(x_i - vertex) * vs^3.
+int sro_vel_field(const nn_sr_params* prm, const float* pos, const float* vel, int32_t n, double* vfield) {
+  Grid g = make_grid(prm);
+  std::vector<int> vox;
+  std::vector<std::vector<int>> hash;
+  int rc = bin_particles(g, pos, n, vox, hash);
+  if (rc) return rc;
+  const int64_t cells = (int64_t)g.nx * g.ny * g.nz;
+  std::fill(vfield, vfield + 3 * cells, 0.0);
+  const double sr = prm->smooth_radius, acoeff = 315.0 / (64.0 * kPi), coeff = g.vs * g.vs * g.vs;
+  const int range = smoothing_range(prm), off = range / 2;
+  for (int i = 0; i < n; ++i)
+    for (int dz = 0; dz < range; ++dz)
+      for (int dy = 0; dy < range; ++dy)
+        for (int dx = 0; dx < range; ++dx) {
+          int nx = vox[3 * i] + dx - off, ny = vox[3 * i + 1] + dy - off, nz = vox[3 * i + 2] + dz - off;
+          for (int w = 0; w < 8; ++w) {
+            int x = nx + kOff[w][0], y = ny + kOff[w][1], z = nz + kOff[w][2];
+            if (x < 0 || y < 0 || z < 0) continue;
+            if (!g.in(x, y, z)) return -8;
+            double d0 = pos[3 * i] - (x * g.vs + g.ox), d1 = pos[3 * i + 1] - (y * g.vs + g.oy),
+                   d2 = pos[3 * i + 2] - (z * g.vs + g.oz);
+            const double f = poly6(d0 * d0 + d1 * d1 + d2 * d2, sr, acoeff) * coeff;
+            if (f == 0.0) continue;
+            for (int k = 0; k < 3; ++k) vfield[k * cells + g.idx(x, y, z)] += vel[3 * i + k] * f;
+          }
+        }
+  return 0;
+}
+
+// process_velocity (srtool.py:1351-1381) at the given mesh vertices [nv,3].
+int sro_mesh_velocity(const nn_sr_params* prm, const double* vfield, const double* vertices, int32_t nv,
+                      double* out) {
+  Grid g = make_grid(prm);
+  const int64_t cells = (int64_t)g.nx * g.ny * g.nz;
+  const double vs = (double)(float)g.vs, ox = (double)(float)g.ox, oy = (double)(float)g.oy,
+               oz = (double)(float)g.oz;
+  for (int i = 0; i < nv; ++i) {
+    const double* p = vertices + 3 * i;
+    float pf[3] = {(float)p[0], (float)p[1], (float)p[2]};
+    int x0, y0, z0;
+    voxel_of(g, pf, x0, y0, z0);
+    const double xd = (p[0] - (x0 * vs + ox)) / vs, yd = (p[1] - (y0 * vs + oy)) / vs, zd = (p[2] - (z0 * vs + oz)) / vs;
+    double acc[3] = {0, 0, 0};
+    for (int a = 0; a < 2; ++a)
+      for (int b = 0; b < 2; ++b)
+        for (int e = 0; e < 2; ++e) {
+          const int x = x0 + a, y = y0 + b, z = z0 + e;
+          if (!g.in(x, y, z)) continue;
+          const double w = (a ? xd : 1 - xd) * (b ? yd : 1 - yd) * (e ? zd : 1 - zd);
+          for (int k = 0; k < 3; ++k) acc[k] += w * vfield[k * cells + g.idx(x, y, z)];
+        }
+    for (int k = 0; k < 3; ++k) out[3 * i + k] = acc[k];
+  }
+  return 0;
 }
 
 }  // extern "C"

@@ -116,3 +116,35 @@ def test_surface_errors(cuda_lib):
     # the context stays usable after an error
     sr.dual_contouring(isolevel=0.0, smooth_radius=0.06, num_particles=len(pos), pos=pos)
     assert sr.num_vertices[None] > 0
+
+
+def test_surface_velocity_matches_oracle(cuda_lib, surf, tmp_path):
+    """SRTool(record_velocity=True): the vertex velocity splat and the mesh velocities
+    (process_velocity) against the oracle at the CUDA mesh's vertices, 1e-5 of the
+    velocities' scale; the mesh itself is the one a run without velocities makes."""
+    pos = ball(seed=15)
+    rng = np.random.default_rng(16)
+    vel = (rng.normal(size=pos.shape) + np.array([0.0, -1.0, 0.5])).astype(np.float32)
+    sr = _tool(record_velocity=True)
+    sr.dual_contouring(isolevel=0.0, smooth_radius=0.06, num_particles=len(pos), pos=torch.from_numpy(pos).cuda(),
+                       velocity=torch.from_numpy(vel).cuda())
+    plain = _tool()
+    plain.dual_contouring(isolevel=0.0, smooth_radius=0.06, num_particles=len(pos), pos=torch.from_numpy(pos).cuda())
+    assert torch.equal(sr.mesh_vertex, plain.mesh_vertex) and torch.equal(sr.mesh_index, plain.mesh_index)
+    nv = sr.num_vertices[None]
+    assert nv > 0 and sr.mesh_velocity.shape == (nv, 3)
+    vf = surf.vel_field(sr.last_params, pos, vel)
+    ref = surf.mesh_velocity(sr.last_params, vf, sr.mesh_vertex.cpu().numpy())
+    assert _scale_err(sr.mesh_velocity.cpu().numpy(), ref) < 1e-5
+    # PLY with normals and velocities
+    path = str(tmp_path / "vel.ply")
+    sr.export_mesh(path, output_normal=True, output_velocity=True)
+    head, body = open(path, "rb").read().split(b"end_header\n", 1)
+    assert b"property float vx" in head
+    v = np.frombuffer(body[: nv * 36], "<f4").reshape(nv, 9)
+    assert np.array_equal(v[:, 6:], sr.mesh_velocity.cpu().numpy())
+    # a tool without velocity recording refuses to export them; one with it needs them
+    with pytest.raises(RuntimeError):
+        plain.export_mesh(str(tmp_path / "x.ply"), output_velocity=True)
+    with pytest.raises(ValueError):
+        sr.dual_contouring(isolevel=0.0, smooth_radius=0.06, num_particles=len(pos), pos=pos)

@@ -72,3 +72,30 @@ def test_oracle_rejects_particles_outside_the_grid(surf):
     pos[5] = [-1.0, 0.5, 0.5]
     with pytest.raises(RuntimeError):
         surf.dual_contouring(default_params(), pos)
+
+
+def test_oracle_velocity_field_of_a_uniform_flow(surf):
+    """A uniform particle velocity u gives vertex velocities u * W, W the poly6
+    weight sum (srtool.py:1159-1190), and mesh velocities that are trilinear blends
+    of those (process_velocity, srtool.py:1351-1381): exact at grid vertices."""
+    pos = block(seed=21, n=(5, 4, 3))
+    prm = default_params()
+    u = np.array([0.5, -2.0, 0.25], np.float32)
+    vf = surf.vel_field(prm, pos, np.tile(u, (len(pos), 1))).reshape(3, -1)
+    w = vf[0] / u[0]
+    assert w.max() > 0
+    assert np.allclose(vf[1], u[1] * w, rtol=1e-12, atol=0) and np.allclose(vf[2], u[2] * w, rtol=1e-12, atol=0)
+    # linear in the velocities
+    rng = np.random.default_rng(3)
+    a, b = rng.normal(size=(2, len(pos), 3)).astype(np.float32)
+    lin = surf.vel_field(prm, pos, a) + surf.vel_field(prm, pos, b) - surf.vel_field(prm, pos, (a + b))
+    assert np.abs(lin).max() < 1e-6 * np.abs(surf.vel_field(prm, pos, a)).max()
+    # at a grid vertex the blend is that vertex's velocity; half-way, the mean of two
+    dims = list(prm.dims)
+    k = int(np.argmax(w))
+    z, y, x = np.unravel_index(k, (dims[2], dims[1], dims[0]))
+    vs = prm.voxel_size
+    pts = np.array([[x * vs, y * vs, z * vs], [(x + 0.5) * vs, y * vs, z * vs]], np.float64)
+    mv = surf.mesh_velocity(prm, vf.reshape(-1), pts)
+    assert np.allclose(mv[0], vf[:, k], rtol=1e-6)
+    assert np.allclose(mv[1], 0.5 * (vf[:, k] + vf[:, k + 1]), rtol=1e-6)
