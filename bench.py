@@ -406,7 +406,8 @@ SR_LAUNCHES = 26  # kernels one SRTool.dual_contouring call launches (three 3-ke
 def run_surface(args, world, rank):
     """SRTool.dual_contouring on the surface workload; one step is one reconstruction.
     `value` = particles / s with the positions resident; `e2e` copies the positions in
-    from pinned host memory and the mesh out, each step."""
+    from pinned host memory and the mesh out, each step. `marching_cubes` times the same
+    pipeline ending in marching cubes (outside the step count)."""
     import torch
 
     from nonnewton_b200.surface import SRTool
@@ -451,6 +452,18 @@ def run_surface(args, world, rank):
     e1.synchronize()
     del hv, hi
     e2e_ms = max_over_ranks(e0.elapsed_time(e1), world)
+    # the same pipeline ending in marching cubes (SRTool.marching_cubes), timed beside it
+    for _ in range(max(args.warmup, 1)):
+        sr.marching_cubes(pos=d_pos, **kw)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    mc_steps = min(args.steps, 10)
+    e0.record(stream)
+    for _ in range(mc_steps):
+        sr.marching_cubes(pos=d_pos, **kw)
+    e1.record(stream)
+    e1.synchronize()
+    mc_ms = max_over_ranks(e0.elapsed_time(e1), world) / mc_steps
+    mc_mesh = {"vertices": sr.num_vertices[None], "triangles": sr.num_indices[None] // 3}
     if rank != 0:
         return
     dims = list(sr.last_params.dims)
@@ -469,6 +482,8 @@ def run_surface(args, world, rank):
                      "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "peak_source": f"{peak_kind} hbm_gbs",
                      "alg_bytes_per_launch": ab, "traffic": None},
         "gpu_launches": SR_LAUNCHES * args.steps,
+        "marching_cubes": {"ms_per_call": mc_ms, "particles_per_s": nf / (mc_ms / 1e3), "calls": mc_steps,
+                           "mesh": mc_mesh},
         "e2e": {"value": nf * args.steps / (e2e_ms / 1e3), "unit": "particles/s", "h2d_bytes_per_step": nf * 12,
                 "d2h_bytes_per_step": nv * 12 + ni * 4},
         "clocks": cs.summary(),

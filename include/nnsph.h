@@ -335,12 +335,24 @@ const char* nn_sr_last_error(const nn_sr_ctx* ctx);
 int nn_sr_dual_contouring(nn_sr_ctx* ctx, const nn_sr_params* params, const float* pos, const float* vel,
                           int32_t n, void* cuda_stream);
 
+/* The same pipeline with marching cubes in place of dual contouring
+   (SRTool.marching_cube_impl, srtool.py:1765-1800, which has no caller in the
+   reference: its public entry is dual_contouring alone). Each cube emits one vertex
+   per crossing edge, in edge order, as the reference does (vertices are not shared
+   between cubes). The triangles come from this library's own case table, derived
+   from the corner states by a face walk (in-corners kept separate on ambiguous
+   faces), not from the reference's 256-case table; the surface is closed. Same
+   arguments, errors and synchronisation as nn_sr_dual_contouring. */
+int nn_sr_marching_cubes(nn_sr_ctx* ctx, const nn_sr_params* params, const float* pos, const float* vel,
+                         int32_t n, void* cuda_stream);
+
 /* The mesh of the last call: counts, and copies into caller device buffers when
    non-NULL: vertices [num_vertices,3] f32, indices [num_indices] i32 (triangles),
    normals [num_vertices,3] f32 (when record_normals was set), velocities
    [num_vertices,3] f32 (when velocities were given). Vertices are numbered
-   by the linear index of their cube, triangles ordered by cube and then by edge
-   (x, y, z edges of the cube's first corner). */
+   by the linear index of their cube (marching cubes: then by edge), triangles
+   ordered by cube and then by edge (dual contouring: the x, y, z edges of the cube's
+   first corner; marching cubes: the case table's order). */
 int nn_sr_get_mesh(nn_sr_ctx* ctx, int32_t* num_vertices, int32_t* num_indices, float* vertices,
                    int32_t* indices, float* normals, float* velocities, void* cuda_stream);
 

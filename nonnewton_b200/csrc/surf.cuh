@@ -746,6 +746,120 @@ __global__ void k_sr_tris(SrDev s, int64_t cells, int pass) {
   }
 }
 
+// ---- 6b. marching cubes (marching_cube_impl, srtool.py:1765-1800) ----------------------
+// The reference's 256-case triangle table is not reproduced. This build's table is
+// computed at compile time from the corner states of each case ("in": value <
+// isolevel): faces list their corners counter-clockwise seen from outside; on a face,
+// every run of in-corners gets one segment from the edge where the walk leaves the run
+// to the edge where it entered it (in-corners stay separate on ambiguous faces, which
+// depends on the face alone, so neighbouring cubes agree and the surface is closed);
+// the segments chain into loops over the crossing edges; loops are taken in order of
+// their smallest edge id, start there, and are fanned as (l0, l[k+1], l[k]).
+#define SR_MC_MAXT 5
+struct SrMcTable {
+  uint16_t edges[256];               // crossing edges of each case
+  uint8_t ntri[256];
+  int8_t tri[256][SR_MC_MAXT][3];    // edge ids
+  bool overflow;                     // a case needs more than SR_MC_MAXT triangles
+};
+
+constexpr int sr_mc_edge_of(const int8_t (&e)[12][2], int c0, int c1) {
+  for (int w = 0; w < 12; ++w)
+    if ((e[w][0] == c0 && e[w][1] == c1) || (e[w][0] == c1 && e[w][1] == c0)) return w;
+  return -1;
+}
+
+constexpr SrMcTable sr_make_mc_table() {
+  // the same corner offsets and edges as c_sr_off and c_sr_edge (srtool.py:775-783, 931-942)
+  const int8_t off[8][3] = {{0, 1, 0}, {1, 1, 0}, {1, 0, 0}, {0, 0, 0}, {0, 1, 1}, {1, 1, 1}, {1, 0, 1}, {0, 0, 1}};
+  const int8_t edge[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6}, {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
+  SrMcTable t{};
+  for (int ci = 0; ci < 256; ++ci) {
+    int next[12] = {-1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1};
+    for (int a = 0; a < 3; ++a)
+      for (int side = 0; side < 2; ++side) {
+        const int u = (a + 1) % 3, v = (a + 2) % 3;
+        int uv[4][2] = {{0, 0}, {1, 0}, {1, 1}, {0, 1}};  // counter-clockwise around +e_a
+        if (side == 0) { uv[1][0] = 0; uv[1][1] = 1; uv[3][0] = 1; uv[3][1] = 0; }
+        int q[4] = {0, 0, 0, 0};
+        for (int k = 0; k < 4; ++k)
+          for (int c = 0; c < 8; ++c)
+            if (off[c][a] == side && off[c][u] == uv[k][0] && off[c][v] == uv[k][1]) q[k] = c;
+        bool in[4] = {false, false, false, false};
+        for (int k = 0; k < 4; ++k) in[k] = (ci >> q[k]) & 1;
+        for (int k = 0; k < 4; ++k) {
+          if (!in[k] || in[(k + 1) % 4]) continue;  // the walk leaves a run of in-corners at q[k]
+          int j = k;
+          while (in[(j + 3) % 4]) j = (j + 3) % 4;  // the run starts at q[j]
+          next[sr_mc_edge_of(edge, q[k], q[(k + 1) % 4])] = sr_mc_edge_of(edge, q[(j + 3) % 4], q[j]);
+        }
+      }
+    bool seen[12] = {false, false, false, false, false, false, false, false, false, false, false, false};
+    int nt = 0;
+    for (int e = 0; e < 12; ++e) {
+      if (next[e] < 0) continue;
+      t.edges[ci] = (uint16_t)(t.edges[ci] | (1u << e));
+      if (seen[e]) continue;
+      int loop[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+      int m = 0;
+      for (int f = e; !seen[f]; f = next[f]) {
+        seen[f] = true;
+        loop[m++] = f;
+      }
+      for (int k = 1; k + 1 < m; ++k) {
+        if (nt == SR_MC_MAXT) { t.overflow = true; break; }
+        t.tri[ci][nt][0] = (int8_t)loop[0];
+        t.tri[ci][nt][1] = (int8_t)loop[k + 1];
+        t.tri[ci][nt][2] = (int8_t)loop[k];
+        ++nt;
+      }
+    }
+    t.ntri[ci] = (uint8_t)nt;
+  }
+  return t;
+}
+static_assert(!sr_make_mc_table().overflow, "a marching-cubes case needs more than SR_MC_MAXT triangles");
+__constant__ SrMcTable c_sr_mc = sr_make_mc_table();
+
+// pass 0: vertices (crossing edges) and indices per cube into vflag / tcount;
+// pass 1: both written at the scanned offsets, in edge order within a cube
+__global__ void k_sr_mc(SrDev s, int64_t cells, int pass) {
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < cells; c += (int64_t)gridDim.x * blockDim.x) {
+    const int x = (int)(c % s.g.nx), y = (int)((c / s.g.nx) % s.g.ny), z = (int)(c / ((int64_t)s.g.nx * s.g.ny));
+    if (pass == 1 && s.vflag[c + 1] == s.vflag[c]) continue;
+    // a cube with a crossing has a nonzero corner, which lies in an active block: the
+    // reference's visit of the cubes around the active vertices reaches every such cube
+    const int ci = sr_cube_mask(s, x, y, z);
+    const uint32_t em = c_sr_mc.edges[ci];
+    if (pass == 0) {
+      s.vflag[c] = __popc(em);
+      s.tcount[c] = 3u * c_sr_mc.ntri[ci];
+      continue;
+    }
+    const int64_t vb = s.vflag[c], tb = s.tcount[c];
+    const int nt = c_sr_mc.ntri[ci];
+    if (vb + __popc(em) > s.max_v || tb + 3 * nt > s.max_i) { sr_fail(s, NN_ERR_CAPACITY); continue; }
+    for (int w = 0; w < 12; ++w) {
+      if (!((em >> w) & 1u)) continue;
+      const int a = c_sr_edge[w][0], b = c_sr_edge[w][1];
+      const int ax = x + c_sr_off[a][0], ay = y + c_sr_off[a][1], az = z + c_sr_off[a][2];
+      const int bx = x + c_sr_off[b][0], by = y + c_sr_off[b][1], bz = z + c_sr_off[b][2];
+      const double v1 = sr_get(s, s.field, ax, ay, az), v2 = sr_get(s, s.field, bx, by, bz);
+      const double delta = v2 - v1;
+      const double t = fabs(delta) < 1e-5 ? 0.5 : ((double)s.iso - v1) / delta;  // vertex_interpolate
+      const double p1[3] = {ax * s.g.dvs + s.g.dox, ay * s.g.dvs + s.g.doy, az * s.g.dvs + s.g.doz};
+      const double p2[3] = {bx * s.g.dvs + s.g.dox, by * s.g.dvs + s.g.doy, bz * s.g.dvs + s.g.doz};
+      const int64_t v = vb + __popc(em & ((1u << w) - 1u));
+      for (int k = 0; k < 3; ++k) s.vert[3 * v + k] = (float)(p1[k] + t * (p2[k] - p1[k]));
+    }
+    for (int q = 0; q < nt; ++q)
+      for (int k = 0; k < 3; ++k) {
+        const int w = c_sr_mc.tri[ci][q][k];
+        s.tri[tb + 3 * q + k] = (int32_t)(vb + __popc(em & ((1u << w) - 1u)));
+      }
+  }
+}
+
 // ---- 7. vertex normals (process_normal) ----------------------------------------------
 __global__ void k_sr_normals(SrDev s, int nv) {
   GRID_STRIDE(i, min(nv, s.max_v)) {
@@ -870,19 +984,22 @@ int nn_sr_destroy(nn_sr_ctx* c) {
 
 const char* nn_sr_last_error(const nn_sr_ctx* c) { return c ? c->err.c_str() : "null context"; }
 
-int nn_sr_dual_contouring(nn_sr_ctx* c, const nn_sr_params* p, const float* pos, const float* vel, int32_t n,
-                          void* stream) {
+// The shared pipeline of SRTool.dual_contouring (srtool.py:1264-1304): binning, splats,
+// smoothing, then dual contouring or marching cubes, normals and velocities.
+static int sr_run(nn_sr_ctx* c, const nn_sr_params* p, const float* pos, const float* vel, int32_t n, void* stream,
+                  bool marching_cubes) {
   if (!c) return NN_ERR_INVALID_ARG;
+  const char* fn = marching_cubes ? "nn_sr_marching_cubes" : "nn_sr_dual_contouring";
   c->have = false;
   if (!p || p->size != (int32_t)sizeof(nn_sr_params) || (!pos && n > 0) || n < 0)
-    return sr_fail_host(c, NN_ERR_INVALID_ARG, "nn_sr_dual_contouring: invalid argument");
+    return sr_fail_host(c, NN_ERR_INVALID_ARG, "%s: invalid argument", fn);
   if (n > c->max_particles)
     return sr_fail_host(c, NN_ERR_CAPACITY, "%d particles exceed the context's %d", n, c->max_particles);
   if (vel && !c->vfix)
     return sr_fail_host(c, NN_ERR_STATE, "velocities given to a context created without NN_SR_VELOCITY");
   if (!(p->voxel_size > 0) || !(p->smooth_radius > 0) || !(p->particle_radius > 0) || p->dims[0] <= 0 ||
       p->dims[1] <= 0 || p->dims[2] <= 0 || p->smooth_iterations < 0 || p->smooth_cells < 0)
-    return sr_fail_host(c, NN_ERR_INVALID_ARG, "nn_sr_dual_contouring: bad parameters");
+    return sr_fail_host(c, NN_ERR_INVALID_ARG, "%s: bad parameters", fn);
   const int64_t cells = (int64_t)p->dims[0] * p->dims[1] * p->dims[2];
   const int bx = (p->dims[0] + NN_SR_BLOCK - 1) / NN_SR_BLOCK, by = (p->dims[1] + NN_SR_BLOCK - 1) / NN_SR_BLOCK,
             bz = (p->dims[2] + NN_SR_BLOCK - 1) / NN_SR_BLOCK;
@@ -961,16 +1078,24 @@ int nn_sr_dual_contouring(nn_sr_ctx* c, const nn_sr_params* p, const float* pos,
     k_sr_smooth<<<grid_c, B, 0, st>>>(s, cells);
     std::swap(s.field, s.tmp);
   }
-  // 6. dual contouring
   SRCK(cudaMemsetAsync(c->vflag, 0, (cells + 1) * sizeof(uint32_t), st));
-  k_sr_dc_flag<<<grid_c, B, 0, st>>>(s, cells);
-  RC(sr_scan(c, c->vflag, cells + 1, st));
-  k_sr_dc_list<<<grid_c, B, 0, st>>>(s, cells);
-  k_sr_dc_point<<<c->sms * 4, 128, 0, st>>>(s, cells);
   SRCK(cudaMemsetAsync(c->tcount, 0, (cells + 1) * sizeof(uint32_t), st));
-  k_sr_tris<<<grid_c, B, 0, st>>>(s, cells, 0);
-  RC(sr_scan(c, c->tcount, cells + 1, st));
-  k_sr_tris<<<grid_c, B, 0, st>>>(s, cells, 1);
+  if (marching_cubes) {
+    // 6b. marching cubes: count, scan, write
+    k_sr_mc<<<grid_c, B, 0, st>>>(s, cells, 0);
+    RC(sr_scan(c, c->vflag, cells + 1, st));
+    RC(sr_scan(c, c->tcount, cells + 1, st));
+    k_sr_mc<<<grid_c, B, 0, st>>>(s, cells, 1);
+  } else {
+    // 6. dual contouring
+    k_sr_dc_flag<<<grid_c, B, 0, st>>>(s, cells);
+    RC(sr_scan(c, c->vflag, cells + 1, st));
+    k_sr_dc_list<<<grid_c, B, 0, st>>>(s, cells);
+    k_sr_dc_point<<<c->sms * 4, 128, 0, st>>>(s, cells);
+    k_sr_tris<<<grid_c, B, 0, st>>>(s, cells, 0);
+    RC(sr_scan(c, c->tcount, cells + 1, st));
+    k_sr_tris<<<grid_c, B, 0, st>>>(s, cells, 1);
+  }
   SRCK(cudaGetLastError());
   uint32_t counts[2];
   int32_t status = 0;
@@ -1005,10 +1130,20 @@ int nn_sr_dual_contouring(nn_sr_ctx* c, const nn_sr_params* p, const float* pos,
   return NN_OK;
 }
 
+int nn_sr_dual_contouring(nn_sr_ctx* c, const nn_sr_params* p, const float* pos, const float* vel, int32_t n,
+                          void* stream) {
+  return sr_run(c, p, pos, vel, n, stream, false);
+}
+
+int nn_sr_marching_cubes(nn_sr_ctx* c, const nn_sr_params* p, const float* pos, const float* vel, int32_t n,
+                         void* stream) {
+  return sr_run(c, p, pos, vel, n, stream, true);
+}
+
 int nn_sr_get_mesh(nn_sr_ctx* c, int32_t* num_vertices, int32_t* num_indices, float* vertices, int32_t* indices,
                    float* normals, float* velocities, void* stream) {
   if (!c) return NN_ERR_INVALID_ARG;
-  if (!c->have) return sr_fail_host(c, NN_ERR_STATE, "no mesh: run nn_sr_dual_contouring first");
+  if (!c->have) return sr_fail_host(c, NN_ERR_STATE, "no mesh: run nn_sr_dual_contouring or nn_sr_marching_cubes first");
   cudaStream_t st = (cudaStream_t)stream;
   if (num_vertices) *num_vertices = c->nv;
   if (num_indices) *num_indices = c->ni;

@@ -12,8 +12,9 @@ from the import:
     sr.export_mesh("out.ply")
 
 `pos` (and `velocity`, with `record_velocity=True`) is a [n, 3] array (torch on the
-GPU, or numpy). The mesh stays on the GPU as torch tensors. Only the dual-contouring
-path exists: the reference's marching cubes (srtool.py:1765-1800) is not built.
+GPU, or numpy). The mesh stays on the GPU as torch tensors. `marching_cubes(...)`
+takes the same arguments and ends the same pipeline with marching cubes
+(srtool.py:1765-1800) instead of dual contouring.
 """
 from __future__ import annotations
 
@@ -49,9 +50,11 @@ def _sr_lib():
         L.nn_sr_last_error.argtypes = [vp]
         L.nn_sr_last_error.restype = C.c_char_p
         L.nn_sr_dual_contouring.argtypes = [vp, C.POINTER(_abi.nn_sr_params), vp, vp, i32, vp]
+        L.nn_sr_marching_cubes.argtypes = [vp, C.POINTER(_abi.nn_sr_params), vp, vp, i32, vp]
         L.nn_sr_get_mesh.argtypes = [vp, C.POINTER(i32), C.POINTER(i32), vp, vp, vp, vp, vp]
         L.nn_sr_get_stage.argtypes = [vp, i32, vp, vp, vp, vp, C.POINTER(C.c_double), vp]
-        for f in ("nn_sr_create", "nn_sr_destroy", "nn_sr_dual_contouring", "nn_sr_get_mesh", "nn_sr_get_stage"):
+        for f in ("nn_sr_create", "nn_sr_destroy", "nn_sr_dual_contouring", "nn_sr_marching_cubes", "nn_sr_get_mesh",
+                  "nn_sr_get_stage"):
             getattr(L, f).restype = C.c_int
         L._sr_bound = True
     return L
@@ -129,6 +132,19 @@ class SRTool:
         """SRTool.dual_contouring (srtool.py:1264-1304). `record_normals` is accepted
         and, as in the reference, ignored: the constructor's flags decide; `velocity`
         is used when the tool records velocities."""
+        return self._run(_sr_lib().nn_sr_dual_contouring, isolevel, smooth_radius, num_particles, pos, velocity,
+                         use_smooth_fluid_field)
+
+    def marching_cubes(self, isolevel, smooth_radius, num_particles, pos, velocity=None,
+                       use_smooth_fluid_field=True, record_normals=True):
+        """The dual_contouring pipeline with marching cubes as the last stage
+        (marching_cube_impl, srtool.py:1765-1800, which the reference defines but never
+        calls). One vertex per crossing edge of each cube, as the reference emits them;
+        the triangles come from the library's own case table (nn_sr_marching_cubes)."""
+        return self._run(_sr_lib().nn_sr_marching_cubes, isolevel, smooth_radius, num_particles, pos, velocity,
+                         use_smooth_fluid_field)
+
+    def _run(self, entry, isolevel, smooth_radius, num_particles, pos, velocity, use_smooth_fluid_field):
         n = int(num_particles)
 
         def dev(a):
@@ -147,8 +163,8 @@ class SRTool:
                                   isolevel, use_smooth_field=use_smooth_fluid_field,
                                   record_normals=self.record_normals)
         stream = C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
-        self._rc(_sr_lib().nn_sr_dual_contouring(self._h, C.byref(prm), C.c_void_p(p.data_ptr()),
-                                                 C.c_void_p(vel.data_ptr()) if vel is not None else None, n, stream))
+        self._rc(entry(self._h, C.byref(prm), C.c_void_p(p.data_ptr()),
+                       C.c_void_p(vel.data_ptr()) if vel is not None else None, n, stream))
         nv, ni = C.c_int32(), C.c_int32()
         self._rc(_sr_lib().nn_sr_get_mesh(self._h, C.byref(nv), C.byref(ni), None, None, None, None, stream))
         self.mesh_vertex = torch.empty((nv.value, 3), dtype=torch.float32, device=self.device)

@@ -144,3 +144,33 @@ def mesh_velocity(params, vfield, vertices):
     _check(L.sro_mesh_velocity(C.byref(params), _p(np.ascontiguousarray(vfield, np.float64)), _p(v), len(v),
                                _p(out)))
     return out
+
+
+def marching_cubes(params: _abi.nn_sr_params, field: np.ndarray, active: np.ndarray, max_vertices: int = 1 << 21,
+                   max_indices: int = 1 << 23) -> dict:
+    """Marching cubes on a given field [z, y, x] and active-block flags."""
+    f = np.ascontiguousarray(field, np.float64).reshape(-1)
+    a = np.ascontiguousarray(active, np.uint8)
+    v = np.zeros((max_vertices, 3), np.float64)
+    idx = np.zeros(max_indices, np.int32)
+    nrm = np.zeros((max_vertices, 3), np.float64)
+    nv, ni = C.c_int32(), C.c_int32()
+    L = lib()
+    L.sro_marching_cubes.argtypes = [C.POINTER(_abi.nn_sr_params), C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
+                                     C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.sro_marching_cubes.restype = C.c_int
+    _check(L.sro_marching_cubes(C.byref(params), _p(f), _p(a), _p(v), max_vertices, _p(idx), max_indices, _p(nrm),
+                                C.byref(nv), C.byref(ni)))
+    return {"vertices": v[: nv.value], "indices": idx[: ni.value], "normals": nrm[: nv.value]}
+
+
+def mc_table():
+    """(triangle count [256], edge ids [256, 12, 3], -1 past the count) of the oracle's
+    marching-cubes triangulation."""
+    nt = np.zeros(256, np.int32)
+    tris = np.zeros((256, 12, 3), np.int32)
+    L = lib()
+    L.sro_mc_table.argtypes = [C.c_void_p, C.c_void_p]
+    L.sro_mc_table.restype = C.c_int
+    _check(L.sro_mc_table(_p(nt), _p(tris)))
+    return nt, tris

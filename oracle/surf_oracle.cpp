@@ -297,6 +297,108 @@ int contour(const Grid& g, double iso, int record_normals, double* vertices, int
   return 0;
 }
 
+// Marching cubes (marching_cube_impl, srtool.py:1765-1800) with this build's own
+// triangulation in place of the reference's 256-case table, which is not reproduced.
+// The triangles of a cube come from its corner states ("in": value < isolevel):
+//   - faces (axis a, side s) list their corners counter-clockwise seen from outside;
+//   - on a face, every run of in-corners gets one segment, from the edge where the
+//     walk leaves the run to the edge where it entered it (in-corners stay separate on
+//     ambiguous faces, a rule that depends on the face alone, so neighbours agree);
+//   - the segments chain into closed loops over the crossing edges; loops are taken
+//     in order of their smallest edge id, each starting there, and fanned from that
+//     edge: (l0, l[k+1], l[k]).
+// Vertices are the crossing edges of each cube in edge order (the reference's atomic
+// counter order is replaced by cube order, as for dual contouring).
+int mc_cube(int ci, int tri[][3]) {
+  int next[12];
+  for (int& e : next) e = -1;
+  for (int a = 0; a < 3; ++a)
+    for (int side = 0; side < 2; ++side) {
+      const int u = (a + 1) % 3, v = (a + 2) % 3;
+      // (u, v) corners of the face in counter-clockwise order around +e_a
+      int uv[4][2] = {{0, 0}, {1, 0}, {1, 1}, {0, 1}};
+      if (side == 0) std::swap(uv[1], uv[3]);
+      int q[4];
+      for (int k = 0; k < 4; ++k)
+        for (int c = 0; c < 8; ++c)
+          if (kOff[c][a] == side && kOff[c][u] == uv[k][0] && kOff[c][v] == uv[k][1]) q[k] = c;
+      auto edge_of = [](int c0, int c1) {
+        for (int w = 0; w < 12; ++w)
+          if ((kEdge[w][0] == c0 && kEdge[w][1] == c1) || (kEdge[w][0] == c1 && kEdge[w][1] == c0)) return w;
+        return -1;
+      };
+      auto in = [&](int k) { return (ci >> q[((k % 4) + 4) % 4]) & 1; };
+      for (int k = 0; k < 4; ++k) {
+        if (!(in(k) && !in(k + 1))) continue;  // leaves a run of in-corners at q[k]
+        int j = k;
+        while (in(j - 1)) --j;  // the run starts at q[j]
+        next[edge_of(q[k], q[(k + 1) % 4])] = edge_of(q[((j - 1) % 4 + 4) % 4], q[((j % 4) + 4) % 4]);
+      }
+    }
+  int nt = 0;
+  bool seen[12] = {false};
+  for (int e = 0; e < 12; ++e) {
+    if (next[e] < 0 || seen[e]) continue;
+    int loop[12], m = 0;
+    for (int f = e; !seen[f]; f = next[f]) {
+      seen[f] = true;
+      loop[m++] = f;
+    }
+    for (int k = 1; k + 1 < m; ++k) {
+      tri[nt][0] = loop[0];
+      tri[nt][1] = loop[k + 1];
+      tri[nt][2] = loop[k];
+      ++nt;
+    }
+  }
+  return nt;
+}
+
+int marching_cubes(const Grid& g, double iso, int record_normals, double* vertices, int32_t max_v, int32_t* indices,
+                   int32_t max_i, double* normals, int32_t* nv, int32_t* ni) {
+  const double vs = (double)(float)g.vs, ox = (double)(float)g.ox, oy = (double)(float)g.oy,
+               oz = (double)(float)g.oz;
+  std::vector<double> pts;
+  std::vector<int32_t> idx;
+  // every cube with a crossing has a corner of nonzero value, so a corner in an active
+  // block: the reference's visit of the cubes around active vertices finds it
+  for (int z = 0; z < g.nz; ++z)
+    for (int y = 0; y < g.ny; ++y)
+      for (int x = 0; x < g.nx; ++x) {
+        const int ci = cube_mask(g, x, y, z, iso);
+        if (ci == 0 || ci == 255) continue;
+        int local[12];
+        const int32_t base = (int32_t)(pts.size() / 3);
+        int cnt = 0;
+        for (int w = 0; w < 12; ++w) {
+          local[w] = -1;
+          if (!edge_cross(ci, w)) continue;
+          const int a = kEdge[w][0], b = kEdge[w][1];
+          const double p1[3] = {(x + kOff[a][0]) * vs + ox, (y + kOff[a][1]) * vs + oy, (z + kOff[a][2]) * vs + oz};
+          const double p2[3] = {(x + kOff[b][0]) * vs + ox, (y + kOff[b][1]) * vs + oy, (z + kOff[b][2]) * vs + oz};
+          const double v1 = g.get(x + kOff[a][0], y + kOff[a][1], z + kOff[a][2]);
+          const double v2 = g.get(x + kOff[b][0], y + kOff[b][1], z + kOff[b][2]);
+          const double delta = v2 - v1;
+          const double t = std::fabs(delta) < 1e-5 ? 0.5 : (iso - v1) / delta;  // vertex_interpolate
+          for (int k = 0; k < 3; ++k) pts.push_back(p1[k] + t * (p2[k] - p1[k]));
+          local[w] = cnt++;
+        }
+        int tri[12][3];
+        const int nt = mc_cube(ci, tri);
+        for (int t = 0; t < nt; ++t)
+          for (int k = 0; k < 3; ++k) idx.push_back(base + local[tri[t][k]]);
+      }
+  const int32_t nvert = (int32_t)(pts.size() / 3);
+  if (nvert > max_v || (int64_t)idx.size() > max_i) return -8;
+  if (vertices) std::memcpy(vertices, pts.data(), sizeof(double) * pts.size());
+  if (indices) std::memcpy(indices, idx.data(), sizeof(int32_t) * idx.size());
+  if (normals && record_normals)
+    for (int i = 0; i < nvert; ++i) normal_at(g, &pts[3 * i], &normals[3 * i]);
+  *nv = nvert;
+  *ni = (int32_t)idx.size();
+  return 0;
+}
+
 // Grid of the parameters, all blocks inactive and every value 0.
 Grid make_grid(const nn_sr_params* prm) {
   Grid g;
@@ -539,6 +641,27 @@ int sro_contour(const nn_sr_params* prm, const double* field, const uint8_t* act
   g.v.assign(field, field + g.v.size());
   g.active.assign(active, active + g.active.size());
   return contour(g, prm->isolevel, prm->record_normals, vertices, max_v, indices, max_i, normals, nv, ni);
+}
+
+// Marching cubes on a given field (values [cells], active flags [blocks]).
+int sro_marching_cubes(const nn_sr_params* prm, const double* field, const uint8_t* active, double* vertices,
+                       int32_t max_v, int32_t* indices, int32_t max_i, double* normals, int32_t* nv, int32_t* ni) {
+  Grid g = make_grid(prm);
+  g.v.assign(field, field + g.v.size());
+  g.active.assign(active, active + g.active.size());
+  return marching_cubes(g, prm->isolevel, prm->record_normals, vertices, max_v, indices, max_i, normals, nv, ni);
+}
+
+// The triangle table that mc_cube gives: per cube index, the triangle count and the
+// edge ids (12 triangles at most; unused entries -1).
+int sro_mc_table(int32_t* ntri, int32_t* tris) {
+  for (int ci = 0; ci < 256; ++ci) {
+    int tri[12][3];
+    ntri[ci] = mc_cube(ci, tri);
+    for (int t = 0; t < 12; ++t)
+      for (int k = 0; k < 3; ++k) tris[(ci * 12 + t) * 3 + k] = t < ntri[ci] ? tri[t][k] : -1;
+  }
+  return 0;
 }
 
 // The whole of SRTool.dual_contouring for n particles. Outputs (each optional):

@@ -50,3 +50,31 @@ def closed_oriented(faces: np.ndarray, nv: int) -> bool:
     if np.any(cnt != 1):
         return False
     return bool(np.all(np.isin(rev, u))) and len(np.unique(f)) == nv
+
+
+def weld(vertices: np.ndarray, faces: np.ndarray, tol: float = 1e-6):
+    """Merge vertices closer than `tol` (marching cubes emits each crossing edge once per
+    cube, and the two copies of an edge's crossing may differ in the last f32 bit);
+    returns (vertices, faces) of the welded mesh."""
+    from scipy.sparse import coo_matrix
+    from scipy.sparse.csgraph import connected_components
+    from scipy.spatial import cKDTree
+
+    v = np.asarray(vertices, np.float64)
+    pairs = cKDTree(v).query_pairs(tol, output_type="ndarray")
+    g = coo_matrix((np.ones(len(pairs)), (pairs[:, 0], pairs[:, 1])), shape=(len(v), len(v)))
+    _, label = connected_components(g, directed=False)
+    first = np.full(label.max() + 1, -1, np.int64)
+    first[label[::-1]] = np.arange(len(v))[::-1]
+    return v[first], label[np.asarray(faces, np.int64).reshape(-1)].reshape(-1, 3)
+
+
+def signed_volume(vertices: np.ndarray, faces: np.ndarray) -> float:
+    v = np.asarray(vertices, np.float64)
+    f = np.asarray(faces, np.int64).reshape(-1, 3)
+    return float(np.einsum("ij,ij->i", v[f[:, 0]], np.cross(v[f[:, 1]], v[f[:, 2]])).sum() / 6.0)
+
+
+# corners of each cube edge and corner offsets (srtool.py:775-783, 931-942)
+CUBE_OFF = np.array([[0, 1, 0], [1, 1, 0], [1, 0, 0], [0, 0, 0], [0, 1, 1], [1, 1, 1], [1, 0, 1], [0, 0, 1]])
+CUBE_EDGE = np.array([[0, 1], [1, 2], [2, 3], [3, 0], [4, 5], [5, 6], [6, 7], [7, 4], [0, 4], [1, 5], [2, 6], [3, 7]])

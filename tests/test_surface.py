@@ -99,3 +99,73 @@ def test_oracle_velocity_field_of_a_uniform_flow(surf):
     mv = surf.mesh_velocity(prm, vf.reshape(-1), pts)
     assert np.allclose(mv[0], vf[:, k], rtol=1e-6)
     assert np.allclose(mv[1], 0.5 * (vf[:, k] + vf[:, k + 1]), rtol=1e-6)
+
+
+def test_oracle_mc_table_is_a_set_of_disks_on_the_crossing_edges(surf):
+    """The marching-cubes case table: every case's triangles use exactly its crossing
+    edges; they form disks whose boundary runs along the cube's faces, as segments
+    between two crossing edges of one face, once each; the count is #edges - 2 #loops."""
+    from .surf_cases import CUBE_EDGE, CUBE_OFF
+
+    nt, tris = surf.mc_table()
+    assert nt[0] == 0 and nt[255] == 0 and nt.max() <= 5
+    for ci in range(256):
+        inside = [(ci >> c) & 1 for c in range(8)]
+        cross = {w for w in range(12) if inside[CUBE_EDGE[w][0]] != inside[CUBE_EDGE[w][1]]}
+        t = tris[ci, : nt[ci]]
+        assert np.all(tris[ci, nt[ci]:] == -1)
+        assert set(t.reshape(-1).tolist()) == cross
+        directed = [(a, b) for tr in t for a, b in ((tr[0], tr[1]), (tr[1], tr[2]), (tr[2], tr[0]))]
+        assert len(set(directed)) == len(directed)
+        boundary = [(a, b) for a, b in directed if (b, a) not in directed]
+        # each crossing edge starts one boundary segment and ends one
+        assert sorted(a for a, _ in boundary) == sorted(cross) == sorted(b for _, b in boundary)
+        for a, b in boundary:  # a segment lies on a face: the two edges share a face
+            ca, cb = CUBE_OFF[CUBE_EDGE[a]], CUBE_OFF[CUBE_EDGE[b]]
+            assert any(np.all(ca[:, k] == ca[0, k]) and np.all(cb[:, k] == ca[0, k]) for k in range(3))
+        nxt = dict(boundary)
+        loops, seen = 0, set()
+        for e in cross:
+            if e in seen:
+                continue
+            loops += 1
+            while e not in seen:
+                seen.add(e)
+                e = nxt[e]
+        assert nt[ci] == len(cross) - 2 * loops
+
+
+def test_oracle_marching_cubes_closes_around_the_ball(surf):
+    """Marching cubes on the ball's field: closed and consistently wound once the per-cube
+    vertices are welded, genus 0, and the same orientation and volume as dual contouring."""
+    from .surf_cases import signed_volume, weld
+
+    prm = default_params()
+    o = surf.dual_contouring(prm, ball(seed=0))
+    mc = surf.marching_cubes(prm, o["field"], o["active"])
+    v, f = weld(mc["vertices"], mc["indices"])
+    assert len(f) > 1000 and closed_oriented(f, len(v)) and len(f) == 2 * len(v) - 4
+    vd = signed_volume(o["vertices"], o["indices"])
+    vm = signed_volume(mc["vertices"], mc["indices"])
+    assert vd > 0 and abs(vm - vd) < 0.02 * vd
+
+
+def test_oracle_marching_cubes_of_an_analytic_sphere(surf):
+    """Every marching-cubes vertex of a sphere's signed distance field lies on an edge
+    crossing, within a small fraction of a voxel of the sphere."""
+    from .surf_cases import weld
+
+    prm = default_params(dims=(48, 48, 48))
+    vs = prm.voxel_size
+    idx = np.stack(np.meshgrid(*[np.arange(48)] * 3, indexing="ij"), -1)
+    c, R = np.array([0.24, 0.23, 0.25]), 0.13
+    sdf = np.linalg.norm(idx * vs - c, axis=-1) - R
+    o = surf.marching_cubes(prm, np.transpose(sdf, (2, 1, 0)), np.ones(8, np.uint8))
+    assert np.abs(np.linalg.norm(o["vertices"] - c, axis=1) - R).max() < 0.05 * vs
+    # a sphere through grid vertices puts several edges' crossings on one point; move it
+    # off the vertices before welding
+    c, R = np.array([0.2413, 0.2327, 0.2491]), 0.1307
+    sdf = np.linalg.norm(idx * vs - c, axis=-1) - R
+    o = surf.marching_cubes(prm, np.transpose(sdf, (2, 1, 0)), np.ones(8, np.uint8))
+    v, f = weld(o["vertices"], o["indices"])
+    assert closed_oriented(f, len(v)) and len(f) == 2 * len(v) - 4
