@@ -202,6 +202,10 @@ class Parameter:
         if p.simulation_method not in (4, None):
             # build_solver (SPH/main.py:196-203)
             raise NotImplementedError(f"Solver type {p.simulation_method} has not been implemented.")
+        if bool(g("useDragForceModel", False)):
+            # the reference's DragForce model is commented out (SPH/main.py:1543-1544), so its
+            # compute_non_pressure_forces (1564-1565) fails on the missing model
+            raise NotImplementedError("useDragForceModel: the reference has no drag force model")
         return p
 
     def flags(self) -> int:

@@ -107,6 +107,8 @@ def test_config_parses_reference_scenes():
     assert p.flags() & _abi.NN_F_IMPLICIT_VISCOSITY and not p.flags() & _abi.NN_F_ELASTICITY
     with pytest.raises(NotImplementedError):
         Parameter.from_config(SimConfig(config={"Configuration": {"simulationMethod": 0}}))
+    with pytest.raises(NotImplementedError):  # the reference's drag hook has no model behind it
+        Parameter.from_config(SimConfig(config={"Configuration": {"simulationMethod": 4, "useDragForceModel": True}}))
 
 
 def test_ply_roundtrip(tmp_path):
