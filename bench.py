@@ -672,8 +672,11 @@ def run_ours(args):
                      "kernel_ms": kms, "launches_per_step": per_step, "list_entries": entries},
         "step_alg_bytes_per_particle": bytes_step,
         "step_roofline_frac": bytes_step * total_ps / (ms_max / 1e3) / 1e9 / hbm,
-        "solver": {k: st[k] for k in ("iterations_v", "iterations", "cg_iterations", "avg_density_err",
-                                      "max_neighbors_seen", "dt", "status")},
+        "solver": dict({k: st[k] for k in ("iterations_v", "iterations", "cg_iterations", "avg_density_err",
+                                           "max_neighbors_seen", "dt", "status")},
+                       # the reference's loop test: avg |rho_adv - rho0| <= maxError % of rho0 (SPH/main.py:1776-1782)
+                       avg_density_err_pct=100.0 * st["avg_density_err"] / sc.param.density0,
+                       max_error_pct=sc.param.max_error),
         "gpu_launches": launches,
         "e2e": {"value": e2e_val, "unit": "particle-steps/s", "h2d_bytes_per_step": int(24 * n),
                 "d2h_bytes_per_step": int(12 * n),
