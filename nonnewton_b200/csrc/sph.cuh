@@ -1037,10 +1037,13 @@ __global__ void k_advect_boundary(Dev d, int do_advect, int do_boundary) {
 
 // ---------------------------------------------------------------------------
 // Synchronisation with the caller's id-order state (meta.pd).
+// Walks the caller's arrays in id order, so its stores are coalesced; the loads come
+// from the slots through slot_of_id (a float4 load uses half of its sector, where a
+// 4-byte store by slot would take a sector for itself).
 __global__ void k_sync_out(Dev d, uint32_t mask) {
   const int n = d.d_n[0];
-  GRID_STRIDE(i, n) {
-    const int id = d.w.id[i];
+  GRID_STRIDE(id, n) {
+    const int i = d.slot_of_id[id];
     const float4 p = d.w.pos[i];
     if (mask & 1u) { d.t.x[3 * id] = p.x; d.t.x[3 * id + 1] = p.y; d.t.x[3 * id + 2] = p.z; }
     if (mask & 2u) { const float4 v = d.w.vel[i]; d.t.v[3 * id] = v.x; d.t.v[3 * id + 1] = v.y; d.t.v[3 * id + 2] = v.z; }
