@@ -182,3 +182,21 @@ def test_marching_cubes_matches_oracle(cuda_lib, surf, case):
     assert vd > 0 and abs(signed_volume(vg, sr.mesh_index.cpu().numpy()) - vd) < 0.03 * vd
     ref = surf.mesh_velocity(prm, surf.vel_field(prm, pos, vel), vg)
     assert _scale_err(sr.mesh_velocity.cpu().numpy(), ref) < 1e-5
+
+
+@pytest.mark.parametrize("method", ["dual_contouring", "marching_cubes"])
+def test_surface_empty_and_single_particle(cuda_lib, surf, method):
+    """No particles: an empty mesh. One particle: the pre-pass skips particle 0
+    (srtool.py:1013), so only the isotropic splat runs, the field has no negative
+    value and no surface results, as in the oracle. The tool stays usable after both."""
+    sr = _tool()
+    run = getattr(sr, method)
+    run(isolevel=0.0, smooth_radius=0.06, num_particles=0, pos=np.zeros((0, 3), np.float32))
+    assert sr.num_vertices[None] == 0 and sr.num_indices[None] == 0 and sr.mesh_vertex.shape == (0, 3)
+    one = np.array([[0.5, 0.5, 0.5]], np.float32)
+    run(isolevel=0.0, smooth_radius=0.06, num_particles=1, pos=one)
+    o = surf.dual_contouring(sr.last_params, one)
+    assert sr.num_vertices[None] == len(o["vertices"]) == 0 and sr.num_indices[None] == 0
+    pos = ball(seed=20)
+    run(isolevel=0.0, smooth_radius=0.06, num_particles=len(pos), pos=pos)
+    assert sr.num_vertices[None] > 0
