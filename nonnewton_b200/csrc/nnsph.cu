@@ -220,7 +220,7 @@ static int launch1(nn_ctx* c, cudaStream_t s, void (*k)(KArgs...), Args... args)
 // The force pass instance for the batch's terms (c->forces_feat) and batch depth.
 template <int U, int... F>
 static void (*forces_pick(int feat, std::integer_sequence<int, F...>))(Dev, int) {
-  static void (*const tbl[])(Dev, int) = {&k_forces<U, F>...};
+  static void (*const tbl[])(Dev, int) = {forces_kernel_of<U, F>()...};
   return tbl[feat];
 }
 static void (*forces_kernel(const nn_ctx* c))(Dev, int) {
