@@ -87,6 +87,7 @@ struct SrDev {
   int32_t max_v, max_i;
   float iso, sr, volume, acoeff;
   float q1_thr, q05_thr;     // largest f32 whose rounded square root is <= 1, <= 0.5
+  float rr_thr;              // smallest f32 whose rounded square root is >= 2 smooth_radius
   int range, off, smooth_cells, record_normals;
 };
 
@@ -221,33 +222,57 @@ __device__ void sr_sym_eig(const double S0[3][3], double lam[3], double V[3][3])
 // can hold a point closer than `reach`, row by row (the voxels of one (y, z) row are
 // one contiguous stretch of the voxel-sorted arrays, whose index k is passed to f);
 // lane `lane` of `lanes` takes every lanes-th row.
+// The particles of the voxel rows (x-runs) of the range around voxel (cx, cy, cz)
+// whose y-z slab comes within `reach` of p, visited by a whole warp. Only about one
+// row in four of the range crosses a particle lattice at half the voxel density, so
+// lanes owning rows would mostly idle: each lane takes one row of a group of 32, a
+// warp scan of the row counts lays their particles end to end, and lane l handles
+// particles l, l + 32, ... of the group, finding its row by a search over the scan.
+// f(k) gets the voxel-sorted index of each particle; `valid` lanes only.
 template <typename F>
-__device__ __forceinline__ void sr_range_rows(const SrDev& s, int cx, int cy, int cz, float px, float py, float pz,
-                                              float reach, int lane, int lanes, F f) {
+__device__ __forceinline__ void sr_range_particles(const SrDev& s, int cx, int cy, int cz, float px, float py,
+                                                   float pz, float reach, int lane, F f) {
   const SrGrid& g = s.g;
+  const unsigned full = 0xffffffffu;
   const int lo = -s.off, hi = s.range - 1 - s.off;
   const float r2 = reach * reach;
   const int x0 = max(cx + lo, 0), x1 = min(cx + hi, g.nx - 1);
-  if (x0 > x1) return;
-  for (int r = lane; r < s.range * s.range; r += lanes) {
-    const int z = cz + lo + r / s.range, y = cy + lo + r % s.range;
-    if (z < 0 || z >= g.nz || y < 0 || y >= g.ny) continue;
-    const float zc = fmaxf(fmaxf(g.oz + z * g.vs - pz, pz - (g.oz + (z + 1) * g.vs)), 0.f);
-    const float yc = fmaxf(fmaxf(g.oy + y * g.vs - py, py - (g.oy + (y + 1) * g.vs)), 0.f);
-    if (yc * yc + zc * zc > r2) continue;
-    const uint32_t b = s.vcount[g.idx(x0, y, z)], e = s.vcount[g.idx(x1, y, z) + 1];
-    for (uint32_t k = b; k < e; ++k) f(k);
+  if (x0 > x1) return;  // warp-uniform
+  const int nrows = s.range * s.range;
+  for (int r0 = 0; r0 < nrows; r0 += 32) {
+    const int r = r0 + lane;
+    uint32_t b = 0, cnt = 0;
+    if (r < nrows) {
+      const int z = cz + lo + r / s.range, y = cy + lo + r % s.range;
+      if (z >= 0 && z < g.nz && y >= 0 && y < g.ny) {
+        const float zc = fmaxf(fmaxf(g.oz + z * g.vs - pz, pz - (g.oz + (z + 1) * g.vs)), 0.f);
+        const float yc = fmaxf(fmaxf(g.oy + y * g.vs - py, py - (g.oy + (y + 1) * g.vs)), 0.f);
+        if (yc * yc + zc * zc <= r2) {
+          b = s.vcount[g.idx(x0, y, z)];
+          cnt = s.vcount[g.idx(x1, y, z) + 1] - b;
+        }
+      }
+    }
+    uint32_t incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t v = __shfl_up_sync(full, incl, o);
+      if (lane >= o) incl += v;
+    }
+    const uint32_t total = __shfl_sync(full, incl, 31);
+    for (uint32_t base = 0; base < total; base += 32) {
+      const uint32_t t = base + lane;
+      int l = 0;  // the first row lane whose inclusive count exceeds t
+#pragma unroll
+      for (int step = 16; step >= 1; step >>= 1)
+        if (__shfl_sync(full, incl, l + step - 1) <= t) l += step;
+      const uint32_t bl = __shfl_sync(full, b, l), il = __shfl_sync(full, incl, l), cl = __shfl_sync(full, cnt, l);
+      if (t < total) f(bl + (t - (il - cl)));
+    }
   }
 }
 
-// |p - q| in f32 with unfused operations (the in-range test must decide the same way
-// as any other f32 evaluation of the same expression)
-__device__ __forceinline__ float sr_dist(float px, float py, float pz, const float* q) {
-  const float dx = __fsub_rn(px, q[0]), dy = __fsub_rn(py, q[1]), dz = __fsub_rn(pz, q[2]);
-  return __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz)));
-}
-
-// One warp per particle: lanes split the rows of the range and the moments are
+// One warp per particle: lanes split the particles of the range and the moments are
 // reduced across the warp with shuffles.
 __global__ void k_sr_aniso_pre(SrDev s) {
   const int lane = threadIdx.x & 31;
@@ -264,11 +289,14 @@ __global__ void k_sr_aniso_pre(SrDev s) {
     double tw = 0.0, m1[3] = {0.0, 0.0, 0.0}, m2[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     int nnb = 0;
     // a margin of one voxel on the pruning distance keeps every pair with w > 0
-    sr_range_rows(s, cx, cy, cz, px, py, pz, rr + s.g.vs, lane, 32, [&](uint32_t k) {
+    sr_range_particles(s, cx, cy, cz, px, py, pz, rr + s.g.vs, lane, [&](uint32_t k) {
       const float4 pj = s.spos[k];
-      const float pjv[3] = {pj.x, pj.y, pj.z};
-      const float dn = sr_dist(px, py, pz, pjv);
-      if (dn < rr) {
+      const float dx = __fsub_rn(px, pj.x), dy = __fsub_rn(py, pj.y), dz = __fsub_rn(pz, pj.z);
+      const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+      // |x_i - x_j| in f32 (unfused, as any f32 evaluation of it) < 2 r_s, decided on
+      // the square: rn(sqrt(d2)) < rr exactly when d2 < rr_thr
+      if (d2 < s.rr_thr) {
+        const float dn = __fsqrt_rn(d2);
         const float q = dn / rr;
         const double w = 1.0 - (double)(q * q * q);  // isoweight, srtool.py:993-999
         const double d[3] = {(double)pj.x - px, (double)pj.y - py, (double)pj.z - pz};
@@ -1029,6 +1057,13 @@ static int sr_run(nn_sr_ctx* c, const nn_sr_params* p, const float* pos, const f
   s.range = (int)std::ceil(4.0 * (double)s.sr / (double)s.g.vs) + 1;  // srtool.py:1137
   s.off = s.range / 2;
   s.smooth_cells = p->smooth_cells;
+  {  // the pre-pass's in-range test rn(sqrt(r2)) < 2 r_s  <=>  r2 < rr_thr
+    const float rr = 2.f * s.sr;
+    float t = rr * rr;
+    while (std::sqrt(t) >= rr) t = std::nextafter(t, 0.f);
+    while (std::sqrt(t) < rr) t = std::nextafter(t, INFINITY);
+    s.rr_thr = t;
+  }
   {  // exact branch tests without the square root: rn(sqrt(t)) <= 1 (0.5)  <=>  t <= q1_thr (q05_thr)
     float t = 1.f;
     while (std::sqrt(std::nextafter(t, INFINITY)) <= 1.f) t = std::nextafter(t, INFINITY);
