@@ -12,7 +12,7 @@ from the import:
     sr.export_mesh("out.ply")
 
 `pos` (and `velocity`, with `record_velocity=True`) is a [n, 3] array (torch on the
-GPU, or numpy). The mesh stays on the GPU as torch tensors. `marching_cubes(...)`
+GPU, numpy, or a field with `to_numpy()` such as the reference example's Taichi field). The mesh stays on the GPU as torch tensors. `marching_cubes(...)`
 takes the same arguments and ends the same pipeline with marching cubes
 (srtool.py:1765-1800) instead of dual contouring.
 """
@@ -148,6 +148,8 @@ class SRTool:
         n = int(num_particles)
 
         def dev(a):
+            if hasattr(a, "to_numpy"):  # a Taichi field, as the reference's callers pass
+                a = a.to_numpy()
             if torch.is_tensor(a):
                 return a[:n].to(device=self.device, dtype=torch.float32).contiguous()
             return torch.as_tensor(np.asarray(a)[:n], dtype=torch.float32, device=self.device).contiguous()

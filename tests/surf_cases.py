@@ -25,6 +25,15 @@ def block(seed=0, n=(12, 10, 8), spacing=0.02, corner=(0.3, 0.25, 0.35), jitter=
     return (p + rng.uniform(-jitter, jitter, size=p.shape)).astype(np.float32)
 
 
+def torus(R=0.12, r=0.045, spacing=0.02, center=0.5):
+    """A solid lattice torus around the y axis, like the reference example's model
+    (SPH/surf_recon/example.py reads a 604-point voxelised torus): 640 particles."""
+    g = np.arange(center - 0.2, center + 0.2 + 1e-9, spacing)
+    p = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    rho = np.hypot(p[:, 0] - center, p[:, 2] - center)
+    return p[(rho - R) ** 2 + (p[:, 1] - center) ** 2 <= r * r].astype(np.float32)
+
+
 def default_params(dims=None, voxel_size=0.01, particle_radius=0.02, smooth_radius=0.06, isolevel=0.0,
                    use_smooth_field=True, record_normals=True, box=1.0):
     """The reference example's settings (SPH/surf_recon/example.py): voxel 0.01,

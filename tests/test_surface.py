@@ -5,7 +5,7 @@ negative field values). No GPU."""
 import numpy as np
 import pytest
 
-from .surf_cases import ball, block, closed_oriented, default_params
+from .surf_cases import ball, block, closed_oriented, default_params, torus
 
 
 @pytest.fixture(scope="module")
@@ -169,3 +169,11 @@ def test_oracle_marching_cubes_of_an_analytic_sphere(surf):
     o = surf.marching_cubes(prm, np.transpose(sdf, (2, 1, 0)), np.ones(8, np.uint8))
     v, f = weld(o["vertices"], o["indices"])
     assert closed_oriented(f, len(v)) and len(f) == 2 * len(v) - 4
+
+
+def test_oracle_torus_has_genus_one(surf):
+    """The reference example's shape: a solid torus of lattice particles gives a closed
+    mesh whose Euler characteristic is 0 (F = 2V), the hole kept open."""
+    o = surf.dual_contouring(default_params(), torus())
+    f, nv = o["indices"].reshape(-1, 3), len(o["vertices"])
+    assert nv > 1000 and closed_oriented(f, nv) and len(f) == 2 * nv
