@@ -174,15 +174,36 @@ def assemble(phases: list[PhaseInfo], param: Parameter, mass_density_default: fl
                        n_fluid=n_fluid, phase_info=info)
 
 
+def geometry_path(geometry_file: str, scene_path: str = "", root: str | None = None) -> str:
+    """Where a scene's `geometryFile` lies. The reference reads
+    `sph_root_path + geometryFile` (SPH/main.py:673), the directory of main.py joined
+    without a separator to paths such as "./data/models/cube.ply", which names a
+    directory "SPH." that does not exist. Here the path is taken relative to `root` when
+    given, else to the first of: the directory holding the scene's data/ folder (the
+    reference's layout, <root>/data/scenes/x.json), the scene's parent and own
+    directories, and the working directory."""
+    if os.path.isabs(geometry_file):
+        return geometry_file
+    if root is not None:
+        return os.path.join(root, geometry_file)
+    cands = []
+    if scene_path:
+        d = os.path.dirname(os.path.abspath(scene_path))
+        cands += [os.path.dirname(os.path.dirname(d)), os.path.dirname(d), d]
+    cands.append(os.getcwd())
+    for c in cands:
+        if os.path.exists(os.path.join(c, geometry_file)):
+            return os.path.join(c, geometry_file)
+    raise FileNotFoundError(f"geometryFile {geometry_file!r} not found relative to any of {cands}")
+
+
 def load_particles(cfg: SimConfig, param: Parameter, root: str | None = None) -> ParticleSet:
     """`load_particles` / `parse_cfg` (SPH/main.py:628-691) for PLY-backed scenes."""
-    root = root if root is not None else (os.path.dirname(os.path.dirname(os.path.abspath(cfg.scene_path)))
-                                          if cfg.scene_path else ".")
     phases = []
 
     def _pos(c, pos=None):
         if pos is None:
-            pos = read_ply_particles(os.path.join(root, c["geometryFile"]))
+            pos = read_ply_particles(geometry_path(c["geometryFile"], cfg.scene_path, root))
         return transform(pos, c)
 
     for cnt, c in enumerate(cfg.get_fluid_cfg()):

@@ -120,3 +120,39 @@ def test_ply_roundtrip(tmp_path):
     f = tmp_path / "p.ply"
     export_ply_particles(x, str(f))
     assert np.array_equal(read_ply_particles(str(f)), x)
+
+
+def test_scene_geometry_resolves_like_the_reference_layout(tmp_path, monkeypatch):
+    """A reference scene (<root>/data/scenes/x.json) names its models as
+    "./data/models/m.ply", relative to <root>, the directory of SPH/main.py; the loader
+    finds them there from any working directory and loads the phases."""
+    import json
+
+    import numpy as np
+
+    from nonnewton_b200.config import Parameter, SimConfig
+    from nonnewton_b200.scene import export_ply_particles, geometry_path, load_particles
+
+    (tmp_path / "data" / "scenes").mkdir(parents=True)
+    (tmp_path / "data" / "models").mkdir(parents=True)
+    g = np.arange(5) * 0.02
+    cube = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3).astype(np.float32)
+    export_ply_particles(cube, str(tmp_path / "data" / "models" / "cube.ply"))
+    scene = {"Configuration": {"particleRadius": 0.01, "simulationMethod": 4},
+             "FluidBlocks": [],
+             "FluidParticles": [{"geometryFile": "./data/models/cube.ply", "translation": [0.5, 0.5, 0.5]}],
+             "SolidParticles": [{"geometryFile": "./data/models/cube.ply", "solidType": "STATIC",
+                                 "translation": [0.2, 0.1, 0.2]}]}
+    path = tmp_path / "data" / "scenes" / "s.json"
+    path.write_text(json.dumps(scene))
+    monkeypatch.chdir("/")
+    import os
+
+    assert os.path.normpath(geometry_path("./data/models/cube.ply", str(path))) == \
+        str(tmp_path / "data" / "models" / "cube.ply")
+    cfg = SimConfig(str(path))
+    ps = load_particles(cfg, Parameter.from_config(cfg))
+    assert ps.x.shape == (250, 3) and ps.n_fluid == 125
+    assert np.allclose(ps.x[:125], cube + 0.5, atol=1e-6)
+    with pytest.raises(FileNotFoundError):
+        geometry_path("./data/models/missing.ply", str(path))
