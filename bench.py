@@ -245,6 +245,7 @@ def run_reference(args):
     print(json.dumps({"impl": "reference", "metric": "particle-steps/s", "value": v, "unit": "particle-steps/s",
                       "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "samples": len(times),
                       "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
+                      "scaling": "weak", "vs_baseline": None,
                       "dtype": "f32", "data": "synthetic (seeded numpy scene generator)",
                       "config": {"workload": name, "particles": n, "fluid": scenes[0].particles.n_fluid},
                       "cpu_baseline": cb,
@@ -391,6 +392,7 @@ def run_reference_surface(args):
     print(json.dumps({"impl": "reference", "metric": "particles/s (surface reconstruction)", "value": v,
                       "unit": "particles/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
                       "samples": len(times), "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
+                      "scaling": "weak", "vs_baseline": None,
                       "dtype": "f32", "data": "synthetic (seeded numpy scene generator)",
                       "config": {"workload": "surface_drop", "particles": int(len(sub))}, "cpu_baseline": cb,
                       "e2e": {"value": v, "unit": "particles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
