@@ -25,6 +25,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -274,8 +275,7 @@ def run_served(args, world, rank):
     barrier(world)
     eng = srv.batch.engine
     l0 = eng.launch_count()
-    clocks_path = os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else "",
-                               f"clocks_rank{rank}.csv")
+    clocks_path = os.path.join(args.clocks_dir, f"clocks_rank{rank}.csv")
     with ClockSampler(clocks_path) as cs:
         torch.cuda.nvtx.range_push("timed")
         res = srv.run(reqs, realtime=True)
@@ -426,8 +426,7 @@ def run_surface(args, world, rank):
     torch.cuda.synchronize()
     barrier(world)
     times = []
-    clocks_path = os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else "",
-                               f"clocks_rank{rank}.csv")
+    clocks_path = os.path.join(args.clocks_dir, f"clocks_rank{rank}.csv")
     with ClockSampler(clocks_path) as cs:
         for _ in range(args.steps):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -548,8 +547,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     barrier(world)
     l0 = eng.launch_count()
-    clocks_path = os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else "",
-                               f"clocks_rank{rank}.csv")
+    clocks_path = os.path.join(args.clocks_dir, f"clocks_rank{rank}.csv")
     # ---- device-resident timing: K steps, state in HBM, one graph replay per step
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -710,6 +708,8 @@ def main():
     ap.add_argument("--plain-sample", type=int, default=48)
     ap.add_argument("--autotune", action="store_true", help="pick block size, unroll and cell factor first")
     ap.add_argument("--tuning", default=None, help="block,unroll,cell_factor (e.g. 128,2,1)")
+    ap.add_argument("--clocks-dir", default=tempfile.gettempdir(),
+                    help="where the nvidia-smi clock samples of the timed region go (clocks_rank<r>.csv)")
     ap.add_argument("--host-loop", action="store_true",
                     help="drive the solver loops from the host instead of CUDA-graph while-nodes "
                          "(for ncu launch lists: ncu does not profile kernel nodes inside conditional nodes)")
