@@ -5,13 +5,16 @@
 // chunleili/nonNewton (cited per function below). It is NOT part of the product:
 // only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg load it.
 //
-// Parity status: the reference's Taichi code cannot run in this environment
-// (taichi is not installed), and the reference stores no golden outputs. The
-// neighbour search and the density / boundary-volume / DFSPH-factor passes are
-// pinned by known answers derived from the reference's fixtures (tests/golden/,
-// generated by tests/golden/make_golden.py) and by an independent numpy
-// restatement; for the solver loops, forces and elasticity, parity is unpinned
-// against a live reference run.
+// Parity status: pinned against the reference's own step. Taichi is not installed
+// here, so tests/golden/make_reference_run.py runs SPH/main.py itself in plain Python
+// against a Taichi stand-in on four small scenes (fluid in a boundary box; with the
+// non-Newtonian model; with an elastic cube; with a rigid cube) and stores the state
+// after each step (tests/golden/ref_*.npz). In the reference-quirks mode this oracle
+// reproduces every recorded field of those runs within 1e-5 of its scale
+// (tests/test_reference_pin.py). The neighbour search and the density /
+// boundary-volume / DFSPH-factor passes are also pinned by known answers derived from
+// the reference's fixtures (tests/golden/make_golden.py) and by an independent numpy
+// restatement.
 //
 // Templated on Real (float = the reference's ti.f32 default, double = the FP64
 // comparison run). Every neighbour loop walks neighbours in ascending particle id.

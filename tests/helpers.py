@@ -60,3 +60,54 @@ def near_cutoff_pairs(x, h, tol_ulps=4):
     ulp = np.spacing(np.float32(h))
     sel = np.abs(d - h) < tol_ulps * ulp
     return {(int(a), int(b)) for a, b in pairs[sel]}
+
+
+# ---- the reference's own step, run once through a Taichi stand-in
+# (tests/golden/make_reference_run.py), stored as tests/golden/ref_<scene>.npz
+REF_SCENES = ("dam", "nonnewton", "elastic", "rigid")
+REF_FIELDS = ("x", "v", "acceleration", "density", "dfsph_factor", "density_adv", "volume", "strain_rate_norm",
+              "nonnewton_viscosity", "stress", "rotations")
+FLUID_ONLY = ("density", "dfsph_factor", "density_adv", "strain_rate_norm", "nonnewton_viscosity")
+
+
+def reference_run(name):
+    """(fixture, config dict, Parameter in quirks mode, ParticleSet) of a reference run:
+    the phases rebuilt from the run's own initial positions and phase ids."""
+    import json
+    import os
+
+    from nonnewton_b200 import scene as S
+    from nonnewton_b200.config import Parameter, SimConfig
+
+    R = dict(np.load(os.path.join(os.path.dirname(__file__), "golden", f"ref_{name}.npz")))
+    cfg = json.loads(R["config"].tobytes().decode())
+    param = Parameter.from_config(SimConfig(config=cfg), quirks=True)
+    phases = []
+    for uid in dict.fromkeys(R["phase_id"].tolist()):
+        m = R["phase_id"] == uid
+        st = S.RIGID if 2000 <= uid < 3000 else S.ELASTIC if uid >= 3000 else S.STATIC
+        phases.append(S.PhaseInfo(uid=uid, material=int(R["material"][m][0]), is_dynamic=bool(R["is_dynamic"][m][0]),
+                                  pos=R["init_x"][m], solid_type=st))
+    return R, cfg, param, S.assemble(phases, param)
+
+
+def reference_steps(R):
+    return sum(1 for k in R if k.startswith("step") and k.endswith("_x"))
+
+
+def reference_errors(R, step, get, nf):
+    """{field: max |ours - reference| / scale} for the fields the run recorded at `step`;
+    fields whose reference scale is below `floor` (stress before any strain, ~1e-10 Pa)
+    are compared against that floor."""
+    floor = {"stress": 1.0}
+    out = {}
+    for k in REF_FIELDS:
+        key = f"step{step}_{k}"
+        if key not in R:
+            continue
+        b = R[key].astype(np.float64)
+        a = np.asarray(get(k), np.float64).reshape(b.shape)
+        if k in FLUID_ONLY:
+            a, b = a[:nf], b[:nf]
+        out[k] = float(np.abs(a - b).max() / max(np.abs(b).max(), floor.get(k, 1e-30)))
+    return out
