@@ -21,6 +21,8 @@ def test_oracle_matches_the_reference_run(name):
     o = O.OracleSim(ps, param, "f32")
     o.initialize()
     assert abs(o.get("volume") - R["init_volume"]).max() <= TOL * abs(R["init_volume"]).max()
+    # the reference's first search runs on the same positions: the same neighbour counts
+    assert (o.neighbors(60)[0] == R["step0_num_neighbors"]).all()
     for s in range(reference_steps(R)):
         o.step(1)
         err = reference_errors(R, s, o.get, ps.n_fluid)
