@@ -114,8 +114,9 @@ class _Rewrite(ast.NodeTransformer):
         return node
 
 
-def load_reference(ref_root: str):
-    """The reference's SPH/main.py, rewritten and executed against the stand-in."""
+def load_reference(ref_root: str, rel_path: str = "SPH/main.py", module: str = "sph_reference"):
+    """A reference source file (SPH/main.py by default), rewritten and executed against
+    the stand-in."""
     sys.path.insert(0, os.path.join(HERE, "refrun"))
     import ti_stub
 
@@ -125,7 +126,7 @@ def load_reference(ref_root: str):
     sys.modules["trimesh"] = trimesh_stub
     for name in ("meshio", "plyfile"):  # read_ply_particles is swapped for the scenes' arrays
         sys.modules.setdefault(name, types.ModuleType(name))
-    path = os.path.join(ref_root, "SPH", "main.py")
+    path = os.path.join(ref_root, rel_path)
     src = open(path).read()
     tree = ast.parse(src)
     tasks = set()
@@ -134,9 +135,9 @@ def load_reference(ref_root: str):
                 and len(n.args) == 3 and isinstance(n.args[1], ast.Attribute)):
             tasks.add(n.args[1].attr)
     tree = ast.fix_missing_locations(_Rewrite(tasks).visit(tree))
-    mod = types.ModuleType("sph_reference")
+    mod = types.ModuleType(module)
     mod.__file__ = path
-    sys.modules["sph_reference"] = mod  # dataclasses look the module up
+    sys.modules[module] = mod  # dataclasses look the module up
     with contextlib.redirect_stdout(io.StringIO()):
         exec(compile(tree, path, "exec"), mod.__dict__)
     return mod

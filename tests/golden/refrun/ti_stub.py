@@ -1,13 +1,14 @@
 """A plain-Python stand-in for the part of Taichi that the reference's SPH/main.py uses,
 so that the reference's own kernels can run (slowly, on the CPU, one particle at a
-time) where Taichi is not installed. TEST INFRASTRUCTURE: only
-tests/golden/make_reference_run.py loads it, to generate golden fixtures.
+time) where Taichi is not installed. TEST INFRASTRUCTURE: only the
+scripts tests/golden/make_reference_*.py load it, to generate golden fixtures.
 
 Semantics kept from Taichi where the reference depends on them:
   - fields are arrays of their dtype (float: f32, int: i32); reading an element gives
     a value (a copy), writing stores it; `for i in field` and ti.grouped(field) visit
-    every index; sparse SNodes are dense arrays (inactive elements read 0, which is
-    all the reference reads of them);
+    every index; under a pointer or dynamic SNode a field is stored per leaf block,
+    which its first write activates, and struct-fors visit the active blocks (bitmasked
+    SNodes are dense: the reference only reads their written elements);
   - vectors and matrices are value types (`Vec`, a numpy array with Taichi's methods);
     with numpy's promotion rules, f32 values combined with Python floats stay f32;
   - ti.func calls are inlined in Taichi, so a `ti.template()` argument is passed by
@@ -16,6 +17,7 @@ Semantics kept from Taichi where the reference depends on them:
 """
 from __future__ import annotations
 
+import builtins
 import itertools
 import types as _types
 
@@ -130,10 +132,17 @@ def _index(key):
 
 
 class Field:
+    """A Taichi field. Placed under a pointer or dynamic SNode it is sparse: storage per
+    leaf block (the dense levels below the last pointer), created by the first write into
+    it (`+= 0` included); reads elsewhere give 0; `for I in field` visits every cell of
+    the active blocks. Otherwise it is one dense array."""
+
     def __init__(self, dtype, shape=None, elem=()):
         self.dtype = _dt(dtype)
         self.elem = tuple(elem)
         self.data = None
+        self.sparse = False
+        self.snode = None
         if shape is not None:
             self._alloc(shape)
 
@@ -142,22 +151,64 @@ class Field:
         self.shape = shape
         self.data = np.zeros(shape + self.elem, self.dtype)
 
+    def _bind_sparse(self, shape, block):
+        self.shape, self.block, self.sparse = tuple(shape), tuple(block), True
+        self.blocks = {}
+
+    def parent(self):
+        return self.snode
+
+    def _where(self, idx):
+        return (tuple(v // b for v, b in zip(idx, self.block)), tuple(v % b for v, b in zip(idx, self.block)))
+
     def __getitem__(self, key):
-        v = self.data[_index(key)]
+        idx = _index(key)
+        if self.sparse:
+            bk, loc = self._where(idx)
+            blk = self.blocks.get(bk)
+            v = np.zeros(self.elem, self.dtype) if blk is None else blk[loc]
+        else:
+            v = self.data[idx]
         if self.elem:
             return np.array(v).view(Vec)
         return self.dtype(v)
 
     def __setitem__(self, key, val):
-        self.data[_index(key)] = np.asarray(val)
+        idx = _index(key)
+        if self.sparse:
+            bk, loc = self._where(idx)
+            blk = self.blocks.get(bk)
+            if blk is None:
+                blk = self.blocks[bk] = np.zeros(self.block + self.elem, self.dtype)
+            blk[loc] = np.asarray(val)
+        else:
+            self.data[idx] = np.asarray(val)
 
     def __iter__(self):
+        if self.sparse:
+            def cells():
+                for bk in sorted(self.blocks):
+                    base = [b * e for b, e in zip(bk, self.block)]
+                    for loc in itertools.product(*[range(e) for e in self.block]):
+                        yield tuple(b + l_ for b, l_ in zip(base, loc))
+            return cells()
         if len(self.shape) == 1:
             return iter(range(self.shape[0]))
         return itertools.product(*[range(s) for s in self.shape])
 
+    def _clear(self):
+        if self.sparse:
+            self.blocks = {}
+            self.lengths = {}
+        else:
+            self.data[...] = 0
+
     def fill(self, v):
-        self.data[...] = np.asarray(v)
+        if self.sparse:
+            for blk in self.blocks.values():
+                blk[...] = np.asarray(v)
+        else:
+            self.data[...] = np.asarray(v)
 
     def to_numpy(self):
         return self.data.copy()
@@ -221,7 +272,7 @@ math = _types.SimpleNamespace(
     mat2=_matrix_of(2, 2), mat3=_matrix_of(3, 3),
     eye=lambda n: np.eye(n, dtype=np.float32).view(Vec), pi=np.pi)
 types = _types.SimpleNamespace(vector=lambda n, dt=float: _vector_of(n, dt),
-                               matrix=lambda n, m, dt=float: _matrix_of(n, m, dt))
+                               matrix=lambda n, m, dt=float: _matrix_of(n, m, dt), ndarray=lambda *a, **kw: None)
 
 
 def Struct(**kw):
@@ -251,7 +302,7 @@ def pow(a, b):  # noqa: A001 - Taichi's name
     return np.power(a, b)
 
 
-sqrt, abs, exp, log, floor, ceil, sin, cos = np.sqrt, np.abs, np.exp, np.log, np.floor, np.ceil, np.sin, np.cos
+sqrt, abs, exp, log, floor, sin, cos = np.sqrt, np.abs, np.exp, np.log, np.floor, np.sin, np.cos
 
 
 def max(*a):  # noqa: A001
@@ -283,25 +334,68 @@ def is_active(*a):
 
 
 class SNode:
-    def __init__(self, shape=()):
-        self.shape = tuple(int(s) for s in shape)
-        self.fields = []
+    """A level of an SNode tree: `kind` (root, dense, pointer, bitmasked, dynamic) over
+    `axes` ("ijk" or one letter) with `dims` cells per axis."""
 
-    def _child(self, axes, shape):
-        shape = (shape,) if np.isscalar(shape) else tuple(shape)
-        return SNode(self.shape + tuple(int(s) for s in shape))
+    def __init__(self, kind="root", axes="", dims=(), parent=None):
+        self.kind, self.axes, self.parent_node = kind, axes, parent
+        dims = [dims] * len(axes) if np.isscalar(dims) else [int(d) for d in np.asarray(dims).reshape(-1)]
+        self.dims = dims
+        self.children, self.fields = [], []
 
-    dense = bitmasked = pointer = _child
+    def _child(self, kind, axes, dims, *a, **kw):
+        c = SNode(kind, axes, dims, self)
+        self.children.append(c)
+        return c
+
+    def dense(self, axes, dims):
+        return self._child("dense", axes, dims)
+
+    def pointer(self, axes, dims):
+        return self._child("pointer", axes, dims)
+
+    def bitmasked(self, axes, dims):
+        return self._child("bitmasked", axes, dims)
+
+    def dynamic(self, axes, n, chunk_size=None):
+        return self._child("dynamic", axes, n)
+
+    def _chain(self):
+        c, n = [], self
+        while n is not None and n.kind != "root":
+            c.append(n)
+            n = n.parent_node
+        return c[::-1]
 
     def place(self, *fs):
+        chain = self._chain()
+        order = []
+        for lv in chain:
+            for ax in lv.axes:
+                if ax not in order:
+                    order.append(ax)
+        shape = {ax: 1 for ax in order}
+        block = {ax: 1 for ax in order}
+        last_ptr = builtins.max([n for n, lv in enumerate(chain) if lv.kind in ("pointer", "dynamic")], default=-1)
+        for n, lv in enumerate(chain):
+            for ax, d in zip(lv.axes, lv.dims):
+                shape[ax] *= d
+                if n > last_ptr or lv.kind == "dynamic":
+                    block[ax] *= d
         for f in fs:
-            f._alloc(self.shape)
+            f.snode = self
+            if last_ptr >= 0:
+                f._bind_sparse([shape[a] for a in order], [block[a] for a in order])
+            else:
+                f._alloc([shape[a] for a in order])
             self.fields.append(f)
         return self
 
     def deactivate_all(self):
         for f in self.fields:
-            f.data[...] = 0
+            f._clear()
+        for c in self.children:
+            c.deactivate_all()
 
 
 root = SNode()
@@ -354,3 +448,39 @@ def _all(x):
 
 def _any(x):
     return bool(np.any(np.asarray(x)))
+
+
+def append(node, idx, v):
+    """ti.append on a dynamic SNode: the next slot of the list at cell `idx`."""
+    f = node.fields[0]
+    key = _index(idx)
+    lens = f.__dict__.setdefault("lengths", {})
+    n = lens.get(key, 0)
+    f[key + (n,)] = v
+    lens[key] = n + 1
+    return n
+
+
+def length(node, idx):
+    return node.fields[0].__dict__.get("lengths", {}).get(_index(idx), 0)
+
+
+def svd(A, dt=None):
+    """A = U diag(s) V^T, singular values in descending order, as Taichi's 3x3 SVD."""
+    U, sv, Vt = np.linalg.svd(np.asarray(A, np.float64))
+    t = np.asarray(A).dtype
+    return U.astype(t).view(Vec), np.diag(sv).astype(t).view(Vec), Vt.T.astype(t).view(Vec)
+
+
+_np_ceil = np.ceil
+
+
+def ceil(x, dtype=None):
+    return _np_ceil(x) if dtype is None else _dt(dtype)(_np_ceil(x))
+
+
+def loop_config(*a, **kw):
+    pass
+
+
+tools = _types.SimpleNamespace(PLYWriter=None)

@@ -224,3 +224,30 @@ def test_surface_torus_from_a_field_object(cuda_lib, surf):
     sr.marching_cubes(isolevel=0, smooth_radius=0.06, num_particles=len(pos), pos=Field(pos))
     v, f = weld(sr.mesh_vertex.cpu().numpy(), sr.mesh_index.cpu().numpy())
     assert closed_oriented(f, len(v)) and len(f) == 2 * len(v)
+
+
+def test_surface_matches_the_reference_run(cuda_lib):
+    """The CUDA surface stages against the reference's own SRTool run
+    (tests/golden/ref_surface.npz, srtool.py through the Taichi stand-in): G and x_bar
+    within 1e-4 of scale, the same active blocks, the splat field within 3e-4 and the
+    smoothed field within 2e-4 of scale (the reference sums its splats in f32), sd 1e-4."""
+    import os
+
+    from nonnewton_b200.surface import SRTool
+
+    R = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_surface.npz"))
+    vs, r, srad, iso = (float(v) for v in R["params"])
+    pos = R["pos"]
+    sr = SRTool([[0, 0, 0], [1, 1, 1]], voxel_size=vs, particle_radius=r, max_num_vertices=20000,
+                max_num_indices=200000, max_num_particles=len(pos))
+    assert sr.grid_dims(srad) == [int(d) for d in R["dims"]]
+    sr.dual_contouring(isolevel=iso, smooth_radius=srad, num_particles=len(pos), pos=pos)
+    s0, s1 = sr.stage(0, len(pos)), sr.stage(1, len(pos))
+    assert _scale_err(s0["G"].cpu().numpy(), R["G"]) < 1e-4 and _scale_err(s0["xbar"].cpu().numpy(), R["xbar"]) < 1e-4
+    dims = [int(d) for d in R["dims"]]
+    nb = [-(-d // 32) for d in dims]
+    act = s0["active"].cpu().numpy().reshape(nb[2], nb[1], nb[0])
+    assert np.array_equal(np.argwhere(act)[:, ::-1], R["blocks"])
+    assert _scale_err(s0["field"].cpu().numpy(), R["field_splat"]) < 3e-4
+    assert abs(s1["sd"] - float(R["sd"])) < 1e-4 * float(R["sd"])
+    assert _scale_err(s1["field"].cpu().numpy(), R["field_smooth"]) < 2e-4
