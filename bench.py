@@ -51,6 +51,13 @@ ALG_BYTES = {
 # 2.4M-particle dam break, from `ncu --set full` captures of the current kernels
 # (profiles/k_build_lists_roofline_2m.md, k_density_adv_roofline_2m.md, k_forces_roofline_2m.md).
 NCU_TRAFFIC_2M = {"build_lists": 493_405_696, "density_adv": 380_488_448, "nonpressure": 430_376_960}
+# what bounds each kernel instead of DRAM, from its ncu capture on the 2.4M scene
+# (profiles/k_*_roofline_2m.md): the HBM fraction above is low because none is DRAM-bound
+LIMITER_2M = {
+    "build_lists": "instruction issue: 73 % issue active, ~216 exact f32 distance tests per particle; DRAM 9 %",
+    "density_adv": "L1 data pipe: 80 % of LSU wavefronts (neighbour gathers); DRAM 18 %",
+    "nonpressure": "gather latency: long-scoreboard stalls lead at 46 % warps active; DRAM 13 %",
+}
 KERNEL_IDS = {"pressure_update": 0, "density_adv": 1, "divergence_update": 2, "density_change": 3,
               "density_factor": 4, "build_lists": 5, "cg_matvec": 6, "nonpressure": 7}
 
@@ -481,7 +488,9 @@ def run_surface(args, world, rank):
                    "mesh": {"vertices": nv, "triangles": ni // 3}},
         "roofline": {"bound": "hbm", "kernel": "whole call", "achieved": achieved, "peak": peaks["hbm_gbs"],
                      "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "peak_source": f"{peak_kind} hbm_gbs",
-                     "alg_bytes_per_launch": ab, "traffic": None},
+                     "alg_bytes_per_launch": ab, "traffic": None,
+                     "limiter": "the anisotropic splat's instruction issue (80 % issue active, 60 % of the call; "
+                                "profiles/surface_launches_drop.md), not memory"},
         "gpu_launches": SR_LAUNCHES * args.steps,
         "marching_cubes": {"ms_per_call": mc_ms, "particles_per_s": nf / (mc_ms / 1e3), "calls": mc_steps,
                            "mesh": mc_mesh},
@@ -669,7 +678,8 @@ def run_ours(args):
                      "frac": achieved / hbm, "peak_source": f"{peak_kind} hbm_gbs",
                      "alg_bytes_per_launch": ab, "traffic": traffic,
                      "traffic_source": "ncu dram bytes of one launch, same kernel and workload" if traffic else None,
-                     "kernel_ms": kms, "launches_per_step": per_step, "list_entries": entries},
+                     "kernel_ms": kms, "launches_per_step": per_step, "list_entries": entries,
+                     "limiter": LIMITER_2M.get(dom) if sc.name == "roofline_2m" else None},
         "step_alg_bytes_per_particle": bytes_step,
         "step_roofline_frac": bytes_step * total_ps / (ms_max / 1e3) / 1e9 / hbm,
         "solver": dict({k: st[k] for k in ("iterations_v", "iterations", "cg_iterations", "avg_density_err",
