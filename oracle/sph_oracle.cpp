@@ -7,8 +7,9 @@
 //
 // Parity status: pinned against the reference's own step. Taichi is not installed
 // here, so tests/golden/make_reference_run.py runs SPH/main.py itself in plain Python
-// against a Taichi stand-in on four small scenes (fluid in a boundary box; with the
-// non-Newtonian model; with an elastic cube; with a rigid cube) and stores the state
+// against a Taichi stand-in on five small scenes (fluid in a boundary box; with the
+// non-Newtonian model; with an elastic cube; with a rigid cube; the reference's own
+// test_deformable.json) and stores the state
 // after each step (tests/golden/ref_*.npz). In the reference-quirks mode this oracle
 // reproduces every recorded field of those runs within 1e-5 of its scale
 // (tests/test_reference_pin.py). The neighbour search and the density /

@@ -246,9 +246,27 @@ def scenes():
     return {"dam": (dam, geo, 6), "nonnewton": (nn, geo, 4), "elastic": (el, geo2, 3), "rigid": (rb, geo2, 4)}
 
 
+def reference_scene_files(ref_root: str):
+    """Scenes of the reference's own data/scenes folder, with their models read from its
+    data/models folder: the elastic fixture test_deformable.json (343 particles)."""
+    sys.path.insert(0, os.path.dirname(HERE))
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from nonnewton_b200.scene import read_ply_particles
+
+    out = {}
+    for name, scene, steps in (("deformable", "test_deformable.json", 5),):
+        cfg = json.load(open(os.path.join(ref_root, "SPH", "data", "scenes", scene)))
+        geo = {}
+        for c in cfg.get("FluidParticles", []) + cfg.get("SolidParticles", []):
+            f = os.path.basename(c["geometryFile"])
+            geo[f] = read_ply_particles(os.path.join(ref_root, "SPH", "data", "models", f))
+        out[name] = (cfg, geo, steps)
+    return out
+
+
 def main(ref_root: str):
     ref = load_reference(ref_root)
-    for name, (cfg, geo, steps) in scenes().items():
+    for name, (cfg, geo, steps) in {**scenes(), **reference_scene_files(ref_root)}.items():
         out = run_scene(ref, cfg, geo, steps)
         path = os.path.join(HERE, f"ref_{name}.npz")
         np.savez_compressed(path, **out)
