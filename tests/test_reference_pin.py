@@ -1,9 +1,9 @@
 """The oracle against the reference's own step: tests/golden/ref_<scene>.npz hold the
 particle state after each step of SPH/main.py itself, run through a plain-Python Taichi
-stand-in (tests/golden/make_reference_run.py) on four small scenes of the reference's
-kinds: a fluid block in a boundary box (surface tension and explicit viscosity on, as
-the reference defaults them), the same with the non-Newtonian model on, with an elastic
-cube, and with a rigid cube. The oracle runs in the reference-quirks mode from the same
+stand-in (tests/golden/make_reference_run.py) on five small scenes: a fluid block in a
+boundary box (surface tension and explicit viscosity on, as the reference defaults
+them), the same with the non-Newtonian model on, with an elastic cube, and with a rigid
+cube, and the reference's own elastic fixture scene test_deformable.json. The oracle runs in the reference-quirks mode from the same
 initial state; every recorded field stays within 2e-5 of its scale (f32 rounding and
 summation order; observed up to 2e-6). No GPU."""
 import pytest
