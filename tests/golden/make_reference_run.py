@@ -248,13 +248,14 @@ def scenes():
 
 def reference_scene_files(ref_root: str):
     """Scenes of the reference's own data/scenes folder, with their models read from its
-    data/models folder: the elastic fixture test_deformable.json (343 particles)."""
+    data/models folder: the elastic fixture test_deformable.json (343 particles) and the
+    neighbour-search fixture test_neighbor.json (9 particles)."""
     sys.path.insert(0, os.path.dirname(HERE))
     sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
     from nonnewton_b200.scene import read_ply_particles
 
     out = {}
-    for name, scene, steps in (("deformable", "test_deformable.json", 5),):
+    for name, scene, steps in (("deformable", "test_deformable.json", 5), ("neighbor9", "test_neighbor.json", 5)):
         cfg = json.load(open(os.path.join(ref_root, "SPH", "data", "scenes", scene)))
         geo = {}
         for c in cfg.get("FluidParticles", []) + cfg.get("SolidParticles", []):

@@ -64,7 +64,7 @@ def near_cutoff_pairs(x, h, tol_ulps=4):
 
 # ---- the reference's own step, run once through a Taichi stand-in
 # (tests/golden/make_reference_run.py), stored as tests/golden/ref_<scene>.npz
-REF_SCENES = ("dam", "nonnewton", "elastic", "rigid", "deformable")
+REF_SCENES = ("dam", "nonnewton", "elastic", "rigid", "deformable", "neighbor9")
 REF_FIELDS = ("x", "v", "acceleration", "density", "dfsph_factor", "density_adv", "volume", "strain_rate_norm",
               "nonnewton_viscosity", "stress", "rotations")
 FLUID_ONLY = ("density", "dfsph_factor", "density_adv", "strain_rate_norm", "nonnewton_viscosity")

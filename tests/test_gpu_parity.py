@@ -222,7 +222,7 @@ def test_lone_particles_step_parity(cuda_lib, n_side):
     assert np.all(np.isfinite(x)) and np.abs(x - sc.particles.x[:nf]).max() > 1e-3  # it moved
 
 
-@pytest.mark.parametrize("name", ["dam", "nonnewton", "elastic", "rigid", "deformable"])
+@pytest.mark.parametrize("name", ["dam", "nonnewton", "elastic", "rigid", "deformable", "neighbor9"])
 def test_gpu_matches_the_reference_run(cuda_lib, name):
     """The CUDA step in the reference-quirks mode against the reference's own step
     (tests/golden/ref_<scene>.npz, SPH/main.py run through a Taichi stand-in), free

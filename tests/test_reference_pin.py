@@ -1,9 +1,10 @@
 """The oracle against the reference's own step: tests/golden/ref_<scene>.npz hold the
 particle state after each step of SPH/main.py itself, run through a plain-Python Taichi
-stand-in (tests/golden/make_reference_run.py) on five small scenes: a fluid block in a
+stand-in (tests/golden/make_reference_run.py) on six small scenes: a fluid block in a
 boundary box (surface tension and explicit viscosity on, as the reference defaults
 them), the same with the non-Newtonian model on, with an elastic cube, and with a rigid
-cube, and the reference's own elastic fixture scene test_deformable.json. The oracle runs in the reference-quirks mode from the same
+cube, and the reference's own fixture scenes test_deformable.json (343 elastic
+particles) and test_neighbor.json (9 fluid particles). The oracle runs in the reference-quirks mode from the same
 initial state; every recorded field stays within 2e-5 of its scale (f32 rounding and
 summation order; observed up to 2e-6). No GPU."""
 import pytest
