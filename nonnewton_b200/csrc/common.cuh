@@ -152,7 +152,15 @@ __device__ __forceinline__ float3 kgrad_r2(float3 r, float r2, const SceneDev& s
 // Neighbour loop in batches of NB_U list entries: the NB_U list loads, then the NB_U
 // gathers of `load`, are issued before any `use`, so several dependent load chains
 // are in flight per thread (the passes are latency-bound on list -> gather).
-template <int NB_U, typename Load, typename Use>
+// STREAM loads the list entries evict-first (__ldcs), leaving L2 to the gathered
+// particle data; the passes of the pressure loop gain from it (see their call sites).
+template <bool STREAM>
+__device__ __forceinline__ int nb_list_load(const int32_t* p) {
+  if constexpr (STREAM) return __ldcs(p);
+  else return __ldg(p);
+}
+
+template <int NB_U, bool STREAM = false, typename Load, typename Use>
 __device__ __forceinline__ void nb_batches(const int32_t* __restrict__ list, int stride, int c, int self, Load load,
                                            Use use) {
   // software pipeline: list entries are loaded PD batches (8 entries) ahead of the
@@ -162,7 +170,7 @@ __device__ __forceinline__ void nb_batches(const int32_t* __restrict__ list, int
 #pragma unroll
   for (int p = 0; p < PD; ++p)
 #pragma unroll
-    for (int u = 0; u < NB_U; ++u) q[p][u] = (p * NB_U + u < c) ? __ldg(list + (size_t)(p * NB_U + u) * stride) : self;
+    for (int u = 0; u < NB_U; ++u) q[p][u] = (p * NB_U + u < c) ? nb_list_load<STREAM>(list + (size_t)(p * NB_U + u) * stride) : self;
   for (int k = 0; k < c; k += NB_U) {
     int j[NB_U];
 #pragma unroll
@@ -174,7 +182,7 @@ __device__ __forceinline__ void nb_batches(const int32_t* __restrict__ list, int
 #pragma unroll
     for (int u = 0; u < NB_U; ++u) {
       const int kk = k + PD * NB_U + u;
-      q[PD - 1][u] = (kk < c) ? __ldg(list + (size_t)kk * stride) : self;
+      q[PD - 1][u] = (kk < c) ? nb_list_load<STREAM>(list + (size_t)kk * stride) : self;
     }
     decltype(load(0)) g[NB_U];
 #pragma unroll

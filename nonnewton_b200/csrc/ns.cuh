@@ -277,7 +277,7 @@ __global__ void __launch_bounds__(NS_WARPS * 32) k_build_lists(Dev d) {
     const int ly = __shfl_sync(full, cy, 0), lz = __shfl_sync(full, cz, 0), ls = __shfl_sync(full, scn, 0);
     const bool uniform = __all_sync(full, !valid || (cy == ly && cz == lz && scn == ls));
     auto append = [&](int j) {
-      if (cnt < d.max_nb) d.nbr[(size_t)cnt * d.cap + i] = j;
+      if (cnt < d.max_nb) __stcs(&d.nbr[(size_t)cnt * d.cap + i], j);  // streaming store (see k_density_adv)
       ++cnt;
     };
     if (uniform) {

@@ -198,6 +198,10 @@ __global__ void k_alpha_times_dt(Dev d) {
 
 // compute_density_adv (SPH/main.py:1647-1667). mode 0: first call of pressure_solve,
 // also alpha *= 1/dt^2 (1771); mode 1: iteration, FP64 error (1793-1797).
+// This pass and k_pressure_update, the pressure loop, read their lists evict-first
+// (nb_batches<U, true>) and the list build writes them streaming: -2 % here and
+// -10 % in k_pressure_update, the step 3.475 -> 3.435 ms on the 2.4M scene (the other
+// passes measured flat or slower with it).
 template <int U>
 __global__ void NN_PASS_REGS k_density_adv(Dev d, int mode) {
   const int n = d.d_n[0];
@@ -212,7 +216,7 @@ __global__ void NN_PASS_REGS k_density_adv(Dev d, int mode) {
       const float3 xi = f3(d.w.pos[i]);
       const float3 vi = f3(d.w.vel[i]);
       float delta = 0.f;
-      nb_batches<U>(d.nbr + i, d.cap, d.nbr_cnt[i], i,
+      nb_batches<U, true>(d.nbr + i, d.cap, d.nbr_cnt[i], i,
                  [&](int j) { return GPV{__ldg(&d.w.pos[j]), __ldg(&d.w.vel[j])}; },
                  [&](int, const GPV& g) {
                    const float3 r = xi - f3(g.p);
@@ -256,7 +260,7 @@ __global__ void NN_PASS_REGS k_pressure_update(Dev d) {
       const float k_i = d.kappa[i];
       float4 v4 = d.w.vel[i];
       float3 vi = f3(v4);
-      nb_batches<U>(d.nbr + i, d.cap, d.nbr_cnt[i], i, load, [&](int, const GPK& g) {
+      nb_batches<U, true>(d.nbr + i, d.cap, d.nbr_cnt[i], i, load, [&](int, const GPK& g) {
         const float3 r = xi - f3(g.p);
         if (w_fluid(g.p.w)) {
           const float k_sum = k_i + g.k;
@@ -270,7 +274,7 @@ __global__ void NN_PASS_REGS k_pressure_update(Dev d) {
       const float Vi = fabsf(pi.w);
       const float inv_dt = 1.f / dt;
       float3 ai = make_float3(0.f, 0.f, 0.f);
-      nb_batches<U>(d.nbr + i, d.cap, d.nbr_cnt[i], i, load, [&](int, const GPK& g) {
+      nb_batches<U, true>(d.nbr + i, d.cap, d.nbr_cnt[i], i, load, [&](int, const GPK& g) {
         if (!w_fluid(g.p.w) || !(fabsf(g.k) > s.eps)) return;
         const float3 r = f3(g.p) - xi;  // x_fluid - x_solid, as the fluid computes it
         const float3 vc = kgrad_r2(r, dot3(r, r), s) * (-Vi) * ((-dt * 1.f) * g.k);
