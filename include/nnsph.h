@@ -220,6 +220,13 @@ int nn_step(nn_ctx* ctx, int32_t nsteps, uint32_t flags);
 /* One sub-step method on the bound state (reads and writes nn_state). */
 int nn_run_pass(nn_ctx* ctx, int32_t pass);
 
+/* animate_particles (SPH/main.py:283-309), which SPHBase.step calls after advect: the
+   next nn_step moves every particle of `scene`, static ones included, by
+   displacement[3] (the sum of the scene's animeFile rows for the current frame),
+   between advection and the boundary clamp; the step then clears it. Enqueued on the
+   context's stream. */
+int nn_set_animation(nn_ctx* ctx, int32_t scene, const float* displacement);
+
 /* meta.ns.num_neighbors / meta.ns.neighbors (SPH/main.py:780-781) materialised in
    particle-id space, each row sorted by id and padded with -1. Device outputs:
    num_neighbors [n] int32, neighbors [n, width] int32. */

@@ -62,6 +62,8 @@ struct SceneDyn {
   int32_t pad;
   double cg_alpha, cg_beta;       // PCG scalars of the current iteration
   int64_t steps;
+  float anim[3];                  // animate_particles displacement of the next step
+  int32_t pad2;
 };
 
 // Accumulator slots per scene (each NN_STRIPES doubles).

@@ -437,7 +437,7 @@ static int enq_step(nn_ctx* c, cudaStream_t s) {
   RC(enq_substep(c, s));
   RC(enq_elastic(c, s));
   RC(enq_rigid(c, s));
-  RC(launch(c, s, k_advect_boundary, 256, c->n, d, 1, 1));
+  RC(launch(c, s, k_advect_boundary, 256, c->n, d, 1, 1, 1));
   return launch1(c, s, k_step_end, d);
 }
 
@@ -992,14 +992,24 @@ int nn_run_pass(nn_ctx* c, int32_t pass) {
     case NN_PASS_NON_PRESSURE_ADVECT: RC(launch(c, s, k_np_advect, 256, c->n, d)); break;
     case NN_PASS_PRESSURE_SOLVE: if (c->any_fluid) RC(enq_pressure(c, s, 0)); break;
     case NN_PASS_ELASTICITY: RC(enq_elastic(c, s)); break;
-    case NN_PASS_ADVECT: RC(launch(c, s, k_advect_boundary, 256, c->n, d, 1, 0)); break;
-    case NN_PASS_ENFORCE_BOUNDARY: RC(launch(c, s, k_advect_boundary, 256, c->n, d, 0, 1)); break;
+    case NN_PASS_ADVECT: RC(launch(c, s, k_advect_boundary, 256, c->n, d, 1, 0, 0)); break;
+    case NN_PASS_ENFORCE_BOUNDARY: RC(launch(c, s, k_advect_boundary, 256, c->n, d, 0, 1, 0)); break;
     case NN_PASS_SUBSTEP: RC(enq_substep(c, s)); break;
     case NN_PASS_RIGID: RC(enq_rigid(c, s)); break;
     default: break;
   }
   RC(enq_sync_out(c, s, SM_ALL));
   CK(cudaStreamSynchronize(s));
+  return NN_OK;
+}
+
+int nn_set_animation(nn_ctx* c, int32_t scene, const float* displacement) {
+  RC(check_ready(c));
+  if (!displacement || scene < 0 || scene >= (int32_t)c->scenes.size())
+    return fail(c, NN_ERR_INVALID_ARG, "nn_set_animation: scene %d of %d", scene, (int)c->scenes.size());
+  // pageable source: staged before the call returns, applied in stream order
+  CK(cudaMemcpyAsync(&c->d_dyn[scene].anim[0], displacement, 3 * sizeof(float), cudaMemcpyHostToDevice,
+                     run_stream(c)));
   return NN_OK;
 }
 

@@ -415,7 +415,10 @@ __global__ void k_set_int(int32_t* p, int32_t v) {
 
 __global__ void k_step_end(Dev d) {
   const int ns = d.d_n[1];
-  for (int sc = threadIdx.x; sc < ns; sc += blockDim.x) d.dyn[sc].steps += 1;
+  for (int sc = threadIdx.x; sc < ns; sc += blockDim.x) {
+    d.dyn[sc].steps += 1;
+    d.dyn[sc].anim[0] = d.dyn[sc].anim[1] = d.dyn[sc].anim[2] = 0.f;  // one step only
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1013,12 +1016,24 @@ __global__ void k_el_init(Dev d) {
 // ---------------------------------------------------------------------------
 // advect (SPH/main.py:1086-1093) + enforce_boundary_3D for FLUID then SOLID
 // (SPH/main.py:1044-1080; each particle is handled by the loop of its material).
-__global__ void k_advect_boundary(Dev d, int do_advect, int do_boundary) {
+// do_anim (the step's call only): animate_particles (SPH/main.py:283-309, called by
+// SPHBase.step between advect and the boundary clamp) moves every particle of the
+// scene, static ones too, by the displacement nn_set_animation stored for this step.
+__global__ void k_advect_boundary(Dev d, int do_advect, int do_boundary, int do_anim) {
   const int n = d.d_n[0];
   GRID_STRIDE(i, n) {
     const uint32_t fl = d.w.flags[i];
-    if (!(fl & NN_CLS_DYNAMIC)) continue;
     const int scn = slot_scene(fl);
+    const float* an = d.dyn[scn].anim;
+    const bool move = do_anim && (an[0] != 0.f || an[1] != 0.f || an[2] != 0.f);
+    if (!(fl & NN_CLS_DYNAMIC)) {
+      if (move) {
+        float4 p = d.w.pos[i];
+        p.x += an[0]; p.y += an[1]; p.z += an[2];
+        d.w.pos[i] = p;
+      }
+      continue;
+    }
     const SceneDev& s = d.sc[scn];
     const float dt = d.dyn[scn].dt;
     float4 p = d.w.pos[i];
@@ -1030,6 +1045,7 @@ __global__ void k_advect_boundary(Dev d, int do_advect, int do_boundary) {
       }
       p.x += dt * v.x; p.y += dt * v.y; p.z += dt * v.z;
     }
+    if (move) { p.x += an[0]; p.y += an[1]; p.z += an[2]; }
     if (do_boundary) {
       float pos[3] = {p.x, p.y, p.z};
       float nrm[3] = {0.f, 0.f, 0.f};

@@ -43,6 +43,8 @@ def lib():
         L.nn_initialize.argtypes = [vp]
         L.nn_step.argtypes = [vp, i32, u32]
         L.nn_run_pass.argtypes = [vp, i32]
+        L.nn_set_animation.argtypes = [vp, i32, C.POINTER(C.c_float)]
+        L.nn_set_animation.restype = C.c_int
         L.nn_get_neighbors.argtypes = [vp, vp, vp, i32]
         L.nn_get_stats.argtypes = [vp, i32, C.POINTER(_abi.nn_stats)]
         L.nn_launch_count.argtypes = [vp]
@@ -148,6 +150,11 @@ class Engine:
     def step(self, nsteps: int = 1, sync: bool = True, host_loop: bool = False):
         flags = (_abi.NN_STEP_SYNC_STATE if sync else 0) | (_abi.NN_STEP_HOST_LOOP if host_loop else 0)
         self._rc(self.L.nn_step(self.h, int(nsteps), flags))
+
+    def set_animation(self, scene: int, displacement):
+        """The next step moves every particle of `scene` by `displacement` (3 floats)."""
+        d = (C.c_float * 3)(*[float(v) for v in displacement])
+        self._rc(self.L.nn_set_animation(self.h, int(scene), d))
 
     def run_pass(self, p: int):
         self._rc(self.L.nn_run_pass(self.h, int(p)))

@@ -27,8 +27,14 @@ STATIC, RIGID, ELASTIC = 0, 1, 2
 
 
 # --------------------------------------------------------------------------- PLY
-def read_ply_particles(path: str) -> np.ndarray:
-    """Vertex positions [n,3] float32 from an ASCII or binary little-endian PLY."""
+_PLY_TYPES = {"float": "<f4", "float32": "<f4", "double": "<f8", "float64": "<f8", "int": "<i4", "int32": "<i4",
+              "uchar": "u1", "uint8": "u1", "char": "i1", "int8": "i1", "short": "<i2", "int16": "<i2",
+              "ushort": "<u2", "uint16": "<u2", "uint": "<u4", "uint32": "<u4"}
+
+
+def read_ply_vertex_data(path: str) -> dict:
+    """The vertex properties of an ASCII or binary little-endian PLY by name, each with its
+    declared type (what plyfile's PlyData.read(path)["vertex"] gives the reference)."""
     with open(path, "rb") as f:
         data = f.read()
     end = data.find(b"end_header")
@@ -52,21 +58,29 @@ def read_ply_particles(path: str) -> np.ndarray:
                 nvert = int(t[2])
         elif t[0] == "property" and in_vertex:
             props.append((t[-1], t[1]))
-    names = [p[0] for p in props]
     if fmt == "ascii":
         rows = data[body_start:].decode("ascii").split("\n")
         vals = [r.split() for r in rows if r.strip()][:nvert]
-        arr = np.array([[float(v) for v in r[: len(names)]] for r in vals], dtype=np.float64)
-        cols = [names.index(c) for c in ("x", "y", "z")]
-        return arr[:, cols].astype(np.float32)
+        cols = list(zip(*[r[: len(props)] for r in vals])) if vals else [[] for _ in props]
+        return {n: np.array([float(v) for v in c], dtype=np.float64).astype(_PLY_TYPES[t])
+                for (n, t), c in zip(props, cols)}
     if fmt == "binary_little_endian":
-        tmap = {"float": "<f4", "float32": "<f4", "double": "<f8", "float64": "<f8", "int": "<i4",
-                "int32": "<i4", "uchar": "u1", "uint8": "u1", "char": "i1", "short": "<i2",
-                "ushort": "<u2", "uint": "<u4"}
-        dt = np.dtype([(n, tmap[t]) for n, t in props])
+        dt = np.dtype([(n, _PLY_TYPES[t]) for n, t in props])
         rec = np.frombuffer(data, dtype=dt, count=nvert, offset=body_start)
-        return np.stack([rec["x"], rec["y"], rec["z"]], axis=1).astype(np.float32)
+        return {n: rec[n].copy() for n, _ in props}
     raise ValueError(f"{path}: unsupported PLY format {fmt}")
+
+
+def read_ply_particles(path: str) -> np.ndarray:
+    """Vertex positions [n,3] float32 from an ASCII or binary little-endian PLY."""
+    v = read_ply_vertex_data(path)
+    return np.stack([v["x"], v["y"], v["z"]], axis=1).astype(np.float32)
+
+
+def read_animation(path: str):
+    """An animeFile (SPH/main.py:283-309): frames [k] and displacements [k,3] float32."""
+    v = read_ply_vertex_data(path)
+    return v["frame"].astype(np.int64), np.stack([v["dx"], v["dy"], v["dz"]], axis=1).astype(np.float32)
 
 
 def export_ply_particles(particles: np.ndarray, filename: str) -> None:

@@ -17,7 +17,7 @@ import torch
 from . import _abi
 from .config import Parameter, SimConfig
 from .engine import Engine
-from .scene import ParticleSet, export_ply_particles, load_particles
+from .scene import ParticleSet, export_ply_particles, geometry_path, load_particles, read_animation
 
 FLUID, SOLID = _abi.NN_FLUID, _abi.NN_SOLID
 
@@ -131,7 +131,19 @@ class SPHBase:
         self.host_loop = False
 
     def step(self):
-        """SPHBase.step (SPH/main.py:915-940) as one CUDA-graph replay."""
+        """SPHBase.step (SPH/main.py:915-940) as one CUDA-graph replay. With an animeFile,
+        the frame's displacement (animate_particles, SPH/main.py:283-309) goes in first:
+        the frame is the number of steps taken, the counter the reference's GUI loop
+        keeps (its noGUI loop has none and fails on such a scene)."""
+        anime = getattr(meta, "anime", None)
+        if anime is not None:
+            frames, disp = anime
+            rows = disp[frames == getattr(meta, "step_num", 0)]
+            if len(rows):
+                d = np.zeros(3, np.float32)
+                for r in rows:  # the reference adds each matching row in turn
+                    d = d + r
+                self.engine.set_animation(0, d)
         self.engine.step(1, sync=True, host_loop=self.host_loop)
         meta.ns._lists = None
         meta.step_num = getattr(meta, "step_num", 0) + 1
@@ -141,7 +153,11 @@ class SPHBase:
 
     def run(self, nsteps: int):
         """`nsteps` steps with the particle state kept resident in cell order between
-        steps; meta.pd is written back once at the end."""
+        steps; meta.pd is written back once at the end (step by step with an animeFile)."""
+        if getattr(meta, "anime", None) is not None:
+            for _ in range(int(nsteps)):
+                self.step()
+            return
         self.engine.step(int(nsteps), sync=True, host_loop=self.host_loop)
         meta.ns._lists = None
         meta.step_num = getattr(meta, "step_num", 0) + int(nsteps)
@@ -250,6 +266,8 @@ def initialize(config: SimConfig | str | dict | None = None, particles: Particle
                                        use_sparse_grid=True, engine=meta.engine)
     meta.num_elastic_bodies = len([p for p in ps.phase_info.values() if getattr(p, "solid_type", 0) == 2])
     meta.step_num = 0
+    anime = meta.config.get_cfg("animeFile", None)
+    meta.anime = read_animation(geometry_path(anime, meta.config.scene_path)) if anime else None
     return meta
 
 
@@ -277,7 +295,8 @@ def save_checkpoint(path: str) -> None:
     torch.cuda.synchronize()
     torch.save({"fields": {k: getattr(meta.pd, k).detach().cpu() for k in CHECKPOINT_FIELDS},
                 "step_num": getattr(meta, "step_num", 0), "config": meta.config.config,
-                "quirks": bool(meta.parm.quirks), "n_fluid": int(meta.fluid_particle_num)}, path)
+                "quirks": bool(meta.parm.quirks), "n_fluid": int(meta.fluid_particle_num),
+                "anime": getattr(meta, "anime", None)}, path)
 
 
 def load_checkpoint(path: str, max_neighbors: int = 64, device="cuda", tuning: dict | None = None):
@@ -290,11 +309,18 @@ def load_checkpoint(path: str, max_neighbors: int = 64, device="cuda", tuning: d
     f = ck["fields"]
     ps = ParticleSet(x=f["x"].numpy(), material=f["material"].numpy(), is_dynamic=f["is_dynamic"].numpy(),
                      phase_id=f["phase_id"].numpy(), mass=f["m"].numpy(), n_fluid=ck["n_fluid"])
-    initialize(SimConfig(config=ck["config"]), particles=ps, quirks=ck["quirks"], max_neighbors=max_neighbors,
+    cfg = {**ck["config"], "Configuration": dict(ck["config"].get("Configuration", {}))}
+    cfg["Configuration"].pop("animeFile", None)  # the table travels in the checkpoint
+    initialize(SimConfig(config=cfg), particles=ps, quirks=ck["quirks"], max_neighbors=max_neighbors,
                device=device, tuning=tuning)
     for k in CHECKPOINT_FIELDS:
         getattr(meta.pd, k).copy_(f[k].to(meta.pd.x.device))
     solver = build_solver()
     solver.initialize()
+    # initialize recomputes the static boundary volumes from the current positions; the
+    # run computed them at the initial ones (an animeFile moves the boundary since)
+    meta.pd.volume.copy_(f["volume"].to(meta.pd.x.device))
     meta.step_num = ck["step_num"]
+    meta.anime = ck.get("anime")
+    meta.config = SimConfig(config=ck["config"])
     return meta, solver

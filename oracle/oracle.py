@@ -46,6 +46,7 @@ def lib():
             getattr(L, f).argtypes = [C.c_void_p]
         L.or_step.argtypes = [C.c_void_p, C.c_int]
         L.or_run_pass.argtypes = [C.c_void_p, C.c_int]
+        L.or_set_animation.argtypes = [C.c_void_p, C.c_void_p]
         L.or_get_field.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
         L.or_set_field.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
         L.or_get_neighbors.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
@@ -99,6 +100,11 @@ class OracleSim:
 
     def run_pass(self, p):
         self._rc(lib().or_run_pass(self.h, int(p)))
+
+    def set_animation(self, d):
+        """Displacement added to every particle by the next step (animate_particles)."""
+        a = np.ascontiguousarray(np.asarray(d, dtype=np.float64).reshape(3))
+        self._rc(lib().or_set_animation(self.h, _ptr(a)))
 
     def get(self, name):
         fid, w = FIELDS[name]

@@ -7,11 +7,11 @@
 //
 // Parity status: pinned against the reference's own step. Taichi is not installed
 // here, so tests/golden/make_reference_run.py runs SPH/main.py itself in plain Python
-// against a Taichi stand-in on five small scenes (fluid in a boundary box; with the
+// against a Taichi stand-in on seven small scenes (fluid in a boundary box; with the
 // non-Newtonian model; with an elastic cube; with a rigid cube; the reference's own
-// test_deformable.json) and stores the state
+// test_deformable.json, test_neighbor.json and test_anime.json) and stores the state
 // after each step (tests/golden/ref_*.npz). In the reference-quirks mode this oracle
-// reproduces every recorded field of those runs within 1e-5 of its scale
+// reproduces every recorded field of those runs within 2e-5 of its scale
 // (tests/test_reference_pin.py). The neighbour search and the density /
 // boundary-volume / DFSPH-factor passes are also pinned by known answers derived from
 // the reference's fixtures (tests/golden/make_golden.py) and by an independent numpy
@@ -196,6 +196,8 @@ class SimBase {
   virtual int set_field(int field, const double* in) = 0;
   virtual int get_neighbors(int32_t* counts, int32_t* lists, int32_t width) = 0;
   virtual int64_t neighbor_total() = 0;
+  // displacement added to every particle by the next step (animate_particles)
+  virtual void set_animation(const double* d) = 0;
   OrStats stats;
   std::string err;
 };
@@ -1124,10 +1126,20 @@ class Sim : public SimBase {
     elasticity_substep();
     rigid_step();  // for rb in meta.rbs: coupling_interval x rb.substep() (SPH/main.py:929-931)
     advect();
+    // animate_particles (SPH/main.py:283-309): every particle, static ones too, moves by
+    // the frame's displacement after advection and before the boundary clamp
+    if (anim[0] != R(0) || anim[1] != R(0) || anim[2] != R(0))
+      for (int i = 0; i < n; ++i)
+        for (int d = 0; d < 3; ++d) x[i][d] += anim[d];
+    anim[0] = anim[1] = anim[2] = R(0);  // one step only
     enforce_boundary(NN_FLUID);
     enforce_boundary(NN_SOLID);
     stats.steps += 1;
     return 0;
+  }
+  R anim[3] = {R(0), R(0), R(0)};
+  void set_animation(const double* d) override {
+    for (int k = 0; k < 3; ++k) anim[k] = R(float(d[k]));
   }
 
   // ---- API -------------------------------------------------------------------
@@ -1228,6 +1240,10 @@ void or_destroy(void* s) { delete static_cast<SimBase*>(s); }
 int or_initialize(void* s) { return static_cast<SimBase*>(s)->initialize(); }
 int or_step(void* s, int nsteps) { return static_cast<SimBase*>(s)->step(nsteps); }
 int or_run_pass(void* s, int pass) { return static_cast<SimBase*>(s)->run_pass(pass); }
+int or_set_animation(void* s, const double* d) {
+  static_cast<SimBase*>(s)->set_animation(d);
+  return 0;
+}
 int or_get_field(void* s, int field, double* out) { return static_cast<SimBase*>(s)->get_field(field, out); }
 int or_set_field(void* s, int field, const double* in) { return static_cast<SimBase*>(s)->set_field(field, in); }
 int or_get_neighbors(void* s, int32_t* counts, int32_t* lists, int32_t width) {

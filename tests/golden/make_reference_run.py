@@ -146,7 +146,7 @@ def load_reference(ref_root: str, rel_path: str = "SPH/main.py", module: str = "
 FIELDS = ("x", "v", "acceleration", "density", "dfsph_factor", "density_adv", "volume")
 
 
-def run_scene(ref, config: dict, geometry: dict, steps: int) -> dict:
+def run_scene(ref, config: dict, geometry: dict, steps: int, anime=None) -> dict:
     """initialize(), build_solver(), solver.initialize() and `steps` solver.step() calls
     of the reference, with the state after the initialisation and after each step."""
     with tempfile.NamedTemporaryFile("w", suffix=".json", delete=False) as f:
@@ -175,12 +175,16 @@ def run_scene(ref, config: dict, geometry: dict, steps: int) -> dict:
     with contextlib.redirect_stdout(io.StringIO()):
         meta.config = ref.SimConfig(scene)
         ref.read_ply_particles = lambda p: geometry[os.path.basename(p)]
+        if anime is not None:  # the animeFile's columns, as plyfile gives them
+            ref.read_ply_particles_with_user_data = lambda p: {
+                "frame": anime[0], "dx": anime[1][:, 0], "dy": anime[1][:, 1], "dz": anime[1][:, 2]}
         ref.initialize()
         solver = ref.build_solver()
         solver.initialize()
         meta.step_num = 0
         out = {f"init_{k}": getattr(meta.pd, k).to_numpy() for k in FIELDS}
         for s in range(steps):
+            meta.frame = s  # the GUI loop's frame counter, which animate_particles reads
             solver.step()
             meta.step_num += 1
             for k in FIELDS:
@@ -198,6 +202,8 @@ def run_scene(ref, config: dict, geometry: dict, steps: int) -> dict:
     out["is_dynamic"] = meta.pd.is_dynamic.to_numpy()
     out["phase_id"] = meta.pd.phase_id.to_numpy()
     out["config"] = np.frombuffer(json.dumps(config).encode(), np.uint8)
+    if anime is not None:
+        out["anime_frames"], out["anime_disp"] = anime
     return out
 
 
@@ -248,27 +254,33 @@ def scenes():
 
 def reference_scene_files(ref_root: str):
     """Scenes of the reference's own data/scenes folder, with their models read from its
-    data/models folder: the elastic fixture test_deformable.json (343 particles) and the
-    neighbour-search fixture test_neighbor.json (9 particles)."""
+    data/models folder: the elastic fixture test_deformable.json (343 particles), the
+    neighbour-search fixture test_neighbor.json (9 particles) and test_anime.json (one
+    particle moved by the animeFile test_anime.ply)."""
     sys.path.insert(0, os.path.dirname(HERE))
     sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
-    from nonnewton_b200.scene import read_ply_particles
+    from nonnewton_b200.scene import read_animation, read_ply_particles
 
     out = {}
-    for name, scene, steps in (("deformable", "test_deformable.json", 5), ("neighbor9", "test_neighbor.json", 5)):
+    for name, scene, steps in (("deformable", "test_deformable.json", 5), ("neighbor9", "test_neighbor.json", 5),
+                               ("anime", "test_anime.json", 8)):
         cfg = json.load(open(os.path.join(ref_root, "SPH", "data", "scenes", scene)))
         geo = {}
         for c in cfg.get("FluidParticles", []) + cfg.get("SolidParticles", []):
             f = os.path.basename(c["geometryFile"])
             geo[f] = read_ply_particles(os.path.join(ref_root, "SPH", "data", "models", f))
-        out[name] = (cfg, geo, steps)
+        af = cfg["Configuration"].get("animeFile")
+        anime = read_animation(os.path.join(ref_root, "SPH", "data", "models", os.path.basename(af))) if af else None
+        out[name] = (cfg, geo, steps, anime)
     return out
 
 
 def main(ref_root: str):
     ref = load_reference(ref_root)
-    for name, (cfg, geo, steps) in {**scenes(), **reference_scene_files(ref_root)}.items():
-        out = run_scene(ref, cfg, geo, steps)
+    runs = {k: v + (None,) for k, v in scenes().items()}
+    runs.update(reference_scene_files(ref_root))
+    for name, (cfg, geo, steps, anime) in runs.items():
+        out = run_scene(ref, cfg, geo, steps, anime)
         path = os.path.join(HERE, f"ref_{name}.npz")
         np.savez_compressed(path, **out)
         print(f"wrote {path}: {len(out['material'])} particles, {steps} steps")

@@ -64,7 +64,7 @@ def near_cutoff_pairs(x, h, tol_ulps=4):
 
 # ---- the reference's own step, run once through a Taichi stand-in
 # (tests/golden/make_reference_run.py), stored as tests/golden/ref_<scene>.npz
-REF_SCENES = ("dam", "nonnewton", "elastic", "rigid", "deformable", "neighbor9")
+REF_SCENES = ("dam", "nonnewton", "elastic", "rigid", "deformable", "neighbor9", "anime")
 REF_FIELDS = ("x", "v", "acceleration", "density", "dfsph_factor", "density_adv", "volume", "strain_rate_norm",
               "nonnewton_viscosity", "stress", "rotations")
 FLUID_ONLY = ("density", "dfsph_factor", "density_adv", "strain_rate_norm", "nonnewton_viscosity")
@@ -81,6 +81,7 @@ def reference_run(name):
 
     R = dict(np.load(os.path.join(os.path.dirname(__file__), "golden", f"ref_{name}.npz")))
     cfg = json.loads(R["config"].tobytes().decode())
+    cfg["Configuration"].pop("animeFile", None)  # its table is in the fixture (reference_animation)
     param = Parameter.from_config(SimConfig(config=cfg), quirks=True)
     phases = []
     for uid in dict.fromkeys(R["phase_id"].tolist()):
@@ -89,6 +90,19 @@ def reference_run(name):
         phases.append(S.PhaseInfo(uid=uid, material=int(R["material"][m][0]), is_dynamic=bool(R["is_dynamic"][m][0]),
                                   pos=R["init_x"][m], solid_type=st))
     return R, cfg, param, S.assemble(phases, param)
+
+
+def reference_animation(R):
+    """(frames, displacements) of the run's animeFile, or None."""
+    return (R["anime_frames"], R["anime_disp"]) if "anime_frames" in R else None
+
+
+def frame_displacement(anime, frame):
+    """The displacement animate_particles (SPH/main.py:283-309) adds at `frame`: the sum
+    of the table's rows for that frame, or None."""
+    if anime is None or not (anime[0] == frame).any():
+        return None
+    return anime[1][anime[0] == frame].astype(np.float32).sum(axis=0)
 
 
 def reference_steps(R):

@@ -156,3 +156,27 @@ def test_scene_geometry_resolves_like_the_reference_layout(tmp_path, monkeypatch
     assert np.allclose(ps.x[:125], cube + 0.5, atol=1e-6)
     with pytest.raises(FileNotFoundError):
         geometry_path("./data/models/missing.ply", str(path))
+
+
+def test_animation_file_reads_as_plyfile_gives_it(tmp_path):
+    """An animeFile (SPH/main.py:283-309) is a PLY whose vertices carry frame, dx, dy and
+    dz; ASCII and binary files give the same table, each column with its declared type."""
+    import numpy as np
+
+    from nonnewton_b200.scene import read_animation, read_ply_vertex_data
+
+    frames = np.array([0, 3, 3, 7], np.int32)
+    disp = np.array([[0.5, 0, 0], [0, -0.25, 0], [0, 0, 0.125], [1, 2, 3]], np.float32)
+    head = "ply\nformat {}\nelement vertex 4\nproperty int frame\nproperty float dx\nproperty float dy\n" \
+           "property float dz\nend_header\n"
+    a = tmp_path / "a.ply"
+    a.write_text(head.format("ascii 1.0") + "".join(f"{f} {x} {y} {z}\n" for f, (x, y, z) in zip(frames, disp)))
+    b = tmp_path / "b.ply"
+    rec = np.zeros(4, np.dtype([("frame", "<i4"), ("dx", "<f4"), ("dy", "<f4"), ("dz", "<f4")]))
+    rec["frame"], rec["dx"], rec["dy"], rec["dz"] = frames, disp[:, 0], disp[:, 1], disp[:, 2]
+    b.write_bytes(head.format("binary_little_endian 1.0").encode() + rec.tobytes())
+    for f in (a, b):
+        v = read_ply_vertex_data(str(f))
+        assert v["frame"].dtype == np.int32 and v["dx"].dtype == np.float32
+        fr, d = read_animation(str(f))
+        assert np.array_equal(fr, frames) and np.array_equal(d, disp)

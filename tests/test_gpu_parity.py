@@ -222,7 +222,34 @@ def test_lone_particles_step_parity(cuda_lib, n_side):
     assert np.all(np.isfinite(x)) and np.abs(x - sc.particles.x[:nf]).max() > 1e-3  # it moved
 
 
-@pytest.mark.parametrize("name", ["dam", "nonnewton", "elastic", "rigid", "deformable", "neighbor9"])
+def test_animation_moves_the_boundary_too(cuda_lib):
+    """animate_particles (SPH/main.py:283-309) through SPHBase.run: the frames of the
+    table (two rows on frame 2, none on 1 and 3) shift every particle, the static
+    boundary box included, between advection and the clamp; eight steps agree with the
+    oracle given the same per-frame displacements."""
+    from .helpers import frame_displacement
+
+    sc = S.dam_break(seed=4, n_side=(8, 8, 8), box=0.3)
+    m, solver, o = _init_both(sc)
+    nf = sc.particles.n_fluid
+    anime = (np.array([0, 2, 2, 4, 5, 6, 7], np.int64),
+             np.array([[0.004, 0, 0], [0, 0.003, 0], [0, 0, -0.002], [-0.005, 0, 0.001], [0, -0.004, 0],
+                       [0.002, 0.002, 0.002], [0, 0, 0.003]], np.float32))
+    m.anime = anime
+    x0 = pd_field(m, "x")[nf:]
+    solver.run(8)
+    for s in range(8):
+        d = frame_displacement(anime, s)
+        if d is not None:
+            o.set_animation(d)
+        o.step(1)
+    _compare(m, o, ["x", "v", "density", "dfsph_factor"], nf)
+    # the box moved as a whole by the table's total
+    assert np.abs(pd_field(m, "x")[nf:] - x0 - anime[1].sum(0)).max() < 1e-5
+    assert m.engine.stats(0)["status"] == 0
+
+
+@pytest.mark.parametrize("name", ["dam", "nonnewton", "elastic", "rigid", "deformable", "neighbor9", "anime"])
 def test_gpu_matches_the_reference_run(cuda_lib, name):
     """The CUDA step in the reference-quirks mode against the reference's own step
     (tests/golden/ref_<scene>.npz, SPH/main.py run through a Taichi stand-in), free
@@ -230,10 +257,11 @@ def test_gpu_matches_the_reference_run(cuda_lib, name):
     from nonnewton_b200 import sph
     from nonnewton_b200.config import SimConfig
 
-    from .helpers import reference_errors, reference_run, reference_steps
+    from .helpers import reference_animation, reference_errors, reference_run, reference_steps
 
     R, cfg, param, ps = reference_run(name)
     m = sph.initialize(SimConfig(config=cfg), particles=ps, quirks=True)
+    m.anime = reference_animation(R)  # what initialize reads from an animeFile
     solver = sph.build_solver()
     solver.initialize()
     for s in range(reference_steps(R)):

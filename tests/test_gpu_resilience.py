@@ -40,6 +40,34 @@ def test_checkpoint_resume_bit_identical(cuda_lib, tmp_path, kind):
     assert np.array_equal(pd_field(m2, "x"), x_ref) and np.array_equal(pd_field(m2, "v"), v_ref)
 
 
+def test_checkpoint_keeps_the_animation(cuda_lib, tmp_path):
+    """A checkpoint carries the animeFile table and the frame count: a resumed run moves
+    by the frames it had not reached, bit-identical to the uninterrupted one."""
+    from nonnewton_b200 import sph
+
+    sc = S.dam_break(seed=2, n_side=(6, 6, 6), box=0.25)
+    anime = (np.array([1, 3, 6, 8], np.int64),
+             np.array([[0.003, 0, 0], [0, 0.002, 0], [0, 0, 0.004], [-0.002, 0, 0]], np.float32))
+    m, solver = gpu_sim(sc)
+    m.anime = anime
+    solver.initialize()
+    for _ in range(10):
+        solver.step()
+    x_ref = pd_field(m, "x")
+    m, solver = gpu_sim(sc)
+    m.anime = anime
+    solver.initialize()
+    for _ in range(5):
+        solver.step()
+    path = str(tmp_path / "ck.pt")
+    sph.save_checkpoint(path)
+    m2, solver2 = sph.load_checkpoint(path)
+    assert m2.step_num == 5 and np.array_equal(m2.anime[0], anime[0])
+    for _ in range(5):
+        solver2.step()
+    assert np.array_equal(pd_field(m2, "x"), x_ref)
+
+
 def test_nonfinite_state_sets_status(cuda_lib):
     import torch
 

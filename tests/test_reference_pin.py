@@ -1,15 +1,17 @@
 """The oracle against the reference's own step: tests/golden/ref_<scene>.npz hold the
 particle state after each step of SPH/main.py itself, run through a plain-Python Taichi
-stand-in (tests/golden/make_reference_run.py) on six small scenes: a fluid block in a
+stand-in (tests/golden/make_reference_run.py) on seven small scenes: a fluid block in a
 boundary box (surface tension and explicit viscosity on, as the reference defaults
 them), the same with the non-Newtonian model on, with an elastic cube, and with a rigid
 cube, and the reference's own fixture scenes test_deformable.json (343 elastic
-particles) and test_neighbor.json (9 fluid particles). The oracle runs in the reference-quirks mode from the same
+particles), test_neighbor.json (9 fluid particles) and test_anime.json (one particle
+moved by an animeFile's per-frame displacements, the frame being the step index, as the
+GUI loop counts it). The oracle runs in the reference-quirks mode from the same
 initial state; every recorded field stays within 2e-5 of its scale (f32 rounding and
 summation order; observed up to 2e-6). No GPU."""
 import pytest
 
-from .helpers import REF_SCENES, reference_errors, reference_run, reference_steps
+from .helpers import REF_SCENES, frame_displacement, reference_animation, reference_errors, reference_run, reference_steps
 
 TOL = 2e-5
 
@@ -24,7 +26,11 @@ def test_oracle_matches_the_reference_run(name):
     assert abs(o.get("volume") - R["init_volume"]).max() <= TOL * abs(R["init_volume"]).max()
     # the reference's first search runs on the same positions: the same neighbour counts
     assert (o.neighbors(60)[0] == R["step0_num_neighbors"]).all()
+    anime = reference_animation(R)
     for s in range(reference_steps(R)):
+        d = frame_displacement(anime, s)
+        if d is not None:
+            o.set_animation(d)
         o.step(1)
         err = reference_errors(R, s, o.get, ps.n_fluid)
         assert err and max(err.values()) < TOL, (s, err)
