@@ -45,58 +45,107 @@ class Batch:
         self.starts: list[int] = []
         self.n = 0
         self.cell_factor = 1
+        self._cparams: dict = {}
+        self._pin = None      # pinned staging buffers (see stage)
+        self._pin_ev = None   # recorded after the last copies out of them
 
     # -- packing -----------------------------------------------------------------
-    def _write_scene(self, sc: Scene, start: int):
-        ps = sc.particles
-        dev = self.pd.x.device
-        sl = slice(start, start + ps.n)
-        x = torch.from_numpy(np.ascontiguousarray(ps.x, np.float32)).to(dev)
-        pd = self.pd
-        pd.x[sl] = x
-        pd.x_0[sl] = x
-        pd.v[sl] = 0
-        pd.acceleration[sl] = 0
-        pd.volume[sl] = sc.param.volume0
-        pd.m[sl] = torch.from_numpy(ps.mass).to(dev)
-        pd.density[sl] = sc.param.density0
-        pd.dfsph_factor[sl] = 0
-        pd.density_adv[sl] = 0
-        pd.material[sl] = torch.from_numpy(ps.material).to(dev)
-        pd.is_dynamic[sl] = torch.from_numpy(ps.is_dynamic).to(dev)
-        pd.phase_id[sl] = torch.from_numpy(ps.phase_id).to(dev)
+    _STAGED = (("x", 3, torch.float32), ("m", 1, torch.float32), ("material", 1, torch.int32),
+               ("is_dynamic", 1, torch.int32), ("phase_id", 1, torch.int32), ("volume", 1, torch.float32),
+               ("density", 1, torch.float32))
 
-    def set(self, scenes: list[Scene], initialize: bool = True):
-        """Pack `scenes` from their initial states and initialise them."""
+    def stage(self, scenes: list[Scene]) -> dict | None:
+        """The initial states of `scenes`, written field by field into pinned host
+        buffers of the batch's capacity (allocated once), so that packing them is one
+        asynchronous copy per field. Host work only: a server stages arriving scenes
+        while the GPU runs the batch."""
+        if not scenes:
+            return None
+        n = sum(sc.particles.n for sc in scenes)
+        if n > self.capacity:
+            raise ValueError(f"{n} particles exceed the batch capacity {self.capacity}")
+        if self._pin is None:
+            self._pin = {name: torch.empty((self.capacity, w) if w > 1 else (self.capacity,), dtype=dt,
+                                           pin_memory=True) for name, w, dt in self._STAGED}
+        if self._pin_ev is not None:
+            self._pin_ev.synchronize()  # the previous staging's copies have left the buffers
+        buf = {name: t.numpy() for name, t in self._pin.items()}
+        off = 0
+        for sc in scenes:
+            p = sc.particles
+            sl = slice(off, off + p.n)
+            buf["x"][sl] = p.x.reshape(-1, 3)
+            buf["m"][sl] = p.mass
+            buf["material"][sl] = p.material
+            buf["is_dynamic"][sl] = p.is_dynamic
+            buf["phase_id"][sl] = p.phase_id
+            buf["volume"][sl] = sc.param.volume0
+            buf["density"][sl] = sc.param.density0
+            off += p.n
+        return {"n": n, **{name: t[:n] for name, t in self._pin.items()}}
+
+    def _write_staged(self, st: dict, start: int):
+        """Rows [start, start + n) from a staging of `stage`: the initial state of each
+        scene (x_0 = x, zero velocity and acceleration, volume0, density0)."""
+        pd = self.pd
+        sl = slice(start, start + st["n"])
+        for name, _, _ in self._STAGED:
+            getattr(pd, name)[sl].copy_(st[name], non_blocking=True)
+        pd.x_0[sl].copy_(pd.x[sl])
+        for name in ("v", "acceleration", "dfsph_factor", "density_adv"):
+            getattr(pd, name)[sl].zero_()
+        self._pin_ev = torch.cuda.Event()
+        self._pin_ev.record()
+
+    def set(self, scenes: list[Scene], initialize: bool = True, staged: dict | None = None):
+        """Pack `scenes` from their initial states and initialise them. `staged` is
+        `stage(scenes)` when the caller made it beforehand."""
         total = sum(sc.particles.n for sc in scenes)
         if total > self.capacity:
             raise ValueError(f"{total} particles exceed the batch capacity {self.capacity}")
         self.scenes, self.starts = list(scenes), []
         start = 0
         for sc in scenes:
-            self._write_scene(sc, start)
             self.starts.append(start)
             start += sc.particles.n
+        if scenes:
+            self._write_staged(staged if staged is not None else self.stage(scenes), 0)
         self.n = total
         self._bind_and_describe()
         if initialize:
             self.engine.initialize()
 
     def _bind_and_describe(self):
+        """Bind the state and describe the scenes. A scene's parameter struct is made
+        when it is packed and reused while it stays resident."""
+        cache = {}
+        for sc in self.scenes:
+            ent = self._cparams.get(id(sc))
+            cache[id(sc)] = ent if ent is not None and ent[0] is sc else (sc, sc.param.to_c())
+        self._cparams = cache
         self.engine.bind(self.pd, self.n)
-        self.engine.set_scenes([(s, sc.particles.n, sc.particles.n_fluid, sc.param.to_c())
+        self.engine.set_scenes([(s, sc.particles.n, sc.particles.n_fluid, cache[id(sc)][1])
                                 for s, sc in zip(self.starts, self.scenes)])
 
-    def repack(self, keep: list[int], new: list[Scene]):
+    def repack(self, keep: list[int], new: list[Scene], staged: dict | None = None):
         """Continuous batching: keep the resident scenes `keep` (indices into the
         current list) with their current states, drop the others, append `new` ones
-        from their initial states. Only the new scenes need initialising, but the
-        static-boundary volumes of all scenes are recomputed (same values)."""
+        from their initial states (`staged` = `stage(new)` when made beforehand). Only
+        the new scenes need initialising, but the static-boundary volumes of all scenes
+        are recomputed (same values)."""
         pd = self.pd
-        rows = [torch.arange(self.starts[k], self.starts[k] + self.scenes[k].particles.n, device=pd.x.device)
-                for k in keep]
-        idx = torch.cat(rows) if rows else torch.zeros(0, dtype=torch.long, device=pd.x.device)
-        m = int(idx.numel())
+        dev = pd.x.device
+        # source row of every kept particle: its new row plus its scene's shift
+        lens = [self.scenes[k].particles.n for k in keep]
+        m = sum(lens)
+        shift, at = [], 0
+        for k, ln in zip(keep, lens):
+            shift.append(self.starts[k] - at)
+            at += ln
+        idx = torch.arange(m, device=dev)
+        if m:
+            idx += torch.repeat_interleave(torch.tensor(shift, dtype=torch.long, device=dev),
+                                           torch.tensor(lens, dtype=torch.long, device=dev), output_size=m)
         for name in ("x", "x_0", "v", "acceleration", "volume", "m", "density", "pressure", "dfsph_factor",
                      "density_adv", "material", "is_dynamic", "phase_id", "strain_rate_norm",
                      "nonnewton_viscosity", "stress", "rotations"):
@@ -110,8 +159,9 @@ class Batch:
         total = start + sum(sc.particles.n for sc in new)
         if total > self.capacity:
             raise ValueError("repack exceeds capacity")
+        if new:
+            self._write_staged(staged if staged is not None else self.stage(new), start)
         for sc in new:
-            self._write_scene(sc, start)
             starts.append(start)
             scenes.append(sc)
             start += sc.particles.n

@@ -61,84 +61,126 @@ class Server:
 
     def run(self, requests: list[Request], realtime: bool = True) -> dict:
         """Serve `requests` (sorted by arrival). With `realtime`, arrival times are
-        seconds of wall clock from the start of the run; otherwise all are queued."""
+        seconds of wall clock from the start of the run; otherwise all are queued.
+
+        The host work of a chunk boundary overlaps the chunk in flight: which requests
+        retire after it is known from the step counts, so the admissions are planned
+        while the GPU runs. Then the loop waits for the chunk, reads the status words
+        (a failed scene retires at once), and enqueues back to back the copy of the
+        finished results into pinned memory, the repack and the next chunk. Results
+        reach their requests when their copy has landed."""
         queue = sorted(requests, key=lambda r: r.arrival)
         qi = 0
         t0 = time.perf_counter()
         now = lambda: time.perf_counter() - t0
         finished = []
         total_ps = 0
-        while qi < len(queue) or self.resident:
-            # retire finished requests
-            done = [r for r in self.resident if r.done_steps >= r.steps]
-            keep_idx = [k for k, r in enumerate(self.resident) if r.done_steps < r.steps]
-            if done:  # one device-to-host copy of all finished results and stats
-                ks = [k for k, r in enumerate(self.resident) if r.done_steps >= r.steps]
-                xs = torch.cat([self.batch.scene_view(k, "x") for k in ks]).cpu().numpy()
-                st = self.batch.engine.stats_range(0, len(self.resident))
-                off = 0
+        cells: dict[int, int] = {}  # grid cells of each request's scene (admission by footprint)
+
+        def cells_of(r):
+            c = cells.get(id(r))
+            if c is None:
+                c = cells[id(r)] = scene_grid_cells(r.scene)
+            return c
+
+        pending = None  # the chunk in flight: (start event, end event, steps)
+        outbox = []     # retired requests whose results are on their way to the host
+
+        def deliver(block: bool):
+            nonlocal outbox
+            left = []
+            for reqs, stats, host, ev in outbox:
+                if not block and not ev.query():
+                    left.append((reqs, stats, host, ev))
+                    continue
+                ev.synchronize()
                 tf = now()
-                for k in ks:
-                    r = self.resident[k]
+                xs = host.numpy()
+                off = 0
+                for r, y in zip(reqs, stats):
                     m = r.scene.particles.n
-                    r.result_x = xs[off:off + m]
+                    r.result_x = xs[off:off + m].copy()
                     off += m
-                    r.stats = st[k]
+                    r.stats = y
                     r.finished = tf
                     finished.append(r)
-            # admit arrived requests that fit
+            outbox = left
+
+        while qi < len(queue) or self.resident or pending is not None:
+            # plan while the chunk in flight runs: who retires after it, who is admitted
+            keep_idx = [k for k, r in enumerate(self.resident) if r.done_steps < r.steps]
             t = now()
             if not self.resident and qi < len(queue) and realtime and queue[qi].arrival > t:
                 time.sleep(max(0.0, queue[qi].arrival - t))
                 t = now()
             new = []
             n_res = sum(self.resident[k].scene.particles.n for k in keep_idx)
-            c_res = sum(scene_grid_cells(self.resident[k].scene) for k in keep_idx)
+            c_res = sum(cells_of(self.resident[k]) for k in keep_idx)
             while qi < len(queue) and (not realtime or queue[qi].arrival <= t):
                 r = queue[qi]
                 if r.scene.particles.n > self.capacity:
                     raise ValueError(f"request {r.rid} exceeds the batch capacity")
-                cells = scene_grid_cells(r.scene)
-                if (n_res + r.scene.particles.n > self.capacity or c_res + cells > self.max_cells
+                c = cells_of(r)
+                if (n_res + r.scene.particles.n > self.capacity or c_res + c > self.max_cells
                         or len(keep_idx) + len(new) >= self.max_scenes):
                     break
                 r.admitted = t
                 new.append(r)
                 n_res += r.scene.particles.n
-                c_res += cells
+                c_res += c
                 qi += 1
-            if done or new:
+            staged = self.batch.stage([r.scene for r in new])  # pinned host copies, made while the GPU runs
+            # the chunk's end: its timing, and failure detection (a scene whose device
+            # status word is set, from a non-finite state or a neighbour overflow, is
+            # evicted at once; the others go on)
+            st = None
+            if pending is not None:
+                e0, e1, k = pending
+                e1.synchronize()
+                ms = e0.elapsed_time(e1) / k
+                self.device_ms += ms * k
+                for r in self.resident:
+                    r.step_ms.extend([ms] * k)
+                st = self.batch.engine.stats_range(0, len(self.resident))
+                for r, y in zip(self.resident, st):
+                    if y["status"] != 0:
+                        r.failed = y["status"]
+                        r.done_steps = r.steps
+                pending = None
+            done_idx = [k for k, r in enumerate(self.resident) if r.done_steps >= r.steps]
+            keep_idx = [k for k, r in enumerate(self.resident) if r.done_steps < r.steps]
+            if done_idx:  # one device-to-host copy of all finished results, into pinned memory
+                xs = torch.cat([self.batch.scene_view(k, "x") for k in done_idx])
+                host = torch.empty(xs.shape, dtype=xs.dtype, pin_memory=True)
+                host.copy_(xs, non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(self.stream)
+                if st is None:
+                    st = self.batch.engine.stats_range(0, len(self.resident))
+                outbox.append(([self.resident[k] for k in done_idx], [st[k] for k in done_idx], host, ev))
+            if done_idx or new:
+                done = bool(done_idx)
                 self.resident = [self.resident[k] for k in keep_idx] + new
                 if self.resident:
                     if self.batch.scenes and (keep_idx or not done):
-                        self.batch.repack(keep_idx, [r.scene for r in new])
-                    else:
-                        self.batch.set([r.scene for r in self.resident])
+                        self.batch.repack(keep_idx, [r.scene for r in new], staged=staged)
+                    else:  # nothing kept: the resident scenes are the new ones
+                        self.batch.set([r.scene for r in self.resident], staged=staged)
                     self.repacks += 1
-            if not self.resident:
-                continue
-            # advance all resident scenes by one chunk
-            k = min(self.chunk, min(r.steps - r.done_steps for r in self.resident))
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(self.stream)
-            self.batch.step(k, sync=True)
-            e1.record(self.stream)
-            e1.synchronize()
-            ms = e0.elapsed_time(e1) / k
-            self.device_ms += ms * k
-            self.chunks += 1
-            for r in self.resident:
-                r.done_steps += k
-                r.step_ms.extend([ms] * k)
-                total_ps += r.scene.particles.n * k
-            # failure detection: a scene whose device status word is set (non-finite
-            # state, neighbour overflow) is evicted at once; the others go on
-            st = self.batch.engine.stats_range(0, len(self.resident))
-            for r, y in zip(self.resident, st):
-                if y["status"] != 0:
-                    r.failed = y["status"]
-                    r.done_steps = r.steps
+            if self.resident:  # advance all resident scenes by one chunk
+                k = min(self.chunk, min(r.steps - r.done_steps for r in self.resident))
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(self.stream)
+                self.batch.step(k, sync=True)
+                e1.record(self.stream)
+                pending = (e0, e1, k)
+                self.chunks += 1
+                for r in self.resident:
+                    r.done_steps += k
+                    total_ps += r.scene.particles.n * k
+            deliver(block=False)
+        deliver(block=True)
         wall = now()
         lat = np.concatenate([np.asarray(r.step_ms) for r in finished]) if finished else np.zeros(1)
         return {
