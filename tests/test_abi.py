@@ -84,6 +84,9 @@ def test_invalid_arguments_are_rejected_without_a_context(lib):
     hi = (C.c_double * 3)(1, 1, 1)
     assert lib.nn_neighbors_noalloc(None, C.c_int32(10), lo, hi, C.c_double(0.04), C.c_int32(8), None, None,
                                     None) == _abi.NN_ERR_INVALID_ARG
+    lib.nn_set_animation.restype = C.c_int
+    d = (C.c_float * 3)(0.01, 0, 0)
+    assert lib.nn_set_animation(None, C.c_int32(0), d) == _abi.NN_ERR_INVALID_ARG
     lib.nn_sr_create.argtypes = [C.c_int32, C.c_int64, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]
     lib.nn_sr_create.restype = C.c_int
     assert lib.nn_sr_create(0, 1000, 10, 10, 0, C.byref(h)) == _abi.NN_ERR_INVALID_ARG
