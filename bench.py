@@ -50,12 +50,12 @@ ALG_BYTES = {
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch on the
 # 2.4M-particle dam break, from `ncu --set full` captures of the current kernels
 # (profiles/k_build_lists_roofline_2m.md, k_density_adv_roofline_2m.md, k_forces_roofline_2m.md).
-NCU_TRAFFIC_2M = {"build_lists": 493_405_696, "density_adv": 380_488_448, "nonpressure": 430_376_960}
+NCU_TRAFFIC_2M = {"build_lists": 495_109_632, "density_adv": 384_678_912, "nonpressure": 430_376_960}
 # what bounds each kernel instead of DRAM, from its ncu capture on the 2.4M scene
 # (profiles/k_*_roofline_2m.md): the HBM fraction above is low because none is DRAM-bound
 LIMITER_2M = {
     "build_lists": "instruction issue: 73 % issue active, ~216 exact f32 distance tests per particle; DRAM 9 %",
-    "density_adv": "L1 data pipe: 80 % of LSU wavefronts (neighbour gathers); DRAM 18 %",
+    "density_adv": "L1 data pipe: 88 % of L1 throughput (neighbour gathers); DRAM 19 %",
     "nonpressure": "gather latency: long-scoreboard stalls lead at 46 % warps active; DRAM 13 %",
 }
 KERNEL_IDS = {"pressure_update": 0, "density_adv": 1, "divergence_update": 2, "density_change": 3,
