@@ -345,7 +345,7 @@ def run_served(args, world, rank):
                 "h2d_bytes_per_step": int(h2d / batch_steps), "d2h_bytes_per_step": int(d2h / batch_steps)},
         "clocks": cs.summary(),
     }
-    if not args.no_cpu_baseline:
+    if not args.no_cpu_baseline and world == 1:  # the CPU baseline is an N=1 measurement
         line["cpu_baseline"] = cpu_baseline([reqs[0].scene], budget_s=args.cpu_budget)
     print(json.dumps(line))
 
@@ -498,7 +498,7 @@ def run_surface(args, world, rank):
                 "d2h_bytes_per_step": nv * 12 + ni * 4},
         "clocks": cs.summary(),
     }
-    if not args.no_cpu_baseline:
+    if not args.no_cpu_baseline and world == 1:  # an N=1 measurement
         from oracle import surf as OS
 
         sub = surface_sample(pos)
@@ -693,7 +693,7 @@ def run_ours(args):
                 "copies": "pinned host <-> device staging on two copy streams, overlapped with the steps"},
         "clocks": cs.summary(),
     }
-    if not args.no_cpu_baseline:
+    if not args.no_cpu_baseline and world == 1:  # the CPU baseline is an N=1 measurement
         line["cpu_baseline"] = cpu_baseline(scenes, budget_s=args.cpu_budget)
     print(json.dumps(line))
     if world > 1:
