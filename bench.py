@@ -104,7 +104,10 @@ class ClockSampler:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.f = open(self.path, "w")
-            dev = os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")[0] or "0"
+            # this rank's GPU: LOCAL_RANK, through CUDA_VISIBLE_DEVICES when that is set
+            local = int(os.environ.get("LOCAL_RANK", "0"))
+            vis = [v for v in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if v.strip()]
+            dev = vis[local] if local < len(vis) else str(local)
             self.p = subprocess.Popen(["nvidia-smi", "-i", dev, f"--query-gpu={q}", "--format=csv,noheader,nounits",
                                        "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
