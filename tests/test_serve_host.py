@@ -1,0 +1,139 @@
+"""The served loop's host logic on CPU: `Server.run` drives a stand-in batch that
+records what it is asked to do (no GPU). Every request is stepped exactly its own
+number of steps while resident, the batch never holds more particles or scenes than
+its limits, requests are admitted in arrival order, and a scene whose status word is
+set is evicted at the end of the chunk that set it, with the others unaffected."""
+import numpy as np
+import pytest
+import torch
+
+from nonnewton_b200 import scene as S
+from nonnewton_b200 import serve as SV
+
+
+class _Event:
+    def __init__(self, enable_timing=False):
+        self.t = None
+
+    def record(self, stream=None):
+        self.t = _Batch.clock
+
+    def synchronize(self):
+        pass
+
+    def query(self):
+        return True
+
+    def elapsed_time(self, other):
+        return float(other.t - self.t)
+
+
+class _Engine:
+    def __init__(self, batch):
+        self.b = batch
+
+    def stats_range(self, first, count):
+        return [{"status": self.b.status.get(id(sc), 0), "avg_density_err": 0.0, "steps": self.b.done[id(sc)]}
+                for sc in self.b.scenes[first:first + count]]
+
+
+class _Batch:
+    """Stands in for Batch: scenes in packing order; a scene's "x" rows hold the
+    number of steps it has taken."""
+    clock = 0
+
+    def __init__(self, capacity, max_scenes, fail=None):
+        self.capacity, self.max_scenes = capacity, max_scenes
+        self.scenes, self.done, self.status = [], {}, {}
+        self.fail = fail or {}  # id(scene) -> step count at which its status word is set
+        self.engine = _Engine(self)
+        self.log = []
+
+    def _check(self):
+        assert sum(sc.particles.n for sc in self.scenes) <= self.capacity
+        assert len(self.scenes) <= self.max_scenes
+
+    def stage(self, scenes):
+        return {"n": sum(sc.particles.n for sc in scenes), "ids": [id(sc) for sc in scenes]} if scenes else None
+
+    def set(self, scenes, initialize=True, staged=None):
+        assert staged is None or staged["ids"] == [id(sc) for sc in scenes]
+        self.scenes = list(scenes)
+        for sc in scenes:
+            self.done[id(sc)] = 0
+        self.log.append(("set", [id(sc) for sc in scenes]))
+        self._check()
+
+    def repack(self, keep, new, staged=None):
+        assert staged is None or staged["ids"] == [id(sc) for sc in new]
+        assert keep == sorted(keep)
+        self.scenes = [self.scenes[k] for k in keep] + list(new)
+        for sc in new:
+            self.done[id(sc)] = 0
+        self.log.append(("repack", [id(sc) for sc in self.scenes]))
+        self._check()
+
+    def step(self, k, sync=True):
+        _Batch.clock += k
+        for sc in self.scenes:
+            self.done[id(sc)] += k
+            at = self.fail.get(id(sc))
+            if at is not None and self.done[id(sc)] >= at:
+                self.status[id(sc)] = -6
+
+    def scene_view(self, k, name):
+        sc = self.scenes[k]
+        return torch.full((sc.particles.n, 3), float(self.done[id(sc)]))
+
+
+@pytest.fixture
+def fake_cuda(monkeypatch):
+    monkeypatch.setattr(torch.cuda, "Event", _Event)
+    empty = torch.empty
+    monkeypatch.setattr(torch, "empty", lambda *a, pin_memory=False, **k: empty(*a, **k))
+    monkeypatch.setattr(torch.cuda, "current_stream", lambda *a, **k: None)
+
+
+def _server(batch, chunk):
+    srv = SV.Server.__new__(SV.Server)
+    srv.capacity, srv.max_scenes, srv.chunk = batch.capacity, batch.max_scenes, chunk
+    srv.max_cells = 1 << 40
+    srv.batch, srv.resident, srv.stream = batch, [], None
+    srv.chunks = srv.repacks = 0
+    srv.device_ms = 0.0
+    return srv
+
+
+@pytest.mark.parametrize("chunk", [1, 3, 10])
+def test_every_request_gets_exactly_its_steps(fake_cuda, chunk):
+    rng = np.random.default_rng(chunk)
+    reqs = []
+    for k in range(14):
+        sc = S.dam_break(seed=k, n_side=(3 + k % 3, 3, 3), box=0.2)
+        reqs.append(SV.Request(k, sc, int(rng.integers(1, 12)), float(k)))
+    cap = sum(r.scene.particles.n for r in reqs[:4])
+    b = _Batch(cap, max_scenes=3)
+    res = _server(b, chunk).run(reqs, realtime=False)
+    assert res["requests"] == len(reqs) and res["failed"] == []
+    fin = {r.rid: r for r in res["finished"]}
+    for r in reqs:
+        assert fin[r.rid].result_x.shape == (r.scene.particles.n, 3)
+        assert np.all(fin[r.rid].result_x == r.steps), (r.rid, r.steps)  # stepped exactly its steps
+        assert len(fin[r.rid].step_ms) == r.steps
+    # admitted in arrival order: each scene's first appearance in the packing log
+    first = []
+    for _, ids in b.log:
+        first += [i for i in ids if i not in first]
+    assert first == [id(r.scene) for r in reqs]
+    assert res["particle_steps"] == sum(r.scene.particles.n * r.steps for r in reqs)
+
+
+def test_a_failing_scene_is_evicted_after_its_chunk(fake_cuda):
+    reqs = [SV.Request(k, S.dam_break(seed=k, n_side=(3, 3, 3), box=0.2), 9, 0.0) for k in range(5)]
+    b = _Batch(10 ** 9, max_scenes=5, fail={id(reqs[1].scene): 2})
+    res = _server(b, chunk=3).run(reqs, realtime=False)
+    fin = {r.rid: r for r in res["finished"]}
+    assert res["failed"] == [1] and fin[1].failed == -6
+    assert np.all(fin[1].result_x == 3)  # retired at the end of the chunk that set its status
+    for k in (0, 2, 3, 4):
+        assert fin[k].failed == 0 and np.all(fin[k].result_x == 9)
