@@ -183,3 +183,36 @@ def test_animation_file_reads_as_plyfile_gives_it(tmp_path):
         assert v["frame"].dtype == np.int32 and v["dx"].dtype == np.float32
         fr, d = read_animation(str(f))
         assert np.array_equal(fr, frames) and np.array_equal(d, disp)
+
+
+def test_animation_frames_reach_the_engine(monkeypatch):
+    """SPHBase.step passes each frame's displacement (the sum of the animeFile rows for
+    that frame, the frame being the number of steps taken) before the step, and only on
+    frames the table names; run(n) then takes its steps one by one."""
+    import types
+
+    import numpy as np
+
+    from nonnewton_b200 import sph
+
+    calls = []
+
+    class Eng:
+        def set_animation(self, scene, d):
+            calls.append(("anim", scene, np.asarray(d, np.float32).copy()))
+
+        def step(self, n, sync=True, host_loop=False):
+            calls.append(("step", n))
+
+    cfg = types.SimpleNamespace(get_cfg=lambda k, d=None: None)
+    m = types.SimpleNamespace(engine=Eng(), parm=types.SimpleNamespace(gravity=0, density0=1000, dt=1e-3),
+                              ns=types.SimpleNamespace(_lists=None), config=cfg, step_num=0,
+                              anime=(np.array([0, 2, 2, 5], np.int64),
+                                     np.array([[1, 0, 0], [0, 2, 0], [0, 0.5, 3], [4, 4, 4]], np.float32)))
+    monkeypatch.setattr(sph, "meta", m)
+    s = sph.SPHBase()
+    s.run(6)
+    assert [c[0] for c in calls] == ["anim", "step", "step", "anim", "step", "step", "step", "anim", "step"]
+    anims = [c for c in calls if c[0] == "anim"]
+    assert np.array_equal(anims[0][2], [1, 0, 0]) and np.array_equal(anims[1][2], [0, 2.5, 3])
+    assert np.array_equal(anims[2][2], [4, 4, 4]) and m.step_num == 6
