@@ -122,6 +122,24 @@ def test_oracle_f32_vs_f64(oracle_lib):
     assert np.abs(a.get("density")[:nf] - b.get("density")[:nf]).max() / 1000 < 1e-4
 
 
+def test_animation_moves_the_static_boundary_rigidly(oracle_lib):
+    """animate_particles (SPH/main.py:283-309) adds the frame's displacement to every
+    particle: the static boundary, which neither advects nor is clamped, moves by
+    exactly that step's displacement (f32 additions), and only in the step it is set for."""
+    sc = S.dam_break(seed=1, n_side=(6, 6, 6), box=0.3)
+    o = oracle_lib.OracleSim(sc.particles, sc.param, "f32")
+    o.initialize()
+    nf = sc.particles.n_fluid
+    x0 = o.get("x")[nf:].astype(np.float32)
+    d = np.array([0.003, -0.002, 0.001], np.float32)
+    o.set_animation(d)
+    o.step(1)
+    x1 = o.get("x")[nf:]
+    assert np.array_equal(x1, (x0 + d).astype(np.float64))
+    o.step(1)  # the displacement applies to one step only
+    assert np.array_equal(o.get("x")[nf:], x1)
+
+
 def test_polar_rotation(oracle_lib):
     rng = np.random.default_rng(0)
     for _ in range(50):
