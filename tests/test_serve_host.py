@@ -137,3 +137,16 @@ def test_a_failing_scene_is_evicted_after_its_chunk(fake_cuda):
     assert np.all(fin[1].result_x == 3)  # retired at the end of the chunk that set its status
     for k in (0, 2, 3, 4):
         assert fin[k].failed == 0 and np.all(fin[k].result_x == 9)
+
+
+def test_realtime_arrivals_wait_and_all_finish(fake_cuda):
+    """With realtime arrivals the loop sleeps while nothing is resident and admits
+    requests only once they have arrived; every request still gets its steps."""
+    reqs = [SV.Request(k, S.dam_break(seed=k, n_side=(3, 3, 3), box=0.2), 4 + k % 3, 0.004 * k) for k in range(8)]
+    b = _Batch(10 ** 9, max_scenes=8)
+    res = _server(b, chunk=2).run(reqs, realtime=True)
+    fin = {r.rid: r for r in res["finished"]}
+    assert res["requests"] == len(reqs) and res["failed"] == []
+    for r in reqs:
+        assert fin[r.rid].admitted >= r.arrival
+        assert np.all(fin[r.rid].result_x == r.steps)
