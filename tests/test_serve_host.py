@@ -150,3 +150,28 @@ def test_realtime_arrivals_wait_and_all_finish(fake_cuda):
     for r in reqs:
         assert fin[r.rid].admitted >= r.arrival
         assert np.all(fin[r.rid].result_x == r.steps)
+
+
+def test_staging_concatenates_the_initial_states(monkeypatch):
+    """Batch.stage writes the scenes' initial states field by field, one after another,
+    into buffers of the batch's capacity, and refuses more particles than that."""
+    from nonnewton_b200.batch import Batch
+
+    empty = torch.empty
+    monkeypatch.setattr(torch, "empty", lambda *a, pin_memory=False, **k: empty(*a, **k))
+    b = Batch.__new__(Batch)
+    b.capacity, b._pin, b._pin_ev = 5000, None, None
+    scs = [S.dam_break(seed=k, n_side=(3 + k, 4, 3), box=0.2 + 0.05 * k) for k in range(3)]
+    st = b.stage(scs)
+    ps = [sc.particles for sc in scs]
+    assert st["n"] == sum(p.n for p in ps)
+    assert np.array_equal(st["x"].numpy(), np.concatenate([p.x for p in ps]))
+    for f, a in (("m", "mass"), ("material", "material"), ("is_dynamic", "is_dynamic"), ("phase_id", "phase_id")):
+        assert np.array_equal(st[f].numpy(), np.concatenate([getattr(p, a) for p in ps])), f
+    assert np.array_equal(st["volume"].numpy(), np.concatenate([np.full(p.n, sc.param.volume0, np.float32)
+                                                                for sc, p in zip(scs, ps)]))
+    assert np.array_equal(st["density"].numpy(), np.concatenate([np.full(p.n, sc.param.density0, np.float32)
+                                                                 for sc, p in zip(scs, ps)]))
+    assert b.stage([]) is None
+    with pytest.raises(ValueError):
+        b.stage([S.dam_break(seed=9, n_side=(20, 20, 20), box=1.0)])
