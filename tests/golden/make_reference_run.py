@@ -13,7 +13,10 @@ values, so the source is rewritten (ast) where the reference relies on that:
     `ti.atomic_add(f[i], v)` go through helpers that store into the field;
   - `a = b` copies vectors (Taichi vectors are values); `all` / `any` reduce arrays.
 The geometry files of the scenes are replaced by the arrays below (read_ply_particles
-is swapped), and meta.config by the scene dicts.
+is swapped), and meta.config by the scene dicts. An animeFile's table is read with
+this build's PLY reader and served to the reference's animate_particles. The run sets
+meta.frame to the step index before each step, as the reference's GUI loop counts it.
+The fixture carries the table, so its tests need no reference files.
 
 Usage: python tests/golden/make_reference_run.py [/path/to/reference]
 """
