@@ -48,11 +48,10 @@ ALG_BYTES = {
     "build_lists": 16 + 4 + 4,                    # pos4, flags -> count; + 4 B per list entry (added live)
 }
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch on the
-# 2.4M-particle dam break, from `ncu --set full` captures of the current kernels
-# (profiles/k_build_lists_roofline_2m.md, k_density_adv_roofline_2m.md, k_forces_roofline_2m.md).
+# 2.4M-particle dam break, from `ncu --set full` captures of the current kernels.
 NCU_TRAFFIC_2M = {"build_lists": 495_109_632, "density_adv": 384_678_912, "nonpressure": 430_376_960}
-# what bounds each kernel instead of DRAM, from its ncu capture on the 2.4M scene
-# (profiles/k_*_roofline_2m.md): the HBM fraction above is low because none is DRAM-bound
+# what bounds each kernel instead of DRAM, from its ncu capture on the 2.4M scene:
+# the HBM fraction above is low because none is DRAM-bound
 LIMITER_2M = {
     "build_lists": "instruction issue: 73 % issue active, ~216 exact f32 distance tests per particle; DRAM 9 %",
     "density_adv": "L1 data pipe: 88 % of L1 throughput (neighbour gathers); DRAM 19 %",
@@ -77,6 +76,17 @@ def load_peaks():
         d = json.load(open(p))
         return d, "measured"
     return PEAKS_FALLBACK, "fallback"
+
+
+def workload_config(sc, world=1):
+    """The `config` object of a bench line, the same in both arms: which workload, its
+    sizes, how it is spread over the ranks and whether its inputs exceed the L2 (so
+    that no flush is needed between timed steps). The working set counts 48 B of state
+    and about 26 four-byte neighbour-list entries per particle."""
+    n = sc.particles.n
+    return {"workload": sc.name, "particles": n, "fluid": sc.particles.n_fluid,
+            "parallelism": f"replicas{world}",
+            "l2": "inputs larger than L2" if n * (48 + 4 * 26) > 126e6 else "inputs smaller than L2; not flushed"}
 
 
 def make_workload(name, seed=0):
@@ -232,34 +242,45 @@ def run_reference(args):
         name = scenes[0].name
     O.build()
     O.set_threads(os.cpu_count())
-    times, psteps = [], 0
+    times, psteps, warm = [], 0, 0
     t_all = time.perf_counter()
+
+    def out_of_budget():
+        return len(times) >= args.steps or time.perf_counter() - t_all >= args.ref_budget
+
     for sc in scenes:
         o = O.OracleSim(sc.particles, sc.param, "f32")
         o.initialize()
-        for _ in range(min(args.warmup, 1)):
-            o.step(1)
+        if warm < args.warmup:  # as many untimed steps as the GPU arm warms up
+            k = args.warmup - warm if args.workload != "served" else min(args.warmup - warm, args.request_steps)
+            o.step(k)
+            warm += k
         for _ in range(args.request_steps if args.workload == "served" else args.steps):
-            if len(times) >= args.steps or time.perf_counter() - t_all >= args.cpu_budget:
+            if out_of_budget():
                 break
             t0 = time.perf_counter()
             o.step(1)
             times.append(time.perf_counter() - t0)
             psteps += sc.particles.n
-        if len(times) >= args.steps or time.perf_counter() - t_all >= args.cpu_budget:
+        if out_of_budget():
             break
     v = psteps / sum(times)
-    n = scenes[0].particles.n
     cb = {"value": v, "unit": "particle-steps/s", "cores": O.get_threads(), "kind": "port",
-          "sample": f"{len(times)} of {args.steps} requested steps of {name} ({psteps} particle-steps), one full "
-                    f"SPH step each, FP32 oracle, OpenMP {O.get_threads()} threads"}
+          "sample": f"{len(times)} timed steps ({args.steps} requested, {args.ref_budget:.0f} s budget) of {name} "
+                    f"({psteps} particle-steps) after {warm} untimed; one full SPH step each, FP32 oracle, "
+                    f"OpenMP {O.get_threads()} threads"}
+    if args.workload == "served":
+        config = {"workload": "served_mixed", "requests": args.requests, "steps_per_request": args.request_steps,
+                  "arrival_rate_per_s": args.rate}
+    else:
+        config = workload_config(scenes[0], args.gpus)
+    # `steps` is the number of steps actually timed (the budget may stop the run early)
     print(json.dumps({"impl": "reference", "metric": "particle-steps/s", "value": v, "unit": "particle-steps/s",
-                      "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "samples": len(times),
-                      "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
+                      "n_gpus": args.gpus, "steps": len(times), "steps_requested": args.steps,
+                      "warmup": warm, "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
                       "scaling": "weak", "vs_baseline": None,
                       "dtype": "f32", "data": "synthetic (seeded numpy scene generator)",
-                      "config": {"workload": name, "particles": n, "fluid": scenes[0].particles.n_fluid},
-                      "cpu_baseline": cb,
+                      "config": config, "cpu_baseline": cb,
                       "e2e": {"value": v, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
                               "d2h_bytes_per_step": 0}}))
 
@@ -492,8 +513,8 @@ def run_surface(args, world, rank):
         "roofline": {"bound": "hbm", "kernel": "whole call", "achieved": achieved, "peak": peaks["hbm_gbs"],
                      "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "peak_source": f"{peak_kind} hbm_gbs",
                      "alg_bytes_per_launch": ab, "traffic": None,
-                     "limiter": "the anisotropic splat's instruction issue (80 % issue active, 60 % of the call; "
-                                "profiles/surface_launches_drop.md), not memory"},
+                     "limiter": "the anisotropic splat's instruction issue (80 % issue active, 60 % of the "
+                                "call in the ncu launch list), not memory"},
         "gpu_launches": SR_LAUNCHES * args.steps,
         "marching_cubes": {"ms_per_call": mc_ms, "particles_per_s": nf / (mc_ms / 1e3), "calls": mc_steps,
                            "mesh": mc_mesh},
@@ -669,12 +690,8 @@ def run_ours(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded numpy scene generator)",
-        "config": {"workload": sc.name, "particles": n, "fluid": sc.particles.n_fluid,
-                   "parallelism": f"replicas{world}",
-                   "l2": ("inputs larger than L2" if n * (48 + 4 * st["max_neighbors_seen"] * 0.75) > 126e6
-                          else "inputs smaller than L2; not flushed"),
-                   "step_graph": "host-driven loops" if args.host_loop else
-                   "CUDA graph with while-node solver loops",
+        "config": workload_config(sc, world),
+        "launch": {"step_graph": "host-driven loops" if args.host_loop else "CUDA graph with while-node solver loops",
                    "tuning": tuning or {"block": 128, "unroll": 2, "cell_factor": 1}},
         "autotune_ms_per_step": tune_ms,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
@@ -711,7 +728,9 @@ def main():
     ap.add_argument("--workload", default="roofline_2m")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of the CPU-baseline sample")
+    ap.add_argument("--ref-budget", type=float, default=150.0,
+                    help="seconds of timed steps of the reference arm at most (it reports how many ran)")
     ap.add_argument("--requests", type=int, default=512)
     ap.add_argument("--request-steps", type=int, default=100, help="steps of each served request")
     ap.add_argument("--rate", type=float, default=200.0, help="Poisson arrival rate of the served workload (1/s)")

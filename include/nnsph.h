@@ -232,6 +232,18 @@ int nn_set_animation(nn_ctx* ctx, int32_t scene, const float* displacement);
    num_neighbors [n] int32, neighbors [n, width] int32. */
 int nn_get_neighbors(nn_ctx* ctx, int32_t* num_neighbors, int32_t* neighbors, int32_t width);
 
+/* Neighbour-list capacity per particle (the reference's fixed 60-wide list,
+   SPH/main.py:777-781, which it overruns silently). Re-allocates the lists for
+   `max_neighbors` entries (1..1024), clears NN_ERR_NEIGHBOR_OVERFLOW from every
+   scene's status word and drops the captured step graphs; the next nn_step or
+   nn_run_pass(NN_PASS_SEARCH) searches again. The caller re-runs the overflowed
+   step from its own copy of the state before it (x and v are the only state a step
+   carries over; the rest is recomputed or lives in the context). With elastic
+   particles the rest lists are re-sized too and rebuilt by the next nn_initialize
+   (from the rest positions x_0, so the rest state is the same); nn_step and
+   nn_run_pass return NN_ERR_STATE until then. Synchronises the device. */
+int nn_set_neighbor_cap(nn_ctx* ctx, int32_t max_neighbors);
+
 /* Statistics of scene `scene` (copies from the device; synchronises the stream). */
 int nn_get_stats(nn_ctx* ctx, int32_t scene, nn_stats* out);
 
@@ -266,14 +278,21 @@ int nn_time_kernel(nn_ctx* ctx, int32_t kernel, int32_t reps, float* ms_out);
    Its scratch is a file-scope device array of NN_NOALLOC_SCRATCH_BYTES that every GPU
    loading the library holds until the process exits. Inputs and outputs are device
    buffers of the caller: x [n,3] float32; num_neighbors [n] and neighbors [n,width]
-   int32, the same rows as nn_get_neighbors (sorted by particle id, padded with -1,
-   at most NN_NOALLOC_MAX_NEIGHBORS per particle). The grid covers the domain of the
-   scene (positions outside it are clamped into the border cells). Returns
-   NN_ERR_CAPACITY beyond NN_NOALLOC_MAX_PARTICLES particles or
-   NN_ERR_CAPACITY when the domain needs more than NN_NOALLOC_MAX_CELLS cells of edge
-   support_radius. The first call on a device looks up the array's address; make it
-   before any stream capture. All calls share the array: calls that overlap on the
-   GPU race. Work is enqueued on `cuda_stream` (NULL = legacy default stream). */
+   int32. num_neighbors[i] is particle i's full neighbour count. Row i holds, sorted
+   by id and padded with -1, the smallest ids among the neighbours the search stored,
+   at most `width` of them: the same rows as nn_get_neighbors of a context whose
+   neighbour cap is NN_NOALLOC_MAX_NEIGHBORS. The search stores every neighbour
+   unless the count exceeds NN_NOALLOC_MAX_NEIGHBORS; such a count is this call's
+   overflow signal, which the caller reads from num_neighbors without a host
+   synchronisation: that row is incomplete (it is drawn from the first
+   NN_NOALLOC_MAX_NEIGHBORS neighbours found, in cell order).
+   The grid covers the domain of the scene (positions outside it are clamped into the
+   border cells). Returns NN_ERR_CAPACITY beyond NN_NOALLOC_MAX_PARTICLES particles or
+   when the domain needs more than NN_NOALLOC_MAX_CELLS cells of edge support_radius,
+   and NN_ERR_CUDA, launching nothing, when a CUDA error from earlier work is pending.
+   The first call in each CUDA context looks up the array's address in that context;
+   make it before any stream capture. All calls share the array: calls that overlap on
+   the GPU race. Work is enqueued on `cuda_stream` (NULL = legacy default stream). */
 #define NN_NOALLOC_MAX_PARTICLES 16384
 #define NN_NOALLOC_MAX_NEIGHBORS 64
 #define NN_NOALLOC_MAX_CELLS     (1 << 18)

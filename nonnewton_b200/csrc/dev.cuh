@@ -43,7 +43,8 @@ struct Dev {
   uint32_t* cell_count;        // [cells + 1] counts, then exclusive starts
   uint32_t* tile_sums;
   int32_t* nbr;                // [max_nb][cap]
-  int32_t* nbr_cnt;            // [cap]
+  int32_t* nbr_cnt;            // [cap] stored entries, min(count, max_nb)
+  int32_t* nbr_raw;            // [cap] full neighbour count, or null (only the allocation-free search keeps it)
   int32_t cap;                 // slot capacity (neighbour list stride)
   int32_t max_nb;
   // non-Newtonian

@@ -85,6 +85,7 @@ struct nn_ctx {
   float2* cg_aux = nullptr;
   float* cg_pinv = nullptr;
   int el_cap = 64, el_stride = 0;
+  bool el_stale = false;               // rest lists re-sized since the last nn_initialize
   int32_t *el_id = nullptr, *el_slot = nullptr, *e_of_id = nullptr, *el_nb = nullptr, *el_cnt = nullptr;
   float4* el_x0 = nullptr;
   float *el_R = nullptr, *el_S = nullptr;
@@ -843,6 +844,7 @@ int nn_set_scenes(nn_ctx* c, int32_t nscenes, const nn_scene_desc* scenes) {
   c->ncells = (int)cells;
   c->ne = (int)el_id.size();
   free_elastic(c);
+  c->el_stale = false;
 
   if (c->ne > 0) {
     c->el_stride = c->ne;
@@ -910,6 +912,10 @@ static int check_ready(nn_ctx* c) {
   if (!c->bound || c->scenes.empty()) return fail(c, NN_ERR_STATE, "bind a state and set scenes first");
   return NN_OK;
 }
+static int check_elastic(nn_ctx* c) {
+  if (c->el_stale) return fail(c, NN_ERR_STATE, "elastic rest lists were re-sized: call nn_initialize first");
+  return NN_OK;
+}
 
 int nn_initialize(nn_ctx* c) {
   RC(check_ready(c));
@@ -938,11 +944,13 @@ int nn_initialize(nn_ctx* c) {
   RC(launch(c, s, KU(k_boundary_volume), c->block, c->n, d, 1));
   RC(enq_sync_out(c, s, SM_VOL));
   CK(cudaStreamSynchronize(s));
+  c->el_stale = false;
   return NN_OK;
 }
 
 int nn_step(nn_ctx* c, int32_t nsteps, uint32_t flags) {
   RC(check_ready(c));
+  RC(check_elastic(c));
   if (nsteps < 0) return fail(c, NN_ERR_INVALID_ARG, "nsteps < 0");
   cudaStream_t s = run_stream(c);
   if (!s) return fail(c, NN_ERR_STATE, "no stream");
@@ -978,6 +986,7 @@ int nn_run_pass(nn_ctx* c, int32_t pass) {
     return NN_OK;
   }
   if (!c->searched) return fail(c, NN_ERR_STATE, "run the neighbour search first");
+  RC(check_elastic(c));
   Dev d = make_dev(c, c->cur);
   RC(launch(c, s, k_sync_in, 256, c->n, d, (uint32_t)SM_ALL));
   RC(launch1(c, s, k_step_dt, d, 0));
@@ -1062,6 +1071,45 @@ int nn_get_neighbors(nn_ctx* c, int32_t* num, int32_t* lists, int32_t width) {
   return NN_OK;
 }
 
+__global__ void k_clear_overflow(Dev d) {
+  const int ns = d.d_n[1];
+  for (int sc = threadIdx.x; sc < ns; sc += blockDim.x)
+    if (d.dyn[sc].status == NN_ERR_NEIGHBOR_OVERFLOW) d.dyn[sc].status = NN_OK;
+}
+
+int nn_set_neighbor_cap(nn_ctx* c, int32_t max_neighbors) {
+  if (!c) return fail(nullptr, NN_ERR_INVALID_ARG, "null context");
+  if (max_neighbors <= 0 || max_neighbors > 1024)
+    return fail(c, NN_ERR_INVALID_ARG, "nn_set_neighbor_cap: %d entries (1..1024)", max_neighbors);
+  cudaStream_t s = run_stream(c);
+  CK(cudaStreamSynchronize(s));
+  if (max_neighbors != c->max_nb) {
+    drop_graphs(c);  // the list pointer and its capacity are graph arguments
+    cudaFree(c->nbr);
+    c->nbr = nullptr;
+    cudaError_t e = dalloc(&c->nbr, (size_t)c->cap * (size_t)max_neighbors);
+    if (e != cudaSuccess) {
+      c->max_nb = 0;
+      return fail(c, NN_ERR_OOM, "nn_set_neighbor_cap: cudaMalloc of %d x %d entries: %s", c->cap, max_neighbors,
+                  cudaGetErrorString(e));
+    }
+    c->max_nb = max_neighbors;
+  }
+  if (c->ne > 0 && max_neighbors != c->el_cap) {  // rest lists: rebuilt from x_0 by the next nn_initialize
+    cudaFree(c->el_nb);
+    c->el_nb = nullptr;
+    if (dalloc(&c->el_nb, (size_t)c->el_stride * (size_t)max_neighbors) != cudaSuccess)
+      return fail(c, NN_ERR_OOM, "nn_set_neighbor_cap: elastic rest lists");
+    CK(cudaMemset(c->el_cnt, 0, (size_t)c->el_stride * sizeof(int32_t)));
+    c->el_stale = true;
+  }
+  if (c->ne == 0 || c->el_stale) c->el_cap = max_neighbors;
+  if (!c->scenes.empty()) RC(launch1(c, s, k_clear_overflow, make_dev(c, c->cur)));
+  c->searched = false;
+  CK(cudaStreamSynchronize(s));
+  return NN_OK;
+}
+
 static void fill_stats(const SceneDyn& y, nn_stats* out) {
   std::memset(out, 0, sizeof(*out));
   out->size = sizeof(*out);
@@ -1109,8 +1157,8 @@ int nn_get_stats(nn_ctx* c, int32_t scene, nn_stats* out) {
 // that loads libnnsph.so holds NN_NOALLOC_SCRATCH_BYTES of device memory until the
 // process exits. All calls share the array, so calls that overlap on the GPU (on
 // different streams, or from several host threads) race; calls on one stream are
-// ordered. The first call on a device looks up the array's device address; make that
-// first call before any stream capture.
+// ordered. The first call in each CUDA context looks up the array's device address
+// in that context; make that first call before any stream capture.
 namespace {
 constexpr size_t kNaAlign = 256;
 constexpr size_t na_round(size_t b) { return (b + kNaAlign - 1) / kNaAlign * kNaAlign; }
@@ -1133,7 +1181,8 @@ constexpr size_t kOffFlags = kOffPos + na_round(kNaN * sizeof(float4));
 constexpr size_t kOffId = kOffFlags + na_round(kNaN * 4);
 constexpr size_t kOffNbr = kOffId + na_round(kNaN * 4);
 constexpr size_t kOffCnt = kOffNbr + na_round(kNaN * kNaNb * 4);
-constexpr size_t kNaEnd = kOffCnt + na_round(kNaN * 4);
+constexpr size_t kOffRaw = kOffCnt + na_round(kNaN * 4);
+constexpr size_t kNaEnd = kOffRaw + na_round(kNaN * 4);
 static_assert(kNaEnd <= NN_NOALLOC_SCRATCH_BYTES, "no-alloc scratch layout exceeds the array");
 }  // namespace
 
@@ -1165,8 +1214,28 @@ __global__ void k_na_gather(Dev d) {
   }
 }
 
+// Device address of the scratch array per CUDA context: a symbol's address belongs to
+// the module loaded in one context, so a caller on another context of the same device
+// (or after cudaDeviceReset) looks it up again. The current context comes from the
+// driver's cuCtxGetCurrent, reached through the runtime (no link against libcuda).
 static std::mutex g_na_mutex;
-static void* g_na_ptr[256] = {nullptr};
+struct NaAddr { int dev; void* ctx; void* ptr; };
+static std::vector<NaAddr> g_na_addr;
+typedef int (*NaCtxGetCurrent)(void**);
+
+static int na_current_context(void** ctx) {
+  static NaCtxGetCurrent fn = nullptr;
+  if (!fn) {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !f)
+      return -1;
+    fn = reinterpret_cast<NaCtxGetCurrent>(f);
+  }
+  *ctx = nullptr;
+  return fn(ctx) == 0 && *ctx ? 0 : -1;
+}
 
 extern "C" int nn_neighbors_noalloc(const float* x, int32_t n, const double* domain_start,
                                     const double* domain_end, double support_radius, int32_t width,
@@ -1195,20 +1264,37 @@ extern "C" int nn_neighbors_noalloc(const float* x, int32_t n, const double* dom
   if (cells > NN_NOALLOC_MAX_CELLS)
     return fail(c, NN_ERR_CAPACITY, "nn_neighbors_noalloc: the domain needs %lld cells of edge h, maximum %d",
                 (long long)cells, NN_NOALLOC_MAX_CELLS);
+  // an error left by earlier, unrelated work is reported as such, before any launch
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return fail(c, NN_ERR_CUDA, "nn_neighbors_noalloc: a CUDA error was pending from earlier work: %s",
+                cudaGetErrorString(e));
   int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess || dev < 0 || dev >= 256) return fail(c, NN_ERR_CUDA, "nn_neighbors_noalloc: cudaGetDevice failed");
+  e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return fail(c, NN_ERR_CUDA, "nn_neighbors_noalloc: cudaGetDevice: %s", cudaGetErrorString(e));
   unsigned char* base = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_na_mutex);
-    if (!g_na_ptr[dev]) {  // once per device, with that device current
+    void* ctx = nullptr;
+    if (na_current_context(&ctx) != 0) {
+      // no context current yet: the runtime makes the device's primary context current
+      // on its first use, here the address lookup
+      void* p = nullptr;
+      e = cudaGetSymbolAddress(&p, g_nn_noalloc_scratch);
+      if (e != cudaSuccess)
+        return fail(c, NN_ERR_CUDA, "nn_neighbors_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+      if (na_current_context(&ctx) != 0) return fail(c, NN_ERR_CUDA, "nn_neighbors_noalloc: no current CUDA context");
+    }
+    for (const NaAddr& a : g_na_addr)
+      if (a.dev == dev && a.ctx == ctx) base = static_cast<unsigned char*>(a.ptr);
+    if (!base) {  // once per device and context, with that device current
       void* p = nullptr;
       e = cudaGetSymbolAddress(&p, g_nn_noalloc_scratch);
       if (e != cudaSuccess || !p)
         return fail(c, NN_ERR_CUDA, "nn_neighbors_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
-      g_na_ptr[dev] = p;
+      g_na_addr.push_back({dev, ctx, p});
+      base = static_cast<unsigned char*>(p);
     }
-    base = static_cast<unsigned char*>(g_na_ptr[dev]);
   }
   if (n == 0) return NN_OK;
   Dev d{};
@@ -1227,6 +1313,7 @@ extern "C" int nn_neighbors_noalloc(const float* x, int32_t n, const double* dom
   d.w.id = reinterpret_cast<int32_t*>(base + kOffId);
   d.nbr = reinterpret_cast<int32_t*>(base + kOffNbr);
   d.nbr_cnt = reinterpret_cast<int32_t*>(base + kOffCnt);
+  d.nbr_raw = reinterpret_cast<int32_t*>(base + kOffRaw);
   d.cap = NN_NOALLOC_MAX_PARTICLES;
   d.max_nb = NN_NOALLOC_MAX_NEIGHBORS;
   d.t.x = const_cast<float*>(x);

@@ -345,6 +345,7 @@ __global__ void __launch_bounds__(NS_WARPS * 32) k_build_lists(Dev d) {
     }
     if (valid) {
       d.nbr_cnt[i] = min(cnt, d.max_nb);
+      if (d.nbr_raw) d.nbr_raw[i] = cnt;
       if (cnt > d.max_nb) set_status(&d.dyn[scn], NN_ERR_NEIGHBOR_OVERFLOW);
     }
     warp_max_to(&d.dyn[scn].max_nb, cnt, valid);
@@ -352,7 +353,8 @@ __global__ void __launch_bounds__(NS_WARPS * 32) k_build_lists(Dev d) {
 }
 
 // meta.ns.num_neighbors / neighbors in particle-id space, rows sorted by id
-// (materialised on demand for parity checks and the elastic rest state).
+// (materialised on demand for parity checks and the elastic rest state). `num` gets
+// the stored count, or the full count where the search kept it (nbr_raw).
 __global__ void k_export_neighbors(Dev d, int32_t* num, int32_t* lists, int width) {
   const int n = d.d_n[0];
   GRID_STRIDE(i, n) {
@@ -377,6 +379,6 @@ __global__ void k_export_neighbors(Dev d, int32_t* num, int32_t* lists, int widt
       }
     }
     for (int k = w; k < width; ++k) row[k] = -1;
-    num[id] = c;
+    num[id] = d.nbr_raw ? d.nbr_raw[i] : c;
   }
 }

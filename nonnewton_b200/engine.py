@@ -165,6 +165,14 @@ class Engine:
         self._rc(self.L.nn_get_neighbors(self.h, _ptr(num), _ptr(lists), int(width)))
         return num, lists
 
+    def set_neighbor_cap(self, max_neighbors: int):
+        """Re-size the neighbour lists (see nn_set_neighbor_cap); clears overflow statuses."""
+        f = self.L.nn_set_neighbor_cap
+        f.argtypes = [C.c_void_p, C.c_int32]
+        f.restype = C.c_int
+        self._rc(f(self.h, int(max_neighbors)))
+        self.max_neighbors = int(max_neighbors)
+
     def stats(self, scene: int = 0) -> dict:
         s = _abi.nn_stats()
         self._rc(self.L.nn_get_stats(self.h, int(scene), C.byref(s)))

@@ -129,6 +129,9 @@ class SPHBase:
         self.dt = meta.parm.dt
         self.engine: Engine = meta.engine
         self.host_loop = False
+        # re-run a step whose neighbour lists overflowed, with a larger cap
+        self.grow_neighbors = True
+        self._snap = None
 
     def step(self):
         """SPHBase.step (SPH/main.py:915-940) as one CUDA-graph replay. With an animeFile,
@@ -136,6 +139,7 @@ class SPHBase:
         the frame is the number of steps taken, the counter the reference's GUI loop
         keeps (its noGUI loop has none and fails on such a scene)."""
         anime = getattr(meta, "anime", None)
+        d = None
         if anime is not None:
             frames, disp = anime
             rows = disp[frames == getattr(meta, "step_num", 0)]
@@ -143,8 +147,7 @@ class SPHBase:
                 d = np.zeros(3, np.float32)
                 for r in rows:  # the reference adds each matching row in turn
                     d = d + r
-                self.engine.set_animation(0, d)
-        self.engine.step(1, sync=True, host_loop=self.host_loop)
+        self._advance(1, d)
         meta.ns._lists = None
         meta.step_num = getattr(meta, "step_num", 0) + 1
         if meta.config.get_cfg("exportPly"):
@@ -158,13 +161,56 @@ class SPHBase:
             for _ in range(int(nsteps)):
                 self.step()
             return
-        self.engine.step(int(nsteps), sync=True, host_loop=self.host_loop)
+        self._advance(int(nsteps))
         meta.ns._lists = None
         meta.step_num = getattr(meta, "step_num", 0) + int(nsteps)
 
+    def _advance(self, nsteps: int, displacement=None):
+        """`nsteps` steps through the engine. The reference's neighbour list has 60
+        slots (SPH/main.py:777-781) and store_neighbors writes past them unchecked
+        (845-847); here the lists have a checked capacity, and with `grow_neighbors`
+        steps whose lists overflowed it are run again from the state before them (x
+        and v, kept on the device) with the capacity raised past the largest count
+        seen. The check reads the scene's status word, one small device-to-host copy
+        per call."""
+        eng = self.engine
+        if not self.grow_neighbors:
+            if displacement is not None:
+                eng.set_animation(0, displacement)
+            eng.step(nsteps, sync=True, host_loop=self.host_loop)
+            return
+        pd = meta.pd
+        if self._snap is None or self._snap[0].shape != pd.x.shape:
+            self._snap = (torch.empty_like(pd.x), torch.empty_like(pd.v))
+        self._snap[0].copy_(pd.x)
+        self._snap[1].copy_(pd.v)
+        while True:
+            if displacement is not None:
+                eng.set_animation(0, displacement)
+            eng.step(nsteps, sync=True, host_loop=self.host_loop)
+            st = eng.stats(0)
+            if st["status"] != _abi.NN_ERR_NEIGHBOR_OVERFLOW or eng.max_neighbors >= 1024:
+                return
+            self._grow_cap(st)
+            pd.x.copy_(self._snap[0])
+            pd.v.copy_(self._snap[1])
+            if getattr(meta, "num_elastic_bodies", 0):
+                eng.initialize()  # re-sized rest lists, rebuilt from x_0 (the same rest state)
+
+    def _grow_cap(self, st):
+        cap = max(st["max_neighbors_seen"], self.engine.max_neighbors) * 5 // 4
+        self.engine.set_neighbor_cap(min(1024, (cap + 7) // 8 * 8))
+
     def initialize(self):
-        """SPHBase.initialize (SPH/main.py:957-960) and the elastic rest state."""
+        """SPHBase.initialize (SPH/main.py:957-960) and the elastic rest state; with
+        `grow_neighbors`, again with larger lists while they overflow."""
         self.engine.initialize()
+        while self.grow_neighbors and self.engine.max_neighbors < 1024:
+            st = self.engine.stats(0)
+            if st["status"] != _abi.NN_ERR_NEIGHBOR_OVERFLOW:
+                break
+            self._grow_cap(st)
+            self.engine.initialize()
         meta.ns._lists = None
 
     def _pass(self, p):

@@ -58,8 +58,7 @@ def cubic_w(r, h):
     return 0.0
 
 
-def main(ref_root=None):
-    ref_root = ref_root or "/root/reference"
+def main(ref_root: str):
     # 9-point neighbour fixture
     ply = os.path.join(ref_root, "SPH/data/models/test_neighbor.ply")
     grid = np.array([[0.03 * i, 0.03 * j, 0.0] for j in range(3) for i in range(3)], dtype=np.float32)
@@ -98,4 +97,6 @@ def main(ref_root=None):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else None)
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {os.path.basename(__file__)} <path of the reference checkout>")
+    main(sys.argv[1])

@@ -197,16 +197,24 @@ def test_animation_frames_reach_the_engine(monkeypatch):
 
     calls = []
 
+    import torch
+
     class Eng:
+        max_neighbors = 64
+
         def set_animation(self, scene, d):
             calls.append(("anim", scene, np.asarray(d, np.float32).copy()))
 
         def step(self, n, sync=True, host_loop=False):
             calls.append(("step", n))
 
+        def stats(self, scene=0):
+            return {"status": 0, "max_neighbors_seen": 30}
+
     cfg = types.SimpleNamespace(get_cfg=lambda k, d=None: None)
+    pd = types.SimpleNamespace(x=torch.zeros(4, 3), v=torch.zeros(4, 3))
     m = types.SimpleNamespace(engine=Eng(), parm=types.SimpleNamespace(gravity=0, density0=1000, dt=1e-3),
-                              ns=types.SimpleNamespace(_lists=None), config=cfg, step_num=0,
+                              ns=types.SimpleNamespace(_lists=None), config=cfg, step_num=0, pd=pd,
                               anime=(np.array([0, 2, 2, 5], np.int64),
                                      np.array([[1, 0, 0], [0, 2, 0], [0, 0.5, 3], [4, 4, 4]], np.float32)))
     monkeypatch.setattr(sph, "meta", m)
@@ -216,3 +224,54 @@ def test_animation_frames_reach_the_engine(monkeypatch):
     anims = [c for c in calls if c[0] == "anim"]
     assert np.array_equal(anims[0][2], [1, 0, 0]) and np.array_equal(anims[1][2], [0, 2.5, 3])
     assert np.array_equal(anims[2][2], [4, 4, 4]) and m.step_num == 6
+
+
+def test_overflowed_step_runs_again_with_larger_lists(monkeypatch):
+    """SPHBase's growth of the neighbour lists (host logic, fake engine): a step that
+    reports NN_ERR_NEIGHBOR_OVERFLOW is run again after the capacity grows past the
+    largest count seen (by a quarter, rounded to 8), from the x and v it started from,
+    with the frame's displacement set again; a clean step is run once."""
+    import types
+
+    import numpy as np
+    import torch
+
+    from nonnewton_b200 import _abi, sph
+
+    calls = []
+
+    class Eng:
+        max_neighbors = 64
+        overflow_once = True
+
+        def set_animation(self, scene, d):
+            calls.append(("anim",))
+
+        def step(self, n, sync=True, host_loop=False):
+            calls.append(("step", n, float(pd.x[0, 0])))
+            pd.x += 1.0  # the step moves the particles
+
+        def stats(self, scene=0):
+            if self.overflow_once:
+                self.overflow_once = False
+                return {"status": _abi.NN_ERR_NEIGHBOR_OVERFLOW, "max_neighbors_seen": 77}
+            return {"status": 0, "max_neighbors_seen": 77}
+
+        def set_neighbor_cap(self, cap):
+            calls.append(("cap", cap))
+            self.max_neighbors = cap
+
+    cfg = types.SimpleNamespace(get_cfg=lambda k, d=None: None)
+    pd = types.SimpleNamespace(x=torch.zeros(4, 3), v=torch.zeros(4, 3))
+    m = types.SimpleNamespace(engine=Eng(), parm=types.SimpleNamespace(gravity=0, density0=1000, dt=1e-3),
+                              ns=types.SimpleNamespace(_lists=None), config=cfg, step_num=0, pd=pd,
+                              anime=(np.array([0], np.int64), np.array([[1, 0, 0]], np.float32)))
+    monkeypatch.setattr(sph, "meta", m)
+    s = sph.SPHBase()
+    s.step()
+    # 77 * 5 / 4 = 96.25 -> 96; the re-run starts from the same x (0.0) and re-sets the frame
+    assert calls == [("anim",), ("step", 1, 0.0), ("cap", 96), ("anim",), ("step", 1, 0.0)]
+    assert float(pd.x[0, 0]) == 1.0 and m.step_num == 1
+    calls.clear()
+    s.step()
+    assert calls == [("step", 1, 1.0)]

@@ -86,28 +86,78 @@ def test_nonfinite_state_sets_status(cuda_lib):
 
 
 def test_neighbor_overflow_sets_status(cuda_lib):
+    """With the growth of the lists turned off, an overflow is reported, not hidden."""
     sc = S.dam_break(seed=1, n_side=(8, 8, 8), box=0.3)
     m, solver = gpu_sim(sc, max_neighbors=16)
+    solver.grow_neighbors = False
     solver.initialize()
     solver.step()
     st = m.engine.stats(0)
     assert st["status"] == _abi.NN_ERR_NEIGHBOR_OVERFLOW and st["max_neighbors_seen"] > 16
 
 
-def test_served_failed_request_is_evicted(cuda_lib):
-    from nonnewton_b200.serve import Request, Server, run_plain
+def test_overflowed_step_is_rerun_with_larger_lists(cuda_lib):
+    """A step whose lists overflow is run again from the state before it with a larger
+    capacity; the result is bit-identical to a context that had room from the start,
+    for single steps and for a resident run of several."""
+    sc = S.dam_break(seed=1, n_side=(8, 8, 8), box=0.3)
+    out = []
+    for cap in (16, 64):
+        m, solver = gpu_sim(sc)
+        solver.initialize()
+        m.engine.set_neighbor_cap(cap)  # too small for the first step: it overflows and runs again
+        for _ in range(3):
+            solver.step()
+        m.engine.set_neighbor_cap(cap)  # and again for the resident run
+        solver.run(4)
+        st = m.engine.stats(0)
+        assert st["status"] == 0 and m.engine.max_neighbors >= st["max_neighbors_seen"]
+        out.append((pd_field(m, "x"), pd_field(m, "v"), m.engine.max_neighbors))
+    assert out[0][2] > 16
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
 
-    reqs = []
-    for k in range(6):
-        sc = S.dam_break(seed=30 + k, n_side=(6, 6, 7), box=0.28)
-        if k == 2:  # poison one particle of one request
-            sc.particles.x[5] = np.nan
-        reqs.append(Request(k, sc, 10, 0.0))
-    srv = Server(capacity=sum(r.scene.particles.n for r in reqs[:3]), max_scenes=3, chunk=5)
-    res = srv.run(reqs, realtime=False)
-    assert res["requests"] == 6 and res["failed"] == [2]
-    alone = [Request(r.rid, r.scene, r.steps, 0.0) for r in reqs if r.rid != 2]
-    run_plain(alone)
-    fin = {r.rid: r for r in res["finished"]}
-    for a in alone:
-        assert np.array_equal(fin[a.rid].result_x, a.result_x)
+
+def test_overlaid_cubes_grow_the_lists(cuda_lib, tmp_path):
+    """The layout of the reference's test_loadparticles.json: six copies of one cube
+    lattice (a stand-in for its cube.ply, 25^3 particles at 0.02 m over [0.26, 0.74] m)
+    placed as fluid, rigid, static and elastic phases at the scene's translations. The
+    copies overlap, up to three particles share a position, and neighbour counts pass
+    the default 64 entries; the reference's 60-entry lists (SPH/main.py:777-781,
+    845-847) are overrun. Here initialize() and the steps grow the lists, the status
+    stays clean and the state finite, and the run equals one with room from the start."""
+    import json
+
+    import torch
+
+    from nonnewton_b200 import sph
+    from nonnewton_b200.config import Parameter, SimConfig
+
+    models = tmp_path / "data" / "models"
+    models.mkdir(parents=True)
+    S.export_ply_particles(S.block([0.26] * 3, [25] * 3, 0.02).astype(np.float32), str(models / "cube.ply"))
+    geo = "./data/models/cube.ply"
+    conf = {"Configuration": {"domainStart": [0.0, 0.0, 0.0], "domainEnd": [2.0, 2.0, 2.0], "particleRadius": 0.01,
+                              "density0": 1000, "simulationMethod": 4, "gravitation": [0.0, -9.81, 0.0],
+                              "timeStepSize": 0.004},
+            "FluidParticles": [{"geometryFile": geo, "translation": [0.0, 0.0, -0.3]},
+                               {"geometryFile": geo, "translation": [0.0, 0.0, 0.3]}],
+            "SolidParticles": [{"geometryFile": geo, "solidType": "RIGID", "translation": [-0.2, -0.2, 0.0]},
+                               {"geometryFile": geo, "solidType": "STATIC", "translation": [0, 0.1, 0.0]},
+                               {"geometryFile": geo, "solidType": "ELASTIC", "translation": [0.4, 0.4, 0.0]},
+                               {"geometryFile": geo, "solidType": "RIGID", "translation": [0.8, 0.8, 0.0]}]}
+    (tmp_path / "scene.json").write_text(json.dumps(conf))
+    cfg = SimConfig(config=conf)
+    ps = S.load_particles(cfg, Parameter.from_config(cfg), root=str(tmp_path))
+    assert ps.n == 6 * 25 ** 3
+    out = []
+    for cap in (64, 256):
+        m = sph.initialize(SimConfig(config=conf), particles=ps, max_neighbors=cap)
+        solver = sph.build_solver()
+        solver.initialize()
+        for _ in range(3):
+            solver.step()
+        st = m.engine.stats(0)
+        assert st["status"] == 0 and torch.isfinite(m.pd.x).all() and torch.isfinite(m.pd.v).all()
+        out.append((pd_field(m, "x"), pd_field(m, "v"), m.engine.max_neighbors, st["max_neighbors_seen"]))
+    assert out[0][2] > 64 and out[0][3] > 64
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
