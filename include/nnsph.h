@@ -203,6 +203,9 @@ int nn_ctx_destroy(nn_ctx* ctx);
 int nn_ctx_set_stream(nn_ctx* ctx, void* cuda_stream);
 const char* nn_last_error(const nn_ctx* ctx);
 int nn_abi_version(void);
+/* Bytes of the arithmetic type of this build: 4 for libnnsph.so (float, the product),
+   8 for libnnsph64.so (the same kernels in double, the FP64 reference run). */
+int nn_real_bytes(void);
 
 /* Bind caller-owned state (meta.pd). */
 int nn_bind_state(nn_ctx* ctx, const nn_state* state);
@@ -243,6 +246,14 @@ int nn_get_neighbors(nn_ctx* ctx, int32_t* num_neighbors, int32_t* neighbors, in
    (from the rest positions x_0, so the rest state is the same); nn_step and
    nn_run_pass return NN_ERR_STATE until then. Synchronises the device. */
 int nn_set_neighbor_cap(nn_ctx* ctx, int32_t max_neighbors);
+
+/* The status word and the largest neighbour count of the last search of `scene`
+   (nn_stats.status and .max_neighbors_seen), copied into host_out[0..1] in stream
+   order without waiting: host_out should be pinned host memory. nn_status_wait
+   blocks until the latest such copy has landed. Lets a caller check a step for
+   overflow when it next needs to, not right after enqueueing it. */
+int nn_status_async(nn_ctx* ctx, int32_t scene, int32_t* host_out);
+int nn_status_wait(nn_ctx* ctx);
 
 /* Statistics of scene `scene` (copies from the device; synchronises the stream). */
 int nn_get_stats(nn_ctx* ctx, int32_t scene, nn_stats* out);

@@ -1,4 +1,6 @@
-"""Build libnnsph.so in-tree for sm_100a with nvcc (no JIT cache, no torch extension)."""
+"""Build libnnsph.so (FP32, the product) and libnnsph64.so (the same source with
+real = double, the FP64 run the FP32 path's error is stated against) in-tree for
+sm_100a with nvcc (no JIT cache, no torch extension)."""
 from __future__ import annotations
 
 import os
@@ -8,6 +10,7 @@ import subprocess
 HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "csrc", "nnsph.cu")
 OUT = os.path.join(HERE, "libnnsph.so")
+OUT64 = os.path.join(HERE, "libnnsph64.so")
 DEPS = [os.path.join(HERE, "csrc", f) for f in os.listdir(os.path.join(HERE, "csrc"))] + [
     os.path.join(HERE, "..", "include", "nnsph.h")]
 
@@ -22,22 +25,27 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found")
 
 
-def needs_build() -> bool:
-    if not os.path.exists(OUT):
+def needs_build(out: str = OUT) -> bool:
+    if not os.path.exists(out):
         return True
-    t = os.path.getmtime(OUT)
+    t = os.path.getmtime(out)
     return any(os.path.getmtime(d) > t for d in DEPS if os.path.exists(d))
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
-    if force or needs_build():
-        cmd = [nvcc(), *NVCC_FLAGS, "-o", OUT + ".tmp", SRC]
-        r = subprocess.run(cmd, capture_output=True, text=True)
-        if r.returncode != 0:
-            raise RuntimeError(f"nvcc failed:\n{r.stdout}\n{r.stderr}")
+    """Both libraries (compiled in parallel); returns the FP32 one's path."""
+    jobs = []
+    for out, extra in ((OUT, []), (OUT64, ["-DNN_FP64"])):
+        if force or needs_build(out):
+            cmd = [nvcc(), *NVCC_FLAGS, *extra, "-o", out + ".tmp", SRC]
+            jobs.append((out, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)))
+    for out, p in jobs:
+        so, se = p.communicate()
+        if p.returncode != 0:
+            raise RuntimeError(f"nvcc failed for {os.path.basename(out)}:\n{so}\n{se}")
         if verbose:
-            print(r.stdout, r.stderr)
-        os.replace(OUT + ".tmp", OUT)
+            print(so, se)
+        os.replace(out + ".tmp", out)
     return OUT
 
 

@@ -13,6 +13,50 @@
 #define NN_CLS_ELASTIC 4u      // member of the elastic model
 #define NN_CLS_VALID 8u        // slot holds a particle
 
+// Arithmetic type of the step. libnnsph.so is built with real = float, the
+// reference's precision (Taichi's default f32). libnnsph64.so is the same source built
+// with NN_FP64 (real = double): the FP64 run of the same kernels that the FP32 path's
+// per-field error is stated against. The caller's state (meta.pd) is float32 in both.
+#ifdef NN_FP64
+typedef double real;
+typedef double2 real2;
+typedef double3 real3;
+typedef double4 real4;
+__host__ __device__ __forceinline__ real2 make_real2(real a, real b) { return make_double2(a, b); }
+__host__ __device__ __forceinline__ real3 make_real3(real a, real b, real c) { return make_double3(a, b, c); }
+__host__ __device__ __forceinline__ real4 make_real4(real a, real b, real c, real e) { return make_double4(a, b, c, e); }
+__device__ __forceinline__ real mul_rn(real a, real b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ real add_rn(real a, real b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ real sqrt_rn(real a) { return __dsqrt_rn(a); }
+__device__ __forceinline__ real fast_div(real a, real b) { return a / b; }
+#define NN_REGS64                         // no register caps: double registers come in pairs
+#else
+typedef float real;
+typedef float2 real2;
+typedef float3 real3;
+typedef float4 real4;
+__host__ __device__ __forceinline__ real2 make_real2(real a, real b) { return make_float2(a, b); }
+__host__ __device__ __forceinline__ real3 make_real3(real a, real b, real c) { return make_float3(a, b, c); }
+__host__ __device__ __forceinline__ real4 make_real4(real a, real b, real c, real e) { return make_float4(a, b, c, e); }
+__device__ __forceinline__ real mul_rn(real a, real b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ real add_rn(real a, real b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ real sqrt_rn(real a) { return __fsqrt_rn(a); }
+__device__ __forceinline__ real fast_div(real a, real b) { return __fdividef(a, b); }
+#define NN_REGS64 __maxnreg__(64)
+#endif
+
+// Read-only loads through the texture path (__ldg), double4 as two double2 loads.
+template <typename T>
+__device__ __forceinline__ T ldg(const T* p) { return __ldg(p); }
+#ifdef NN_FP64
+template <>
+__device__ __forceinline__ double4 ldg<double4>(const double4* p) {
+  const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+  const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+  return make_double4(a.x, a.y, b.x, b.y);
+}
+#endif
+
 // Constants of one scene, derived once on the host (mirrors how Taichi folds the
 // reference's Python floats into f32 literals: SPH/main.py:859-905, 1044-1051).
 struct SceneDev {
@@ -20,36 +64,36 @@ struct SceneDev {
   int32_t start, n, n_fluid;      // id range
   int64_t cell_base;              // first cell key of the scene
   int32_t gx, gy, gz, mbits;      // grid size; rows (y,z) are Morton-ordered with mbits per axis
-  float origin[3];
-  float cell;                     // cell edge (h / nf)
+  real origin[3];
+  real cell;                     // cell edge (h / nf)
   int32_t nf;                     // stencil half-width in cells (cell factor)
-  float h, k_w, k2_w, k_grad, W0; // cubic spline constants
-  float inv_h;
-  float h2_thr;                   // smallest float whose rounded sqrt is >= h
-  float rho0, inv_rho0;
-  float g[3];
-  float eps;
-  float sigma, dia2, w_dia;       // surface tension
-  float visc, visc_b, c01h2;      // explicit viscosity
-  float xmin[3], xmax[3], cf, sticky;
+  real h, k_w, k2_w, k_grad, W0; // cubic spline constants
+  real inv_h;
+  real h2_thr;                   // smallest value whose rounded sqrt is >= h (h^2 in the FP64 build)
+  real rho0, inv_rho0;
+  real g[3];
+  real eps;
+  real sigma, dia2, w_dia;       // surface tension
+  real visc, visc_b, c01h2;      // explicit viscosity
+  real xmin[3], xmax[3], cf, sticky;
   double eta_v_fac;               // maxErrorV * 0.01 * rho0 (multiplied by 1/dt)
   double eta_p;                   // maxError * 0.01 * rho0
   int32_t max_iter_v, max_iter, visco_max_iter, nn_method;
   double visco_tol;
-  float nn_n, nn_K, nn_mu0, nn_muinf, nn_gc, nn_muc, nn_tauy;
-  float mu_newton;                // viscosity * rho0 (implicit solver without a law)
-  float mu_b;                     // visco_boundary * rho0
-  float el_cd, el_co, el_cs;      // isotropic C of Becker 2009 (SPH/main.py:1276-1283)
+  real nn_n, nn_K, nn_mu0, nn_muinf, nn_gc, nn_muc, nn_tauy;
+  real mu_newton;                // viscosity * rho0 (implicit solver without a law)
+  real mu_b;                     // visco_boundary * rho0
+  real el_cd, el_co, el_cs;      // isotropic C of Becker 2009 (SPH/main.py:1276-1283)
   int32_t el_mult;                // elastic substeps per step (quirk: one per elastic phase)
-  float cfl_factor, cfl_min_dt, cfl_max_dt, diameter;
-  float V0, padding;              // volume0 and padding (rigid-body mass, ground clamp)
+  real cfl_factor, cfl_min_dt, cfl_max_dt, diameter;
+  real V0, padding;              // volume0 and padding (rigid-body mass, ground clamp)
   int32_t n_rigid, coupling;      // rigid bodies of the scene, substeps per step
 };
 
 // Mutable per-scene state on the device.
 struct SceneDyn {
-  float dt, inv_dt;               // time step and f32(1/dt)
-  float inv_dt2;                  // f32(1/(dt*dt))
+  real dt, inv_dt;               // time step and f32(1/dt)
+  real inv_dt2;                  // f32(1/(dt*dt))
   int32_t it_v, it_p, it_cg;      // loop counters (reference semantics)
   int32_t act_v, act_p, act_cg;   // 1 while the scene still iterates
   int32_t status;                 // first NN_ERR_* seen
@@ -62,41 +106,41 @@ struct SceneDyn {
   int32_t pad;
   double cg_alpha, cg_beta;       // PCG scalars of the current iteration
   int64_t steps;
-  float anim[3];                  // animate_particles displacement of the next step
+  float anim[3];                 // animate_particles displacement of the next step (set by the host)
   int32_t pad2;
 };
 
 // Accumulator slots per scene (each NN_STRIPES doubles).
 enum { ACC_ERR = 0, ACC_RZ, ACC_PAP, ACC_RR, ACC_BB, ACC_COUNT };
 
-struct Vec3 { float x, y, z; };
-__device__ __forceinline__ float3 f3(float4 a) { return make_float3(a.x, a.y, a.z); }
-__device__ __forceinline__ float3 operator-(float3 a, float3 b) { return make_float3(a.x - b.x, a.y - b.y, a.z - b.z); }
-__device__ __forceinline__ float3 operator+(float3 a, float3 b) { return make_float3(a.x + b.x, a.y + b.y, a.z + b.z); }
-__device__ __forceinline__ float3 operator*(float3 a, float s) { return make_float3(a.x * s, a.y * s, a.z * s); }
-__device__ __forceinline__ float3 operator-(float3 a) { return make_float3(-a.x, -a.y, -a.z); }
-__device__ __forceinline__ void operator+=(float3& a, float3 b) { a.x += b.x; a.y += b.y; a.z += b.z; }
-__device__ __forceinline__ void operator-=(float3& a, float3 b) { a.x -= b.x; a.y -= b.y; a.z -= b.z; }
-__device__ __forceinline__ float dot3(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+struct Vec3 { real x, y, z; };
+__device__ __forceinline__ real3 f3(real4 a) { return make_real3(a.x, a.y, a.z); }
+__device__ __forceinline__ real3 operator-(real3 a, real3 b) { return make_real3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ real3 operator+(real3 a, real3 b) { return make_real3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ real3 operator*(real3 a, real s) { return make_real3(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ real3 operator-(real3 a) { return make_real3(-a.x, -a.y, -a.z); }
+__device__ __forceinline__ void operator+=(real3& a, real3 b) { a.x += b.x; a.y += b.y; a.z += b.z; }
+__device__ __forceinline__ void operator-=(real3& a, real3 b) { a.x -= b.x; a.y -= b.y; a.z -= b.z; }
+__device__ __forceinline__ real dot3(real3 a, real3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 
 // Exact f32 distance as the reference computes it for the in-range test:
 // (x_i - x_j).norm() < support_radius (SPH/main.py:845), no FMA contraction.
-__device__ __forceinline__ float exact_norm(float3 r) {
-  float s = __fadd_rn(__fadd_rn(__fmul_rn(r.x, r.x), __fmul_rn(r.y, r.y)), __fmul_rn(r.z, r.z));
-  return __fsqrt_rn(s);
+__device__ __forceinline__ real exact_norm(real3 r) {
+  real s = add_rn(add_rn(mul_rn(r.x, r.x), mul_rn(r.y, r.y)), mul_rn(r.z, r.z));
+  return sqrt_rn(s);
 }
 
 // cubic_kernel, SPH/main.py:859-880
-__device__ __forceinline__ float kernel_w(float rn, const SceneDev& s) {
-  float q = rn / s.h;
-  float res = 0.f;
+__device__ __forceinline__ real kernel_w(real rn, const SceneDev& s) {
+  real q = rn / s.h;
+  real res = 0.f;
   if (q <= 1.f) {
     if (q <= 0.5f) {
-      float q2 = q * q;
-      float q3 = q2 * q;
+      real q2 = q * q;
+      real q3 = q2 * q;
       res = s.k_w * (6.f * q3 - 6.f * q2 + 1.f);
     } else {
-      float t = 1.f - q;
+      real t = 1.f - q;
       res = s.k2_w * (t * t * t);
     }
   }
@@ -104,17 +148,17 @@ __device__ __forceinline__ float kernel_w(float rn, const SceneDev& s) {
 }
 
 // cubic_kernel_derivative, SPH/main.py:883-905 (rn = |r| passed in)
-__device__ __forceinline__ float3 kernel_grad(float3 r, float rn, const SceneDev& s) {
-  float q = rn / s.h;
-  float3 res = make_float3(0.f, 0.f, 0.f);
+__device__ __forceinline__ real3 kernel_grad(real3 r, real rn, const SceneDev& s) {
+  real q = rn / s.h;
+  real3 res = make_real3(0.f, 0.f, 0.f);
   if (rn > 1e-5f && q <= 1.f) {
-    float den = rn * s.h;
-    float3 gq = make_float3(r.x / den, r.y / den, r.z / den);
-    float f;
+    real den = rn * s.h;
+    real3 gq = make_real3(r.x / den, r.y / den, r.z / den);
+    real f;
     if (q <= 0.5f) {
       f = s.k_grad * q * (3.f * q - 2.f);
     } else {
-      float t = 1.f - q;
+      real t = 1.f - q;
       f = s.k_grad * (-t * t);
     }
     res = gq * f;
@@ -125,28 +169,28 @@ __device__ __forceinline__ float3 kernel_grad(float3 r, float rn, const SceneDev
 // The same cubic spline and gradient as kernel_w / kernel_grad, from r^2 and without
 // divisions (1/h precomputed, 1/|r| from rsqrt): used inside the neighbour loops,
 // where it agrees with the reference expressions to a few ulp.
-__device__ __forceinline__ void kwg_r2(float3 r, float r2, const SceneDev& s, float& w, float3& g) {
-  const float inv_rn = r2 > 0.f ? rsqrtf(r2) : 0.f;
-  const float rn = r2 * inv_rn;
-  const float q = rn * s.inv_h;
-  const float t = 1.f - q;
+__device__ __forceinline__ void kwg_r2(real3 r, real r2, const SceneDev& s, real& w, real3& g) {
+  const real inv_rn = r2 > 0.f ? rsqrt(r2) : 0.f;
+  const real rn = r2 * inv_rn;
+  const real q = rn * s.inv_h;
+  const real t = 1.f - q;
   const bool in = q <= 1.f;
   const bool inner = q <= 0.5f;
   w = in ? (inner ? s.k_w * (6.f * q * q * (q - 1.f) + 1.f) : s.k2_w * (t * t * t)) : 0.f;
-  const float f = inner ? s.k_grad * q * (3.f * q - 2.f) : -s.k_grad * t * t;
-  const float c = (rn > 1e-5f && in) ? f * inv_rn * s.inv_h : 0.f;
-  g = make_float3(r.x * c, r.y * c, r.z * c);
+  const real f = inner ? s.k_grad * q * (3.f * q - 2.f) : -s.k_grad * t * t;
+  const real c = (rn > 1e-5f && in) ? f * inv_rn * s.inv_h : 0.f;
+  g = make_real3(r.x * c, r.y * c, r.z * c);
 }
-__device__ __forceinline__ float kw_r2(float r2, const SceneDev& s) {
-  const float rn = r2 > 0.f ? r2 * rsqrtf(r2) : 0.f;
-  const float q = rn * s.inv_h;
-  const float t = 1.f - q;
-  const float w = q <= 0.5f ? s.k_w * (6.f * q * q * (q - 1.f) + 1.f) : s.k2_w * (t * t * t);
+__device__ __forceinline__ real kw_r2(real r2, const SceneDev& s) {
+  const real rn = r2 > 0.f ? r2 * rsqrt(r2) : 0.f;
+  const real q = rn * s.inv_h;
+  const real t = 1.f - q;
+  const real w = q <= 0.5f ? s.k_w * (6.f * q * q * (q - 1.f) + 1.f) : s.k2_w * (t * t * t);
   return q <= 1.f ? w : 0.f;
 }
-__device__ __forceinline__ float3 kgrad_r2(float3 r, float r2, const SceneDev& s) {
-  float w;
-  float3 g;
+__device__ __forceinline__ real3 kgrad_r2(real3 r, real r2, const SceneDev& s) {
+  real w;
+  real3 g;
   kwg_r2(r, r2, s, w, g);
   return g;
 }
@@ -159,7 +203,7 @@ __device__ __forceinline__ float3 kgrad_r2(float3 r, float r2, const SceneDev& s
 template <bool STREAM>
 __device__ __forceinline__ int nb_list_load(const int32_t* p) {
   if constexpr (STREAM) return __ldcs(p);
-  else return __ldg(p);
+  else return ldg(p);
 }
 
 template <int NB_U, bool STREAM = false, typename Load, typename Use>
@@ -198,7 +242,7 @@ __device__ __forceinline__ void nb_batches(const int32_t* __restrict__ list, int
 // Material of a slot is also kept in the sign of pos.w: the volume is stored
 // positive for fluid and negative for solid particles, so neighbour loops need no
 // separate class gather.
-__device__ __forceinline__ bool w_fluid(float w) { return w > 0.f; }
+__device__ __forceinline__ bool w_fluid(real w) { return w > 0.f; }
 
 __device__ __forceinline__ int slot_scene(uint32_t fl) { return (int)(fl >> NN_SCENE_SHIFT); }
 __device__ __forceinline__ bool cls_fluid(uint32_t fl) { return (fl & (NN_CLS_VALID | NN_CLS_SOLID)) == NN_CLS_VALID; }

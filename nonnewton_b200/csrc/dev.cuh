@@ -4,15 +4,15 @@
 
 // Sorted working set: particles in cell order ("slots").
 struct WorkSet {
-  float4* pos;      // x, y, z, volume (negative for solids)
-  float4* vel;      // v, w = mass (a copy of `mass`, so neighbour loops get it with v)
-  float* mass;
-  float* dens;
-  uint32_t* flags;  // class bits | scene << NN_SCENE_SHIFT
-  int32_t* id;      // particle id of the slot
+  real4* pos;       // x, y, z, volume (negative for solids)
+  real4* vel;       // v, w = mass (a copy of `mass`, so neighbour loops get it with v)
+  real* mass;
+  real* dens;
+  uint32_t* flags;   // class bits | scene << NN_SCENE_SHIFT
+  int32_t* id;       // particle id of the slot
 };
 
-// Caller-owned state in particle-id order (meta.pd).
+// Caller-owned state in particle-id order (meta.pd): float32 in both builds.
 struct Truth {
   float* x; float* x_0; float* v; float* a;
   float* volume; float* m; float* density; float* dfsph_factor; float* density_adv;
@@ -31,10 +31,10 @@ struct Dev {
   WorkSet w;                   // current sorted set
   WorkSet wo;                  // previous sorted set (resident re-sort source)
   const int32_t* src_from_truth; // device flag: 1 = gather from Truth, 0 = from wo
-  float4* acc4;                // accelerations (slot order)
-  float* alpha;
-  float* rho_adv;
-  float* kappa;
+  real4* acc4;                 // accelerations (slot order)
+  real* alpha;
+  real* rho_adv;
+  real* kappa;
   int32_t* slot_of_id;
   // neighbour search
   uint32_t* key;               // per source index
@@ -48,23 +48,23 @@ struct Dev {
   int32_t cap;                 // slot capacity (neighbour list stride)
   int32_t max_nb;
   // non-Newtonian
-  float* srn;
-  float* mu;
+  real* srn;
+  real* mu;
   // implicit viscosity CG (slot order)
-  float4* cg_x; float4* cg_r; float4* cg_z; float4* cg_p; float4* cg_Ap; float4* cg_b;
-  float2* cg_aux;              // fluid: mu_i, m_i / rho_i; solid: 0, 1 if dynamic
-  float* cg_pinv;              // [6][cap] symmetric inverse of the diagonal block
+  real4* cg_x; real4* cg_r; real4* cg_z; real4* cg_p; real4* cg_Ap; real4* cg_b;
+  real2* cg_aux;               // fluid: mu_i, m_i / rho_i; solid: 0, 1 if dynamic
+  real* cg_pinv;               // [6][cap] symmetric inverse of the diagonal block
   // elasticity (e-space: elastic particles in id order)
   int32_t* el_id;              // [Ne] particle id
   int32_t* el_slot;            // [Ne] current slot
   int32_t* e_of_id;            // [cap] elastic index or -1
-  float4* el_x0;               // [Ne] rest position, rest volume
+  real4* el_x0;                // [Ne] rest position, rest volume
   int32_t* el_nb;              // [rest_cap][Ne] rest neighbours (elastic indices)
   int32_t* el_cnt;             // [Ne]
   int32_t el_cap;              // rest list capacity
   int32_t el_stride;           // Ne capacity
-  float* el_R;                 // [9][Ne]
-  float* el_S;                 // [6][Ne]
+  real* el_R;                  // [9][Ne]
+  real* el_S;                  // [6][Ne]
   // rigid bodies ("r-space")
   int32_t n_rb;
   const int32_t* rb_of_id;     // [cap] body index or -1

@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstddef>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -76,24 +77,25 @@ struct nn_ctx {
   double* d_acc = nullptr;
   int32_t* d_scene_of_id = nullptr;
   int32_t* d_src_flag = nullptr;
-  float4* acc4 = nullptr;
-  float *alpha = nullptr, *rho_adv = nullptr, *kappa = nullptr, *srn = nullptr, *mu = nullptr;
+  real4* acc4 = nullptr;
+  real *alpha = nullptr, *rho_adv = nullptr, *kappa = nullptr, *srn = nullptr, *mu = nullptr;
   int32_t* slot_of_id = nullptr;
   uint32_t *key = nullptr, *rank = nullptr, *cell_count = nullptr, *tile_sums = nullptr;
   int32_t *src = nullptr, *nbr = nullptr, *nbr_cnt = nullptr;
-  float4 *cg_x = nullptr, *cg_r = nullptr, *cg_z = nullptr, *cg_p = nullptr, *cg_Ap = nullptr, *cg_b = nullptr;
-  float2* cg_aux = nullptr;
-  float* cg_pinv = nullptr;
+  real4 *cg_x = nullptr, *cg_r = nullptr, *cg_z = nullptr, *cg_p = nullptr, *cg_Ap = nullptr, *cg_b = nullptr;
+  real2* cg_aux = nullptr;
+  real* cg_pinv = nullptr;
   int el_cap = 64, el_stride = 0;
   bool el_stale = false;               // rest lists re-sized since the last nn_initialize
   int32_t *el_id = nullptr, *el_slot = nullptr, *e_of_id = nullptr, *el_nb = nullptr, *el_cnt = nullptr;
-  float4* el_x0 = nullptr;
-  float *el_R = nullptr, *el_S = nullptr;
+  real4* el_x0 = nullptr;
+  real *el_R = nullptr, *el_S = nullptr;
   int n_rb = 0, rb_rounds = 0, coupling_max = 1;
   int32_t *rb_of_id = nullptr, *rb_round = nullptr;
   double *rb_acc = nullptr, *rb_rest = nullptr, *rb_cm = nullptr, *rb_R = nullptr;
   int32_t* d_any = nullptr;
   int32_t* h_any = nullptr;            // pinned
+  cudaEvent_t status_ev = nullptr;     // recorded after nn_status_async's copy
   int32_t* d_body = nullptr;
   int64_t fixed_nodes_per_step = 0;    // kernel nodes outside loop bodies (graph mode)
   int64_t graph_replays = 0;
@@ -478,16 +480,17 @@ static int capture_step(nn_ctx* c, cudaStream_t s, int parity) {
 }
 
 // ---- scene setup ----------------------------------------------------------------------
-static float host_kernel_w(float rn, float h, float k_w, float k2_w) {
-  float q = rn / h;
-  float res = 0.f;
-  if (q <= 1.f) {
-    if (q <= 0.5f) {
-      float q2 = q * q;
-      float q3 = q2 * q;
-      res = k_w * (6.f * q3 - 6.f * q2 + 1.f);
+// cubic_kernel (SPH/main.py:859-880) on the host, in the arithmetic type of the build
+static real host_kernel_w(real rn, real h, real k_w, real k2_w) {
+  real q = rn / h;
+  real res = 0;
+  if (q <= 1) {
+    if (q <= real(0.5)) {
+      real q2 = q * q;
+      real q3 = q2 * q;
+      res = k_w * (6 * q3 - 6 * q2 + 1);
     } else {
-      float t = 1.f - q;
+      real t = 1 - q;
       res = k2_w * (t * t * t);
     }
   }
@@ -506,7 +509,7 @@ static SceneDev make_scene(const nn_scene_desc& sd, int64_t cell_base, int el_mu
   int g[3];
   const double cell = h / cell_factor;
   for (int k = 0; k < 3; ++k) {
-    s.origin[k] = (float)(p.domain_start[k] - 2.0 * h);
+    s.origin[k] = (real)(p.domain_start[k] - 2.0 * h);
     double ext = (p.domain_end[k] - p.domain_start[k]) + 4.0 * h;
     g[k] = (int)std::min(65535.0, std::max(1.0, std::ceil(ext / cell) + 1.0));
   }
@@ -514,38 +517,42 @@ static SceneDev make_scene(const nn_scene_desc& sd, int64_t cell_base, int el_mu
   int mb = 0;
   while ((1 << mb) < std::max(g[1], g[2])) ++mb;
   s.mbits = mb;
-  s.cell = (float)cell;
+  s.cell = (real)cell;
   s.nf = cell_factor;
-  s.h = (float)h;
-  s.inv_h = (float)(1.0 / h);
+  s.h = (real)h;
+  s.inv_h = (real)(1.0 / h);
+#ifdef NN_FP64
+  s.h2_thr = s.h * s.h;  // the search tests r2 < h^2 in double
+#else
   {  // exact squared cut-off: sqrt_rn(r2) < h  <=>  r2 < h2_thr
     float t = s.h * s.h;
     while (t > 0.f && std::sqrt(t) >= s.h) t = std::nextafter(t, 0.f);
     while (std::sqrt(t) < s.h) t = std::nextafter(t, INFINITY);
     s.h2_thr = t;
   }
+#endif
   const double k = 8.0 / kPi / (h * h * h);
-  s.k_w = (float)k;
-  s.k2_w = (float)(k * 2.0);
-  s.k_grad = (float)(6.0 * (8.0 / kPi) / (h * h * h));
+  s.k_w = (real)k;
+  s.k2_w = (real)(k * 2.0);
+  s.k_grad = (real)(6.0 * (8.0 / kPi) / (h * h * h));
   s.W0 = host_kernel_w(0.f, s.h, s.k_w, s.k2_w);
-  s.rho0 = (float)p.density0;
-  s.inv_rho0 = (float)(1.0 / p.density0);
-  for (int q = 0; q < 3; ++q) s.g[q] = (float)p.gravity[q];
-  s.eps = (float)p.eps;
-  s.sigma = (float)p.surface_tension;
+  s.rho0 = (real)p.density0;
+  s.inv_rho0 = (real)(1.0 / p.density0);
+  for (int q = 0; q < 3; ++q) s.g[q] = (real)p.gravity[q];
+  s.eps = (real)p.eps;
+  s.sigma = (real)p.surface_tension;
   const double dia = 2.0 * p.particle_radius;
-  s.dia2 = (float)(dia * dia);
-  s.w_dia = host_kernel_w(std::sqrt((float)dia * (float)dia), s.h, s.k_w, s.k2_w);
-  s.visc = (float)p.viscosity;
-  s.visc_b = (float)p.boundary_viscosity;
-  s.c01h2 = (float)(0.01 * h * h);
+  s.dia2 = (real)(dia * dia);
+  s.w_dia = host_kernel_w(std::sqrt((real)dia * (real)dia), s.h, s.k_w, s.k2_w);
+  s.visc = (real)p.viscosity;
+  s.visc_b = (real)p.boundary_viscosity;
+  s.c01h2 = (real)(0.01 * h * h);
   for (int q = 0; q < 3; ++q) {
-    s.xmin[q] = (float)(p.domain_start[q] + p.padding);
-    s.xmax[q] = (float)(p.domain_end[q] - p.padding);
+    s.xmin[q] = (real)(p.domain_start[q] + p.padding);
+    s.xmax[q] = (real)(p.domain_end[q] - p.padding);
   }
-  s.cf = (float)p.collision_coeff;
-  s.sticky = (float)p.sticky_coeff;
+  s.cf = (real)p.collision_coeff;
+  s.sticky = (real)p.sticky_coeff;
   s.eta_v_fac = p.max_error_v * 0.01 * p.density0;
   s.eta_p = p.max_error * 0.01 * p.density0;
   s.max_iter_v = std::min(std::max(p.max_iterations_v, 0), 100000);
@@ -553,28 +560,28 @@ static SceneDev make_scene(const nn_scene_desc& sd, int64_t cell_base, int el_mu
   s.visco_max_iter = std::min(std::max(p.visco_max_iter, 0), 100000);
   s.nn_method = p.nonnewton_method;
   s.visco_tol = p.visco_max_error;
-  s.nn_n = (float)p.power_index;
-  s.nn_K = (float)p.consistency_index;
-  s.nn_mu0 = (float)p.viscosity0;
-  s.nn_muinf = (float)p.viscosity_inf;
-  s.nn_gc = (float)p.critical_strain_rate;
-  s.nn_muc = (float)p.mu_c;
-  s.nn_tauy = (float)p.yield_stress;
-  s.mu_newton = (float)(p.viscosity * p.density0);
-  s.mu_b = (float)(p.visco_boundary * p.density0);
+  s.nn_n = (real)p.power_index;
+  s.nn_K = (real)p.consistency_index;
+  s.nn_mu0 = (real)p.viscosity0;
+  s.nn_muinf = (real)p.viscosity_inf;
+  s.nn_gc = (real)p.critical_strain_rate;
+  s.nn_muc = (real)p.mu_c;
+  s.nn_tauy = (real)p.yield_stress;
+  s.mu_newton = (real)(p.viscosity * p.density0);
+  s.mu_b = (real)(p.visco_boundary * p.density0);
   double E = p.youngs_modulus, nu = p.poisson_ratio;
   if (p.flags & NN_F_QUIRKS) { E = 25e4; nu = 0.33; }  // SPH/main.py:1188-1189
   const double f = E / ((1.0 + nu) * (1.0 - 2.0 * nu));
-  s.el_cd = (float)(f * (1.0 - nu));
-  s.el_co = (float)(f * nu);
-  s.el_cs = (float)(f * 0.5 * (1.0 - 2.0 * nu));
+  s.el_cd = (real)(f * (1.0 - nu));
+  s.el_co = (real)(f * nu);
+  s.el_cs = (real)(f * 0.5 * (1.0 - 2.0 * nu));
   s.el_mult = el_mult;
-  s.cfl_factor = (float)p.cfl_factor;
-  s.cfl_min_dt = (float)p.cfl_min_dt;
-  s.cfl_max_dt = (float)p.cfl_max_dt;
-  s.diameter = (float)dia;
-  s.V0 = (float)p.volume0;
-  s.padding = (float)p.padding;
+  s.cfl_factor = (real)p.cfl_factor;
+  s.cfl_min_dt = (real)p.cfl_min_dt;
+  s.cfl_max_dt = (real)p.cfl_max_dt;
+  s.diameter = (real)dia;
+  s.V0 = (real)p.volume0;
+  s.padding = (real)p.padding;
   s.coupling = std::max(p.coupling_interval, 1);
   return s;
 }
@@ -603,6 +610,8 @@ static void free_elastic(nn_ctx* c) {
 extern "C" {
 
 int nn_abi_version(void) { return NNSPH_ABI_VERSION; }
+
+int nn_real_bytes(void) { return (int)sizeof(real); }
 
 const char* nn_last_error(const nn_ctx* c) { return c ? c->err.c_str() : g_err; }
 
@@ -650,6 +659,8 @@ int nn_ctx_create(int32_t max_particles, int32_t max_scenes, int32_t max_neighbo
   if (cudaStreamCreateWithFlags(&c->side, cudaStreamDefault) != cudaSuccess ||
       cudaStreamCreateWithFlags(&c->own, cudaStreamDefault) != cudaSuccess)
     return bail(fail(nullptr, NN_ERR_CUDA, "cudaStreamCreate failed"));
+  if (cudaEventCreateWithFlags(&c->status_ev, cudaEventDisableTiming) != cudaSuccess)
+    return bail(fail(nullptr, NN_ERR_CUDA, "cudaEventCreate failed"));
   if (max_cells > 0) {
     int rc = ensure_cells(c, max_cells);
     if (rc != NN_OK) return bail(rc);
@@ -676,6 +687,7 @@ int nn_ctx_destroy(nn_ctx* c) {
   cudaFree(c->rb_of_id); cudaFree(c->rb_round); cudaFree(c->rb_acc); cudaFree(c->rb_rest); cudaFree(c->rb_cm);
   cudaFree(c->rb_R);
   if (c->h_any) cudaFreeHost(c->h_any);
+  if (c->status_ev) cudaEventDestroy(c->status_ev);
   if (c->side) cudaStreamDestroy(c->side);
   if (c->own) cudaStreamDestroy(c->own);
   delete c;
@@ -814,9 +826,9 @@ int nn_set_scenes(nn_ctx* c, int32_t nscenes, const nn_scene_desc* scenes) {
     cells += (int64_t)s.gx * ((int64_t)1 << (2 * s.mbits));
     sdev.push_back(s);
     SceneDyn y{};
-    y.dt = (float)sd.params.dt;
-    y.inv_dt = (float)(1.0 / (double)y.dt);
-    y.inv_dt2 = (float)(1.0 / ((double)y.dt * (double)y.dt));
+    y.dt = (real)sd.params.dt;
+    y.inv_dt = (real)(1.0 / (double)y.dt);
+    y.inv_dt2 = (real)(1.0 / ((double)y.dt * (double)y.dt));
     sdyn[k] = y;
     c->any_fluid |= sd.n_fluid > 0;
     c->any_div |= sd.n_fluid > 0 && (sd.params.flags & NN_F_DIVERGENCE);
@@ -1110,6 +1122,23 @@ int nn_set_neighbor_cap(nn_ctx* c, int32_t max_neighbors) {
   return NN_OK;
 }
 
+int nn_status_async(nn_ctx* c, int32_t scene, int32_t* host_out) {
+  RC(check_ready(c));
+  if (!host_out || scene < 0 || scene >= (int)c->scenes.size())
+    return fail(c, NN_ERR_INVALID_ARG, "nn_status_async: bad arguments");
+  static_assert(offsetof(SceneDyn, max_nb) == offsetof(SceneDyn, status) + sizeof(int32_t), "status, max_nb adjacent");
+  cudaStream_t s = run_stream(c);
+  CK(cudaMemcpyAsync(host_out, &c->d_dyn[scene].status, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  CK(cudaEventRecord(c->status_ev, s));
+  return NN_OK;
+}
+
+int nn_status_wait(nn_ctx* c) {
+  if (!c) return fail(nullptr, NN_ERR_INVALID_ARG, "null context");
+  CK(cudaEventSynchronize(c->status_ev));
+  return NN_OK;
+}
+
 static void fill_stats(const SceneDyn& y, nn_stats* out) {
   std::memset(out, 0, sizeof(*out));
   out->size = sizeof(*out);
@@ -1177,7 +1206,7 @@ constexpr size_t kOffSrc = kOffRank + na_round(kNaN * 4);
 constexpr size_t kOffCells = kOffSrc + na_round(kNaN * 4);
 constexpr size_t kOffTiles = kOffCells + na_round((kNaC + 1) * 4);
 constexpr size_t kOffPos = kOffTiles + na_round(((kNaC + 1) / SCAN_TILE + 2) * 4);
-constexpr size_t kOffFlags = kOffPos + na_round(kNaN * sizeof(float4));
+constexpr size_t kOffFlags = kOffPos + na_round(kNaN * sizeof(real4));
 constexpr size_t kOffId = kOffFlags + na_round(kNaN * 4);
 constexpr size_t kOffNbr = kOffId + na_round(kNaN * 4);
 constexpr size_t kOffCnt = kOffNbr + na_round(kNaN * kNaNb * 4);
@@ -1208,7 +1237,7 @@ __global__ void k_na_gather(Dev d) {
   const int n = d.d_n[0];
   GRID_STRIDE(i, n) {
     const int s = d.src[i];
-    d.w.pos[i] = make_float4(d.t.x[3 * s], d.t.x[3 * s + 1], d.t.x[3 * s + 2], 0.f);
+    d.w.pos[i] = make_real4(d.t.x[3 * s], d.t.x[3 * s + 1], d.t.x[3 * s + 2], 0.f);
     d.w.flags[i] = NN_CLS_VALID;
     d.w.id[i] = s;
   }
@@ -1308,7 +1337,7 @@ extern "C" int nn_neighbors_noalloc(const float* x, int32_t n, const double* dom
   d.src = reinterpret_cast<int32_t*>(base + kOffSrc);
   d.cell_count = reinterpret_cast<uint32_t*>(base + kOffCells);
   d.tile_sums = reinterpret_cast<uint32_t*>(base + kOffTiles);
-  d.w.pos = reinterpret_cast<float4*>(base + kOffPos);
+  d.w.pos = reinterpret_cast<real4*>(base + kOffPos);
   d.w.flags = reinterpret_cast<uint32_t*>(base + kOffFlags);
   d.w.id = reinterpret_cast<int32_t*>(base + kOffId);
   d.nbr = reinterpret_cast<int32_t*>(base + kOffNbr);
@@ -1338,5 +1367,7 @@ extern "C" int nn_neighbors_noalloc(const float* x, int32_t n, const double* dom
   return NN_OK;
 }
 
-// Surface reconstruction (SRTool): kernels and its C ABI.
+#ifndef NN_FP64
+// Surface reconstruction (SRTool): kernels and its C ABI (FP32 build only).
 #include "surf.cuh"
+#endif

@@ -21,11 +21,11 @@
       for (bool valid = i < (n); _once; _once = 0)
 
 // Cell key of a position in scene s: Morton(cy, cz) * gx + cx + cell_base.
-__device__ __forceinline__ uint32_t cell_key(const SceneDev& s, float x, float y, float z, int* cx_out, int* cy_out,
+__device__ __forceinline__ uint32_t cell_key(const SceneDev& s, real x, real y, real z, int* cx_out, int* cy_out,
                                              int* cz_out) {
-  int cx = (int)floorf((x - s.origin[0]) / s.cell);
-  int cy = (int)floorf((y - s.origin[1]) / s.cell);
-  int cz = (int)floorf((z - s.origin[2]) / s.cell);
+  int cx = (int)floor((x - s.origin[0]) / s.cell);
+  int cy = (int)floor((y - s.origin[1]) / s.cell);
+  int cz = (int)floor((z - s.origin[2]) / s.cell);
   cx = min(max(cx, 0), s.gx - 1);
   cy = min(max(cy, 0), s.gy - 1);
   cz = min(max(cz, 0), s.gz - 1);
@@ -45,13 +45,13 @@ __global__ void k_keys(Dev d) {
   const bool truth = mode != 0;
   const float* __restrict__ X = mode == 2 ? d.t.x_0 : d.t.x;
   GRID_STRIDE(s, n) {
-    float x, y, z;
+    real x, y, z;
     int sc;
     if (truth) {
       x = X[3 * s]; y = X[3 * s + 1]; z = X[3 * s + 2];
       sc = d.scene_of_id[s];
     } else {
-      float4 p = d.wo.pos[s];
+      real4 p = d.wo.pos[s];
       x = p.x; y = p.y; z = p.z;
       sc = slot_scene(d.wo.flags[s]);
     }
@@ -200,20 +200,20 @@ __global__ void k_gather(Dev d) {
   const float* __restrict__ X = mode == 2 ? d.t.x_0 : d.t.x;
   FOR_SLOTS_WARP(i, valid, n) {
     uint32_t fl = 0u;
-    float vm = 0.f;
+    real vm = 0.f;
     if (valid) {
       int s = d.src[i];
       int id;
-      float4 p, v;
-      float m, rho;
+      real4 p, v;
+      real m, rho;
       if (truth) {
         id = s;
         int sc = d.scene_of_id[id];
-        const float vol = d.t.volume[id];
-        p = make_float4(X[3 * id], X[3 * id + 1], X[3 * id + 2],
+        const real vol = d.t.volume[id];
+        p = make_real4(X[3 * id], X[3 * id + 1], X[3 * id + 2],
                         d.t.material[id] == NN_SOLID ? -vol : vol);  // signed volume: solid < 0
         m = d.t.m[id];
-        v = make_float4(d.t.v[3 * id], d.t.v[3 * id + 1], d.t.v[3 * id + 2], m);  // vel.w carries the mass
+        v = make_real4(d.t.v[3 * id], d.t.v[3 * id + 1], d.t.v[3 * id + 2], m);  // vel.w carries the mass
         rho = d.t.density[id];
         fl = class_bits(d.t.material[id], d.t.is_dynamic[id], d.t.phase_id[id], d.sc[sc]) |
              ((uint32_t)sc << NN_SCENE_SHIFT);
@@ -232,10 +232,10 @@ __global__ void k_gather(Dev d) {
       d.w.flags[i] = fl;
       d.w.id[i] = id;
       d.slot_of_id[id] = i;
-      vm = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z);
+      vm = sqrt(v.x * v.x + v.y * v.y + v.z * v.z);
     }
     const bool cfl = valid && (fl & NN_CLS_DYNAMIC) && (d.sc[slot_scene(fl)].flags & NN_F_CFL);
-    warp_max_to(&d.dyn[slot_scene(fl)].vmax_bits, __float_as_uint(vm), cfl);
+    warp_max_to(&d.dyn[slot_scene(fl)].vmax_bits, __float_as_uint((float)vm), cfl);
   }
 }
 
@@ -248,30 +248,31 @@ __global__ void k_gather(Dev d) {
 // into shared memory with coalesced loads, in chunks of NS_CHUNK; each lane then tests
 // its own 3-cell window from shared memory. Other warps read candidates directly.
 // The in-range test sqrt_rn(r2) < h is evaluated as r2 < h2_thr, where h2_thr is the
-// smallest float whose correctly rounded square root is >= h (exactly equivalent).
+// smallest float whose correctly rounded square root is >= h (exactly equivalent; the
+// FP64 build tests r2 < h^2 in double).
 #define NS_WARPS 8
 #define NS_CHUNK 128
-__device__ __forceinline__ float exact_r2(float3 r) {
-  return __fadd_rn(__fadd_rn(__fmul_rn(r.x, r.x), __fmul_rn(r.y, r.y)), __fmul_rn(r.z, r.z));
+__device__ __forceinline__ real exact_r2(real3 r) {
+  return add_rn(add_rn(mul_rn(r.x, r.x), mul_rn(r.y, r.y)), mul_rn(r.z, r.z));
 }
 
 __global__ void __launch_bounds__(NS_WARPS * 32) k_build_lists(Dev d) {
-  __shared__ float4 stage_all[NS_WARPS][NS_CHUNK];
-  float4* stage = stage_all[threadIdx.x >> 5];
+  __shared__ real4 stage_all[NS_WARPS][NS_CHUNK];
+  real4* stage = stage_all[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
   const unsigned full = 0xffffffffu;
   const int n = d.d_n[0];
   FOR_SLOTS_WARP(i, valid, n) {
     int cnt = 0, scn = 0, cx = 0, cy = 0, cz = 0;
-    float4 pi = make_float4(0.f, 0.f, 0.f, 0.f);
+    real4 pi = make_real4(0.f, 0.f, 0.f, 0.f);
     if (valid) {
       scn = slot_scene(d.w.flags[i]);
       pi = d.w.pos[i];
       cell_key(d.sc[scn], pi.x, pi.y, pi.z, &cx, &cy, &cz);
     }
     const SceneDev& s = d.sc[scn];
-    const float3 xi = f3(pi);
-    const float thr = s.h2_thr;
+    const real3 xi = f3(pi);
+    const real thr = s.h2_thr;
     const int x0 = max(cx - s.nf, 0), x1 = min(cx + s.nf, s.gx - 1);
     // lane 0 is always valid (the warp's first slot is below n)
     const int ly = __shfl_sync(full, cy, 0), lz = __shfl_sync(full, cz, 0), ls = __shfl_sync(full, scn, 0);
@@ -298,7 +299,7 @@ __global__ void __launch_bounds__(NS_WARPS * 32) k_build_lists(Dev d) {
           if (valid) { b = d.cell_count[row + x0]; e = d.cell_count[row + x1 + 1]; }
           for (uint32_t c0 = rb; c0 < re; c0 += NS_CHUNK) {
             const uint32_t c1 = min(c0 + NS_CHUNK, re);
-            for (uint32_t t = lane; t < c1 - c0; t += 32) stage[t] = __ldg(&d.w.pos[c0 + t]);
+            for (uint32_t t = lane; t < c1 - c0; t += 32) stage[t] = ldg(&d.w.pos[c0 + t]);
             __syncwarp();
             const uint32_t lo = max(b, c0), hi = min(e, c1);
             // tests first, into a hit mask per group of 32 candidates (no stores in the
@@ -306,7 +307,7 @@ __global__ void __launch_bounds__(NS_WARPS * 32) k_build_lists(Dev d) {
             // the hits appended in ascending slot order
             for (uint32_t g0 = lo; g0 < hi; g0 += 32) {
               const uint32_t len = min(32u, hi - g0);
-              const float4* st = stage + (g0 - c0);
+              const real4* st = stage + (g0 - c0);
               uint32_t m = 0u, k = 0u;
               for (; k + 4 <= len; k += 4) {  // four independent tests
                 const uint32_t h0 = exact_r2(xi - f3(st[k])) < thr;
@@ -338,7 +339,7 @@ __global__ void __launch_bounds__(NS_WARPS * 32) k_build_lists(Dev d) {
           const uint32_t b = d.cell_count[row + x0], e = d.cell_count[row + x1 + 1];
           for (uint32_t j = b; j < e; ++j) {
             if ((int)j == i) continue;
-            if (exact_r2(xi - f3(__ldg(&d.w.pos[j]))) < thr) append((int)j);
+            if (exact_r2(xi - f3(ldg(&d.w.pos[j]))) < thr) append((int)j);
           }
         }
       }

@@ -16,7 +16,7 @@
   for (int _k = 0, _c = (d).nbr_cnt[i]; _k < _c; ++_k)     \
     for (int j = (d).nbr[(size_t)_k * (d).cap + (i)], _o = 1; _o; _o = 0)
 
-struct GPV { float4 p, v; };
+struct GPV { real4 p, v; };
 
 // ---------------------------------------------------------------------------
 // compute_static_boundary_volume / compute_moving_boundary_volume (SPH/main.py:1010-1035)
@@ -27,13 +27,13 @@ __global__ void k_boundary_volume(Dev d, int moving) {
     const uint32_t fl = d.w.flags[i];
     if (moving ? !cls_dyn_solid(fl) : !cls_static_solid(fl)) continue;
     const SceneDev& s = d.sc[slot_scene(fl)];
-    const float3 xi = f3(d.w.pos[i]);
-    float delta = s.W0;
+    const real3 xi = f3(d.w.pos[i]);
+    real delta = s.W0;
     // plain loads: this pass writes pos.w of solid slots (the sign never changes)
     nb_batches<U>(d.nbr + i, d.cap, d.nbr_cnt[i], i, [&](int j) { return d.w.pos[j]; },
-               [&](int, float4 pj) {
+               [&](int, real4 pj) {
                  if (!w_fluid(pj.w)) {
-                   const float3 r = xi - f3(pj);
+                   const real3 r = xi - f3(pj);
                    delta += kw_r2(dot3(r, r), s);
                  }
                });
@@ -47,7 +47,7 @@ __global__ void k_clear_acc(Dev d) {
   GRID_STRIDE(i, n) {
     const uint32_t fl = d.w.flags[i];
     const SceneDev& s = d.sc[slot_scene(fl)];
-    d.acc4[i] = cls_static_solid(fl) ? make_float4(0.f, 0.f, 0.f, 0.f) : make_float4(s.g[0], s.g[1], s.g[2], 0.f);
+    d.acc4[i] = cls_static_solid(fl) ? make_real4(0.f, 0.f, 0.f, 0.f) : make_real4(s.g[0], s.g[1], s.g[2], 0.f);
   }
 }
 
@@ -64,33 +64,33 @@ __global__ void k_density_factor(Dev d, int do_density, int do_factor) {
     const uint32_t fl = valid ? d.w.flags[i] : 0u;
     const bool work = valid && cls_fluid(fl);
     const int scn = slot_scene(fl);
-    float rho = 0.f;
+    real rho = 0.f;
     if (work) {
       const SceneDev& s = d.sc[scn];
-      const float4 pi = d.w.pos[i];
-      const float3 xi = f3(pi);
-      const float3 vi = f3(d.w.vel[i]);
+      const real4 pi = d.w.pos[i];
+      const real3 xi = f3(pi);
+      const real3 vi = f3(d.w.vel[i]);
       const int c = d.nbr_cnt[i];
-      float den = 0.f, sum_grad = 0.f, dd = 0.f;
-      float3 gpi = make_float3(0.f, 0.f, 0.f);
-      auto body = [&](float4 pj, float4 vj) {
-        const float3 r = xi - f3(pj);
-        float w;
-        float3 g;
+      real den = 0.f, sum_grad = 0.f, dd = 0.f;
+      real3 gpi = make_real3(0.f, 0.f, 0.f);
+      auto body = [&](real4 pj, real4 vj) {
+        const real3 r = xi - f3(pj);
+        real w;
+        real3 g;
         kwg_r2(r, dot3(r, r), s, w, g);
-        const float V = fabsf(pj.w);
+        const real V = fabs(pj.w);
         den += V * w;
-        const float3 gpj = g * (-V);
+        const real3 gpj = g * (-V);
         if (w_fluid(pj.w)) sum_grad += dot3(gpj, gpj);
         gpi -= gpj;
         if (CHANGE) dd += V * dot3(vi - f3(vj), g);
       };
       if constexpr (CHANGE) {
-        nb_batches<U>(d.nbr + i, d.cap, c, i, [&](int j) { return GPV{__ldg(&d.w.pos[j]), __ldg(&d.w.vel[j])}; },
+        nb_batches<U>(d.nbr + i, d.cap, c, i, [&](int j) { return GPV{ldg(&d.w.pos[j]), ldg(&d.w.vel[j])}; },
                       [&](int, const GPV& g) { body(g.p, g.v); });
       } else {
-        nb_batches<U>(d.nbr + i, d.cap, c, i, [&](int j) { return __ldg(&d.w.pos[j]); },
-                      [&](int, float4 pj) { body(pj, pj); });
+        nb_batches<U>(d.nbr + i, d.cap, c, i, [&](int j) { return ldg(&d.w.pos[j]); },
+                      [&](int, real4 pj) { body(pj, pj); });
       }
       if (do_density) {
         rho = pi.w * s.W0;
@@ -100,9 +100,9 @@ __global__ void k_density_factor(Dev d, int do_density, int do_factor) {
       }
       if (do_factor) {
         sum_grad += dot3(gpi, gpi);
-        float alpha = sum_grad > 1e-6f ? -1.f / sum_grad : 0.f;
+        real alpha = sum_grad > 1e-6f ? -1.f / sum_grad : 0.f;
         if (CHANGE && d.dyn[scn].act_v) {
-          dd = fmaxf(dd, 0.f);
+          dd = fmax(dd, real(0));
           if (c < 20) dd = 0.f;
           d.rho_adv[i] = dd;
           alpha = alpha * d.dyn[scn].inv_dt;
@@ -111,7 +111,7 @@ __global__ void k_density_factor(Dev d, int do_density, int do_factor) {
         d.alpha[i] = alpha;
       }
     }
-    if (do_density) warp_max_to(&d.dyn[scn].max_density_bits, __float_as_uint(rho), work);
+    if (do_density) warp_max_to(&d.dyn[scn].max_density_bits, __float_as_uint((float)rho), work);
   }
 }
 
@@ -128,19 +128,19 @@ __global__ void NN_PASS_REGS k_density_change(Dev d, int mode) {
     double err = 0.0;
     if (work) {
       const SceneDev& s = d.sc[scn];
-      const float3 xi = f3(d.w.pos[i]);
-      const float3 vi = f3(d.w.vel[i]);
+      const real3 xi = f3(d.w.pos[i]);
+      const real3 vi = f3(d.w.vel[i]);
       const int c = d.nbr_cnt[i];
-      float dd = 0.f;
-      nb_batches<U>(d.nbr + i, d.cap, c, i, [&](int j) { return GPV{__ldg(&d.w.pos[j]), __ldg(&d.w.vel[j])}; },
+      real dd = 0.f;
+      nb_batches<U>(d.nbr + i, d.cap, c, i, [&](int j) { return GPV{ldg(&d.w.pos[j]), ldg(&d.w.vel[j])}; },
                  [&](int, const GPV& g) {
-                   const float3 r = xi - f3(g.p);
-                   dd += fabsf(g.p.w) * dot3(vi - f3(g.v), kgrad_r2(r, dot3(r, r), s));
+                   const real3 r = xi - f3(g.p);
+                   dd += fabs(g.p.w) * dot3(vi - f3(g.v), kgrad_r2(r, dot3(r, r), s));
                  });
-      dd = fmaxf(dd, 0.f);
+      dd = fmax(dd, real(0));
       if (c < 20) dd = 0.f;
       d.rho_adv[i] = dd;
-      float a = d.alpha[i];
+      real a = d.alpha[i];
       if (mode == 0) {
         a = a * d.dyn[scn].inv_dt;
         d.alpha[i] = a;
@@ -154,7 +154,7 @@ __global__ void NN_PASS_REGS k_density_change(Dev d, int mode) {
 
 // divergence_solver_iteration_kernel (SPH/main.py:1721-1760). The pushes onto
 // dynamic solids (1755-1760) are omitted: clear_accelerations (1552) discards them.
-struct GPK { float4 p; float k; };
+struct GPK { real4 p; real k; };
 template <int U>
 __global__ void NN_PASS_REGS k_divergence_update(Dev d) {
   const int n = d.d_n[0];
@@ -164,21 +164,21 @@ __global__ void NN_PASS_REGS k_divergence_update(Dev d) {
     const int scn = slot_scene(fl);
     if (!d.dyn[scn].act_v) continue;
     const SceneDev& s = d.sc[scn];
-    const float dt = d.dyn[scn].dt;
-    const float3 xi = f3(d.w.pos[i]);
-    const float k_i = d.kappa[i];
-    float3 dv = make_float3(0.f, 0.f, 0.f);
-    nb_batches<U>(d.nbr + i, d.cap, d.nbr_cnt[i], i, [&](int j) { return GPK{__ldg(&d.w.pos[j]), __ldg(&d.kappa[j])}; },
+    const real dt = d.dyn[scn].dt;
+    const real3 xi = f3(d.w.pos[i]);
+    const real k_i = d.kappa[i];
+    real3 dv = make_real3(0.f, 0.f, 0.f);
+    nb_batches<U>(d.nbr + i, d.cap, d.nbr_cnt[i], i, [&](int j) { return GPK{ldg(&d.w.pos[j]), ldg(&d.kappa[j])}; },
                [&](int, const GPK& g) {
-                 const float3 r = xi - f3(g.p);
+                 const real3 r = xi - f3(g.p);
                  if (w_fluid(g.p.w)) {
-                   const float k_sum = k_i + g.k;
-                   if (fabsf(k_sum) > s.eps) dv -= kgrad_r2(r, dot3(r, r), s) * (-g.p.w) * (dt * k_sum);
-                 } else if (fabsf(k_i) > s.eps) {
+                   const real k_sum = k_i + g.k;
+                   if (fabs(k_sum) > s.eps) dv -= kgrad_r2(r, dot3(r, r), s) * (-g.p.w) * (dt * k_sum);
+                 } else if (fabs(k_i) > s.eps) {
                    dv += kgrad_r2(r, dot3(r, r), s) * g.p.w * ((-dt * 1.f) * k_i);
                  }
                });
-    float4 v = d.w.vel[i];
+    real4 v = d.w.vel[i];
     v.x += dv.x; v.y += dv.y; v.z += dv.z;
     d.w.vel[i] = v;
   }
@@ -212,20 +212,20 @@ __global__ void NN_PASS_REGS k_density_adv(Dev d, int mode) {
     double err = 0.0;
     if (work) {
       const SceneDev& s = d.sc[scn];
-      const float dt = d.dyn[scn].dt;
-      const float3 xi = f3(d.w.pos[i]);
-      const float3 vi = f3(d.w.vel[i]);
-      float delta = 0.f;
+      const real dt = d.dyn[scn].dt;
+      const real3 xi = f3(d.w.pos[i]);
+      const real3 vi = f3(d.w.vel[i]);
+      real delta = 0.f;
       nb_batches<U, true>(d.nbr + i, d.cap, d.nbr_cnt[i], i,
-                 [&](int j) { return GPV{__ldg(&d.w.pos[j]), __ldg(&d.w.vel[j])}; },
+                 [&](int j) { return GPV{ldg(&d.w.pos[j]), ldg(&d.w.vel[j])}; },
                  [&](int, const GPV& g) {
-                   const float3 r = xi - f3(g.p);
-                   delta += fabsf(g.p.w) * dot3(vi - f3(g.v), kgrad_r2(r, dot3(r, r), s));
+                   const real3 r = xi - f3(g.p);
+                   delta += fabs(g.p.w) * dot3(vi - f3(g.v), kgrad_r2(r, dot3(r, r), s));
                  });
-      float da = d.w.dens[i] * s.inv_rho0 + dt * delta;
-      da = fmaxf(da, 1.f);
+      real da = d.w.dens[i] * s.inv_rho0 + dt * delta;
+      da = fmax(da, real(1));
       d.rho_adv[i] = da;
-      float a = d.alpha[i];
+      real a = d.alpha[i];
       if (mode != 1) {
         // mode 2 also applies the divergence solve's closing alpha *= dt (1713)
         if (mode == 2 && d.dyn[scn].div_ran) a = a * d.dyn[scn].dt;
@@ -252,35 +252,35 @@ __global__ void NN_PASS_REGS k_pressure_update(Dev d) {
     const int scn = slot_scene(fl);
     if (!d.dyn[scn].act_p) continue;
     const SceneDev& s = d.sc[scn];
-    const float dt = d.dyn[scn].dt;
-    const float4 pi = d.w.pos[i];
-    const float3 xi = f3(pi);
-    auto load = [&](int j) { return GPK{__ldg(&d.w.pos[j]), __ldg(&d.kappa[j])}; };
+    const real dt = d.dyn[scn].dt;
+    const real4 pi = d.w.pos[i];
+    const real3 xi = f3(pi);
+    auto load = [&](int j) { return GPK{ldg(&d.w.pos[j]), ldg(&d.kappa[j])}; };
     if (fluid) {
-      const float k_i = d.kappa[i];
-      float4 v4 = d.w.vel[i];
-      float3 vi = f3(v4);
+      const real k_i = d.kappa[i];
+      real4 v4 = d.w.vel[i];
+      real3 vi = f3(v4);
       nb_batches<U, true>(d.nbr + i, d.cap, d.nbr_cnt[i], i, load, [&](int, const GPK& g) {
-        const float3 r = xi - f3(g.p);
+        const real3 r = xi - f3(g.p);
         if (w_fluid(g.p.w)) {
-          const float k_sum = k_i + g.k;
-          if (fabsf(k_sum) > s.eps) vi -= kgrad_r2(r, dot3(r, r), s) * (-g.p.w) * (dt * k_sum);
-        } else if (fabsf(k_i) > s.eps) {
+          const real k_sum = k_i + g.k;
+          if (fabs(k_sum) > s.eps) vi -= kgrad_r2(r, dot3(r, r), s) * (-g.p.w) * (dt * k_sum);
+        } else if (fabs(k_i) > s.eps) {
           vi += kgrad_r2(r, dot3(r, r), s) * g.p.w * ((-dt * 1.f) * k_i);
         }
       });
-      d.w.vel[i] = make_float4(vi.x, vi.y, vi.z, v4.w);
+      d.w.vel[i] = make_real4(vi.x, vi.y, vi.z, v4.w);
     } else {
-      const float Vi = fabsf(pi.w);
-      const float inv_dt = 1.f / dt;
-      float3 ai = make_float3(0.f, 0.f, 0.f);
+      const real Vi = fabs(pi.w);
+      const real inv_dt = 1.f / dt;
+      real3 ai = make_real3(0.f, 0.f, 0.f);
       nb_batches<U, true>(d.nbr + i, d.cap, d.nbr_cnt[i], i, load, [&](int, const GPK& g) {
-        if (!w_fluid(g.p.w) || !(fabsf(g.k) > s.eps)) return;
-        const float3 r = f3(g.p) - xi;  // x_fluid - x_solid, as the fluid computes it
-        const float3 vc = kgrad_r2(r, dot3(r, r), s) * (-Vi) * ((-dt * 1.f) * g.k);
+        if (!w_fluid(g.p.w) || !(fabs(g.k) > s.eps)) return;
+        const real3 r = f3(g.p) - xi;  // x_fluid - x_solid, as the fluid computes it
+        const real3 vc = kgrad_r2(r, dot3(r, r), s) * (-Vi) * ((-dt * 1.f) * g.k);
         ai -= vc * inv_dt;
       });
-      float4 a = d.acc4[i];
+      real4 a = d.acc4[i];
       a.x += ai.x; a.y += ai.y; a.z += ai.z;
       d.acc4[i] = a;
     }
@@ -363,14 +363,14 @@ __global__ void k_step_dt(Dev d, int do_cfl) {
     SceneDyn& y = d.dyn[sc];
     const SceneDev& s = d.sc[sc];
     if (do_cfl && (s.flags & NN_F_CFL)) {
-      const float vm = __uint_as_float(y.vmax_bits);
+      const real vm = __uint_as_float(y.vmax_bits);
       double dtn = s.cfl_max_dt;
       if (vm > 1e-9f) dtn = (double)s.cfl_factor * 0.4 * (double)s.diameter / (double)vm;
       dtn = fmin(fmax(dtn, (double)s.cfl_min_dt), (double)s.cfl_max_dt);
-      y.dt = (float)dtn;
+      y.dt = (real)dtn;
     }
-    y.inv_dt = (float)(1.0 / (double)y.dt);
-    y.inv_dt2 = (float)(1.0 / ((double)y.dt * (double)y.dt));
+    y.inv_dt = (real)(1.0 / (double)y.dt);
+    y.inv_dt2 = (real)(1.0 / ((double)y.dt * (double)y.dt));
     y.vmax_bits = 0u;
   }
 }
@@ -381,9 +381,9 @@ __global__ void k_np_advect(Dev d) {
   GRID_STRIDE(i, n) {
     const uint32_t fl = d.w.flags[i];
     if (!cls_fluid(fl) || !(fl & NN_CLS_DYNAMIC)) continue;
-    const float dt = d.dyn[slot_scene(fl)].dt;
-    const float4 a = d.acc4[i];
-    float4 v = d.w.vel[i];
+    const real dt = d.dyn[slot_scene(fl)].dt;
+    const real4 a = d.acc4[i];
+    real4 v = d.w.vel[i];
     v.x += dt * a.x; v.y += dt * a.y; v.z += dt * a.z;
     d.w.vel[i] = v;
   }
@@ -424,22 +424,22 @@ __global__ void k_step_end(Dev d) {
 // ---------------------------------------------------------------------------
 // NonNewton viscosity laws (SPH/main.py:404-459); quirk mode keeps the Newtonian
 // branch that the reference's int-vs-Enum dispatch always takes (387-402).
-__device__ __forceinline__ float nn_law(float g, const SceneDev& s) {
+__device__ __forceinline__ real nn_law(real g, const SceneDev& s) {
   const int method = (s.flags & NN_F_QUIRKS) ? NN_NEWTONIAN : s.nn_method;
   switch (method) {
-    case NN_POWER_LAW: return s.nn_K * powf(g, s.nn_n - 1.f);
-    case NN_CROSS: return s.nn_muinf + (s.nn_mu0 - s.nn_muinf) / (1.f + powf(s.nn_K * g, s.nn_n));
-    case NN_CASSON: { float q = sqrtf(s.nn_muc) + sqrtf(s.nn_tauy / g); return q * q; }
+    case NN_POWER_LAW: return s.nn_K * pow(g, s.nn_n - 1.f);
+    case NN_CROSS: return s.nn_muinf + (s.nn_mu0 - s.nn_muinf) / (1.f + pow(s.nn_K * g, s.nn_n));
+    case NN_CASSON: { real q = sqrt(s.nn_muc) + sqrt(s.nn_tauy / g); return q * q; }
     case NN_CARREAU:
       if (s.flags & NN_F_CARREAU_TEXTBOOK)
-        return s.nn_muinf + (s.nn_mu0 - s.nn_muinf) * powf(1.f + (s.nn_K * g) * (s.nn_K * g), (s.nn_n - 1.f) / 2.f);
-      return s.nn_muinf + (s.nn_mu0 - s.nn_muinf) / (1.f + powf(s.nn_K * g * g, (1.f - s.nn_n) / 2.f));
+        return s.nn_muinf + (s.nn_mu0 - s.nn_muinf) * pow(1.f + (s.nn_K * g) * (s.nn_K * g), (s.nn_n - 1.f) / 2.f);
+      return s.nn_muinf + (s.nn_mu0 - s.nn_muinf) / (1.f + pow(s.nn_K * g * g, (1.f - s.nn_n) / 2.f));
     case NN_BINGHAM:
       if (g < s.nn_gc) return s.nn_mu0;
       return s.nn_gc * (s.nn_mu0 - s.nn_muinf) / g + s.nn_muinf;
     case NN_HERSCHEL_BULKLEY:
       if (g < s.nn_gc) return s.nn_mu0;
-      return (s.nn_mu0 * s.nn_gc - s.nn_K * powf(s.nn_gc, s.nn_n)) / g + s.nn_K * powf(g, s.nn_n - 1.f);
+      return (s.nn_mu0 * s.nn_gc - s.nn_K * pow(s.nn_gc, s.nn_n)) / g + s.nn_K * pow(g, s.nn_n - 1.f);
     default: return s.nn_mu0;
   }
 }
@@ -453,7 +453,7 @@ __device__ __forceinline__ float nn_law(float g, const SceneDev& s) {
 // the boundary-viscosity reaction from their fluid neighbours (the reference scatters
 // it, 1459-1460). The velocity update of non_pressure_advect cannot join this pass:
 // the viscosity reads the neighbours' velocities.
-struct GF { float4 p, v; float rho; int id; };  // v.w = mass
+struct GF { real4 p, v; real rho; int id; };  // v.w = mass
 // Terms compiled into an instance of the force pass (the host picks the instance
 // that covers every scene of the batch; the scene flags still gate each term).
 #define FF_ST 1  // surface tension
@@ -477,48 +477,48 @@ __device__ __forceinline__ void forces_body(Dev d, int clear) {
         (FF & FF_VI) && cls_dyn_solid(fl) && !implicit && (s.flags & NN_F_VISCOSITY) && s.visc_b != 0.f;
     const bool nn_on = (FF & FF_SR) && (s.flags & NN_F_NONNEWTON);
     const bool sr_on = nn_on && (fluid || quirks);
-    const float4 pi = d.w.pos[i];
-    const float3 xi = f3(pi);
-    const float3 vi = f3(d.w.vel[i]);
-    float4 a;
-    if (clear) a = cls_static_solid(fl) ? make_float4(0.f, 0.f, 0.f, 0.f) : make_float4(s.g[0], s.g[1], s.g[2], 0.f);
+    const real4 pi = d.w.pos[i];
+    const real3 xi = f3(pi);
+    const real3 vi = f3(d.w.vel[i]);
+    real4 a;
+    if (clear) a = cls_static_solid(fl) ? make_real4(0.f, 0.f, 0.f, 0.f) : make_real4(s.g[0], s.g[1], s.g[2], 0.f);
     else a = d.acc4[i];
-    float3 st = make_float3(0.f, 0.f, 0.f), vs = make_float3(0.f, 0.f, 0.f), rf = make_float3(0.f, 0.f, 0.f);
-    float S[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // strain-rate sum: 00 11 22 01 02 12
+    real3 st = make_real3(0.f, 0.f, 0.f), vs = make_real3(0.f, 0.f, 0.f), rf = make_real3(0.f, 0.f, 0.f);
+    real S[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // strain-rate sum: 00 11 22 01 02 12
     int last_id = -1;                             // quirk: the last neighbour in id order survives
     if (st_on || vi_on || vb_on || sr_on) {
-      const float mi = d.w.mass[i];
-      const float rho_i = d.w.dens[i];
-      const float Vi = fabsf(pi.w);
+      const real mi = d.w.mass[i];
+      const real rho_i = d.w.dens[i];
+      const real Vi = fabs(pi.w);
       const bool need_rho = vi_on || vb_on;  // density and id only where a term reads them
       nb_batches<U>(d.nbr + i, d.cap, d.nbr_cnt[i], i,
                     [&](int j) {
-                      return GF{__ldg(&d.w.pos[j]), __ldg(&d.w.vel[j]), need_rho ? __ldg(&d.w.dens[j]) : 1.f,
-                                quirks ? __ldg(&d.w.id[j]) : 0};
+                      return GF{ldg(&d.w.pos[j]), ldg(&d.w.vel[j]), need_rho ? ldg(&d.w.dens[j]) : 1.f,
+                                quirks ? ldg(&d.w.id[j]) : 0};
                     },
                     [&](int, const GF& g) {
-                      const float3 r = xi - f3(g.p);
-                      const float r2 = dot3(r, r);
-                      float w;
-                      float3 gw;
+                      const real3 r = xi - f3(g.p);
+                      const real r2 = dot3(r, r);
+                      real w;
+                      real3 gw;
                       kwg_r2(r, r2, s, w, gw);
                       const bool jf = w_fluid(g.p.w);
-                      const float mj = g.v.w;
+                      const real mj = g.v.w;
                       if (jf && st_on) st -= (r * (s.sigma / mi * mj)) * (r2 > s.dia2 ? w : s.w_dia);
                       if (vi_on) {
-                        const float v_xy = dot3(vi - f3(g.v), r);
+                        const real v_xy = dot3(vi - f3(g.v), r);
                         if (jf) vs += gw * (10.f * s.visc * (mj / g.rho) * v_xy / (r2 + s.c01h2));
                         else if (s.visc_b != 0.f)
-                          vs += gw * (10.f * s.visc_b * (s.rho0 * fabsf(g.p.w) / rho_i) * v_xy / (r2 + s.c01h2));
+                          vs += gw * (10.f * s.visc_b * (s.rho0 * fabs(g.p.w) / rho_i) * v_xy / (r2 + s.c01h2));
                       }
                       if (vb_on && jf) {  // reaction on a dynamic solid: the fluid's term with i <-> j
-                        const float3 rr = -r;
-                        const float v_xy = dot3(f3(g.v) - vi, rr);
+                        const real3 rr = -r;
+                        const real v_xy = dot3(f3(g.v) - vi, rr);
                         rf += (-gw) * (10.f * s.visc_b * (s.rho0 * Vi / g.rho) * v_xy / (r2 + s.c01h2));
                       }
                       if (sr_on) {
-                        const float3 vji = f3(g.v) - vi;
-                        const float t[6] = {(vji.x * gw.x + vji.x * gw.x) * mj, (vji.y * gw.y + vji.y * gw.y) * mj,
+                        const real3 vji = f3(g.v) - vi;
+                        const real t[6] = {(vji.x * gw.x + vji.x * gw.x) * mj, (vji.y * gw.y + vji.y * gw.y) * mj,
                                             (vji.z * gw.z + vji.z * gw.z) * mj, (vji.x * gw.y + vji.y * gw.x) * mj,
                                             (vji.x * gw.z + vji.z * gw.x) * mj, (vji.y * gw.z + vji.z * gw.y) * mj};
                         const bool take = g.id > last_id;
@@ -532,21 +532,21 @@ __device__ __forceinline__ void forces_body(Dev d, int clear) {
     if (vi_on) { a.x += vs.x; a.y += vs.y; a.z += vs.z; }
     if (vb_on) { a.x -= rf.x; a.y -= rf.y; a.z -= rf.z; }
     d.acc4[i] = a;
-    float mu = s.mu_newton;
+    real mu = s.mu_newton;
     if (nn_on) {
-      float g = 0.f;
+      real g = 0.f;
       if (sr_on) {
-        float nrm2;
+        real nrm2;
         if (quirks) {
           nrm2 = S[0] * S[0] + S[1] * S[1] + S[2] * S[2] + 2.f * (S[3] * S[3] + S[4] * S[4] + S[5] * S[5]);
         } else {
-          const float sc = 0.5f / d.w.dens[i];
-          float D[6];
+          const real sc = 0.5f / d.w.dens[i];
+          real D[6];
 #pragma unroll
           for (int k = 0; k < 6; ++k) D[k] = S[k] * sc;
           nrm2 = D[0] * D[0] + D[1] * D[1] + D[2] * D[2] + 2.f * (D[3] * D[3] + D[4] * D[4] + D[5] * D[5]);
         }
-        g = sqrtf(nrm2);
+        g = sqrt(nrm2);
         mu = nn_law(g, s);
       } else {
         mu = 0.f;
@@ -556,8 +556,8 @@ __device__ __forceinline__ void forces_body(Dev d, int clear) {
     }
     // CG coefficients: (mu, m / rho) of a fluid slot; (0, 1) marks a dynamic solid
     if (implicit)
-      d.cg_aux[i] = fluid ? make_float2(mu, d.w.mass[i] / d.w.dens[i])
-                          : make_float2(0.f, cls_dyn_solid(fl) ? 1.f : 0.f);
+      d.cg_aux[i] = fluid ? make_real2(mu, d.w.mass[i] / d.w.dens[i])
+                          : make_real2(0.f, cls_dyn_solid(fl) ? 1.f : 0.f);
   }
 }
 
@@ -569,7 +569,7 @@ __device__ __forceinline__ void forces_body(Dev d, int clear) {
 template <int U, int FF>
 __global__ void k_forces(Dev d, int clear) { forces_body<U, FF>(d, clear); }
 template <int U, int FF>
-__global__ void __maxnreg__(64) k_forces_r64(Dev d, int clear) { forces_body<U, FF>(d, clear); }
+__global__ void NN_REGS64 k_forces_r64(Dev d, int clear) { forces_body<U, FF>(d, clear); }
 template <int U, int FF>
 constexpr void (*forces_kernel_of())(Dev, int) {
   if constexpr ((FF & FF_VI) != 0) return &k_forces<U, FF>;
@@ -592,43 +592,43 @@ __device__ __forceinline__ bool cg_row(const Dev& d, int i, uint32_t fl) {
 
 // A p for one row; in the setup also the diagonal block D and the right-hand-side
 // correction of moving boundaries (SETUP: `vec` is the velocity field).
-struct GCG { float4 p, x; float2 a; };
+struct GCG { real4 p, x; real2 a; };
 template <int U, bool SETUP>
-__device__ __forceinline__ float3 cg_apply(const Dev& d, int i, const float4* __restrict__ vec, float3 vi,
-                                           const SceneDev& s, float dt, float* D, float3* bcorr) {
-  const float3 xi = f3(d.w.pos[i]);
-  const float2 ai = d.cg_aux[i];
-  const float mi = d.w.mass[i];
-  const float rho_i = d.w.dens[i];
-  float3 acc = vi * mi;
-  const float cdt = dt * 10.f;
-  const float cb = cdt * s.mu_b * mi * s.rho0 / (rho_i * rho_i);
+__device__ __forceinline__ real3 cg_apply(const Dev& d, int i, const real4* __restrict__ vec, real3 vi,
+                                           const SceneDev& s, real dt, real* D, real3* bcorr) {
+  const real3 xi = f3(d.w.pos[i]);
+  const real2 ai = d.cg_aux[i];
+  const real mi = d.w.mass[i];
+  const real rho_i = d.w.dens[i];
+  real3 acc = vi * mi;
+  const real cdt = dt * 10.f;
+  const real cb = cdt * s.mu_b * mi * s.rho0 / (rho_i * rho_i);
   nb_batches<U>(d.nbr + i, d.cap, d.nbr_cnt[i], i,
              [&](int j) {
                GCG g;
-               g.p = __ldg(&d.w.pos[j]);
-               g.x = __ldg(&vec[j]);
-               g.a = __ldg(&d.cg_aux[j]);
+               g.p = ldg(&d.w.pos[j]);
+               g.x = ldg(&vec[j]);
+               g.a = ldg(&d.cg_aux[j]);
                return g;
              },
              [&](int, const GCG& g) {
-               const float3 r = xi - f3(g.p);
-               const float r2 = dot3(r, r);
-               const float3 gw = kgrad_r2(r, r2, s);
-               const float w = __fdividef(1.f, r2 + s.c01h2);
-               float c;
-               float3 diff;
+               const real3 r = xi - f3(g.p);
+               const real r2 = dot3(r, r);
+               const real3 gw = kgrad_r2(r, r2, s);
+               const real w = fast_div(1.f, r2 + s.c01h2);
+               real c;
+               real3 diff;
                if (w_fluid(g.p.w)) {
                  c = cdt * 0.5f * (ai.x + g.a.x) * ai.y * g.a.y;
                  diff = vi - f3(g.x);
                } else {
-                 c = cb * fabsf(g.p.w);
+                 c = cb * fabs(g.p.w);
                  diff = vi;
                  if (SETUP && g.a.y > 0.f) *bcorr -= gw * (c * dot3(r, f3(g.x)) * w);  // dynamic solid
                }
                acc -= gw * (c * dot3(r, diff) * w);
                if (SETUP) {
-                 const float cw = c * w;
+                 const real cw = c * w;
                  D[0] -= cw * gw.x * r.x; D[1] -= cw * gw.y * r.y; D[2] -= cw * gw.z * r.z;
                  D[3] -= cw * gw.x * r.y; D[4] -= cw * gw.x * r.z; D[5] -= cw * gw.y * r.z;
                }
@@ -636,14 +636,14 @@ __device__ __forceinline__ float3 cg_apply(const Dev& d, int i, const float4* __
   return acc;
 }
 
-__device__ __forceinline__ float3 sym_apply(const float* P, float3 v) {  // P: 00 11 22 01 02 12
-  return make_float3(P[0] * v.x + P[3] * v.y + P[4] * v.z, P[3] * v.x + P[1] * v.y + P[5] * v.z,
+__device__ __forceinline__ real3 sym_apply(const real* P, real3 v) {  // P: 00 11 22 01 02 12
+  return make_real3(P[0] * v.x + P[3] * v.y + P[4] * v.z, P[3] * v.x + P[1] * v.y + P[5] * v.z,
                      P[4] * v.x + P[5] * v.y + P[2] * v.z);
 }
 
 // 64 registers (from 72): 8 blocks of 128 per SM instead of 7
 template <int U>
-__global__ void __maxnreg__(64) k_cg_setup(Dev d) {
+__global__ void NN_REGS64 k_cg_setup(Dev d) {
   const int n = d.d_n[0];
   FOR_SLOTS_WARP(i, valid, n) {
     const uint32_t fl = valid ? d.w.flags[i] : 0u;
@@ -652,29 +652,29 @@ __global__ void __maxnreg__(64) k_cg_setup(Dev d) {
     double rr = 0, bb = 0, rz = 0;
     if (work) {
       const SceneDev& s = d.sc[scn];
-      const float dt = d.dyn[scn].dt;
-      const float mi = d.w.mass[i];
-      const float3 vi = f3(d.w.vel[i]);
-      float D[6] = {mi, mi, mi, 0.f, 0.f, 0.f};
-      float3 bc = make_float3(0.f, 0.f, 0.f);
-      const float3 Av = cg_apply<U, true>(d, i, d.w.vel, vi, s, dt, D, &bc);
-      const float3 b = vi * mi + bc;
+      const real dt = d.dyn[scn].dt;
+      const real mi = d.w.mass[i];
+      const real3 vi = f3(d.w.vel[i]);
+      real D[6] = {mi, mi, mi, 0.f, 0.f, 0.f};
+      real3 bc = make_real3(0.f, 0.f, 0.f);
+      const real3 Av = cg_apply<U, true>(d, i, d.w.vel, vi, s, dt, D, &bc);
+      const real3 b = vi * mi + bc;
       // symmetric 3x3 inverse in double
       double a00 = D[0], a11 = D[1], a22 = D[2], a01 = D[3], a02 = D[4], a12 = D[5];
       double c00 = a11 * a22 - a12 * a12, c01 = a02 * a12 - a01 * a22, c02 = a01 * a12 - a02 * a11;
       double det = a00 * c00 + a01 * c01 + a02 * c02;
       double id = 1.0 / det;
-      float P[6] = {(float)(c00 * id), (float)((a00 * a22 - a02 * a02) * id), (float)((a00 * a11 - a01 * a01) * id),
-                    (float)(c01 * id), (float)(c02 * id), (float)((a01 * a02 - a00 * a12) * id)};
+      real P[6] = {(real)(c00 * id), (real)((a00 * a22 - a02 * a02) * id), (real)((a00 * a11 - a01 * a01) * id),
+                    (real)(c01 * id), (real)(c02 * id), (real)((a01 * a02 - a00 * a12) * id)};
 #pragma unroll
       for (int k = 0; k < 6; ++k) d.cg_pinv[(size_t)k * d.cap + i] = P[k];
-      const float3 r = b - Av;
-      const float3 z = sym_apply(P, r);
-      d.cg_b[i] = make_float4(b.x, b.y, b.z, 0.f);
-      d.cg_x[i] = make_float4(vi.x, vi.y, vi.z, 0.f);
-      d.cg_r[i] = make_float4(r.x, r.y, r.z, 0.f);
-      d.cg_z[i] = make_float4(z.x, z.y, z.z, 0.f);
-      d.cg_p[i] = make_float4(z.x, z.y, z.z, 0.f);
+      const real3 r = b - Av;
+      const real3 z = sym_apply(P, r);
+      d.cg_b[i] = make_real4(b.x, b.y, b.z, 0.f);
+      d.cg_x[i] = make_real4(vi.x, vi.y, vi.z, 0.f);
+      d.cg_r[i] = make_real4(r.x, r.y, r.z, 0.f);
+      d.cg_z[i] = make_real4(z.x, z.y, z.z, 0.f);
+      d.cg_p[i] = make_real4(z.x, z.y, z.z, 0.f);
       rr = (double)r.x * r.x + (double)r.y * r.y + (double)r.z * r.z;
       bb = (double)b.x * b.x + (double)b.y * b.y + (double)b.z * b.z;
       rz = (double)r.x * z.x + (double)r.y * z.y + (double)r.z * z.z;
@@ -723,9 +723,9 @@ __global__ void k_cg_matvec(Dev d) {
     double pap = 0;
     if (work) {
       const SceneDev& s = d.sc[scn];
-      const float3 p = f3(d.cg_p[i]);
-      const float3 Ap = cg_apply<U, false>(d, i, d.cg_p, p, s, d.dyn[scn].dt, nullptr, nullptr);
-      d.cg_Ap[i] = make_float4(Ap.x, Ap.y, Ap.z, 0.f);
+      const real3 p = f3(d.cg_p[i]);
+      const real3 Ap = cg_apply<U, false>(d, i, d.cg_p, p, s, d.dyn[scn].dt, nullptr, nullptr);
+      d.cg_Ap[i] = make_real4(Ap.x, Ap.y, Ap.z, 0.f);
       pap = (double)p.x * Ap.x + (double)p.y * Ap.y + (double)p.z * Ap.z;
     }
     scene_add(d.acc, ACC_PAP, 0, scn, work, pap);
@@ -740,18 +740,18 @@ __global__ void k_cg_update(Dev d) {
     const bool work = valid && cg_row(d, i, fl) && d.dyn[scn].act_cg;
     double rr = 0, rz = 0;
     if (work) {
-      const float al = (float)d.dyn[scn].cg_alpha;
-      float3 x = f3(d.cg_x[i]), r = f3(d.cg_r[i]);
-      const float3 p = f3(d.cg_p[i]), Ap = f3(d.cg_Ap[i]);
+      const real al = (real)d.dyn[scn].cg_alpha;
+      real3 x = f3(d.cg_x[i]), r = f3(d.cg_r[i]);
+      const real3 p = f3(d.cg_p[i]), Ap = f3(d.cg_Ap[i]);
       x += p * al;
       r -= Ap * al;
-      float P[6];
+      real P[6];
 #pragma unroll
       for (int k = 0; k < 6; ++k) P[k] = d.cg_pinv[(size_t)k * d.cap + i];
-      const float3 z = sym_apply(P, r);
-      d.cg_x[i] = make_float4(x.x, x.y, x.z, 0.f);
-      d.cg_r[i] = make_float4(r.x, r.y, r.z, 0.f);
-      d.cg_z[i] = make_float4(z.x, z.y, z.z, 0.f);
+      const real3 z = sym_apply(P, r);
+      d.cg_x[i] = make_real4(x.x, x.y, x.z, 0.f);
+      d.cg_r[i] = make_real4(r.x, r.y, r.z, 0.f);
+      d.cg_z[i] = make_real4(z.x, z.y, z.z, 0.f);
       rr = (double)r.x * r.x + (double)r.y * r.y + (double)r.z * r.z;
       rz = (double)r.x * z.x + (double)r.y * z.y + (double)r.z * z.z;
     }
@@ -808,10 +808,10 @@ __global__ void k_cg_pupdate(Dev d) {
     const uint32_t fl = d.w.flags[i];
     const int scn = slot_scene(fl);
     if (!cg_row(d, i, fl) || !d.dyn[scn].act_cg) continue;
-    const float be = (float)d.dyn[scn].cg_beta;
-    const float3 z = f3(d.cg_z[i]), p = f3(d.cg_p[i]);
-    const float3 np = z + p * be;
-    d.cg_p[i] = make_float4(np.x, np.y, np.z, 0.f);
+    const real be = (real)d.dyn[scn].cg_beta;
+    const real3 z = f3(d.cg_z[i]), p = f3(d.cg_p[i]);
+    const real3 np = z + p * be;
+    d.cg_p[i] = make_real4(np.x, np.y, np.z, 0.f);
   }
 }
 
@@ -826,18 +826,18 @@ __global__ void k_cg_finish(Dev d, int advect) {
     const int scn = slot_scene(fl);
     const SceneDev& s = d.sc[scn];
     if (s.n_fluid == 0) continue;
-    const float dt = d.dyn[scn].dt;
-    float4 a = d.acc4[i];
-    const float4 v4 = d.w.vel[i];
+    const real dt = d.dyn[scn].dt;
+    real4 a = d.acc4[i];
+    const real4 v4 = d.w.vel[i];
     if (scene_implicit(s)) {
-      const float inv_dt = d.dyn[scn].inv_dt;
-      const float3 x = f3(d.cg_x[i]);
+      const real inv_dt = d.dyn[scn].inv_dt;
+      const real3 x = f3(d.cg_x[i]);
       a.x += (x.x - v4.x) * inv_dt;
       a.y += (x.y - v4.y) * inv_dt;
       a.z += (x.z - v4.z) * inv_dt;
       d.acc4[i] = a;
     }
-    if (advect && (fl & NN_CLS_DYNAMIC)) d.w.vel[i] = make_float4(v4.x + dt * a.x, v4.y + dt * a.y, v4.z + dt * a.z, v4.w);
+    if (advect && (fl & NN_CLS_DYNAMIC)) d.w.vel[i] = make_real4(v4.x + dt * a.x, v4.y + dt * a.y, v4.z + dt * a.z, v4.w);
   }
 }
 
@@ -857,16 +857,16 @@ __global__ void k_el_rotations(Dev d, int rep) {
     const uint32_t fl = d.w.flags[i];
     const SceneDev& s = d.sc[slot_scene(fl)];
     if (rep >= s.el_mult) continue;
-    const float3 xi = f3(d.w.pos[i]);
-    const float3 x0i = f3(d.el_x0[e]);
-    const float mi = d.w.mass[i];
-    float A[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    const real3 xi = f3(d.w.pos[i]);
+    const real3 x0i = f3(d.el_x0[e]);
+    const real mi = d.w.mass[i];
+    real A[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     const int c = d.el_cnt[e];
     for (int k = 0; k < c; ++k) {
       const int je = d.el_nb[(size_t)k * d.el_stride + e];
-      const float3 xji = f3(d.w.pos[d.el_slot[je]]) - xi;
-      const float3 xji0 = f3(d.el_x0[je]) - x0i;
-      const float wgt = mi * kernel_w(sqrtf(dot3(xji0, xji0)), s);
+      const real3 xji = f3(d.w.pos[d.el_slot[je]]) - xi;
+      const real3 xji0 = f3(d.el_x0[je]) - x0i;
+      const real wgt = mi * kernel_w(sqrt(dot3(xji0, xji0)), s);
       A[0] += xji.x * xji0.x * wgt; A[1] += xji.x * xji0.y * wgt; A[2] += xji.x * xji0.z * wgt;
       A[3] += xji.y * xji0.x * wgt; A[4] += xji.y * xji0.y * wgt; A[5] += xji.y * xji0.z * wgt;
       A[6] += xji.z * xji0.x * wgt; A[7] += xji.z * xji0.y * wgt; A[8] += xji.z * xji0.z * wgt;
@@ -874,7 +874,7 @@ __global__ void k_el_rotations(Dev d, int rep) {
     double Ad[3][3], Rd[3][3];
     for (int k = 0; k < 9; ++k) Ad[k / 3][k % 3] = (double)A[k];
     closest_rotation(Ad, Rd);
-    for (int k = 0; k < 9; ++k) d.el_R[(size_t)k * d.el_stride + e] = (float)Rd[k / 3][k % 3];
+    for (int k = 0; k < 9; ++k) d.el_R[(size_t)k * d.el_stride + e] = (real)Rd[k / 3][k % 3];
   }
 }
 
@@ -886,31 +886,31 @@ __global__ void k_el_stress(Dev d, int rep) {
     const uint32_t fl = d.w.flags[i];
     const SceneDev& s = d.sc[slot_scene(fl)];
     if (rep >= s.el_mult) continue;
-    const float3 xi = f3(d.w.pos[i]);
-    const float3 x0i = f3(d.el_x0[e]);
-    float R[9];
+    const real3 xi = f3(d.w.pos[i]);
+    const real3 x0i = f3(d.el_x0[e]);
+    real R[9];
 #pragma unroll
     for (int k = 0; k < 9; ++k) R[k] = d.el_R[(size_t)k * d.el_stride + e];
-    float G[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    real G[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     const int c = d.el_cnt[e];
     for (int k = 0; k < c; ++k) {
       const int je = d.el_nb[(size_t)k * d.el_stride + e];
-      const float4 x0j = d.el_x0[je];
-      const float3 xji = f3(d.w.pos[d.el_slot[je]]) - xi;
-      const float3 xji0 = f3(x0j) - x0i;
+      const real4 x0j = d.el_x0[je];
+      const real3 xji = f3(d.w.pos[d.el_slot[je]]) - xi;
+      const real3 xji0 = f3(x0j) - x0i;
       // u_ji = R^T x_ji - x0_ji
-      float3 u = make_float3(R[0] * xji.x + R[3] * xji.y + R[6] * xji.z - xji0.x,
+      real3 u = make_real3(R[0] * xji.x + R[3] * xji.y + R[6] * xji.z - xji0.x,
                              R[1] * xji.x + R[4] * xji.y + R[7] * xji.z - xji0.y,
                              R[2] * xji.x + R[5] * xji.y + R[8] * xji.z - xji0.z);
       u = u * x0j.w;
-      const float3 gw = kernel_grad(xji0, sqrtf(dot3(xji0, xji0)), s);
+      const real3 gw = kernel_grad(xji0, sqrt(dot3(xji0, xji0)), s);
       G[0] -= u.x * gw.x; G[1] -= u.x * gw.y; G[2] -= u.x * gw.z;
       G[3] -= u.y * gw.x; G[4] -= u.y * gw.y; G[5] -= u.y * gw.z;
       G[6] -= u.z * gw.x; G[7] -= u.z * gw.y; G[8] -= u.z * gw.z;
     }
-    const float e0 = G[0], e1 = G[4], e2 = G[8];
-    const float e3 = 0.5f * (G[1] + G[3]), e4 = 0.5f * (G[2] + G[6]), e5 = 0.5f * (G[5] + G[7]);
-    float S[6];
+    const real e0 = G[0], e1 = G[4], e2 = G[8];
+    const real e3 = 0.5f * (G[1] + G[3]), e4 = 0.5f * (G[2] + G[6]), e5 = 0.5f * (G[5] + G[7]);
+    real S[6];
     S[0] = s.el_cd * e0 + s.el_co * e1 + s.el_co * e2;
     S[1] = s.el_co * e0 + s.el_cd * e1 + s.el_co * e2;
     S[2] = s.el_co * e0 + s.el_co * e1 + s.el_cd * e2;
@@ -922,8 +922,8 @@ __global__ void k_el_stress(Dev d, int rep) {
   }
 }
 
-__device__ __forceinline__ float3 sym6_mul(const float* M, float3 v) {  // symMatTimesVec 1328-1332
-  return make_float3(M[0] * v.x + M[3] * v.y + M[4] * v.z, M[3] * v.x + M[1] * v.y + M[5] * v.z,
+__device__ __forceinline__ real3 sym6_mul(const real* M, real3 v) {  // symMatTimesVec 1328-1332
+  return make_real3(M[0] * v.x + M[3] * v.y + M[4] * v.z, M[3] * v.x + M[1] * v.y + M[5] * v.z,
                      M[4] * v.x + M[5] * v.y + M[2] * v.z);
 }
 
@@ -935,37 +935,37 @@ __global__ void k_el_forces(Dev d, int rep) {
     const uint32_t fl = d.w.flags[i];
     const SceneDev& s = d.sc[slot_scene(fl)];
     if (rep >= s.el_mult) continue;
-    const float4 x0i4 = d.el_x0[e];
-    const float3 x0i = f3(x0i4);
-    const float Vi = x0i4.w;
-    float Ri[9], Si[6];
+    const real4 x0i4 = d.el_x0[e];
+    const real3 x0i = f3(x0i4);
+    const real Vi = x0i4.w;
+    real Ri[9], Si[6];
 #pragma unroll
     for (int k = 0; k < 9; ++k) Ri[k] = d.el_R[(size_t)k * d.el_stride + e];
 #pragma unroll
     for (int k = 0; k < 6; ++k) Si[k] = d.el_S[(size_t)k * d.el_stride + e];
-    float3 f = make_float3(0.f, 0.f, 0.f);
+    real3 f = make_real3(0.f, 0.f, 0.f);
     const int c = d.el_cnt[e];
     for (int k = 0; k < c; ++k) {
       const int je = d.el_nb[(size_t)k * d.el_stride + e];
-      const float4 x0j = d.el_x0[je];
-      const float3 xji0 = f3(x0j) - x0i;
-      const float3 gw0 = kernel_grad(xji0, sqrtf(dot3(xji0, xji0)), s);
-      const float3 dji = gw0 * Vi;
-      const float3 dij = gw0 * (-x0j.w);
-      float Sj[6], Rj[9];
+      const real4 x0j = d.el_x0[je];
+      const real3 xji0 = f3(x0j) - x0i;
+      const real3 gw0 = kernel_grad(xji0, sqrt(dot3(xji0, xji0)), s);
+      const real3 dji = gw0 * Vi;
+      const real3 dij = gw0 * (-x0j.w);
+      real Sj[6], Rj[9];
 #pragma unroll
       for (int q = 0; q < 6; ++q) Sj[q] = d.el_S[(size_t)q * d.el_stride + je];
 #pragma unroll
       for (int q = 0; q < 9; ++q) Rj[q] = d.el_R[(size_t)q * d.el_stride + je];
-      const float3 fij = sym6_mul(Sj, dji) * (-x0j.w);
-      const float3 fji = sym6_mul(Si, dij) * (-Vi);
+      const real3 fij = sym6_mul(Sj, dji) * (-x0j.w);
+      const real3 fji = sym6_mul(Si, dij) * (-Vi);
       f.x += (Rj[0] * fij.x + Rj[1] * fij.y + Rj[2] * fij.z) - (Ri[0] * fji.x + Ri[1] * fji.y + Ri[2] * fji.z);
       f.y += (Rj[3] * fij.x + Rj[4] * fij.y + Rj[5] * fij.z) - (Ri[3] * fji.x + Ri[4] * fji.y + Ri[5] * fji.z);
       f.z += (Rj[6] * fij.x + Rj[7] * fij.y + Rj[8] * fij.z) - (Ri[6] * fji.x + Ri[7] * fji.y + Ri[8] * fji.z);
     }
     f = f * 0.5f;
-    const float mi = d.w.mass[i];
-    float4 a = d.acc4[i];
+    const real mi = d.w.mass[i];
+    real4 a = d.acc4[i];
     a.x += f.x / mi; a.y += f.y / mi; a.z += f.z / mi;
     d.acc4[i] = a;
   }
@@ -987,16 +987,16 @@ __global__ void k_el_init(Dev d) {
     const bool q = (s.flags & NN_F_QUIRKS) != 0;
     const int cap = q ? min(50, d.el_cap) : d.el_cap;
     const int ph = d.t.phase_id[id];
-    const float3 xi = f3(d.w.pos[i]);
-    const float mi = d.w.mass[i];
-    float den = mi * s.W0;
+    const real3 xi = f3(d.w.pos[i]);
+    const real mi = d.w.mass[i];
+    real den = mi * s.W0;
     int c = 0;
     NB_LOOP(d, i, j) {
       const int jid = d.w.id[j];
       const int je = d.e_of_id[jid];
       const bool member = q ? (je >= 0) : (je >= 0 && d.t.phase_id[jid] == ph);
-      const float3 r = xi - f3(d.w.pos[j]);
-      const float wj = d.w.mass[j] * kernel_w(sqrtf(dot3(r, r)), s);
+      const real3 r = xi - f3(d.w.pos[j]);
+      const real wj = d.w.mass[j] * kernel_w(sqrt(dot3(r, r)), s);
       if (q || member) den += wj;
       if (member) {
         if (c < cap) d.el_nb[(size_t)c * d.el_stride + e] = je;
@@ -1004,8 +1004,8 @@ __global__ void k_el_init(Dev d) {
       }
     }
     d.el_cnt[e] = min(c, cap);
-    const float3 x0 = make_float3(d.t.x_0[3 * id], d.t.x_0[3 * id + 1], d.t.x_0[3 * id + 2]);
-    d.el_x0[e] = make_float4(x0.x, x0.y, x0.z, mi / den);
+    const real3 x0 = make_real3(d.t.x_0[3 * id], d.t.x_0[3 * id + 1], d.t.x_0[3 * id + 2]);
+    d.el_x0[e] = make_real4(x0.x, x0.y, x0.z, mi / den);
 #pragma unroll
     for (int k = 0; k < 9; ++k) d.el_R[(size_t)k * d.el_stride + e] = (k % 4 == 0) ? 1.f : 0.f;
 #pragma unroll
@@ -1028,38 +1028,38 @@ __global__ void k_advect_boundary(Dev d, int do_advect, int do_boundary, int do_
     const bool move = do_anim && (an[0] != 0.f || an[1] != 0.f || an[2] != 0.f);
     if (!(fl & NN_CLS_DYNAMIC)) {
       if (move) {
-        float4 p = d.w.pos[i];
+        real4 p = d.w.pos[i];
         p.x += an[0]; p.y += an[1]; p.z += an[2];
         d.w.pos[i] = p;
       }
       continue;
     }
     const SceneDev& s = d.sc[scn];
-    const float dt = d.dyn[scn].dt;
-    float4 p = d.w.pos[i];
-    float4 v = d.w.vel[i];
+    const real dt = d.dyn[scn].dt;
+    real4 p = d.w.pos[i];
+    real4 v = d.w.vel[i];
     if (do_advect) {
       if (cls_dyn_solid(fl)) {
-        const float4 a = d.acc4[i];
+        const real4 a = d.acc4[i];
         v.x += dt * a.x; v.y += dt * a.y; v.z += dt * a.z;
       }
       p.x += dt * v.x; p.y += dt * v.y; p.z += dt * v.z;
     }
     if (move) { p.x += an[0]; p.y += an[1]; p.z += an[2]; }
     if (do_boundary) {
-      float pos[3] = {p.x, p.y, p.z};
-      float nrm[3] = {0.f, 0.f, 0.f};
-      float q[3] = {p.x, p.y, p.z};
+      real pos[3] = {p.x, p.y, p.z};
+      real nrm[3] = {0.f, 0.f, 0.f};
+      real q[3] = {p.x, p.y, p.z};
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
         if (pos[k] > s.xmax[k]) { nrm[k] += 1.f; q[k] = s.xmax[k]; }
         if (pos[k] <= s.xmin[k]) { nrm[k] += -1.f; q[k] = s.xmin[k]; }
       }
       p.x = q[0]; p.y = q[1]; p.z = q[2];
-      const float len = sqrtf(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
+      const real len = sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
       if (len > 1e-6f) {
-        const float3 nn = make_float3(nrm[0] / len, nrm[1] / len, nrm[2] / len);
-        const float vd = (1.f + s.cf) * (v.x * nn.x + v.y * nn.y + v.z * nn.z);
+        const real3 nn = make_real3(nrm[0] / len, nrm[1] / len, nrm[2] / len);
+        const real vd = (1.f + s.cf) * (v.x * nn.x + v.y * nn.y + v.z * nn.z);
         v.x -= nn.x * vd; v.y -= nn.y * vd; v.z -= nn.z * vd;
         v.x *= s.sticky; v.y *= s.sticky; v.z *= s.sticky;
       }
@@ -1080,11 +1080,11 @@ __global__ void k_sync_out(Dev d, uint32_t mask) {
   const int n = d.d_n[0];
   GRID_STRIDE(id, n) {
     const int i = d.slot_of_id[id];
-    const float4 p = d.w.pos[i];
+    const real4 p = d.w.pos[i];
     if (mask & 1u) { d.t.x[3 * id] = p.x; d.t.x[3 * id + 1] = p.y; d.t.x[3 * id + 2] = p.z; }
-    if (mask & 2u) { const float4 v = d.w.vel[i]; d.t.v[3 * id] = v.x; d.t.v[3 * id + 1] = v.y; d.t.v[3 * id + 2] = v.z; }
-    if (mask & 4u) { const float4 a = d.acc4[i]; d.t.a[3 * id] = a.x; d.t.a[3 * id + 1] = a.y; d.t.a[3 * id + 2] = a.z; }
-    if (mask & 8u) d.t.volume[id] = fabsf(p.w);
+    if (mask & 2u) { const real4 v = d.w.vel[i]; d.t.v[3 * id] = v.x; d.t.v[3 * id + 1] = v.y; d.t.v[3 * id + 2] = v.z; }
+    if (mask & 4u) { const real4 a = d.acc4[i]; d.t.a[3 * id] = a.x; d.t.a[3 * id + 1] = a.y; d.t.a[3 * id + 2] = a.z; }
+    if (mask & 8u) d.t.volume[id] = fabs(p.w);
     if (mask & 16u) d.t.density[id] = d.w.dens[i];
     if (mask & 32u) d.t.dfsph_factor[id] = d.alpha[i];
     if (mask & 64u) d.t.density_adv[id] = d.rho_adv[i];
@@ -1109,15 +1109,15 @@ __global__ void k_sync_in(Dev d, uint32_t mask) {
   const int n = d.d_n[0];
   GRID_STRIDE(i, n) {
     const int id = d.w.id[i];
-    float4 p = d.w.pos[i];
+    real4 p = d.w.pos[i];
     if (mask & 1u) { p.x = d.t.x[3 * id]; p.y = d.t.x[3 * id + 1]; p.z = d.t.x[3 * id + 2]; }
     if (mask & 8u) p.w = cls_solid(d.w.flags[i]) ? -d.t.volume[id] : d.t.volume[id];
     d.w.pos[i] = p;
-    float m = d.w.mass[i];  // vel.w carries the mass
+    real m = d.w.mass[i];  // vel.w carries the mass
     if (mask & 256u) { m = d.t.m[id]; d.w.mass[i] = m; }
-    if (mask & 2u) d.w.vel[i] = make_float4(d.t.v[3 * id], d.t.v[3 * id + 1], d.t.v[3 * id + 2], m);
+    if (mask & 2u) d.w.vel[i] = make_real4(d.t.v[3 * id], d.t.v[3 * id + 1], d.t.v[3 * id + 2], m);
     else if (mask & 256u) d.w.vel[i].w = m;
-    if (mask & 4u) d.acc4[i] = make_float4(d.t.a[3 * id], d.t.a[3 * id + 1], d.t.a[3 * id + 2], 0.f);
+    if (mask & 4u) d.acc4[i] = make_real4(d.t.a[3 * id], d.t.a[3 * id + 1], d.t.a[3 * id + 2], 0.f);
     if (mask & 16u) d.w.dens[i] = d.t.density[id];
     if (mask & 32u) d.alpha[i] = d.t.dfsph_factor[id];
     if (mask & 64u) d.rho_adv[i] = d.t.density_adv[id];
@@ -1167,7 +1167,7 @@ __global__ void k_rigid_ground(Dev d, int round, int rep) {
     if (!cls_solid(fl)) continue;
     const SceneDev& s = d.sc[slot_scene(fl)];
     if (!(s.flags & NN_F_RIGID) || round >= s.n_rigid || rep >= s.coupling) continue;
-    float4 p = d.w.pos[i];
+    real4 p = d.w.pos[i];
     if (p.y < s.padding) { p.y = s.padding; d.w.pos[i] = p; }
   }
 }
@@ -1181,10 +1181,10 @@ __global__ void k_rigid_com(Dev d, int round, int rest) {
     if (b >= 0) {
       const SceneDev& s = d.sc[slot_scene(d.w.flags[i])];
       const double m = (double)(s.V0 * d.w.dens[i]);
-      float3 x;
+      real3 x;
       if (rest) {
         const int id = d.w.id[i];
-        x = make_float3(d.t.x_0[3 * id], d.t.x_0[3 * id + 1], d.t.x_0[3 * id + 2]);
+        x = make_real3(d.t.x_0[3 * id], d.t.x_0[3 * id + 1], d.t.x_0[3 * id + 2]);
       } else {
         x = f3(d.w.pos[i]);
       }
@@ -1215,7 +1215,7 @@ __global__ void k_rigid_A(Dev d, int round) {
       const SceneDev& s = d.sc[slot_scene(d.w.flags[i])];
       const double m = (double)(s.V0 * d.w.dens[i]);
       const int id = d.w.id[i];
-      const float4 x = d.w.pos[i];
+      const real4 x = d.w.pos[i];
       const double p[3] = {(double)x.x - d.rb_cm[3 * b], (double)x.y - d.rb_cm[3 * b + 1],
                            (double)x.z - d.rb_cm[3 * b + 2]};
       const double q[3] = {(double)d.t.x_0[3 * id] - d.rb_rest[3 * b], (double)d.t.x_0[3 * id + 1] - d.rb_rest[3 * b + 1],
@@ -1255,10 +1255,10 @@ __global__ void k_rigid_apply(Dev d, int round) {
     const double q[3] = {(double)d.t.x_0[3 * id] - d.rb_rest[3 * b], (double)d.t.x_0[3 * id + 1] - d.rb_rest[3 * b + 1],
                          (double)d.t.x_0[3 * id + 2] - d.rb_rest[3 * b + 2]};
     const double* R = &d.rb_R[9 * b];
-    float4 p = d.w.pos[i];
-    p.x = (float)(d.rb_cm[3 * b] + R[0] * q[0] + R[1] * q[1] + R[2] * q[2]);
-    p.y = (float)(d.rb_cm[3 * b + 1] + R[3] * q[0] + R[4] * q[1] + R[5] * q[2]);
-    p.z = (float)(d.rb_cm[3 * b + 2] + R[6] * q[0] + R[7] * q[1] + R[8] * q[2]);
+    real4 p = d.w.pos[i];
+    p.x = (real)(d.rb_cm[3 * b] + R[0] * q[0] + R[1] * q[1] + R[2] * q[2]);
+    p.y = (real)(d.rb_cm[3 * b + 1] + R[3] * q[0] + R[4] * q[1] + R[5] * q[2]);
+    p.z = (real)(d.rb_cm[3 * b + 2] + R[6] * q[0] + R[7] * q[1] + R[8] * q[2]);
     d.w.pos[i] = p;
   }
 }

@@ -2,6 +2,8 @@
 
 The CUDA library is the only compute path: if `libnnsph.so` is missing or no CUDA
 device is present, constructing an Engine raises. There is no CPU fallback.
+`precision="f64"` binds libnnsph64.so instead, the same kernels built with double
+arithmetic (the FP64 run the FP32 path's error is measured against).
 """
 from __future__ import annotations
 
@@ -14,8 +16,10 @@ from . import _abi
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libnnsph.so")
+LIB_PATHS = {"f32": LIB_PATH, "f64": os.path.join(HERE, "libnnsph64.so")}
+REAL_BYTES = {"f32": 4, "f64": 8}
 
-_lib = None
+_libs = {}
 
 
 class NNError(RuntimeError):
@@ -24,13 +28,13 @@ class NNError(RuntimeError):
         self.code = code
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not os.path.exists(LIB_PATH):
-            raise ImportError(f"{LIB_PATH} is missing: build it with `python __graft_entry__.py build` "
+def lib(precision: str = "f32"):
+    if precision not in _libs:
+        path = LIB_PATHS[precision]
+        if not os.path.exists(path):
+            raise ImportError(f"{path} is missing: build it with `python __graft_entry__.py build` "
                               "(or nonnewton_b200.build.build())")
-        L = C.CDLL(LIB_PATH)
+        L = C.CDLL(path)
         vp, i32, i64, u32 = C.c_void_p, C.c_int32, C.c_int64, C.c_uint32
         L.nn_abi_version.restype = C.c_int
         L.nn_last_error.restype = C.c_char_p
@@ -59,9 +63,12 @@ def lib():
                      "nn_set_block_size"):
             getattr(L, name).restype = C.c_int
         if L.nn_abi_version() != 1:
-            raise ImportError("libnnsph.so ABI version mismatch")
-        _lib = L
-    return _lib
+            raise ImportError(f"{os.path.basename(path)}: ABI version mismatch")
+        L.nn_real_bytes.restype = C.c_int
+        if L.nn_real_bytes() != REAL_BYTES[precision]:
+            raise ImportError(f"{os.path.basename(path)} computes in {L.nn_real_bytes()}-byte reals, not {precision}")
+        _libs[precision] = L
+    return _libs[precision]
 
 
 def _ptr(t):
@@ -72,7 +79,7 @@ class Engine:
     """One nn_ctx: capacities fixed at creation, state bound from torch tensors."""
 
     def __init__(self, max_particles: int, max_scenes: int = 1, max_neighbors: int = 64, max_cells: int = 0,
-                 device=None):
+                 device=None, precision: str = "f32"):
         if not torch.cuda.is_available():
             raise RuntimeError("nonnewton_b200 needs a CUDA device (the SPH step runs only as sm_100a kernels)")
         dev = torch.device(device if device is not None else "cuda")
@@ -80,7 +87,8 @@ class Engine:
             dev = torch.device("cuda", torch.cuda.current_device())
         self.device = dev
         torch.cuda.set_device(self.device)
-        self.L = lib()
+        self.precision = precision
+        self.L = lib(precision)
         h = C.c_void_p()
         self._rc(self.L.nn_ctx_create(int(max_particles), int(max_scenes), int(max_neighbors), int(max_cells),
                                       C.byref(h)), None)
@@ -172,6 +180,20 @@ class Engine:
         f.restype = C.c_int
         self._rc(f(self.h, int(max_neighbors)))
         self.max_neighbors = int(max_neighbors)
+
+    def status_async(self, out: torch.Tensor, scene: int = 0):
+        """Enqueue the copy of (status, max_neighbors_seen) of `scene` into `out`, two
+        int32 in pinned host memory (see nn_status_async); status_wait() waits for it."""
+        f = self.L.nn_status_async
+        f.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
+        f.restype = C.c_int
+        self._rc(f(self.h, int(scene), C.c_void_p(out.data_ptr())))
+
+    def status_wait(self):
+        f = self.L.nn_status_wait
+        f.argtypes = [C.c_void_p]
+        f.restype = C.c_int
+        self._rc(f(self.h))
 
     def stats(self, scene: int = 0) -> dict:
         s = _abi.nn_stats()

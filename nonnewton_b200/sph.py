@@ -97,6 +97,9 @@ class NeighborhoodSearchSparse:
         self._lists = None
 
     def run_search(self):
+        solver = getattr(meta, "solver", None)
+        if solver is not None:
+            solver._settle()  # a pending step check may still change the positions
         self.engine.run_pass(_abi.NN_PASS_SEARCH)
         self._lists = None
 
@@ -132,6 +135,9 @@ class SPHBase:
         # re-run a step whose neighbour lists overflowed, with a larger cap
         self.grow_neighbors = True
         self._snap = None
+        self._status = None
+        self._pending = None       # the last call's unchecked status copy
+        self._last_max = None      # largest neighbour count last seen
 
     def step(self):
         """SPHBase.step (SPH/main.py:915-940) as one CUDA-graph replay. With an animeFile,
@@ -169,33 +175,72 @@ class SPHBase:
         """`nsteps` steps through the engine. The reference's neighbour list has 60
         slots (SPH/main.py:777-781) and store_neighbors writes past them unchecked
         (845-847); here the lists have a checked capacity, and with `grow_neighbors`
-        steps whose lists overflowed it are run again from the state before them (x
-        and v, kept on the device) with the capacity raised past the largest count
-        seen. The check reads the scene's status word, one small device-to-host copy
-        per call."""
+        work whose lists overflowed it runs again from the state before it (x and v,
+        kept on the device) with the capacity raised past the largest count seen.
+
+        A call whose last known neighbour count is within a quarter of the capacity
+        reads the scene's status right after its steps (one host synchronisation).
+        Otherwise the status is copied to pinned memory without waiting and checked
+        when the next call (or stats()) begins; in the rare case that it overflowed,
+        the state it started from is restored and its steps run again, checked, before
+        the new work. Until then meta.pd holds that call's unverified result."""
         eng = self.engine
         if not self.grow_neighbors:
             if displacement is not None:
                 eng.set_animation(0, displacement)
             eng.step(nsteps, sync=True, host_loop=self.host_loop)
             return
+        self._settle()
         pd = meta.pd
         if self._snap is None or self._snap[0].shape != pd.x.shape:
             self._snap = (torch.empty_like(pd.x), torch.empty_like(pd.v))
+            self._status = torch.zeros(2, dtype=torch.int32, pin_memory=torch.cuda.is_available())
         self._snap[0].copy_(pd.x)
         self._snap[1].copy_(pd.v)
+        near = self._last_max is None or 4 * self._last_max >= 3 * eng.max_neighbors
+        if displacement is not None:
+            eng.set_animation(0, displacement)
+        eng.step(nsteps, sync=True, host_loop=self.host_loop)
+        if near:
+            self._check(nsteps, displacement)
+        else:
+            eng.status_async(self._status)
+            self._pending = (nsteps, displacement)
+
+    def _check(self, nsteps, displacement):
+        """Status after the steps just enqueued: on overflow, grow and run them again."""
+        eng = self.engine
         while True:
-            if displacement is not None:
-                eng.set_animation(0, displacement)
-            eng.step(nsteps, sync=True, host_loop=self.host_loop)
             st = eng.stats(0)
+            self._last_max = st["max_neighbors_seen"]
             if st["status"] != _abi.NN_ERR_NEIGHBOR_OVERFLOW or eng.max_neighbors >= 1024:
                 return
-            self._grow_cap(st)
-            pd.x.copy_(self._snap[0])
-            pd.v.copy_(self._snap[1])
-            if getattr(meta, "num_elastic_bodies", 0):
-                eng.initialize()  # re-sized rest lists, rebuilt from x_0 (the same rest state)
+            self._rerun(nsteps, displacement, st["max_neighbors_seen"])
+
+    def _rerun(self, nsteps, displacement, seen):
+        eng = self.engine
+        cap = max(seen, eng.max_neighbors) * 5 // 4
+        eng.set_neighbor_cap(min(1024, (cap + 7) // 8 * 8))
+        meta.pd.x.copy_(self._snap[0])
+        meta.pd.v.copy_(self._snap[1])
+        if getattr(meta, "num_elastic_bodies", 0):
+            eng.initialize()  # re-sized rest lists, rebuilt from x_0 (the same rest state)
+        if displacement is not None:
+            eng.set_animation(0, displacement)
+        eng.step(nsteps, sync=True, host_loop=self.host_loop)
+
+    def _settle(self):
+        """Check the previous call's status copy (see _advance)."""
+        if self._pending is None:
+            return
+        nsteps, displacement = self._pending
+        self._pending = None
+        self.engine.status_wait()
+        status, seen = (int(v) for v in self._status)
+        self._last_max = seen
+        if status == _abi.NN_ERR_NEIGHBOR_OVERFLOW:
+            self._rerun(nsteps, displacement, seen)
+            self._check(nsteps, displacement)
 
     def _grow_cap(self, st):
         cap = max(st["max_neighbors_seen"], self.engine.max_neighbors) * 5 // 4
@@ -204,6 +249,7 @@ class SPHBase:
     def initialize(self):
         """SPHBase.initialize (SPH/main.py:957-960) and the elastic rest state; with
         `grow_neighbors`, again with larger lists while they overflow."""
+        self._settle()
         self.engine.initialize()
         while self.grow_neighbors and self.engine.max_neighbors < 1024:
             st = self.engine.stats(0)
@@ -214,6 +260,7 @@ class SPHBase:
         meta.ns._lists = None
 
     def _pass(self, p):
+        self._settle()
         self.engine.run_pass(p)
 
     def clear_accelerations(self):
@@ -236,6 +283,7 @@ class SPHBase:
         self._pass(_abi.NN_PASS_ADVECT)
 
     def stats(self) -> dict:
+        self._settle()
         return self.engine.stats(0)
 
 
@@ -282,12 +330,14 @@ def build_solver():
     """`build_solver` (SPH/main.py:196-203)."""
     solver_type = meta.config.get_cfg("simulationMethod")
     if solver_type == 4:
-        return DFSPHSolver()
+        meta.solver = DFSPHSolver()
+        return meta.solver
     raise NotImplementedError(f"Solver type {solver_type} has not been implemented.")
 
 
 def initialize(config: SimConfig | str | dict | None = None, particles: ParticleSet | None = None,
-               quirks: bool = False, max_neighbors: int = 64, device="cuda", tuning: dict | None = None):
+               quirks: bool = False, max_neighbors: int = 64, device="cuda", tuning: dict | None = None,
+               precision: str = "f32"):
     """`initialize()` (SPH/main.py:1870-1895): parameters, particles, fields, the
     neighbour search object and the CUDA engine (which also sets up elastic bodies)."""
     if isinstance(config, str):
@@ -297,13 +347,14 @@ def initialize(config: SimConfig | str | dict | None = None, particles: Particle
     if config is not None:
         meta.config = config
     meta.parm = Parameter.from_config(meta.config, quirks=quirks)
+    meta.solver = None
     ps = particles if particles is not None else load_particles(meta.config, meta.parm)
     meta.phase_info = ps.phase_info
     meta.particle_max_num = ps.n
     meta.fluid_particle_num = ps.n_fluid
     meta.pd = ParticleData(ps.n, device=device)
     initialize_particles(meta.pd, ps, meta.parm)
-    meta.engine = Engine(max(ps.n, 1), 1, max_neighbors, device=device)
+    meta.engine = Engine(max(ps.n, 1), 1, max_neighbors, device=device, precision=precision)
     if tuning:
         meta.engine.set_tuning(tuning.get("block", 0), tuning.get("unroll", 0), tuning.get("cell_factor", 0))
     meta.engine.bind(meta.pd)

@@ -211,6 +211,12 @@ def test_animation_frames_reach_the_engine(monkeypatch):
         def stats(self, scene=0):
             return {"status": 0, "max_neighbors_seen": 30}
 
+        def status_async(self, out, scene=0):
+            out[0], out[1] = 0, 30
+
+        def status_wait(self):
+            pass
+
     cfg = types.SimpleNamespace(get_cfg=lambda k, d=None: None)
     pd = types.SimpleNamespace(x=torch.zeros(4, 3), v=torch.zeros(4, 3))
     m = types.SimpleNamespace(engine=Eng(), parm=types.SimpleNamespace(gravity=0, density0=1000, dt=1e-3),
@@ -275,3 +281,57 @@ def test_overflowed_step_runs_again_with_larger_lists(monkeypatch):
     calls.clear()
     s.step()
     assert calls == [("step", 1, 1.0)]
+
+
+def test_unchecked_step_is_checked_by_the_next_call(monkeypatch):
+    """Far from the capacity, a step's status is copied without waiting and read when
+    the next call begins: an overflow found there restores the x, v that step started
+    from and runs it again (checked) before the new step (host logic, fake engine)."""
+    import types
+
+    import torch
+
+    from nonnewton_b200 import _abi, sph
+
+    calls = []
+    reports = iter([(0, 20), (_abi.NN_ERR_NEIGHBOR_OVERFLOW, 70), (0, 20)])  # async copies of steps 2, 3, 4
+
+    class Eng:
+        max_neighbors = 64
+
+        def set_animation(self, scene, d):
+            pass
+
+        def step(self, n, sync=True, host_loop=False):
+            calls.append(("step", float(pd.x[0, 0])))
+            pd.x += 1.0
+
+        def stats(self, scene=0):
+            calls.append(("stats",))
+            return {"status": 0, "max_neighbors_seen": 20}
+
+        def status_async(self, out, scene=0):
+            calls.append(("async",))
+            out[0], out[1] = next(reports)
+
+        def status_wait(self):
+            pass
+
+        def set_neighbor_cap(self, cap):
+            calls.append(("cap", cap))
+            self.max_neighbors = cap
+
+    cfg = types.SimpleNamespace(get_cfg=lambda k, d=None: None)
+    pd = types.SimpleNamespace(x=torch.zeros(4, 3), v=torch.zeros(4, 3))
+    m = types.SimpleNamespace(engine=Eng(), parm=types.SimpleNamespace(gravity=0, density0=1000, dt=1e-3),
+                              ns=types.SimpleNamespace(_lists=None), config=cfg, step_num=0, pd=pd, anime=None)
+    monkeypatch.setattr(sph, "meta", m)
+    s = sph.SPHBase()
+    s.step()  # no count known yet: checked at once
+    s.step()  # 20 of 64: status copied without waiting
+    s.step()  # the copy says clean; this step's copy goes out unchecked
+    assert calls == [("step", 0.0), ("stats",), ("step", 1.0), ("async",), ("step", 2.0), ("async",)]
+    calls.clear()
+    s.step()  # the third step overflowed (70 seen): restored to x = 2 and run again first
+    assert calls == [("cap", 88), ("step", 2.0), ("stats",), ("step", 3.0), ("async",)]
+    assert float(pd.x[0, 0]) == 4.0 and m.step_num == 4

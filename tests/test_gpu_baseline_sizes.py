@@ -1,0 +1,124 @@
+"""Parity at the benchmark scenes' own sizes (the configurations the bench names),
+not on test-sized stand-ins:
+
+  - dam break, 23,002 particles (8,000 fluid in a 15,002-particle boundary box),
+    all 100 steps in lockstep with the FP32 oracle: each step starts from the same
+    x and v on both sides (the oracle takes the CUDA path's), iteration counts are
+    equal, fields agree within 1e-4 of their scale, and the DFSPH average density
+    error ends at or below maxError (0.1 % of rho0) every step, the reference's
+    stopping rule (SPH/main.py:1695-1703, 1778-1784);
+  - shear-thinning drop, 135,201 particles (Cross law, implicit viscosity CG, CFL),
+    20 steps in lockstep: the same, plus CG iteration counts within one and the CFL
+    time step equal;
+  - fluid + elastic block, 175,870 particles, the full 200 steps: after every step
+    the neighbour lists of all particles, searched on the current positions, equal
+    the oracle's search (the reference's rule p_i != p_j and |x_i - x_j| < h in f32,
+    SPH/main.py:836-847) as sorted id sets, pairs within 4 ulp of h excepted; the
+    lists are symmetric, the status stays clean and the state finite.
+"""
+import numpy as np
+import pytest
+import torch
+
+from nonnewton_b200 import _abi
+from nonnewton_b200 import scene as S
+
+from .helpers import gpu_sim, oracle_sim, pd_field, rel_err
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-4
+FIELDS = ("x", "v", "acceleration", "density", "dfsph_factor", "density_adv")
+FLUID_ONLY = ("density", "dfsph_factor", "density_adv")
+
+
+def _lockstep(sc, steps, cg=False):
+    m, solver = gpu_sim(sc)
+    solver.initialize()
+    o = oracle_sim(sc)
+    o.initialize()
+    nf = sc.particles.n_fluid
+    eta = sc.param.max_error * 0.01 * sc.param.density0
+    worst = {k: 0.0 for k in FIELDS}
+    iters = []
+    for k in range(steps):
+        o.set("x", pd_field(m, "x"))
+        o.set("v", pd_field(m, "v"))
+        solver.step()
+        o.step(1)
+        gs, os_ = m.engine.stats(0), o.stats()
+        assert gs["status"] == 0, (k, gs)
+        assert (gs["iterations_v"], gs["iterations"]) == (os_["iterations_v"], os_["iterations"]), (k, gs, os_)
+        if cg:
+            assert abs(gs["cg_iterations"] - os_["cg_iterations"]) <= 1, (k, gs, os_)
+            assert abs(gs["dt"] - os_["dt"]) <= 1e-6 * os_["dt"], (k, gs["dt"], os_["dt"])
+        if gs["iterations"] + 1 < sc.param.max_iterations:  # the loop stopped on the error, not the cap
+            assert gs["avg_density_err"] <= eta + 1e-9, (k, gs)
+        for name in FIELDS:
+            g, r = pd_field(m, name), o.get(name)
+            if name in FLUID_ONLY:
+                g, r = g[:nf], r[:nf]
+            e = rel_err(g, r)
+            worst[name] = max(worst[name], e)
+            assert e < TOL, f"step {k} {name}: {e:.2e}"
+        iters.append((gs["iterations_v"], gs["iterations"], gs["cg_iterations"]))
+    return m, worst, iters
+
+
+def test_dam_break_23k_lockstep_100_steps(cuda_lib):
+    sc = S.dam_break(seed=0)
+    assert sc.particles.n == 23002 and sc.particles.n_fluid == 8000
+    m, worst, iters = _lockstep(sc, 100)
+    assert max(i[1] for i in iters) >= 1  # the pressure solve iterated
+    print("dam break 23k, 100 steps, worst per-field error:", {k: f"{v:.1e}" for k, v in worst.items()})
+
+
+def test_shear_thinning_drop_135k_lockstep(cuda_lib):
+    sc = S.shear_thinning_drop(seed=0)
+    assert sc.particles.n == 135201 and sc.param.implicit_viscosity
+    m, worst, iters = _lockstep(sc, 20, cg=True)
+    assert sum(i[2] for i in iters) > 0  # the viscosity CG iterated
+    print("drop 135k, 20 steps, worst per-field error:", {k: f"{v:.1e}" for k, v in worst.items()})
+
+
+def _cutoff_tie(x, h, i, j, ulps=4):
+    d = np.linalg.norm(x[i].astype(np.float64) - x[j].astype(np.float64))
+    return abs(d - h) < ulps * float(np.spacing(np.float32(h)))
+
+
+def test_fluid_elastic_176k_lists_every_step(cuda_lib):
+    sc = S.fluid_elastic(seed=0)
+    n = sc.particles.n
+    assert n == 175870
+    m, solver = gpu_sim(sc)
+    solver.initialize()
+    o = oracle_sim(sc)
+    h = sc.param.support_radius
+    width = 64
+    ties = 0
+    for k in range(sc.steps):
+        solver.step()
+        m.ns.run_search()  # the lists of the current positions
+        num, lists = m.engine.neighbors(n, width)
+        x = m.pd.x.detach()
+        st = m.engine.stats(0)
+        assert st["status"] == 0 and st["max_neighbors_seen"] <= width, (k, st)
+        assert torch.isfinite(x).all() and torch.isfinite(m.pd.v).all(), k
+        # symmetry of all lists: j lists i exactly when i lists j
+        rows = torch.arange(n, device=x.device)[:, None].expand(-1, width)
+        mask = lists >= 0
+        i_, j_ = rows[mask].long(), lists[mask].long()
+        assert torch.equal(torch.sort(i_ * n + j_).values, torch.sort(j_ * n + i_).values), k
+        # every particle's list against the oracle's search on the same positions
+        xh = x.cpu().numpy()
+        o.set("x", xh)
+        o.run_pass(_abi.NN_PASS_SEARCH)
+        on, ol = o.neighbors(width)
+        gn, gl = num.cpu().numpy(), lists.cpu().numpy()
+        bad = np.nonzero((gn != on) | np.any(gl != ol, axis=1))[0]
+        for i in bad:
+            a = set(gl[i, : gn[i]].tolist())
+            b = set(ol[i, : on[i]].tolist())
+            for j in a ^ b:
+                assert _cutoff_tie(xh, h, i, j), (k, int(i), int(j))
+                ties += 1
+    print(f"fluid + elastic 176k: {sc.steps} steps, lists equal to the oracle's every step ({ties} cut-off ties)")

@@ -1,5 +1,11 @@
-"""Per-field error of the FP32 GPU step against the FP64 run of the same algorithm
-(the oracle in double precision), from identical initial states, free-running.
+"""Per-field error of the FP32 GPU step against FP64 runs, from identical initial
+states, free-running:
+
+  - against the FP64 build of the same CUDA kernels (libnnsph64.so: the same source
+    with double arithmetic; the caller's float32 state is read once at the start and
+    the run stays resident in double) on the benchmark scenes at their own sizes;
+  - against the FP64 run of the same algorithm on the CPU (the oracle in double
+    precision) on small scenes.
 
 The bounds are the stated accuracy of the FP32 path; the measured values are printed
 (pytest -s) and recorded in the design notes."""
@@ -63,3 +69,59 @@ def test_fp32_vs_fp64_per_field(cuda_lib, name, steps, bounds):
     print(f"\nFP32 GPU vs FP64 oracle, {name}, {steps} steps: " + ", ".join(f"{k} {v:.2e}" for k, v in errs.items()))
     for f, b in bounds.items():
         assert errs[f] < b, (f, errs[f])
+
+
+def _run_build(sc, precision, steps):
+    """Fields after `steps` resident steps of the CUDA build of `precision`."""
+    import torch
+
+    from nonnewton_b200 import sph
+    from nonnewton_b200.config import SimConfig
+
+    m = sph.initialize(SimConfig(config=sc.config), particles=sc.particles, quirks=sc.param.quirks,
+                       precision=precision)
+    assert m.engine.precision == precision
+    solver = sph.build_solver()
+    solver.initialize()
+    solver.run(steps)
+    st = m.engine.stats(0)
+    out = {k: pd_field(m, k) for k in ("x", "v", "density", "stress")}
+    out["stats"] = st
+    m.engine.close()
+    torch.cuda.empty_cache()
+    return out
+
+
+@pytest.mark.parametrize("name,steps,bounds", [
+    ("roofline_2m", 50, {"x": 1e-5, "v": 1e-2, "density": 1e-3}),
+    ("shear_thinning_drop", 200, {"x": 1e-3, "v": 5e-2, "density": 2e-2}),
+    ("fluid_elastic", 200, {"x": 1e-3, "v": 5e-2, "density": 2e-2, "stress": 5e-2}),
+])
+def test_fp32_vs_fp64_build_at_bench_sizes(cuda_lib, name, steps, bounds):
+    """The FP32 product path against the FP64 build of the same kernels, free-running
+    from the same float32 initial state over the scene's own step count: the error of
+    each field (max |FP32 - FP64| over the field's scale, and the RMS of the same)."""
+    sc = {"roofline_2m": S.roofline_scene, "shear_thinning_drop": S.shear_thinning_drop,
+          "fluid_elastic": S.fluid_elastic}[name](seed=0)
+    a = _run_build(sc, "f32", steps)
+    b = _run_build(sc, "f64", steps)
+    nf = sc.particles.n_fluid
+    el = np.nonzero(np.asarray(sc.particles.phase_id) >= 3000)[0]
+    errs, rms = {}, {}
+    for f in bounds:
+        g, r = a[f], b[f]
+        if f == "density":
+            g, r = g[:nf], r[:nf]
+        elif f == "stress":
+            g, r = g[el], r[el]
+        scale = max(np.abs(r).max(), 1e-30)
+        errs[f] = float(np.abs(g - r).max() / scale)
+        rms[f] = float(np.sqrt(np.mean((g - r) ** 2)) / scale)
+    sa, sb = a["stats"], b["stats"]
+    print(f"\nFP32 vs FP64 build, {name} ({sc.particles.n} particles), {steps} steps: "
+          + ", ".join(f"{k} max {errs[k]:.2e} rms {rms[k]:.2e}" for k in errs)
+          + f"; last step iterations (div, pressure, cg) f32 {sa['iterations_v'], sa['iterations'], sa['cg_iterations']}"
+          + f" f64 {sb['iterations_v'], sb['iterations'], sb['cg_iterations']}")
+    assert sa["status"] == 0 and sb["status"] == 0
+    for f, bd in bounds.items():
+        assert errs[f] < bd, (f, errs[f])
