@@ -285,92 +285,134 @@ def run_reference(args):
                               "d2h_bytes_per_step": 0}}))
 
 
-def run_served(args, world, rank):
-    """The mixed served workload: Poisson arrivals of dam-break requests (fluid count
-    log-uniform in [2k, 128k], box at 50 % fill, Cross law with mu0 ~ U[0.1, 20],
-    n ~ U[0.5, 1], implicit viscosity), K steps each, continuously batched; the plain
-    per-scene loop runs a seeded sample of the same requests one after another."""
+def served_measure(args, world, rank):
+    """The mixed served workload: one seeded stream of Poisson-arriving dam-break
+    requests (fluid count log-uniform in [2k, 128k], box at 50 % fill, Cross law with
+    mu0 ~ U[0.1, 20], n ~ U[0.5, 1], implicit viscosity), K steps each, continuously
+    batched; with N ranks, each serves its shard of the stream (serve_sharded). The
+    server's pools come from the device memory budget, capped at --capacity resident
+    particles; its launch shape is autotuned on the first full packing of its shard
+    (untimed). The plain per-scene loop runs a seeded sample of the same requests one
+    after another. Returns every figure of the served block (on every rank)."""
     import torch
 
     from nonnewton_b200 import scene as S
-    from nonnewton_b200.serve import Request, Server, run_plain
+    from nonnewton_b200.autotune import QUICK_CANDIDATES
+    from nonnewton_b200.serve import Request, Server, run_plain, scene_grid_cells
+    from nonnewton_b200.shard import serve_sharded, shard_requests
 
-    nreq = args.requests
-    work = S.mixed_workload(n_requests=nreq, seed=1000 + rank, rate=args.rate, steps=args.request_steps)
+    work = S.mixed_workload(n_requests=args.requests, seed=1000, rate=args.rate, steps=args.request_steps)
     reqs = [Request(k, sc, args.request_steps, t) for k, (t, sc) in enumerate(work)]
+    mine = [reqs[k] for k in shard_requests(reqs, world)[rank]]
+    srv = Server(capacity=args.capacity, max_scenes=args.max_scenes, chunk=args.chunk,
+                 tune_candidates=QUICK_CANDIDATES)
+    # the first full packing of this rank's stream: what the autotuner and the roofline use
+    pack, n, c = [], 0, 0
+    for r in mine:
+        cr = scene_grid_cells(r.scene)
+        if not srv.fits(n, c, r.scene.particles.n, cr) or len(pack) >= args.max_scenes:
+            break
+        pack.append(r.scene)
+        n += r.scene.particles.n
+        c += cr
+    tuning = None
+    if not args.no_served_autotune:
+        srv.batch.set(pack)
+        tuning = srv.tune()
     # warm-up: a small served run (captures the step graphs of the server context)
-    srv = Server(capacity=args.capacity, max_scenes=args.max_scenes, chunk=args.chunk)
-    warm = [Request(-1 - k, sc, max(args.warmup, 1), 0.0) for k, (t, sc) in enumerate(work[:4])]
+    warm = [Request(-1 - k, sc, max(args.warmup, 1), 0.0) for k, sc in enumerate(pack[:4])]
     srv.run(warm, realtime=False)
     torch.cuda.synchronize()
     barrier(world)
     eng = srv.batch.engine
     l0 = eng.launch_count()
-    clocks_path = os.path.join(args.clocks_dir, f"clocks_rank{rank}.csv")
+    clocks_path = os.path.join(args.clocks_dir, f"clocks_served_rank{rank}.csv")
     with ClockSampler(clocks_path) as cs:
-        torch.cuda.nvtx.range_push("timed")
-        res = srv.run(reqs, realtime=True)
+        torch.cuda.nvtx.range_push("timed_served")
+        res = serve_sharded(srv, reqs, world, rank, realtime=True)
         torch.cuda.nvtx.range_pop()
     launches = eng.launch_count() - l0
-    wall_max = max_over_ranks(res["wall_s"], world)
-    dev_s = max_over_ranks(res["particle_steps"] / max(res["device_throughput"], 1e-9), world)
-    total_ps = sum_over_ranks(float(res["particle_steps"]), world)
-    # plain per-scene loop on a sample
-    rng = np.random.default_rng(7)
-    sample = [reqs[k] for k in sorted(rng.choice(len(reqs), size=min(args.plain_sample, len(reqs)), replace=False))]
+    comb = res["combined"]
+    # plain per-scene loop on a sample of this rank's requests, and alone-vs-mix agreement
+    rng = np.random.default_rng(7 + rank)
+    k_plain = min(args.plain_sample, len(mine))
+    sample = [mine[k] for k in sorted(rng.choice(len(mine), size=k_plain, replace=False))]
     plain_reqs = [Request(r.rid, r.scene, r.steps, 0.0) for r in sample]
     plain = run_plain(plain_reqs)
-    # alone-vs-mix agreement on the sample
     fin = {r.rid: r for r in res["finished"]}
     mix_err = max(float(np.abs(fin[p.rid].result_x - p.result_x).max()) for p in plain_reqs)
-    # roofline of the dominant kernel on a full batch
-    first = [r.scene for r in reqs]
-    pack, n = [], 0
-    for sc in first:
-        if n + sc.particles.n > args.capacity or len(pack) >= args.max_scenes:
-            break
-        pack.append(sc)
-        n += sc.particles.n
+    plain_tp = sum_over_ranks(plain["throughput"], world)  # N independent per-scene loops
+    mix_err = max_over_ranks(mix_err, world)
+    max_err_pct = max_over_ranks(res["max_density_err_pct"], world)
+    failed = sum_over_ranks(float(len(res["failed"])), world)
+    # bytes copied per batch step on this rank: each request's initial state in (x, mass
+    # and three int32 class fields), its final positions out
+    h2d = sum(r.scene.particles.n * (12 + 4 + 4 * 3) for r in res["finished"])
+    d2h = sum(r.scene.particles.n * 12 for r in res["finished"])
+    bsteps = max(res["batch_steps"], 1)
+    return {
+        "srv": srv, "pack": pack, "reqs": reqs, "clocks": cs.summary(), "launches": launches,
+        "block": {
+            "workload": "served_mixed", "requests": args.requests, "steps_per_request": args.request_steps,
+            "arrival_rate_per_s": args.rate, "ranks": world,
+            "throughput_wall": comb["particle_steps"] / comb["wall_s"], "wall_s": comb["wall_s"],
+            "device_throughput": comb["device_throughput"],
+            "plain_throughput": plain_tp, "plain_requests": k_plain * world,
+            "ratio_served_over_plain": (comb["particle_steps"] / comb["wall_s"]) / plain_tp,
+            "step_ms_p50": comb["step_ms_p50"], "step_ms_p99": comb["step_ms_p99"],
+            "step_latency": "CUDA-event pair around each step's graph launch, every step of every request; the "
+                            "first step after a repack includes the repack",
+            "request_s_p50": res["request_s_p50"], "request_s_p99": res["request_s_p99"],
+            "max_avg_density_err_pct": max_err_pct, "max_error_pct": 0.1,
+            "density_err_basis": "largest DFSPH average density error at the end of any step of any request",
+            "failed_requests": int(failed), "alone_vs_mix_max_abs_dx": mix_err,
+            "capacity_particles": srv.capacity, "hbm_budget_bytes": srv.budget,
+            "chunk_steps": args.chunk, "repacks": res["repacks"], "chunks": res["chunks"],
+            "tuning": tuning["best"] if tuning else None,
+        },
+        "h2d_bytes_per_step": int(h2d / bsteps), "d2h_bytes_per_step": int(d2h / bsteps),
+        "particle_steps": comb["particle_steps"], "wall_s": comb["wall_s"], "device_s": comb["device_s"],
+    }
+
+
+def run_served(args, world, rank):
+    """`--workload served`: the served workload's own bench line."""
+    import torch
+
+    m = served_measure(args, world, rank)
+    srv, pack, blk = m["srv"], m["pack"], m["block"]
+    # roofline of the dominant kernel on the first full packing
+    n = sum(sc.particles.n for sc in pack)
     srv.batch.set(pack)
     srv.batch.step(2, sync=False)
+    eng = srv.batch.engine
     kms = {k: eng.time_kernel(KERNEL_IDS[k], reps=10) for k in ("pressure_update", "density_adv", "build_lists",
                                                                 "density_factor", "cg_matvec")}
+    torch.cuda.synchronize()
     peaks, peak_kind = load_peaks()
     if rank != 0:
         return
     dom = "density_adv"
     achieved = ALG_BYTES[dom] * n / (kms[dom] / 1e3) / 1e9
     hbm = peaks["hbm_gbs"]
-    h2d = sum(r.scene.particles.n * (12 + 4 + 4 * 3) for r in reqs)
-    d2h = sum(r.scene.particles.n * 12 for r in reqs)
-    batch_steps = max(res["chunks"], 1)
     line = {
-        "metric": "particle-steps/s (served, continuous batching)", "value": total_ps / dev_s,
+        "metric": "particle-steps/s (served, continuous batching)", "value": m["particle_steps"] / m["device_s"],
         "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": res["step_ms_p50"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "ms_per_step": blk["step_ms_p50"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded numpy scene generator, Poisson arrivals)",
-        "config": {"workload": "served_mixed", "requests": nreq, "steps_per_request": args.request_steps,
-                   "arrival_rate_per_s": args.rate, "capacity_particles": args.capacity,
-                   "max_scenes": args.max_scenes, "chunk_steps": args.chunk,
-                   "l2": "inputs larger than L2", "parallelism": f"scenes sharded over {world} rank(s)"},
-        "served": {"throughput_wall": total_ps / wall_max, "wall_s": wall_max,
-                   "step_ms_p50": res["step_ms_p50"], "step_ms_p99": res["step_ms_p99"],
-                   "request_s_p50": res["request_s_p50"], "request_s_p99": res["request_s_p99"],
-                   "repacks": res["repacks"], "chunks": res["chunks"],
-                   "max_avg_density_err": res["max_density_err"]},
-        "plain": {"throughput": plain["throughput"], "requests": plain["requests"],
-                  "ratio_served_over_plain": (total_ps / wall_max) / plain["throughput"],
-                  "alone_vs_mix_max_abs_dx": mix_err},
+        "config": {"workload": "served_mixed", "requests": args.requests, "steps_per_request": args.request_steps,
+                   "arrival_rate_per_s": args.rate},
+        "served": blk,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "peak_source": f"{peak_kind} hbm_gbs", "alg_bytes_per_launch":
                      ALG_BYTES[dom] * n, "traffic": None, "kernel_ms": kms, "particles": n},
-        "gpu_launches": launches,
-        "e2e": {"value": total_ps / wall_max, "unit": "particle-steps/s",
-                "h2d_bytes_per_step": int(h2d / batch_steps), "d2h_bytes_per_step": int(d2h / batch_steps)},
-        "clocks": cs.summary(),
+        "gpu_launches": m["launches"],
+        "e2e": {"value": blk["throughput_wall"], "unit": "particle-steps/s",
+                "h2d_bytes_per_step": m["h2d_bytes_per_step"], "d2h_bytes_per_step": m["d2h_bytes_per_step"]},
+        "clocks": m["clocks"],
     }
     if not args.no_cpu_baseline and world == 1:  # the CPU baseline is an N=1 measurement
-        line["cpu_baseline"] = cpu_baseline([reqs[0].scene], budget_s=args.cpu_budget)
+        line["cpu_baseline"] = cpu_baseline([m["reqs"][0].scene], budget_s=args.cpu_budget)
     print(json.dumps(line))
 
 
@@ -674,6 +716,16 @@ def run_ours(args):
     e2e_ms = max_over_ranks(t0.elapsed_time(t1), world)
     e2e_val = total_ps / (e2e_ms / 1e3)
     peaks, peak_kind = load_peaks()
+    served = None
+    if args.workload == "roofline_2m" and not args.no_served:
+        # the headline comparison of the served form with the plain loop, on the mixed
+        # workload, in the same run (every rank takes part: it has collectives)
+        del st_x, st_v, st_o, h_x, h_v, h_out
+        eng.close()
+        sph.meta.pd = sph.meta.engine = sph.meta.ns = sph.meta.solver = None
+        del m, pd, solver
+        torch.cuda.empty_cache()
+        served = served_measure(args, world, rank)["block"]
     if rank != 0:
         if world > 1:
             torch.distributed.destroy_process_group()
@@ -713,6 +765,8 @@ def run_ours(args):
                 "copies": "pinned host <-> device staging on two copy streams, overlapped with the steps"},
         "clocks": cs.summary(),
     }
+    if served is not None:
+        line["served"] = served
     if not args.no_cpu_baseline and world == 1:  # the CPU baseline is an N=1 measurement
         line["cpu_baseline"] = cpu_baseline(scenes, budget_s=args.cpu_budget)
     print(json.dumps(line))
@@ -738,6 +792,9 @@ def main():
     ap.add_argument("--max-scenes", type=int, default=256)
     ap.add_argument("--chunk", type=int, default=10, help="steps between admissions")
     ap.add_argument("--plain-sample", type=int, default=48)
+    ap.add_argument("--no-served", action="store_true", help="leave the served block out of the default line")
+    ap.add_argument("--no-served-autotune", action="store_true",
+                    help="serve with the default launch shape instead of tuning it on the first packing")
     ap.add_argument("--autotune", action="store_true", help="pick block size, unroll and cell factor first")
     ap.add_argument("--tuning", default=None, help="block,unroll,cell_factor (e.g. 128,2,1)")
     ap.add_argument("--clocks-dir", default=tempfile.gettempdir(),

@@ -166,6 +166,9 @@ typedef struct nn_stats {
   double dt;                      /* time step used by the last step */
   double max_density;             /* printed at SPH/main.py:1548 */
   int64_t steps;                  /* steps taken since nn_initialize */
+  double max_avg_density_err;     /* largest avg_density_err at the end of any step since
+                                     nn_set_scenes: the DFSPH error of every step, not only
+                                     the last */
 } nn_stats;
 
 typedef struct nn_ctx nn_ctx;
@@ -193,6 +196,10 @@ enum nn_pass {
 /* step flags */
 #define NN_STEP_SYNC_STATE  (1u << 0)  /* write the state back to nn_state after the last step */
 #define NN_STEP_HOST_LOOP   (1u << 1)  /* drive solver loops from the host (no CUDA graph) */
+#define NN_STEP_RESUME      (1u << 2)  /* continue from the state the last nn_step left resident on
+                                          the device instead of reading nn_state again (for one launch
+                                          per step without a write-back in between); NN_ERR_STATE if
+                                          anything since that step changed the context or its state */
 
 /* ---- context ------------------------------------------------------------
    Replaces: initialize() allocations (SPH/main.py:1870-1895) — ParticleData sizes,

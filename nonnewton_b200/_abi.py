@@ -62,6 +62,7 @@ NN_HERSCHEL_BULKLEY = 6
 
 NN_STEP_SYNC_STATE = 1 << 0
 NN_STEP_HOST_LOOP = 1 << 1
+NN_STEP_RESUME = 1 << 2
 
 
 class nn_scene_params(C.Structure):
@@ -158,6 +159,7 @@ class nn_stats(C.Structure):
         ("dt", C.c_double),
         ("max_density", C.c_double),
         ("steps", C.c_int64),
+        ("max_avg_density_err", C.c_double),
     ]
 
     def as_dict(self):

@@ -4,8 +4,8 @@ Knobs (see nn_set_tuning): threads per block of the neighbour passes, neighbour
 chains each thread keeps in flight ("unroll": how many neighbours of a particle a
 thread gathers at once) and the cell factor f (cells of edge h / f with a
 (2f+1)-cell stencil). The tuner times each candidate on the actual batch, from the
-batch's initial state, and keeps the fastest; results are cached per device, scene
-mix and particle count (rounded to a power of two).
+batch's initial state after a few untimed steps, and keeps the fastest; results are
+cached per device, scene mix and particle count (rounded to a power of two).
 """
 from __future__ import annotations
 
@@ -17,6 +17,9 @@ import torch
 
 DEFAULT_CANDIDATES = [dict(block=b, unroll=u, cell_factor=f)
                       for b, u, f in itertools.product((128, 256, 512), (2, 4, 8), (1, 2))]
+
+# a shorter list for tuning inside a served run (block x chains, cell factor 1)
+QUICK_CANDIDATES = [dict(block=b, unroll=u, cell_factor=1) for b, u in itertools.product((128, 256), (2, 4))]
 
 _cache: dict = {}
 
@@ -46,10 +49,17 @@ def apply(batch, cfg: dict) -> None:
     batch.cell_factor = cfg["cell_factor"]
 
 
-def autotune(batch, candidates=None, steps: int = 3, warmup: int = 2, cache_path: str | None = None) -> dict:
+def _sync():
+    torch.cuda.synchronize()
+
+
+def autotune(batch, candidates=None, steps: int = 3, warmup: int = 5, cache_path: str | None = None) -> dict:
     """Try `candidates` on `batch` (re-initialised from its scenes' initial states for
     each), leave the best applied and the batch re-initialised; returns
-    {"best": cfg, "ms": {cfg: ms}}."""
+    {"best": cfg, "ms": {cfg: ms}, "errors": {cfg: message}}. A candidate that fails
+    (a launch shape that does not fit, for example) is recorded with its error; an
+    error that persists on the device stops the tuning; RuntimeError when no
+    candidate ran."""
     key = _key(batch)
     if cache_path and os.path.exists(cache_path) and not _cache:
         try:
@@ -62,19 +72,22 @@ def autotune(batch, candidates=None, steps: int = 3, warmup: int = 2, cache_path
         batch.set(batch.scenes)
         return _cache[key]
     scenes = list(batch.scenes)
-    results = {}
+    results, errors = {}, {}
     for cfg in candidates or DEFAULT_CANDIDATES:
+        key_c = json.dumps(cfg, sort_keys=True)
         try:
             apply(batch, cfg)
             batch.set(scenes)
-            results[json.dumps(cfg, sort_keys=True)] = time_steps(batch, steps, warmup)
-        except Exception as e:  # a candidate that does not fit (e.g. cells) is skipped
-            results[json.dumps(cfg, sort_keys=True)] = float("inf")
-            last_error = e  # noqa: F841
+            results[key_c] = time_steps(batch, steps, warmup)
+        except Exception as e:
+            errors[key_c] = f"{type(e).__name__}: {e}"
+            _sync()  # raises if the failure left the device in an error state
+    if not results:
+        raise RuntimeError(f"autotune: no candidate ran: {errors}")
     best = json.loads(min(results, key=results.get))
     apply(batch, best)
     batch.set(scenes)
-    out = {"best": best, "ms": results}
+    out = {"best": best, "ms": results, "errors": errors}
     _cache[key] = out
     if cache_path:
         try:

@@ -170,8 +170,8 @@ class Batch:
         self.engine.initialize()
 
     # -- stepping ----------------------------------------------------------------
-    def step(self, nsteps: int = 1, sync: bool = True):
-        self.engine.step(nsteps, sync=sync)
+    def step(self, nsteps: int = 1, sync: bool = True, resume: bool = False):
+        self.engine.step(nsteps, sync=sync, resume=resume)
 
     def scene_view(self, k: int, name: str) -> torch.Tensor:
         s = self.starts[k]

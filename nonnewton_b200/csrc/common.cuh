@@ -108,6 +108,7 @@ struct SceneDyn {
   int64_t steps;
   float anim[3];                 // animate_particles displacement of the next step (set by the host)
   int32_t pad2;
+  double max_avg_p;               // largest avg_p at the end of a step since the scene was set
 };
 
 // Accumulator slots per scene (each NN_STRIPES doubles).

@@ -71,6 +71,7 @@ struct nn_ctx {
   WorkSet set[2]{};
   int cur = 0;                         // set holding the current slots
   bool searched = false;
+  bool resident_ok = false;            // the slots hold the state the last nn_step left
   int32_t* d_n = nullptr;
   SceneDev* d_sc = nullptr;
   SceneDyn* d_dyn = nullptr;
@@ -751,6 +752,7 @@ int nn_bind_state(nn_ctx* c, const nn_state* st) {
   c->state = *st;
   c->bound = true;
   c->searched = false;
+  c->resident_ok = false;
   return NN_OK;
 }
 
@@ -916,6 +918,7 @@ int nn_set_scenes(nn_ctx* c, int32_t nscenes, const nn_scene_desc* scenes) {
     CK(cudaGetLastError());
   }
   c->searched = false;
+  c->resident_ok = false;
   return NN_OK;
 }
 
@@ -931,6 +934,7 @@ static int check_elastic(nn_ctx* c) {
 
 int nn_initialize(nn_ctx* c) {
   RC(check_ready(c));
+  c->resident_ok = false;
   cudaStream_t s = run_stream(c);
   // Elasticity constructors run before solver.initialize() (SPH/main.py:1889-1895, 1915).
   // Their rest neighbourhoods come from a search over the rest positions x_0 (equal to
@@ -967,8 +971,12 @@ int nn_step(nn_ctx* c, int32_t nsteps, uint32_t flags) {
   cudaStream_t s = run_stream(c);
   if (!s) return fail(c, NN_ERR_STATE, "no stream");
   const bool host = (flags & NN_STEP_HOST_LOOP) != 0;
+  const bool resume = (flags & NN_STEP_RESUME) != 0;
+  if (resume && !c->resident_ok)
+    return fail(c, NN_ERR_STATE, "NN_STEP_RESUME: no state left resident by a previous nn_step");
   for (int k = 0; k < nsteps; ++k) {
-    CK(cudaMemsetAsync(c->d_src_flag, k == 0 ? 1 : 0, sizeof(int32_t), s));
+    // the first step reads the caller's state, unless it resumes from the resident slots
+    CK(cudaMemsetAsync(c->d_src_flag, (k == 0 && !resume) ? 1 : 0, sizeof(int32_t), s));
     if (host) {
       RC(enq_step(c, s));
     } else {
@@ -983,12 +991,14 @@ int nn_step(nn_ctx* c, int32_t nsteps, uint32_t flags) {
   if (flags & NN_STEP_SYNC_STATE) RC(enq_sync_out(c, s, SM_ALL));
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(c, NN_ERR_CUDA, "nn_step: %s", cudaGetErrorString(e));
+  if (nsteps > 0) c->resident_ok = true;
   return NN_OK;
 }
 
 int nn_run_pass(nn_ctx* c, int32_t pass) {
   RC(check_ready(c));
   if (pass < 0 || pass >= NN_PASS_COUNT) return fail(c, NN_ERR_INVALID_ARG, "unknown pass %d", pass);
+  c->resident_ok = false;
   cudaStream_t s = run_stream(c);
   if (pass == NN_PASS_SEARCH) {
     CK(cudaMemsetAsync(c->d_src_flag, 1, sizeof(int32_t), s));
@@ -1038,6 +1048,7 @@ int nn_time_kernel(nn_ctx* c, int32_t kernel, int32_t reps, float* ms_out) {
   RC(check_ready(c));
   if (!ms_out || reps <= 0 || kernel < 0 || kernel >= NN_K_COUNT) return fail(c, NN_ERR_INVALID_ARG, "nn_time_kernel: bad arguments");
   if (!c->searched) return fail(c, NN_ERR_STATE, "run a step first");
+  c->resident_ok = false;  // the timed update kernels change the slots' velocities
   cudaStream_t s = run_stream(c);
   Dev d = make_dev(c, c->cur);
   RC(launch1(c, s, k_force_active, d));
@@ -1118,6 +1129,7 @@ int nn_set_neighbor_cap(nn_ctx* c, int32_t max_neighbors) {
   if (c->ne == 0 || c->el_stale) c->el_cap = max_neighbors;
   if (!c->scenes.empty()) RC(launch1(c, s, k_clear_overflow, make_dev(c, c->cur)));
   c->searched = false;
+  c->resident_ok = false;
   CK(cudaStreamSynchronize(s));
   return NN_OK;
 }
@@ -1156,6 +1168,7 @@ static void fill_stats(const SceneDyn& y, nn_stats* out) {
   std::memcpy(&md, &bits, sizeof(md));
   out->max_density = md;
   out->steps = y.steps;
+  out->max_avg_density_err = y.max_avg_p;
 }
 
 int nn_get_stats_range(nn_ctx* c, int32_t first, int32_t count, nn_stats* out) {

@@ -417,6 +417,7 @@ __global__ void k_step_end(Dev d) {
   const int ns = d.d_n[1];
   for (int sc = threadIdx.x; sc < ns; sc += blockDim.x) {
     d.dyn[sc].steps += 1;
+    if (d.sc[sc].n_fluid > 0) d.dyn[sc].max_avg_p = fmax(d.dyn[sc].max_avg_p, d.dyn[sc].avg_p);
     d.dyn[sc].anim[0] = d.dyn[sc].anim[1] = d.dyn[sc].anim[2] = 0.f;  // one step only
   }
 }

@@ -155,8 +155,11 @@ class Engine:
     def initialize(self):
         self._rc(self.L.nn_initialize(self.h))
 
-    def step(self, nsteps: int = 1, sync: bool = True, host_loop: bool = False):
-        flags = (_abi.NN_STEP_SYNC_STATE if sync else 0) | (_abi.NN_STEP_HOST_LOOP if host_loop else 0)
+    def step(self, nsteps: int = 1, sync: bool = True, host_loop: bool = False, resume: bool = False):
+        """nsteps steps; `sync` writes the state back to the bound fields at the end,
+        `resume` continues from the state the previous step left on the device."""
+        flags = ((_abi.NN_STEP_SYNC_STATE if sync else 0) | (_abi.NN_STEP_HOST_LOOP if host_loop else 0)
+                 | (_abi.NN_STEP_RESUME if resume else 0))
         self._rc(self.L.nn_step(self.h, int(nsteps), flags))
 
     def set_animation(self, scene: int, displacement):

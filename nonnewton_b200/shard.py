@@ -52,3 +52,32 @@ def combine_metrics(local: dict, world: int) -> dict:
     out.update(particle_steps=float(s[0]), requests=int(s[1]), wall_s=float(m[0]), device_s=float(m[1]))
     out["throughput"] = out["particle_steps"] / out["wall_s"] if out["wall_s"] > 0 else 0.0
     return out
+
+
+def serve_sharded(server, requests, world: int, rank: int, realtime: bool = True) -> dict:
+    """Serve this rank's shard of one arrival stream (every rank passes the same
+    `requests`; shard_requests picks the same disjoint shards on each). Each request
+    keeps its arrival time, so a rank sees a thinned copy of the stream. Returns the
+    server's local result with "mine" (the request ids served here) and "combined":
+    particle-steps and requests summed, wall and device time max-reduced, and the
+    step-latency percentiles over the steps of all ranks."""
+    import numpy as np
+
+    idx = shard_requests(requests, world)[rank]
+    res = server.run([requests[k] for k in idx], realtime=realtime)
+    local = {"particle_steps": float(res["particle_steps"]), "requests": res["requests"], "wall_s": res["wall_s"],
+             "device_s": server.device_ms / 1e3}
+    comb = combine_metrics(local, world)
+    lat = np.asarray(res["step_ms"], np.float64)
+    if world > 1:
+        import torch.distributed as dist
+
+        parts = [None] * world
+        dist.all_gather_object(parts, lat.tolist())
+        lat = np.concatenate([np.asarray(p, np.float64) for p in parts])
+    comb["step_ms_p50"] = float(np.percentile(lat, 50))
+    comb["step_ms_p99"] = float(np.percentile(lat, 99))
+    comb["device_throughput"] = comb["particle_steps"] / comb["device_s"] if comb["device_s"] > 0 else 0.0
+    res["mine"] = [requests[k].rid for k in idx]
+    res["combined"] = comb
+    return res

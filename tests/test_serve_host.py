@@ -45,6 +45,7 @@ class _Batch:
     def __init__(self, capacity, max_scenes, fail=None):
         self.capacity, self.max_scenes = capacity, max_scenes
         self.scenes, self.done, self.status = [], {}, {}
+        self.resumable = False
         self.fail = fail or {}  # id(scene) -> step count at which its status word is set
         self.engine = _Engine(self)
         self.log = []
@@ -59,6 +60,7 @@ class _Batch:
     def set(self, scenes, initialize=True, staged=None):
         assert staged is None or staged["ids"] == [id(sc) for sc in scenes]
         self.scenes = list(scenes)
+        self.resumable = False
         for sc in scenes:
             self.done[id(sc)] = 0
         self.log.append(("set", [id(sc) for sc in scenes]))
@@ -68,12 +70,15 @@ class _Batch:
         assert staged is None or staged["ids"] == [id(sc) for sc in new]
         assert keep == sorted(keep)
         self.scenes = [self.scenes[k] for k in keep] + list(new)
+        self.resumable = False
         for sc in new:
             self.done[id(sc)] = 0
         self.log.append(("repack", [id(sc) for sc in self.scenes]))
         self._check()
 
-    def step(self, k, sync=True):
+    def step(self, k, sync=True, resume=False):
+        assert not resume or self.resumable  # resume only what the last step left resident
+        self.resumable = True
         _Batch.clock += k
         for sc in self.scenes:
             self.done[id(sc)] += k
@@ -94,14 +99,10 @@ def fake_cuda(monkeypatch):
     monkeypatch.setattr(torch.cuda, "current_stream", lambda *a, **k: None)
 
 
-def _server(batch, chunk):
-    srv = SV.Server.__new__(SV.Server)
-    srv.capacity, srv.max_scenes, srv.chunk = batch.capacity, batch.max_scenes, chunk
-    srv.max_cells = 1 << 40
-    srv.batch, srv.resident, srv.stream = batch, [], None
-    srv.chunks = srv.repacks = 0
-    srv.device_ms = 0.0
-    return srv
+def _server(batch, chunk, **kw):
+    kw.setdefault("max_cells", 1 << 40)
+    return SV.Server(capacity=batch.capacity, max_scenes=batch.max_scenes, chunk=chunk, batch=batch,
+                     hbm_free=1 << 62, hbm_reserve=0, **kw)
 
 
 @pytest.mark.parametrize("chunk", [1, 3, 10])
@@ -175,3 +176,72 @@ def test_staging_concatenates_the_initial_states(monkeypatch):
     assert b.stage([]) is None
     with pytest.raises(ValueError):
         b.stage([S.dam_break(seed=9, n_side=(20, 20, 20), box=1.0)])
+
+
+def test_pools_are_sized_from_the_device_budget(fake_cuda):
+    """Without a cap, the batch's particle and cell pools are the largest whose
+    footprint fits the free memory minus the reserve; a cap smaller than that wins;
+    a batch that does not fit the budget is refused."""
+    gib = 1 << 30
+    b = _Batch(10 ** 12, max_scenes=4)
+    srv = SV.Server(max_scenes=4, batch=b, hbm_free=10 * gib, hbm_reserve=2 * gib)
+    per = SV.footprint_bytes(1, 64) + 4 * SV.CELL_BYTES  # 4 cells per particle
+    assert srv.budget == 8 * gib and srv.capacity == 8 * gib // per and srv.max_cells == 4 * srv.capacity
+    assert SV.footprint_bytes(srv.capacity, 64, srv.max_cells) <= srv.budget
+    assert SV.footprint_bytes(srv.capacity + 1, 64, srv.max_cells + 4) > srv.budget
+    capped = SV.Server(capacity=1000, max_scenes=4, batch=b, hbm_free=10 * gib, hbm_reserve=2 * gib)
+    assert capped.capacity == 1000 and capped.max_cells == 4000
+    with pytest.raises(ValueError):
+        SV.Server(capacity=1000, max_cells=10 ** 10, max_scenes=4, batch=b, hbm_free=10 * gib, hbm_reserve=2 * gib)
+    with pytest.raises(ValueError):
+        SV.Server(max_scenes=4, batch=b, hbm_free=gib, hbm_reserve=2 * gib)
+
+
+def test_admission_follows_the_footprint_model(fake_cuda):
+    """A budget that holds the particles of two requests and the grid cells of one
+    (a small cell pool) admits them one at a time: the cell pool binds."""
+    reqs = [SV.Request(k, S.dam_break(seed=k, n_side=(3, 3, 3), box=0.2), 3, 0.0) for k in range(3)]
+    n = reqs[0].scene.particles.n
+    cells = SV.scene_grid_cells(reqs[0].scene)
+    budget = SV.footprint_bytes(2 * n, 64, cells)
+    b = _Batch(2 * n, max_scenes=4)
+    srv = SV.Server(capacity=2 * n, max_cells=cells, max_scenes=4, chunk=3, batch=b, hbm_free=budget,
+                    hbm_reserve=0)
+    res = srv.run(reqs, realtime=False)
+    assert res["requests"] == 3 and all(len(ids) == 1 for _, ids in b.log)
+    assert srv.fits(0, 0, n, cells) and not srv.fits(0, 1, n, cells) and not srv.fits(2 * n, 0, 1, 0)
+
+
+def test_autotune_records_failures_and_needs_one_success(monkeypatch):
+    """The tuner keeps every candidate's error, picks the fastest that ran, and raises
+    when none ran."""
+    from nonnewton_b200 import autotune as AT
+
+    class Eng:
+        def __init__(self):
+            self.cfg = None
+
+        def set_tuning(self, b, u, f):
+            if b == 512:
+                raise RuntimeError("candidate does not fit")
+            self.cfg = (b, u, f)
+
+    class B:
+        n, scenes, cell_factor = 100, [], 1
+
+        def __init__(self):
+            self.engine = Eng()
+
+        def set(self, scenes):
+            pass
+
+    monkeypatch.setattr(AT, "_key", lambda batch: f"key{id(batch)}")
+    monkeypatch.setattr(AT, "_sync", lambda: None)
+    monkeypatch.setattr(AT, "time_steps", lambda batch, steps, warmup: {128: 3.0, 256: 2.0}[batch.engine.cfg[0]])
+    cands = [dict(block=b, unroll=2, cell_factor=1) for b in (128, 256, 512)]
+    b = B()
+    out = AT.autotune(b, candidates=cands)
+    assert out["best"]["block"] == 256 and b.engine.cfg == (256, 2, 1)
+    assert len(out["errors"]) == 1 and "does not fit" in next(iter(out["errors"].values()))
+    with pytest.raises(RuntimeError):
+        AT.autotune(B(), candidates=[dict(block=512, unroll=2, cell_factor=1)])
