@@ -94,6 +94,10 @@ def make_workload(name, seed=0):
 
     if name == "roofline_2m":
         return [S.roofline_scene(seed=seed)]
+    if name == "roofline_2m_packed":
+        # the same scene with the fluid packed to 0.95 of its spacing: the pressure solve
+        # iterates several times in the first steps (for per-iteration costs and launch lists)
+        return [S.roofline_scene(seed=seed, spacing_factor=0.95)]
     if name == "dam_break":
         return [S.dam_break(seed=seed)]
     if name == "shear_thinning_drop":
