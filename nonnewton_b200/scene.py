@@ -390,9 +390,10 @@ def roofline_scene(seed=0, counts=(200, 100, 100), r=0.005, quirks=False, steps=
     corner of a 4 x 2 x 2 m one-layer boundary box (401*201*201 - 399*199*199 =
     400,002 particles); Carreau mu0=1, mu_inf=0.001, lambda=0.5 (K = lambda^2 in the
     reference form), n=0.6; h = 0.02 m. `spacing_factor` < 1 packs the fluid lattice
-    closer: the lattice at 2r sits near 800 kg/m^3 (volume0 = 0.8 (2r)^3), and at 0.95
-    the pressure solve iterates from the first steps (the oracle on a 40 x 30 x 30 block:
-    8, 5 and 3 pressure iterations in steps 1 to 3, then 1)."""
+    closer: the lattice at 2r sits near 800 kg/m^3 (volume0 = 0.8 (2r)^3), so the plain
+    scene has no pressure for hundreds of steps; at 0.92 it starts near 1,027 kg/m^3,
+    and once the column falls the pressure solve iterates several times per step (the
+    oracle on the same block at r = 0.02: 3 to 5 iterations per step after 80 steps)."""
     h = 4 * r
     sp = 2 * r
     rng = np.random.default_rng(seed)

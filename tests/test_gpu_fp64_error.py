@@ -71,16 +71,21 @@ def test_fp32_vs_fp64_per_field(cuda_lib, name, steps, bounds):
         assert errs[f] < b, (f, errs[f])
 
 
-def _engine(sc, precision):
+def _engine(sc, precision, nudge=False):
     """ParticleData + Engine of one scene for the CUDA build of `precision` (the pieces
     sph.initialize assembles, without its global `meta`, so that two builds can hold
-    the same scene at once)."""
+    the same scene at once). `nudge` moves every fluid position up by one float32 ulp."""
+    import torch
+
     from nonnewton_b200.engine import Engine
     from nonnewton_b200.sph import ParticleData, initialize_particles
 
     ps = sc.particles
     pd = ParticleData(ps.n)
     initialize_particles(pd, ps, sc.param)
+    if nudge:
+        x = pd.x[: ps.n_fluid]
+        x.copy_(torch.nextafter(x, torch.full_like(x, float("inf"))))
     eng = Engine(ps.n, 1, 64, precision=precision)
     eng.bind(pd)
     eng.set_scenes([(0, ps.n, ps.n_fluid, sc.param.to_c())])
@@ -195,8 +200,19 @@ def test_fp32_vs_fp64_build_at_bench_sizes(cuda_lib, name, steps, lockstep, boun
         eng.close()
         del pd
         torch.cuda.empty_cache()
+    # the flow's own sensitivity: the FP64 build against itself, the fluid's initial
+    # positions moved by one float32 ulp
+    pd, eng = _engine(sc, "f64", nudge=True)
+    eng.step(steps, sync=True)
+    nudged = _fields(pd, names, nf, el)
+    eng.close()
+    del pd
+    torch.cuda.empty_cache()
     err = _errors(out["f32"], out["f64"], floors)
+    sens = _errors(nudged, out["f64"], floors)
     print(f"FP32 vs FP64 build, {name}, free-running {steps} steps: "
           + ", ".join(f"{f} max {err[f][0]:.2e} rms {err[f][1]:.2e}" for f in names))
+    print(f"FP64 vs FP64 with the fluid moved by one float32 ulp, {name}, {steps} steps: "
+          + ", ".join(f"{f} max {sens[f][0]:.2e} rms {sens[f][1]:.2e}" for f in names))
     for f in names:
         assert err[f][1] < 0.05, (f, err[f])  # a sanity bound on the RMS divergence
