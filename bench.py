@@ -611,8 +611,8 @@ def run_ours(args):
     sc = scenes[0]
     tuning, tune_ms = None, None
     if args.tuning:
-        b_, u_, f_ = (int(t) for t in args.tuning.split(","))
-        tuning = {"block": b_, "unroll": u_, "cell_factor": f_}
+        t_ = [int(t) for t in args.tuning.split(",")]
+        tuning = {"block": t_[0], "unroll": t_[1], "cell_factor": t_[2], "x_split": t_[3] if len(t_) > 3 else 0}
     if args.autotune:
         from nonnewton_b200.autotune import autotune
         from nonnewton_b200.batch import Batch
@@ -629,8 +629,10 @@ def run_ours(args):
     n = sc.particles.n
     eng = m.engine
     stream = torch.cuda.current_stream()
-    if args.presteps:  # advance the scene first (untimed, through the step graph)
-        eng.step(args.presteps, sync=True)
+    if args.presteps:
+        # advance the scene first (untimed, resident, through the step graph); the
+        # object API's run() grows the neighbour lists if the scene outgrows them
+        solver.run(args.presteps)
     # warm-up (also captures the step graphs)
     eng_step = lambda k, sync: eng.step(k, sync=sync, host_loop=args.host_loop)
     eng_step(max(args.warmup, 1), True)
@@ -813,7 +815,7 @@ def main():
     ap.add_argument("--no-served-autotune", action="store_true",
                     help="serve with the default launch shape instead of tuning it on the first packing")
     ap.add_argument("--autotune", action="store_true", help="pick block size, unroll and cell factor first")
-    ap.add_argument("--tuning", default=None, help="block,unroll,cell_factor (e.g. 128,2,1)")
+    ap.add_argument("--tuning", default=None, help="block,unroll,cell_factor[,x_split] (e.g. 128,2,1,2)")
     ap.add_argument("--clocks-dir", default=tempfile.gettempdir(),
                     help="where the nvidia-smi clock samples of the timed region go (clocks_rank<r>.csv)")
     ap.add_argument("--host-loop", action="store_true",

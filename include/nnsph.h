@@ -328,6 +328,13 @@ int nn_set_block_size(nn_ctx* ctx, int32_t threads);
    cell factor takes effect at the next nn_set_scenes, which must follow. */
 int nn_set_tuning(nn_ctx* ctx, int32_t block, int32_t unroll, int32_t cell_factor);
 
+/* Tuning knob of the cell layout (0 = default, 1..4): x cells per cell edge. Cells
+   are h/x_split long in x and h / cell_factor in y and z; the list build then tests
+   the x cells within h of each particle's cell, (2 x_split + 1) / x_split of h in x
+   instead of 3 h, in the same 9 contiguous rows. The neighbour sets do not depend on
+   it. Takes effect at the next nn_set_scenes, which must follow. */
+int nn_set_x_split(nn_ctx* ctx, int32_t x_split);
+
 /* ---- Surface reconstruction (SPH/surf_recon/srtool.py, SRTool) ------------------
    The particle-to-mesh step after the simulation: fluid field on a vertex grid (an
    isotropic poly6 splat and the anisotropic Yu-Turk splat), one value-weighted

@@ -46,6 +46,7 @@ def time_steps(batch, steps: int, warmup: int) -> float:
 
 def apply(batch, cfg: dict) -> None:
     batch.engine.set_tuning(cfg["block"], cfg["unroll"], cfg["cell_factor"])
+    batch.engine.set_x_split(cfg.get("x_split", 0))
     batch.cell_factor = cfg["cell_factor"]
 
 

@@ -16,15 +16,16 @@ from .scene import Scene
 from .sph import ParticleData
 
 
-def scene_grid_cells(sc: Scene, cell_factor: int = 1) -> int:
-    """Cells of the scene's grid (edge h / cell_factor, Morton-ordered rows), as
-    libnnsph lays it out."""
+def scene_grid_cells(sc: Scene, cell_factor: int = 1, x_split: int = 1) -> int:
+    """Cells of the scene's grid (edge h / cell_factor in y and z, that divided by
+    x_split in x; Morton-ordered rows), as libnnsph lays it out."""
     p = sc.param
     h = p.support_radius
     g = []
     for k in range(3):
         ext = (p.domain_end[k] - p.domain_start[k]) + 4 * h
-        g.append(int(min(65535, max(1, np.ceil(ext / (h / cell_factor)) + 1))))
+        edge = h / cell_factor / (x_split if k == 0 else 1)
+        g.append(int(min(65535, max(1, np.ceil(ext / edge) + 1))))
     mb = 0
     while (1 << mb) < max(g[1], g[2]):
         mb += 1

@@ -65,8 +65,10 @@ struct SceneDev {
   int64_t cell_base;              // first cell key of the scene
   int32_t gx, gy, gz, mbits;      // grid size; rows (y,z) are Morton-ordered with mbits per axis
   real origin[3];
-  real cell;                     // cell edge (h / nf)
-  int32_t nf;                     // stencil half-width in cells (cell factor)
+  real cell;                     // cell edge in y and z (h / nf)
+  int32_t nf;                     // stencil half-width in y and z cells (cell factor)
+  real cellx;                    // cell edge in x (cell / x split)
+  int32_t nfx;                    // stencil half-width in x cells (nf * x split)
   real h, k_w, k2_w, k_grad, W0; // cubic spline constants
   real inv_h;
   real h2_thr;                   // smallest value whose rounded sqrt is >= h (h^2 in the FP64 build)

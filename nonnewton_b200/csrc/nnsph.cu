@@ -45,6 +45,7 @@ cudaError_t dalloc(T** p, size_t count) {
 // the fastest of block {128, 256, 512} x chains {2, 4, 8} x cell factor {1, 2}).
 #define NN_DEFAULT_BLOCK 128
 #define NN_DEFAULT_UNROLL 2
+#define NN_DEFAULT_XSPLIT 1
 
 struct nn_ctx {
   int cap = 0, max_scenes = 0, max_nb = 0;
@@ -58,6 +59,7 @@ struct nn_ctx {
   int block = NN_DEFAULT_BLOCK;
   int unroll = NN_DEFAULT_UNROLL;      // neighbour chains in flight per thread (2, 4, 8)
   int cell_factor = 1;                 // cells of edge h / cell_factor
+  int x_split = NN_DEFAULT_XSPLIT;     // x cells per cell edge
   // state binding and scenes
   nn_state state{};
   bool bound = false;
@@ -498,7 +500,8 @@ static real host_kernel_w(real rn, real h, real k_w, real k2_w) {
   return res;
 }
 
-static SceneDev make_scene(const nn_scene_desc& sd, int64_t cell_base, int el_mult, int cell_factor = 1) {
+static SceneDev make_scene(const nn_scene_desc& sd, int64_t cell_base, int el_mult, int cell_factor = 1,
+                           int x_split = 1) {
   const nn_scene_params& p = sd.params;
   SceneDev s{};
   s.flags = p.flags;
@@ -509,10 +512,11 @@ static SceneDev make_scene(const nn_scene_desc& sd, int64_t cell_base, int el_mu
   const double h = p.support_radius;
   int g[3];
   const double cell = h / cell_factor;
+  const double cellx = cell / x_split;  // x cells may be shorter: rows stay contiguous in x
   for (int k = 0; k < 3; ++k) {
     s.origin[k] = (real)(p.domain_start[k] - 2.0 * h);
     double ext = (p.domain_end[k] - p.domain_start[k]) + 4.0 * h;
-    g[k] = (int)std::min(65535.0, std::max(1.0, std::ceil(ext / cell) + 1.0));
+    g[k] = (int)std::min(65535.0, std::max(1.0, std::ceil(ext / (k == 0 ? cellx : cell)) + 1.0));
   }
   s.gx = g[0]; s.gy = g[1]; s.gz = g[2];
   int mb = 0;
@@ -520,6 +524,8 @@ static SceneDev make_scene(const nn_scene_desc& sd, int64_t cell_base, int el_mu
   s.mbits = mb;
   s.cell = (real)cell;
   s.nf = cell_factor;
+  s.cellx = (real)cellx;
+  s.nfx = cell_factor * x_split;
   s.h = (real)h;
   s.inv_h = (real)(1.0 / h);
 #ifdef NN_FP64
@@ -729,6 +735,18 @@ int nn_set_tuning(nn_ctx* c, int32_t block, int32_t unroll, int32_t cell_factor)
   return NN_OK;
 }
 
+int nn_set_x_split(nn_ctx* c, int32_t x_split) {
+  if (!c) return fail(nullptr, NN_ERR_INVALID_ARG, "null context");
+  if (x_split == 0) x_split = NN_DEFAULT_XSPLIT;
+  if (x_split < 1 || x_split > 4) return fail(c, NN_ERR_INVALID_ARG, "x split %d (1..4)", x_split);
+  if (x_split != c->x_split) {
+    drop_graphs(c);
+    c->scenes.clear();  // the cell layout changes: set the scenes again
+  }
+  c->x_split = x_split;
+  return NN_OK;
+}
+
 int64_t nn_launch_count(const nn_ctx* cc) {
   nn_ctx* c = const_cast<nn_ctx*>(cc);
   if (!c) return -1;
@@ -814,7 +832,7 @@ int nn_set_scenes(nn_ctx* c, int32_t nscenes, const nn_scene_desc* scenes) {
     if (el_mult > 0)
       for (int i = sd.start; i < sd.start + sd.n; ++i)
         if (q || (mat[i] == NN_SOLID && ph[i] >= NN_PHASE_ELASTIC_BASE)) el_id.push_back(i);
-    SceneDev s = make_scene(sd, cells, el_mult, c->cell_factor);
+    SceneDev s = make_scene(sd, cells, el_mult, c->cell_factor, c->x_split);
     // rigid bodies of the scene (RIGID phases: dynamic solids with phase ids 2000..2999)
     if (sd.params.flags & NN_F_RIGID) {
       std::vector<int> rp;

@@ -23,7 +23,7 @@
 // Cell key of a position in scene s: Morton(cy, cz) * gx + cx + cell_base.
 __device__ __forceinline__ uint32_t cell_key(const SceneDev& s, real x, real y, real z, int* cx_out, int* cy_out,
                                              int* cz_out) {
-  int cx = (int)floor((x - s.origin[0]) / s.cell);
+  int cx = (int)floor((x - s.origin[0]) / s.cellx);
   int cy = (int)floor((y - s.origin[1]) / s.cell);
   int cz = (int)floor((z - s.origin[2]) / s.cell);
   cx = min(max(cx, 0), s.gx - 1);
@@ -273,7 +273,7 @@ __global__ void __launch_bounds__(NS_WARPS * 32) k_build_lists(Dev d) {
     const SceneDev& s = d.sc[scn];
     const real3 xi = f3(pi);
     const real thr = s.h2_thr;
-    const int x0 = max(cx - s.nf, 0), x1 = min(cx + s.nf, s.gx - 1);
+    const int x0 = max(cx - s.nfx, 0), x1 = min(cx + s.nfx, s.gx - 1);
     // lane 0 is always valid (the warp's first slot is below n)
     const int ly = __shfl_sync(full, cy, 0), lz = __shfl_sync(full, cz, 0), ls = __shfl_sync(full, scn, 0);
     const bool uniform = __all_sync(full, !valid || (cy == ly && cz == lz && scn == ls));
@@ -285,8 +285,8 @@ __global__ void __launch_bounds__(NS_WARPS * 32) k_build_lists(Dev d) {
       // every bound below is warp-uniform: the lanes past the end of the array carry
       // scene 0, so the scene of lane 0 is used (all valid lanes share it)
       const SceneDev& su = d.sc[ls];
-      const int wx0 = max(__reduce_min_sync(full, valid ? cx : 0x7fffffff) - su.nf, 0);
-      const int wx1 = min(__reduce_max_sync(full, valid ? cx : -1) + su.nf, su.gx - 1);
+      const int wx0 = max(__reduce_min_sync(full, valid ? cx : 0x7fffffff) - su.nfx, 0);
+      const int wx1 = min(__reduce_max_sync(full, valid ? cx : -1) + su.nfx, su.gx - 1);
       for (int dz = -su.nf; dz <= su.nf; ++dz) {
         const int zz = lz + dz;
         if (zz < 0 || zz >= su.gz) continue;

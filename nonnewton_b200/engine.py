@@ -94,6 +94,7 @@ class Engine:
                                       C.byref(h)), None)
         self.h = h
         self.max_neighbors = max_neighbors
+        self.x_split = 1
         self._state = None
         self._scenes = None
         self._keep = []
@@ -126,6 +127,14 @@ class Engine:
         f.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]
         f.restype = C.c_int
         self._rc(f(self.h, int(block), int(unroll), int(cell_factor)))
+
+    def set_x_split(self, x_split: int = 0):
+        """x cells per cell edge of the search grid (see nn_set_x_split); set_scenes again after."""
+        f = self.L.nn_set_x_split
+        f.argtypes = [C.c_void_p, C.c_int32]
+        f.restype = C.c_int
+        self._rc(f(self.h, int(x_split)))
+        self.x_split = int(x_split) if x_split else 1
 
     def bind(self, pd, n: int | None = None) -> None:
         """Bind the fields of `pd`; `n` active particles (default: all rows)."""

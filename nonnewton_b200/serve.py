@@ -161,10 +161,12 @@ class Server:
         total_ps = 0
         cells: dict[int, int] = {}  # grid cells of each request's scene (admission by footprint)
 
+        layout = (getattr(self.batch, "cell_factor", 1), getattr(getattr(self.batch, "engine", None), "x_split", 1))
+
         def cells_of(r):
             c = cells.get(id(r))
             if c is None:
-                c = cells[id(r)] = scene_grid_cells(r.scene)
+                c = cells[id(r)] = scene_grid_cells(r.scene, *layout)
             return c
 
         pending = None  # the chunk in flight: (events, steps)

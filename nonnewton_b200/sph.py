@@ -357,6 +357,7 @@ def initialize(config: SimConfig | str | dict | None = None, particles: Particle
     meta.engine = Engine(max(ps.n, 1), 1, max_neighbors, device=device, precision=precision)
     if tuning:
         meta.engine.set_tuning(tuning.get("block", 0), tuning.get("unroll", 0), tuning.get("cell_factor", 0))
+        meta.engine.set_x_split(tuning.get("x_split", 0))
     meta.engine.bind(meta.pd)
     meta.engine.set_scenes([(0, ps.n, ps.n_fluid, meta.parm.to_c())])
     meta.ns = NeighborhoodSearchSparse(meta.pd.x, ps.n, meta.parm.support_radius, meta.parm.domain_size,

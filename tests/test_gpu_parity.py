@@ -180,10 +180,13 @@ def test_resident_run_equals_steps(cuda_lib):
 
 
 @pytest.mark.parametrize("tuning", [dict(block=128, unroll=8, cell_factor=2), dict(block=512, unroll=2, cell_factor=1),
-                                    dict(block=64, unroll=4, cell_factor=2)])
+                                    dict(block=64, unroll=4, cell_factor=2),
+                                    dict(block=128, unroll=2, cell_factor=1, x_split=2),
+                                    dict(block=128, unroll=2, cell_factor=1, x_split=4),
+                                    dict(block=256, unroll=4, cell_factor=2, x_split=3)])
 def test_tuning_invariance(cuda_lib, tuning):
-    """Launch shape and cell size change neither the neighbour sets nor (beyond
-    summation-order rounding) the trajectory."""
+    """Launch shape and cell layout (cell factor, x cells per cell edge) change neither
+    the neighbour sets nor (beyond summation-order rounding) the trajectory."""
     from nonnewton_b200 import sph
     from nonnewton_b200.config import SimConfig
 

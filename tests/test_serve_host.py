@@ -226,6 +226,9 @@ def test_autotune_records_failures_and_needs_one_success(monkeypatch):
                 raise RuntimeError("candidate does not fit")
             self.cfg = (b, u, f)
 
+        def set_x_split(self, x):
+            pass
+
     class B:
         n, scenes, cell_factor = 100, [], 1
 
