@@ -1,9 +1,9 @@
 """Autotuner of the step's launch shape.
 
-Knobs (see nn_set_tuning): threads per block of the neighbour passes, neighbour
-chains each thread keeps in flight ("unroll": how many neighbours of a particle a
-thread gathers at once) and the cell factor f (cells of edge h / f with a
-(2f+1)-cell stencil). The tuner times each candidate on the actual batch, from the
+Knobs (see nn_set_tuning, nn_set_x_split): threads per block of the neighbour
+passes, neighbour chains each thread keeps in flight ("unroll": how many neighbours of
+a particle a thread gathers at once), the cell factor f (cells of edge h / f with a
+(2f+1)-cell stencil) and the x split (x cells per cell edge). The tuner times each candidate on the actual batch, from the
 batch's initial state after a few untimed steps, and keeps the fastest; results are
 cached per device, scene mix and particle count (rounded to a power of two).
 """
@@ -15,8 +15,10 @@ import os
 
 import torch
 
-DEFAULT_CANDIDATES = [dict(block=b, unroll=u, cell_factor=f)
-                      for b, u, f in itertools.product((128, 256, 512), (2, 4, 8), (1, 2))]
+DEFAULT_CANDIDATES = ([dict(block=b, unroll=u, cell_factor=1, x_split=x)
+                       for b, u, x in itertools.product((128, 256, 512), (2, 4, 8), (1, 2))]
+                      + [dict(block=b, unroll=u, cell_factor=2, x_split=1)
+                         for b, u in itertools.product((128, 256, 512), (2, 4, 8))])
 
 # a shorter list for tuning inside a served run (block x chains, cell factor 1)
 QUICK_CANDIDATES = [dict(block=b, unroll=u, cell_factor=1) for b, u in itertools.product((128, 256), (2, 4))]

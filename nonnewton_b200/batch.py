@@ -24,7 +24,7 @@ def scene_grid_cells(sc: Scene, cell_factor: int = 1, x_split: int = 1) -> int:
     g = []
     for k in range(3):
         ext = (p.domain_end[k] - p.domain_start[k]) + 4 * h
-        edge = h / cell_factor / (x_split if k == 0 else 1)
+        edge = h / cell_factor * (1.0 + 1e-3) / (x_split if k == 0 else 1)  # the library's 0.1 % margin
         g.append(int(min(65535, max(1, np.ceil(ext / edge) + 1))))
     mb = 0
     while (1 << mb) < max(g[1], g[2]):

@@ -18,6 +18,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libnnsph.so")
 LIB_PATHS = {"f32": LIB_PATH, "f64": os.path.join(HERE, "libnnsph64.so")}
 REAL_BYTES = {"f32": 4, "f64": 8}
+X_SPLIT_DEFAULT = 2  # x cells per cell edge of a new context (the library's NN_DEFAULT_XSPLIT)
 
 _libs = {}
 
@@ -94,7 +95,8 @@ class Engine:
                                       C.byref(h)), None)
         self.h = h
         self.max_neighbors = max_neighbors
-        self.x_split = 1
+        self.x_split = X_SPLIT_DEFAULT
+        self.set_x_split(X_SPLIT_DEFAULT)
         self._state = None
         self._scenes = None
         self._keep = []
@@ -134,7 +136,7 @@ class Engine:
         f.argtypes = [C.c_void_p, C.c_int32]
         f.restype = C.c_int
         self._rc(f(self.h, int(x_split)))
-        self.x_split = int(x_split) if x_split else 1
+        self.x_split = int(x_split) if x_split else X_SPLIT_DEFAULT
 
     def bind(self, pd, n: int | None = None) -> None:
         """Bind the fields of `pd`; `n` active particles (default: all rows)."""
