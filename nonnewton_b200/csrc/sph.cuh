@@ -86,10 +86,10 @@ __global__ void k_density_factor(Dev d, int do_density, int do_factor) {
         if (CHANGE) dd += V * dot3(vi - f3(vj), g);
       };
       if constexpr (CHANGE) {
-        nb_batches<U>(d.nbr + i, d.cap, c, i, [&](int j) { return GPV{ldg(&d.w.pos[j]), ldg(&d.w.vel[j])}; },
+        nb_batches<U>(d.nbr + i, d.cap, c, i, [&](int j) { return GPV{pos_of(d, j), ldg(&d.w.vel[j])}; },
                       [&](int, const GPV& g) { body(g.p, g.v); });
       } else {
-        nb_batches<U>(d.nbr + i, d.cap, c, i, [&](int j) { return ldg(&d.w.pos[j]); },
+        nb_batches<U>(d.nbr + i, d.cap, c, i, [&](int j) { return pos_of(d, j); },
                       [&](int, real4 pj) { body(pj, pj); });
       }
       if (do_density) {
@@ -132,7 +132,7 @@ __global__ void NN_PASS_REGS k_density_change(Dev d, int mode) {
       const real3 vi = f3(d.w.vel[i]);
       const int c = d.nbr_cnt[i];
       real dd = 0.f;
-      nb_batches<U>(d.nbr + i, d.cap, c, i, [&](int j) { return GPV{ldg(&d.w.pos[j]), ldg(&d.w.vel[j])}; },
+      nb_batches<U>(d.nbr + i, d.cap, c, i, [&](int j) { return GPV{pos_of(d, j), ldg(&d.w.vel[j])}; },
                  [&](int, const GPV& g) {
                    const real3 r = xi - f3(g.p);
                    dd += fabs(g.p.w) * dot3(vi - f3(g.v), kgrad_r2(r, dot3(r, r), s));
@@ -168,7 +168,7 @@ __global__ void NN_PASS_REGS k_divergence_update(Dev d) {
     const real3 xi = f3(d.w.pos[i]);
     const real k_i = d.kappa[i];
     real3 dv = make_real3(0.f, 0.f, 0.f);
-    nb_batches<U>(d.nbr + i, d.cap, d.nbr_cnt[i], i, [&](int j) { return GPK{ldg(&d.w.pos[j]), ldg(&d.kappa[j])}; },
+    nb_batches<U>(d.nbr + i, d.cap, d.nbr_cnt[i], i, [&](int j) { return GPK{pos_of(d, j), ldg(&d.kappa[j])}; },
                [&](int, const GPK& g) {
                  const real3 r = xi - f3(g.p);
                  if (w_fluid(g.p.w)) {
@@ -217,7 +217,7 @@ __global__ void NN_PASS_REGS k_density_adv(Dev d, int mode) {
       const real3 vi = f3(d.w.vel[i]);
       real delta = 0.f;
       nb_batches<U, true>(d.nbr + i, d.cap, d.nbr_cnt[i], i,
-                 [&](int j) { return GPV{ldg(&d.w.pos[j]), ldg(&d.w.vel[j])}; },
+                 [&](int j) { return GPV{pos_of(d, j), ldg(&d.w.vel[j])}; },
                  [&](int, const GPV& g) {
                    const real3 r = xi - f3(g.p);
                    delta += fabs(g.p.w) * dot3(vi - f3(g.v), kgrad_r2(r, dot3(r, r), s));
@@ -255,7 +255,7 @@ __global__ void NN_PASS_REGS k_pressure_update(Dev d) {
     const real dt = d.dyn[scn].dt;
     const real4 pi = d.w.pos[i];
     const real3 xi = f3(pi);
-    auto load = [&](int j) { return GPK{ldg(&d.w.pos[j]), ldg(&d.kappa[j])}; };
+    auto load = [&](int j) { return GPK{pos_of(d, j), ldg(&d.kappa[j])}; };
     if (fluid) {
       const real k_i = d.kappa[i];
       real4 v4 = d.w.vel[i];
@@ -494,7 +494,7 @@ __device__ __forceinline__ void forces_body(Dev d, int clear) {
       const bool need_rho = vi_on || vb_on;  // density and id only where a term reads them
       nb_batches<U>(d.nbr + i, d.cap, d.nbr_cnt[i], i,
                     [&](int j) {
-                      return GF{ldg(&d.w.pos[j]), ldg(&d.w.vel[j]), need_rho ? ldg(&d.w.dens[j]) : 1.f,
+                      return GF{pos_of(d, j), ldg(&d.w.vel[j]), need_rho ? ldg(&d.w.dens[j]) : 1.f,
                                 quirks ? ldg(&d.w.id[j]) : 0};
                     },
                     [&](int, const GF& g) {
@@ -607,7 +607,7 @@ __device__ __forceinline__ real3 cg_apply(const Dev& d, int i, const real4* __re
   nb_batches<U>(d.nbr + i, d.cap, d.nbr_cnt[i], i,
              [&](int j) {
                GCG g;
-               g.p = ldg(&d.w.pos[j]);
+               g.p = pos_of(d, j);
                g.x = ldg(&vec[j]);
                g.a = ldg(&d.cg_aux[j]);
                return g;
