@@ -20,12 +20,6 @@ struct Truth {
   float* srn; float* mu; float* stress; float* rot;
 };
 
-// A neighbour's position + volume in the neighbour passes. NN_POS_TEX builds fetch it
-// through the texture path, whose data pipe is separate from the one serving the
-// other gathers (ld.global); the positions are read-only in those passes.
-struct Dev;
-__device__ __forceinline__ real4 pos_of(const Dev& d, int j);
-
 struct Dev {
   // sizes (device-resident so a captured graph serves any batch composition)
   const int32_t* d_n;          // [0] particles, [1] scenes, [2] total cells, [3] elastic particles
@@ -35,7 +29,6 @@ struct Dev {
   const int32_t* scene_of_id;  // scene of each particle id
   Truth t;
   WorkSet w;                   // current sorted set
-  unsigned long long tex_pos;  // texture object over w.pos (NN_POS_TEX builds), else 0
   WorkSet wo;                  // previous sorted set (resident re-sort source)
   const int32_t* src_from_truth; // device flag: 1 = gather from Truth, 0 = from wo
   real4* acc4;                 // accelerations (slot order)
@@ -86,10 +79,5 @@ struct Dev {
   int32_t* body_count;         // [4] executed loop bodies (div, pressure, cg, elastic)
 };
 
-__device__ __forceinline__ real4 pos_of(const Dev& d, int j) {
-#if defined(NN_POS_TEX) && !defined(NN_FP64)
-  return tex1Dfetch<float4>((cudaTextureObject_t)d.tex_pos, j);
-#else
-  return ldg(&d.w.pos[j]);
-#endif
-}
+// A neighbour's position + volume in the neighbour passes (read-only there).
+__device__ __forceinline__ real4 pos_of(const Dev& d, int j) { return ldg(&d.w.pos[j]); }

@@ -71,7 +71,6 @@ struct nn_ctx {
   int el_mult_max = 0;
   // device buffers
   WorkSet set[2]{};
-  cudaTextureObject_t tex_pos[2] = {0, 0};  // NN_POS_TEX builds: texture objects over set[k].pos
   int cur = 0;                         // set holding the current slots
   bool searched = false;
   bool resident_ok = false;            // the slots hold the state the last nn_step left
@@ -152,7 +151,6 @@ static Dev make_dev(nn_ctx* c, int cur) {
               s.material, s.is_dynamic, s.phase_id, s.strain_rate_norm, s.nonnewton_viscosity, s.stress, s.rotations};
   d.w = c->set[cur];
   d.wo = c->set[1 - cur];
-  d.tex_pos = (unsigned long long)c->tex_pos[cur];
   d.src_from_truth = c->d_src_flag;
   d.acc4 = c->acc4;
   d.alpha = c->alpha;
@@ -653,19 +651,6 @@ int nn_ctx_create(int32_t max_particles, int32_t max_scenes, int32_t max_neighbo
     AL(c->set[k].pos, N); AL(c->set[k].vel, N); AL(c->set[k].mass, N); AL(c->set[k].dens, N);
     AL(c->set[k].flags, N); AL(c->set[k].id, N);
   }
-#if defined(NN_POS_TEX) && !defined(NN_FP64)
-  for (int k = 0; k < 2; ++k) {
-    cudaResourceDesc rd{};
-    rd.resType = cudaResourceTypeLinear;
-    rd.res.linear.devPtr = c->set[k].pos;
-    rd.res.linear.desc = cudaCreateChannelDesc<float4>();
-    rd.res.linear.sizeInBytes = N * sizeof(float4);
-    cudaTextureDesc td{};
-    td.readMode = cudaReadModeElementType;
-    if (cudaCreateTextureObject(&c->tex_pos[k], &rd, &td, nullptr) != cudaSuccess)
-      return bail(fail(nullptr, NN_ERR_CUDA, "cudaCreateTextureObject failed"));
-  }
-#endif
   AL(c->d_n, 4); AL(c->d_sc, (size_t)max_scenes); AL(c->d_dyn, (size_t)max_scenes);
   AL(c->d_acc, (size_t)max_scenes * ACC_COUNT * NN_STRIPES);
   AL(c->d_scene_of_id, N); AL(c->d_src_flag, 1); AL(c->acc4, N);
@@ -701,8 +686,6 @@ int nn_ctx_create(int32_t max_particles, int32_t max_scenes, int32_t max_neighbo
 int nn_ctx_destroy(nn_ctx* c) {
   if (!c) return NN_OK;
   drop_graphs(c);
-  for (int k = 0; k < 2; ++k)
-    if (c->tex_pos[k]) cudaDestroyTextureObject(c->tex_pos[k]);
   for (int k = 0; k < 2; ++k) {
     cudaFree(c->set[k].pos); cudaFree(c->set[k].vel); cudaFree(c->set[k].mass); cudaFree(c->set[k].dens);
     cudaFree(c->set[k].flags); cudaFree(c->set[k].id);

@@ -158,25 +158,55 @@ __global__ void k_scatter(Dev d) {
 }
 
 // In-cell order by particle id, so that the slot order (and every neighbour sum)
-// does not depend on the atomics of k_keys.
+// does not depend on the atomics of k_keys. A cell of up to NS_SORT_SMALL particles
+// is sorted by its own thread (insertion sort); a crowded cell (a cluster) by the
+// whole warp: each lane ranks some of its particles by counting the smaller ids, so
+// a cell of n particles takes n^2 / 32 steps per lane instead of about n^2 / 4 on one
+// thread. Particle ids are distinct, so the ranks are a permutation. The scratch of
+// the warp path is the key array, which nothing reads after k_scatter.
+#define NS_SORT_SMALL 24
 __global__ void k_cell_sort(Dev d) {
   const int nc = d.d_n[2];
   const bool truth = *d.src_from_truth != 0;
-  GRID_STRIDE(c, nc) {
-    uint32_t b = d.cell_count[c], e = d.cell_count[c + 1];
-    if (e - b < 2) continue;
-    for (uint32_t i = b + 1; i < e; ++i) {
-      int s = d.src[i];
-      int ids = truth ? s : d.wo.id[s];
-      uint32_t j = i;
-      while (j > b) {
-        int sp = d.src[j - 1];
-        int idp = truth ? sp : d.wo.id[sp];
-        if (idp <= ids) break;
-        d.src[j] = sp;
-        --j;
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  FOR_SLOTS_WARP(c, valid, nc) {
+    uint32_t b = 0, e = 0;
+    if (valid) { b = d.cell_count[c]; e = d.cell_count[c + 1]; }
+    const uint32_t n = e - b;
+    if (n >= 2 && n <= NS_SORT_SMALL) {
+      for (uint32_t i = b + 1; i < e; ++i) {
+        int s = d.src[i];
+        int ids = truth ? s : d.wo.id[s];
+        uint32_t j = i;
+        while (j > b) {
+          int sp = d.src[j - 1];
+          int idp = truth ? sp : d.wo.id[sp];
+          if (idp <= ids) break;
+          d.src[j] = sp;
+          --j;
+        }
+        d.src[j] = s;
       }
-      d.src[j] = s;
+    }
+    unsigned big = __ballot_sync(full, n > NS_SORT_SMALL);
+    while (big) {
+      const int l = __ffs(big) - 1;
+      big &= big - 1;
+      const uint32_t bb = __shfl_sync(full, b, l), ee = __shfl_sync(full, e, l);
+      for (uint32_t k = bb + lane; k < ee; k += 32) d.key[k] = (uint32_t)d.src[k];
+      __syncwarp();
+      for (uint32_t k = bb + lane; k < ee; k += 32) {
+        const int s = (int)d.key[k];
+        const int ids = truth ? s : d.wo.id[s];
+        uint32_t rank = 0;
+        for (uint32_t j = bb; j < ee; ++j) {
+          const int sj = (int)d.key[j];
+          rank += (uint32_t)((truth ? sj : d.wo.id[sj]) < ids);
+        }
+        d.src[bb + rank] = s;
+      }
+      __syncwarp();
     }
   }
 }
