@@ -49,14 +49,14 @@ ALG_BYTES = {
 }
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch on the
 # 2.4M-particle dam break, from `ncu --set full` captures of the current kernels.
-NCU_TRAFFIC_2M = {"build_lists": 494899456, "density_adv": 380777216,
+NCU_TRAFFIC_2M = {"build_lists": 477530368, "density_adv": 380777216,
                   "nonpressure": 431172096, "density_factor": 371440896,
                   "density_change": 366368512, "divergence_update": 376274432,
                   "pressure_update": 383854080, "cg_matvec": 406361600}
 # what bounds each kernel instead of DRAM, from its ncu capture on the 2.4M scene:
 # the HBM fraction above is low because none is DRAM-bound
 LIMITER_2M = {
-    "build_lists": "instruction issue: 71 % issue active, ~216 exact f32 distance tests per particle; DRAM 9 %",
+    "build_lists": "instruction issue: 72 % issue active, ~160 exact f32 distance tests per particle, two per packed f32x2 instruction; DRAM 13 %",
     "density_adv": "L1 data pipe: LSU wavefronts at 84 % of peak (neighbour gathers); DRAM 18 %",
     "nonpressure": "L1 data pipe and gather latency: LSU wavefronts 62 %, 46 % warps active; DRAM 13 %",
     "density_factor": "L1 data pipe: LSU wavefronts 67 % of peak; DRAM 14 %",

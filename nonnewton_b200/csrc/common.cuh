@@ -282,6 +282,36 @@ __device__ __forceinline__ void scene_add(double* acc, int quantity, int nscenes
   (void)nscenes_stride;
 }
 
+// FP64 partial sums of NQ quantities that a lane keeps for the scene it last worked
+// on, across the iterations of a grid-stride loop: they go to the scene's striped
+// accumulators (scene_add) when any lane of the warp moves on to another scene, and
+// at the end of the kernel, instead of once per iteration. add() and flush() must be
+// called by all 32 lanes.
+template <int NQ>
+struct LaneSums {
+  double v[NQ];
+  int scn = -1;
+  __device__ __forceinline__ LaneSums() {
+#pragma unroll
+    for (int k = 0; k < NQ; ++k) v[k] = 0.0;
+  }
+  __device__ __forceinline__ void flush(double* acc, const int (&q)[NQ]) {
+#pragma unroll
+    for (int k = 0; k < NQ; ++k) scene_add(acc, q[k], 0, scn >= 0 ? scn : 0, scn >= 0, v[k]);
+#pragma unroll
+    for (int k = 0; k < NQ; ++k) v[k] = 0.0;
+    scn = -1;
+  }
+  __device__ __forceinline__ void add(double* acc, const int (&q)[NQ], bool work, int scene, const double (&x)[NQ]) {
+    if (__any_sync(0xffffffffu, work && scn >= 0 && scene != scn)) flush(acc, q);
+    if (work) {
+#pragma unroll
+      for (int k = 0; k < NQ; ++k) v[k] += x[k];
+      scn = scene;
+    }
+  }
+};
+
 // Warp-aggregated atomicMax: lanes that target the same address combine first.
 // Must be called by all 32 lanes.
 __device__ __forceinline__ void warp_max_to(unsigned* addr, unsigned val, bool valid) {

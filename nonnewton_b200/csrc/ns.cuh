@@ -286,9 +286,55 @@ __device__ __forceinline__ real exact_r2(real3 r) {
   return add_rn(add_rn(mul_rn(r.x, r.x), mul_rn(r.y, r.y)), mul_rn(r.z, r.z));
 }
 
+#ifndef NN_FP64
+// Staged candidates of the FP32 build are tested two at a time with sm_100's packed
+// f32x2 arithmetic, half the arithmetic instructions of the issue-bound test loop, and
+// with results bit-identical to exact_r2 (so the lists are unchanged):
+//  - x_j + (-x_i) is the exact negation of x_i - x_j (one add.rn.f32x2);
+//  - each square is fma.rn.f32x2(d, d, +0), which rounds d*d once, as mul.rn does.
+//    A packed mul.rn.f32x2 feeding the packed add was measured to be contracted into a
+//    fused multiply-add by ptxas, which moves r2 by a rounding step in about a quarter
+//    of the pairs; an fma with a +0 addend cannot be folded into the add that follows,
+//    since that would change its result;
+//  - the two sums are add.rn.f32x2, in the reference's order.
+// The stage holds x, y and z planes, so one 8-byte shared load yields a pair (t even);
+// the lower 32 bits hold candidate t.
+#define NS_PACKED 1
+__device__ __forceinline__ uint64_t add_rn_x2(uint64_t a, uint64_t b) {
+  uint64_t d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ uint64_t sq_rn_x2(uint64_t a) {
+  uint64_t d;
+  asm("fma.rn.f32x2 %0, %1, %1, %2;" : "=l"(d) : "l"(a), "l"(0ull));
+  return d;
+}
+__device__ __forceinline__ uint64_t splat_x2(float v) {
+  const uint64_t u = __float_as_uint(v);
+  return u | (u << 32);
+}
+__device__ __forceinline__ uint32_t pair_hits(const float* sx, const float* sy, const float* sz, uint32_t t,
+                                              uint64_t nx, uint64_t ny, uint64_t nz, float thr) {
+  const uint64_t dx = add_rn_x2(*reinterpret_cast<const uint64_t*>(sx + t), nx);
+  const uint64_t dy = add_rn_x2(*reinterpret_cast<const uint64_t*>(sy + t), ny);
+  const uint64_t dz = add_rn_x2(*reinterpret_cast<const uint64_t*>(sz + t), nz);
+  const uint64_t r2 = add_rn_x2(add_rn_x2(sq_rn_x2(dx), sq_rn_x2(dy)), sq_rn_x2(dz));
+  return (uint32_t)(__uint_as_float((uint32_t)r2) < thr) |
+         ((uint32_t)(__uint_as_float((uint32_t)(r2 >> 32)) < thr) << 1);
+}
+#endif
+
 __global__ void __launch_bounds__(NS_WARPS * 32) k_build_lists(Dev d) {
+#ifdef NS_PACKED
+  __shared__ __align__(16) float stage_xyz[3][NS_WARPS][NS_CHUNK];
+  float* sx = stage_xyz[0][threadIdx.x >> 5];
+  float* sy = stage_xyz[1][threadIdx.x >> 5];
+  float* sz = stage_xyz[2][threadIdx.x >> 5];
+#else
   __shared__ real4 stage_all[NS_WARPS][NS_CHUNK];
   real4* stage = stage_all[threadIdx.x >> 5];
+#endif
   const int lane = threadIdx.x & 31;
   const unsigned full = 0xffffffffu;
   const int n = d.d_n[0];
@@ -303,6 +349,9 @@ __global__ void __launch_bounds__(NS_WARPS * 32) k_build_lists(Dev d) {
     const SceneDev& s = d.sc[scn];
     const real3 xi = f3(pi);
     const real thr = s.h2_thr;
+#ifdef NS_PACKED
+    const uint64_t nx = splat_x2(-xi.x), ny = splat_x2(-xi.y), nz = splat_x2(-xi.z);
+#endif
     const int x0 = max(cx - s.nfx, 0), x1 = min(cx + s.nfx, s.gx - 1);
     // lane 0 is always valid (the warp's first slot is below n)
     const int ly = __shfl_sync(full, cy, 0), lz = __shfl_sync(full, cz, 0), ls = __shfl_sync(full, scn, 0);
@@ -329,6 +378,37 @@ __global__ void __launch_bounds__(NS_WARPS * 32) k_build_lists(Dev d) {
           if (valid) { b = d.cell_count[row + x0]; e = d.cell_count[row + x1 + 1]; }
           for (uint32_t c0 = rb; c0 < re; c0 += NS_CHUNK) {
             const uint32_t c1 = min(c0 + NS_CHUNK, re);
+#ifdef NS_PACKED
+            for (uint32_t t = lane; t < c1 - c0; t += 32) {
+              const real4 p = ldg(&d.w.pos[c0 + t]);
+              sx[t] = p.x; sy[t] = p.y; sz[t] = p.z;
+            }
+            // a pair that ends past an odd chunk end reads one more entry (< NS_CHUNK,
+            // which is even): give it a defined value; its bit is masked below
+            if (lane == 0 && ((c1 - c0) & 1u)) { sx[c1 - c0] = 0.f; sy[c1 - c0] = 0.f; sz[c1 - c0] = 0.f; }
+            __syncwarp();
+            const uint32_t lo = max(b, c0), hi = min(e, c1);
+            // groups of up to 32 candidates from an even stage index (one below lo when
+            // lo - c0 is odd; that bit is cleared), tested in pairs
+            for (uint32_t g = (lo - c0) & ~1u; lo < hi && g < hi - c0; g += 32) {
+              const uint32_t len = min(32u, hi - c0 - g);
+              uint32_t m = 0u, k = 0u;
+              for (; k + 4 <= len; k += 4) {  // two independent pairs
+                const uint32_t p0 = pair_hits(sx, sy, sz, g + k, nx, ny, nz, thr);
+                const uint32_t p1 = pair_hits(sx, sy, sz, g + k + 2, nx, ny, nz, thr);
+                m |= (p0 | (p1 << 2)) << k;
+              }
+              for (; k < len; k += 2) m |= pair_hits(sx, sy, sz, g + k, nx, ny, nz, thr) << k;
+              if (len < 32u) m &= (1u << len) - 1u;
+              if (c0 + g < lo) m &= ~1u;
+              const uint32_t self = (uint32_t)i - (c0 + g);
+              if (self < 32u) m &= ~(1u << self);
+              while (m) {
+                append((int)(c0 + g + __ffs(m) - 1));
+                m &= m - 1u;
+              }
+            }
+#else
             for (uint32_t t = lane; t < c1 - c0; t += 32) stage[t] = ldg(&d.w.pos[c0 + t]);
             __syncwarp();
             const uint32_t lo = max(b, c0), hi = min(e, c1);
@@ -354,6 +434,7 @@ __global__ void __launch_bounds__(NS_WARPS * 32) k_build_lists(Dev d) {
                 m &= m - 1u;
               }
             }
+#endif
             __syncwarp();
           }
         }

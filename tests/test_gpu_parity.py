@@ -77,6 +77,32 @@ def test_neighbor_lists_bit_exact(cuda_lib, seed):
     assert set(bad.tolist()) <= tie_ids, f"{len(bad)} rows differ outside cut-off ties"
 
 
+def test_neighbor_lists_exact_at_the_cutoff(cuda_lib):
+    """No tie exceptions: a fluid lattice at spacing h / 2, so that the pairs two steps
+    apart along an axis sit at the cut-off, with every fluid coordinate moved by -3..3
+    ulp at random, puts thousands of pairs within a few ulp of h. Both sides evaluate the
+    reference's f32 expression with separately rounded operations (SPH/main.py:845; the
+    list build two candidates at a time with packed f32x2 arithmetic), so the lists equal
+    the oracle's exactly."""
+    sc = S.dam_break(seed=0, n_side=(16, 16, 16), box=0.6, jitter=0.0)
+    nf = sc.particles.n_fluid
+    x = np.asarray(sc.particles.x, np.float32).copy()
+    bits = x[:nf].view(np.int32)  # positive coordinates: +k on the bits is +k ulp
+    bits += np.random.default_rng(5).integers(-3, 4, size=bits.shape, dtype=np.int32)
+    sc.particles.x = x
+    ties = near_cutoff_pairs(x, sc.param.support_radius)
+    assert len(ties) > 1000, len(ties)
+    m, solver = gpu_sim(sc)
+    m.ns.run_search()
+    o = oracle_sim(sc)
+    o.run_pass(_abi.NN_PASS_SEARCH)
+    on, ol = o.neighbors(60)
+    gn = m.ns.num_neighbors.cpu().numpy()
+    gl = m.ns.neighbors.cpu().numpy()
+    bad = np.nonzero((gn != on) | np.any(gl != ol, axis=1))[0]
+    assert len(bad) == 0, f"{len(bad)} rows differ ({len(ties)} pairs within 4 ulp of h)"
+
+
 def _init_both(sc, **kw):
     m, solver = gpu_sim(sc, **kw)
     solver.initialize()
