@@ -47,12 +47,15 @@ ALG_BYTES = {
     "nonpressure": 4 + 16 + 16 + 4 + 4 + 16 + 4 + 4 + 8,  # flags, pos4, vel4, mass, dens -> acc4, srn, mu, aux2
     "build_lists": 16 + 4 + 4,                    # pos4, flags -> count; + 4 B per list entry (added live)
 }
+# the density change that also computes the non-pressure terms (run in the divergence
+# loop's predicted last body) reads mass and density besides and writes acc4, srn, mu, aux2
+ALG_BYTES["density_change_np"] = ALG_BYTES["density_change"] + 4 + 4 + 16 + 4 + 4 + 8
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch on the
 # 2.4M-particle dam break, from `ncu --set full` captures of the current kernels.
 NCU_TRAFFIC_2M = {"build_lists": 477530368, "density_adv": 380777216,
                   "nonpressure": 431172096, "density_factor": 371440896,
                   "density_change": 366368512, "divergence_update": 376274432,
-                  "pressure_update": 383854080, "cg_matvec": 406361600}
+                  "pressure_update": 383854080, "cg_matvec": 406361600, "density_change_np": 436444416}
 # what bounds each kernel instead of DRAM, from its ncu capture on the 2.4M scene:
 # the HBM fraction above is low because none is DRAM-bound
 LIMITER_2M = {
@@ -64,9 +67,11 @@ LIMITER_2M = {
     "divergence_update": "L1 data pipe: LSU wavefronts 65 % of peak, 64 % issue active; DRAM 20 %",
     "pressure_update": "L1 data pipe: LSU wavefronts 72 % of peak; DRAM 24 %",
     "cg_matvec": "L1 data pipe: LSU wavefronts 84 % of peak; DRAM 15 %",
+    "density_change_np": "gather latency with the folded force terms: LSU wavefronts 60 %, issue 63 %, "
+                         "46 % warps active at 64 registers; DRAM 12 %",
 }
 KERNEL_IDS = {"pressure_update": 0, "density_adv": 1, "divergence_update": 2, "density_change": 3,
-              "density_factor": 4, "build_lists": 5, "cg_matvec": 6, "nonpressure": 7}
+              "density_factor": 4, "build_lists": 5, "cg_matvec": 6, "nonpressure": 7, "density_change_np": 8}
 
 
 def step_bytes(iters_v, iters_p, iters_cg, f_el, implicit):
@@ -662,15 +667,20 @@ def run_ours(args):
     value = total_ps / (ms_max / 1e3)
     # ---- roofline of the dominant kernel: timed live on the current slots
     implicit = bool(sc.param.implicit_viscosity)
+    # when the last step took its non-pressure terms from the divergence loop's last
+    # density change, the force pass skipped the scene and that body ran the NP instance
+    folded = bool(st["nonpressure_folded"])
     kms = {}
     for k in ("pressure_update", "density_adv", "build_lists", "density_factor", "divergence_update",
-              "density_change", "nonpressure") + (("cg_matvec",) if implicit else ()):
+              "density_change") + (("density_change_np",) if folded else ("nonpressure",)) + \
+             (("cg_matvec",) if implicit else ()):
         kms[k] = eng.time_kernel(KERNEL_IDS[k], reps=10)
     # launches per step of each timed kernel at the iteration counts of the last step;
     # the dominant kernel is the one with the largest time per step
     it_v, it_p = st["iterations_v"] + 1, st["iterations"] + 1
-    per_step = {"build_lists": 1, "density_factor": 1, "nonpressure": 1, "density_adv": it_p + 1,
-                "pressure_update": it_p, "divergence_update": it_v, "density_change": it_v,
+    per_step = {"build_lists": 1, "density_factor": 1, "nonpressure": 0 if folded else 1,
+                "density_adv": it_p + 1, "pressure_update": it_p, "divergence_update": it_v,
+                "density_change": it_v - (1 if folded else 0), "density_change_np": 1 if folded else 0,
                 "cg_matvec": st["cg_iterations"]}
     dom = max(kms, key=lambda k: kms[k] * per_step[k])
     num_nb, _ = eng.neighbors(n, 1)
@@ -761,7 +771,8 @@ def run_ours(args):
         "data": "synthetic (seeded numpy scene generator)",
         "config": workload_config(sc, world),
         "launch": {"step_graph": "host-driven loops" if args.host_loop else "CUDA graph with while-node solver loops",
-                   "tuning": tuning or {"block": 128, "unroll": 2, "cell_factor": 1}},
+                   "tuning": tuning or {"block": 128, "unroll": 2, "cell_factor": 1},
+                   "nonpressure": "in the divergence loop's last density change" if folded else "force pass"},
         "autotune_ms_per_step": tune_ms,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "peak_source": f"{peak_kind} hbm_gbs",

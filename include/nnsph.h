@@ -169,6 +169,12 @@ typedef struct nn_stats {
   double max_avg_density_err;     /* largest avg_density_err at the end of any step since
                                      nn_set_scenes: the DFSPH error of every step, not only
                                      the last */
+  int32_t nonpressure_folded;     /* 1 when the last nn_step took the fluid's non-pressure
+                                     terms (compute_non_pressure_forces, 1557-1567) from the
+                                     divergence loop's last density change instead of the
+                                     force pass: every scene with fluid runs the divergence
+                                     solve, none needs the explicit viscosity or quirk mode,
+                                     and the loop ran as many bodies as in the step before */
 } nn_stats;
 
 typedef struct nn_ctx nn_ctx;
@@ -281,6 +287,7 @@ enum nn_kernel_id {
   NN_K_BUILD_LISTS,           /* store_neighbors */
   NN_K_CG_MATVEC,             /* implicit viscosity matrix-vector product */
   NN_K_NONPRESSURE,           /* surface tension + explicit viscosity */
+  NN_K_DENSITY_CHANGE_NP,     /* compute_density_change with the non-pressure terms */
   NN_K_COUNT
 };
 /* Average duration in ms of `reps` launches of one kernel on the current slots,

@@ -105,12 +105,15 @@ struct SceneDyn {
   double avg_v, avg_p;            // last average density errors
   double cg_rz, cg_bnorm2, cg_rel;
   int32_t div_ran;                // divergence solve ran this step (alpha bookkeeping)
-  int32_t pad;
+  int32_t np_body;                // divergence loop body (0-based) whose density change also computes
+                                  // the non-pressure terms: the last body of the previous step
   double cg_alpha, cg_beta;       // PCG scalars of the current iteration
   int64_t steps;
   float anim[3];                 // animate_particles displacement of the next step (set by the host)
-  int32_t pad2;
+  int32_t np_last;                // index of the last divergence loop body of the last step
   double max_avg_p;               // largest avg_p at the end of a step since the scene was set
+  int32_t np_fresh;               // this step's non-pressure terms came from body np_body, the last
+  int32_t pad;
 };
 
 // Accumulator slots per scene (each NN_STRIPES doubles).

@@ -68,6 +68,8 @@ struct nn_ctx {
   int n = 0, ncells = 0, ne = 0;
   bool any_fluid = false, any_div = false, any_nonnewton = false, any_implicit = false, any_cfl = false;
   int forces_feat = 0;                 // FF_* terms of the force pass any scene needs
+  bool fold_np = false;                // the step takes the fluid's non-pressure terms from the
+                                       // divergence loop's last density change (no force pass)
   int el_mult_max = 0;
   // device buffers
   WorkSet set[2]{};
@@ -117,7 +119,7 @@ static uint64_t feature_sig(const nn_ctx* c) {
   return (uint64_t)c->any_fluid | ((uint64_t)c->any_div << 1) | ((uint64_t)c->any_nonnewton << 2) |
          ((uint64_t)c->any_implicit << 3) | ((uint64_t)std::min(c->el_mult_max, 255) << 8) |
          ((uint64_t)(c->ne > 0) << 16) | ((uint64_t)c->block << 20) |
-         ((uint64_t)c->forces_feat << 40);
+         ((uint64_t)c->forces_feat << 40) | ((uint64_t)c->fold_np << 48);
 }
 
 static thread_local char g_err[512];
@@ -330,20 +332,23 @@ static int enq_search(nn_ctx* c, cudaStream_t s) {
 
 // DFSPHSolver.divergence_solve (SPH/main.py:1683-1713). In the fused step the first
 // density change and alpha *= 1/dt were done by k_density_factor<CHANGE> and the
-// closing alpha *= dt is folded into the pressure solve's first pass (fused = true).
+// closing alpha *= dt is folded into the pressure solve's first pass (fused = true);
+// with c->fold_np the loop's density change also computes the fluid's non-pressure terms.
 static int enq_divergence(nn_ctx* c, cudaStream_t s, bool fused) {
   Dev d = make_dev(c, c->cur);
   const int B = c->block;
+  const bool np = fused && c->fold_np;
   if (!fused) RC(launch1(c, s, k_solver_begin, d, 0));
   RC(solver_loop(c, s, false,
                  [&](cudaStream_t q) {
-                   return fused ? NN_OK : launch(c, q, KU(k_density_change), B, c->n, make_dev(c, c->cur), 0);
+                   return fused ? NN_OK : launch(c, q, KU(k_density_change), B, c->n, make_dev(c, c->cur), 0, 0);
                  },
                  [&](cudaStream_t q) {
                    Dev e = make_dev(c, c->cur);
                    RC(launch(c, q, KU(k_divergence_update), B, c->n, e));
-                   RC(launch(c, q, KU(k_density_change), B, c->n, e, 1));
-                   return launch1(c, q, k_solver_check, e, 0);
+                   RC(launch(c, q, KU(k_density_change), B, c->n, e, 1, np ? 1 : 0));
+                   if (np) RC(launch(c, q, KU(k_density_change_np), B, c->n, e, 1, 1));
+                   return launch1(c, q, k_solver_check, e, 0, np ? 1 : 0);
                  }));
   return fused ? NN_OK : launch(c, s, k_alpha_times_dt, 256, c->n, d);
 }
@@ -362,13 +367,14 @@ static int enq_pressure(nn_ctx* c, cudaStream_t s, int init_mode) {
                        Dev e = make_dev(c, c->cur);
                        RC(launch(c, q, KU(k_pressure_update), B, c->n, e));
                        RC(launch(c, q, KU(k_density_adv), B, c->n, e, 1));
-                       return launch1(c, q, k_solver_check, e, 1);
+                       return launch1(c, q, k_solver_check, e, 1, 0);
                      });
 }
 
 // compute_non_pressure_forces (SPH/main.py:1557-1567), with the substep's
 // clear_accelerations when `clear`, then the implicit viscosity and, when `advect`,
-// non_pressure_advect.
+// non_pressure_advect. The force pass skips the scenes whose terms the divergence loop
+// already computed (SceneDyn::np_fresh).
 static int enq_nonpressure(nn_ctx* c, cudaStream_t s, int advect, int clear) {
   Dev d = make_dev(c, c->cur);
   const int B = c->block;
@@ -439,7 +445,7 @@ static int enq_step(nn_ctx* c, cudaStream_t s) {
   Dev d = make_dev(c, c->cur);
   RC(launch1(c, s, k_step_dt, d, 1));
   RC(launch(c, s, KU(k_boundary_volume), c->block, c->n, d, 1));
-  RC(launch(c, s, k_clear_acc, 256, c->n, d));
+  RC(launch(c, s, k_clear_acc, 256, c->n, d, c->fold_np ? 1 : 0));
   RC(enq_substep(c, s));
   RC(enq_elastic(c, s));
   RC(enq_rigid(c, s));
@@ -823,6 +829,7 @@ int nn_set_scenes(nn_ctx* c, int32_t nscenes, const nn_scene_desc* scenes) {
   c->any_fluid = c->any_div = c->any_nonnewton = c->any_implicit = c->any_cfl = false;
   c->forces_feat = 0;
   c->el_mult_max = 0;
+  bool all_div = true;                 // every scene with fluid runs the divergence solve
   for (int k = 0; k < nscenes; ++k) {
     const nn_scene_desc& sd = scenes[k];
     const bool q = (sd.params.flags & NN_F_QUIRKS) != 0;
@@ -857,6 +864,7 @@ int nn_set_scenes(nn_ctx* c, int32_t nscenes, const nn_scene_desc* scenes) {
     sdyn[k] = y;
     c->any_fluid |= sd.n_fluid > 0;
     c->any_div |= sd.n_fluid > 0 && (sd.params.flags & NN_F_DIVERGENCE);
+    if (sd.n_fluid > 0 && !(sd.params.flags & NN_F_DIVERGENCE)) all_div = false;
     c->any_nonnewton |= (sd.params.flags & NN_F_NONNEWTON) != 0;
     c->any_implicit |= sd.n_fluid > 0 && (sd.params.flags & NN_F_IMPLICIT_VISCOSITY) && !q;
     c->any_cfl |= (sd.params.flags & NN_F_CFL) != 0;
@@ -869,6 +877,10 @@ int nn_set_scenes(nn_ctx* c, int32_t nscenes, const nn_scene_desc* scenes) {
       if (q) c->forces_feat |= FF_Q;
     }
   }
+  // the force pass's terms ride on the divergence loop's last density change unless a
+  // scene skips the divergence solve or needs the explicit viscosity or quirk mode
+  c->fold_np = c->any_fluid && all_div && (c->forces_feat & (FF_VI | FF_Q)) == 0;
+  c->body_nodes[0] = c->fold_np ? 4 : 3;  // the folded density change is a second launch per body
   if (cells >= (int64_t)0x7fffffff) return fail(c, NN_ERR_CAPACITY, "%lld grid cells exceed the 32-bit key space", (long long)cells);
   if (cells > c->max_cells) drop_graphs(c);  // the scan grids were sized for the old table
   RC(ensure_cells(c, cells));
@@ -1038,7 +1050,7 @@ int nn_run_pass(nn_ctx* c, int32_t pass) {
   switch (pass) {
     case NN_PASS_STATIC_BOUNDARY_VOLUME: RC(launch(c, s, KU(k_boundary_volume), c->block, c->n, d, 0)); break;
     case NN_PASS_MOVING_BOUNDARY_VOLUME: RC(launch(c, s, KU(k_boundary_volume), c->block, c->n, d, 1)); break;
-    case NN_PASS_CLEAR_ACCELERATIONS: RC(launch(c, s, k_clear_acc, 256, c->n, d)); break;
+    case NN_PASS_CLEAR_ACCELERATIONS: RC(launch(c, s, k_clear_acc, 256, c->n, d, 0)); break;
     case NN_PASS_DENSITIES: RC(launch(c, s, KU2(k_density_factor, false), c->block, c->n, d, 1, 0)); break;
     case NN_PASS_DFSPH_FACTOR: RC(launch(c, s, KU2(k_density_factor, false), c->block, c->n, d, 0, 1)); break;
     case NN_PASS_DIVERGENCE_SOLVE: if (c->any_div) RC(enq_divergence(c, s, false)); break;
@@ -1084,7 +1096,8 @@ int nn_time_kernel(nn_ctx* c, int32_t kernel, int32_t reps, float* ms_out) {
       case NN_K_PRESSURE_UPDATE: return launch(c, s, KU(k_pressure_update), B, c->n, d);
       case NN_K_DENSITY_ADV: return launch(c, s, KU(k_density_adv), B, c->n, d, 1);
       case NN_K_DIVERGENCE_UPDATE: return launch(c, s, KU(k_divergence_update), B, c->n, d);
-      case NN_K_DENSITY_CHANGE: return launch(c, s, KU(k_density_change), B, c->n, d, 1);
+      case NN_K_DENSITY_CHANGE: return launch(c, s, KU(k_density_change), B, c->n, d, 1, 0);
+      case NN_K_DENSITY_CHANGE_NP: return launch(c, s, KU(k_density_change_np), B, c->n, d, 1, 0);
       case NN_K_DENSITY_FACTOR: return launch(c, s, KU2(k_density_factor, false), B, c->n, d, 1, 1);
       case NN_K_BUILD_LISTS: return launch(c, s, k_build_lists, NS_WARPS * 32, c->n, d);
       case NN_K_CG_MATVEC: return launch(c, s, KU(k_cg_matvec), B, c->n, d);
@@ -1192,6 +1205,7 @@ static void fill_stats(const SceneDyn& y, nn_stats* out) {
   out->max_density = md;
   out->steps = y.steps;
   out->max_avg_density_err = y.max_avg_p;
+  out->nonpressure_folded = y.np_fresh;
 }
 
 int nn_get_stats_range(nn_ctx* c, int32_t first, int32_t count, nn_stats* out) {

@@ -41,13 +41,20 @@ __global__ void k_boundary_volume(Dev d, int moving) {
   }
 }
 
-// clear_accelerations_kernel (SPH/main.py:945-951)
-__global__ void k_clear_acc(Dev d) {
+// clear_accelerations_kernel (SPH/main.py:945-951). With `solid_terms` also what the
+// force pass would write for the solid slots of scenes with fluid (strain rate and
+// viscosity 0, CG coefficients (0, 1 if dynamic)): the step sets it when the fluid's
+// non-pressure terms come from the divergence loop's last density change instead.
+__global__ void k_clear_acc(Dev d, int solid_terms) {
   const int n = d.d_n[0];
   GRID_STRIDE(i, n) {
     const uint32_t fl = d.w.flags[i];
     const SceneDev& s = d.sc[slot_scene(fl)];
     d.acc4[i] = cls_static_solid(fl) ? make_real4(0.f, 0.f, 0.f, 0.f) : make_real4(s.g[0], s.g[1], s.g[2], 0.f);
+    if (solid_terms && !cls_fluid(fl) && s.n_fluid > 0) {
+      if (s.flags & NN_F_NONNEWTON) { d.srn[i] = 0.f; d.mu[i] = 0.f; }
+      if (scene_implicit(s)) d.cg_aux[i] = make_real2(0.f, cls_dyn_solid(fl) ? 1.f : 0.f);
+    }
   }
 }
 
@@ -115,16 +122,35 @@ __global__ void k_density_factor(Dev d, int do_density, int do_factor) {
   }
 }
 
+__device__ __forceinline__ real nn_law(real g, const SceneDev& s);
+__device__ __forceinline__ real strain_rate_norm(const real (&S)[6], real rho_i, bool quirks);
+
 // compute_density_change (SPH/main.py:1610-1645). mode 0: first call of
 // divergence_solve, also applies alpha *= 1/dt (1688); mode 1: solver iteration,
 // accumulates the FP64 density error (1669-1675, 1717-1719).
-template <int U>
-__global__ void NN_PASS_REGS k_density_change(Dev d, int mode) {
+//
+// NP: the fluid's non-pressure terms of compute_non_pressure_forces (SPH/main.py:
+// 1557-1567) in the same pass: surface tension (1387-1414), the strain rate and the
+// viscosity law (461-492, 404-459) and the implicit viscosity's coefficients. They read
+// the positions and the velocities that the force pass would read: the velocities left
+// by the divergence solve, whose loop always ends with this pass after its last update
+// (it runs at least once, SPH/main.py:1695). Results are the force pass's, term for term
+// and in neighbour order. Only the body predicted to be the scene's last (np_body: the
+// last body of its previous step) runs this instance; when the prediction holds,
+// k_solver_check marks the terms fresh and the force pass skips the scene. The step
+// uses it when no scene needs the force pass's other terms (explicit viscosity, quirk
+// mode); the solids' outputs come from k_clear_acc.
+// `sel` = 1 in such a loop: the plain instance skips, and the NP instance takes, the
+// scenes whose np_body this body is; 0: every scene.
+template <int U, bool NP>
+__device__ __forceinline__ void density_change_body(Dev d, int mode, int sel) {
   const int n = d.d_n[0];
   FOR_SLOTS_WARP(i, valid, n) {
     uint32_t fl = valid ? d.w.flags[i] : 0u;
     const int scn = slot_scene(fl);
-    bool work = valid && cls_fluid(fl) && d.dyn[scn].act_v;
+    const SceneDyn& y = d.dyn[scn];
+    const bool np_here = sel && y.it_v == y.np_body;
+    bool work = valid && cls_fluid(fl) && y.act_v && (NP ? (np_here || !sel) : !np_here);
     double err = 0.0;
     if (work) {
       const SceneDev& s = d.sc[scn];
@@ -132,11 +158,50 @@ __global__ void NN_PASS_REGS k_density_change(Dev d, int mode) {
       const real3 vi = f3(d.w.vel[i]);
       const int c = d.nbr_cnt[i];
       real dd = 0.f;
-      nb_batches<U>(d.nbr + i, d.cap, c, i, [&](int j) { return GPV{pos_of(d, j), ldg(&d.w.vel[j])}; },
-                 [&](int, const GPV& g) {
-                   const real3 r = xi - f3(g.p);
-                   dd += fabs(g.p.w) * dot3(vi - f3(g.v), kgrad_r2(r, dot3(r, r), s));
-                 });
+      if constexpr (!NP) {
+        nb_batches<U>(d.nbr + i, d.cap, c, i, [&](int j) { return GPV{pos_of(d, j), ldg(&d.w.vel[j])}; },
+                   [&](int, const GPV& g) {
+                     const real3 r = xi - f3(g.p);
+                     dd += fabs(g.p.w) * dot3(vi - f3(g.v), kgrad_r2(r, dot3(r, r), s));
+                   });
+      } else {
+        const bool st_on = (s.flags & NN_F_SURFACE_TENSION) != 0;
+        const bool sr_on = (s.flags & NN_F_NONNEWTON) != 0;
+        const real mi = d.w.mass[i];
+        real3 st = make_real3(0.f, 0.f, 0.f);
+        real S[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // strain-rate sum: 00 11 22 01 02 12
+        nb_batches<U>(d.nbr + i, d.cap, c, i, [&](int j) { return GPV{pos_of(d, j), ldg(&d.w.vel[j])}; },
+                   [&](int, const GPV& g) {
+                     const real3 r = xi - f3(g.p);
+                     const real r2 = dot3(r, r);
+                     real w;
+                     real3 gw;
+                     kwg_r2(r, r2, s, w, gw);
+                     dd += fabs(g.p.w) * dot3(vi - f3(g.v), gw);
+                     const real mj = g.v.w;
+                     if (st_on && w_fluid(g.p.w)) st -= (r * (s.sigma / mi * mj)) * (r2 > s.dia2 ? w : s.w_dia);
+                     if (sr_on) {
+                       const real3 vji = f3(g.v) - vi;
+                       const real t[6] = {(vji.x * gw.x + vji.x * gw.x) * mj, (vji.y * gw.y + vji.y * gw.y) * mj,
+                                           (vji.z * gw.z + vji.z * gw.z) * mj, (vji.x * gw.y + vji.y * gw.x) * mj,
+                                           (vji.x * gw.z + vji.z * gw.x) * mj, (vji.y * gw.z + vji.z * gw.y) * mj};
+#pragma unroll
+                       for (int k = 0; k < 6; ++k) S[k] += t[k];
+                     }
+                   });
+        real4 a = make_real4(s.g[0], s.g[1], s.g[2], 0.f);
+        if (st_on) { a.x += st.x; a.y += st.y; a.z += st.z; }
+        d.acc4[i] = a;
+        const real rho_i = d.w.dens[i];
+        real mu = s.mu_newton;
+        if (sr_on) {
+          const real g = strain_rate_norm(S, rho_i, false);
+          mu = nn_law(g, s);
+          d.srn[i] = g;
+          d.mu[i] = mu;
+        }
+        if (scene_implicit(s)) d.cg_aux[i] = make_real2(mu, mi / rho_i);
+      }
       dd = fmax(dd, real(0));
       if (c < 20) dd = 0.f;
       d.rho_adv[i] = dd;
@@ -153,6 +218,12 @@ __global__ void NN_PASS_REGS k_density_change(Dev d, int mode) {
     if (mode == 1) scene_add(d.acc, ACC_ERR, 0, scn, work, err);
   }
 }
+template <int U>
+__global__ void NN_PASS_REGS k_density_change(Dev d, int mode, int sel) { density_change_body<U, false>(d, mode, sel); }
+// The NP instance is capped at 64 registers: uncapped it takes 79 (6 blocks of 128 per
+// SM) and ran 0.455 ms on the 2.4M scene, capped 0.428 ms (44 bytes spilled).
+template <int U>
+__global__ void NN_REGS64 k_density_change_np(Dev d, int mode, int sel) { density_change_body<U, true>(d, mode, sel); }
 
 // divergence_solver_iteration_kernel (SPH/main.py:1721-1760). The pushes onto
 // dynamic solids (1755-1760) are omitted: clear_accelerations (1552) discards them.
@@ -295,7 +366,9 @@ __global__ void NN_PASS_REGS k_pressure_update(Dev d) {
 // Loop control after each solver iteration: per-scene average error against eta,
 // the reference's iteration counting (SPH/main.py:1695-1703, 1778-1784), and the
 // CUDA graph while-condition (any scene still iterating).
-__global__ void k_solver_check(Dev d, int which /*0 div, 1 pressure*/) {
+// `fold`: the divergence loop runs the non-pressure terms in body np_body (k_density_change
+// NP); when a scene stops, its terms are fresh if that body was its last.
+__global__ void k_solver_check(Dev d, int which /*0 div, 1 pressure*/, int fold) {
   __shared__ int any;
   if (threadIdx.x == 0) any = 0;
   __syncthreads();
@@ -310,6 +383,7 @@ __global__ void k_solver_check(Dev d, int which /*0 div, 1 pressure*/) {
     double avg = err / (double)s.n_fluid;
     double eta = which == 0 ? (1.0 / (double)y.dt) * s.eta_v_fac : s.eta_p;
     int* it = which == 0 ? &y.it_v : &y.it_p;
+    const int body = *it;  // 0-based index of the body that just ran
     int mx = which == 0 ? s.max_iter_v : s.max_iter;
     if (which == 0) y.avg_v = avg; else y.avg_p = avg;
     if (avg <= eta) {
@@ -319,6 +393,10 @@ __global__ void k_solver_check(Dev d, int which /*0 div, 1 pressure*/) {
       if (*it >= max(mx, 1)) *act = 0;
     }
     if (!(avg == avg)) { set_status(&y, NN_ERR_NAN); *act = 0; }
+    if (which == 0 && !*act) {
+      y.np_last = body;
+      y.np_fresh = fold && body == y.np_body;
+    }
     if (*act) any = 1;
   }
   __syncthreads();
@@ -339,7 +417,11 @@ __global__ void k_solver_begin(Dev d, int which /*0 div, 1 pressure, 2 cg*/) {
     SceneDyn& y = d.dyn[sc];
     const SceneDev& s = d.sc[sc];
     int on = s.n_fluid > 0;
-    if (which == 0) { on = on && (s.flags & NN_F_DIVERGENCE); y.act_v = on; y.it_v = 0; y.div_ran = on; }
+    if (which == 0) {
+      on = on && (s.flags & NN_F_DIVERGENCE);
+      y.act_v = on; y.it_v = 0; y.div_ran = on;
+      y.np_body = min(max(y.np_last, 0), max(s.max_iter_v, 1) - 1);  // as many bodies as last step
+    }
     else if (which == 1) { y.act_p = on; y.it_p = 0; }
     else { y.it_cg = 0; }
     any |= on;
@@ -356,6 +438,7 @@ __global__ void k_step_reset(Dev d) {
     y.max_nb = 0;
     y.it_v = y.it_p = y.it_cg = 0;
     y.div_ran = 0;
+    y.np_fresh = 0;
   }
 }
 
@@ -401,6 +484,7 @@ __global__ void k_force_active(Dev d) {
     const bool on = d.sc[sc].n_fluid > 0;
     y.act_v = y.act_p = on;
     y.act_cg = on && scene_implicit(d.sc[sc]);
+    y.np_fresh = 0;
   }
 }
 
@@ -452,6 +536,23 @@ __device__ __forceinline__ real nn_law(real g, const SceneDev& s) {
 
 
 
+// calcStrainRate's norm (SPH/main.py:461-492) of the strain-rate sum S (00 11 22 01 02
+// 12): sqrt(D:D) with D = S / (2 rho_i); in quirk mode the norm of S itself, since the
+// reference takes the norm before the 0.5 / rho scaling (491-492).
+__device__ __forceinline__ real strain_rate_norm(const real (&S)[6], real rho_i, bool quirks) {
+  real nrm2;
+  if (quirks) {
+    nrm2 = S[0] * S[0] + S[1] * S[1] + S[2] * S[2] + 2.f * (S[3] * S[3] + S[4] * S[4] + S[5] * S[5]);
+  } else {
+    const real sc = 0.5f / rho_i;
+    real D[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) D[k] = S[k] * sc;
+    nrm2 = D[0] * D[0] + D[1] * D[1] + D[2] * D[2] + 2.f * (D[3] * D[3] + D[4] * D[4] + D[5] * D[5]);
+  }
+  return sqrt(nrm2);
+}
+
 // compute_non_pressure_forces (SPH/main.py:1557-1567) in one neighbour pass:
 // [clear_accelerations (1552)] + SurfaceTension (1387-1414) + NonNewton strain rate
 // and law (461-492, 404-459) + ViscosityModel (1426-1468), and the per-particle
@@ -475,6 +576,7 @@ __device__ __forceinline__ void forces_body(Dev d, int clear) {
     const int scn = slot_scene(fl);
     const SceneDev& s = d.sc[scn];
     if (s.n_fluid == 0) continue;  // the reference runs the substep only with fluid
+    if (d.dyn[scn].np_fresh) continue;  // computed by the divergence loop's last density change
     const bool implicit = scene_implicit(s);
     const bool quirks = (FF & FF_Q) && (s.flags & NN_F_QUIRKS);
     const bool st_on = (FF & FF_ST) && fluid && (s.flags & NN_F_SURFACE_TENSION);
@@ -542,17 +644,7 @@ __device__ __forceinline__ void forces_body(Dev d, int clear) {
     if (nn_on) {
       real g = 0.f;
       if (sr_on) {
-        real nrm2;
-        if (quirks) {
-          nrm2 = S[0] * S[0] + S[1] * S[1] + S[2] * S[2] + 2.f * (S[3] * S[3] + S[4] * S[4] + S[5] * S[5]);
-        } else {
-          const real sc = 0.5f / d.w.dens[i];
-          real D[6];
-#pragma unroll
-          for (int k = 0; k < 6; ++k) D[k] = S[k] * sc;
-          nrm2 = D[0] * D[0] + D[1] * D[1] + D[2] * D[2] + 2.f * (D[3] * D[3] + D[4] * D[4] + D[5] * D[5]);
-        }
-        g = sqrt(nrm2);
+        g = strain_rate_norm(S, d.w.dens[i], quirks);
         mu = nn_law(g, s);
       } else {
         mu = 0.f;
