@@ -3,8 +3,11 @@
 - PLY read/write of `x, y, z` float vertices (the reference's `read_ply_particles`
   and `export_ply_particles`, SPH/main.py:121-124, 184-190), without plyfile.
 - `transform` (SPH/main.py:133-144) and `fill_tank` (SPH/main.py:147-181) without
-  trimesh: rotation about the point-cloud centroid, then translation; the tank is a
-  lattice of spacing 2r filling the padded domain up to `height`.
+  trimesh, restating what the trimesh calls compute (trimesh is not installed here and
+  the reference pins no version): the rotation is about the origin (trimesh's
+  center_mass of the face-less mesh the reference builds from a point cloud), then the
+  translation; the tank is the filled voxelisation of a box, a lattice at integer
+  multiples of the pitch 2r.
 - `load_particles` (SPH/main.py:628-691): phases ordered fluid -> static solid ->
   rigid solid -> elastic solid, with the reference's phase_id bases 0 / 1000 / 2000 /
   3000.
@@ -96,7 +99,16 @@ def export_ply_particles(particles: np.ndarray, filename: str) -> None:
 
 
 def transform(points: np.ndarray, cfg: dict) -> np.ndarray:
-    """Rotate about the centroid (rotationAxis, rotationAngle in degrees), then translate."""
+    """`transform` (SPH/main.py:133-144): rotation by rotationAngle degrees about
+    rotationAxis through `trimesh.Trimesh(vertices=points).center_mass`, then the
+    translation, in float64.
+
+    The reference's mesh has vertices and no faces. trimesh's mass properties integrate
+    over the triangles (the divergence-theorem integrals of its `triangles.mass_properties`),
+    so the volume is 0, and for a volume below its zero tolerance trimesh returns a center
+    of mass of (0, 0, 0). The rotation is therefore about the axis through the origin,
+    not through the point cloud's centroid (in the reference's test_transform.json this
+    swings cube.ply, [0.26, 0.74]^3, partly below y = 0)."""
     pts = np.asarray(points, dtype=np.float64)
     ang = cfg.get("rotationAngle")
     axis = cfg.get("rotationAxis")
@@ -105,27 +117,36 @@ def transform(points: np.ndarray, cfg: dict) -> np.ndarray:
         k = k / np.linalg.norm(k)
         th = np.deg2rad(ang)
         K = np.array([[0, -k[2], k[1]], [k[2], 0, -k[0]], [-k[1], k[0], 0]])
-        R = np.eye(3) + math.sin(th) * K + (1 - math.cos(th)) * (K @ K)
-        c = pts.mean(axis=0)
-        pts = (pts - c) @ R.T + c
+        R = math.cos(th) * np.eye(3) + math.sin(th) * K + (1 - math.cos(th)) * np.outer(k, k)
+        pts = pts @ R.T
     t = cfg.get("translation")
     if t is not None:
         pts = pts + np.asarray(t, dtype=np.float64)
     return pts
 
 
-def lattice(lo, hi, spacing) -> np.ndarray:
-    """Points of a regular lattice with the given spacing inside [lo, hi] (inclusive)."""
-    axes = [np.arange(lo[d], hi[d] + 0.5 * spacing, spacing) for d in range(3)]
+def fill_tank(param: Parameter, height: float) -> np.ndarray:
+    """`fill_tank` (SPH/main.py:147-181): `mesh.voxelized(pitch=2r).fill().points` of the
+    box [domain_start + padding, (domain_end - padding) with y = height].
+
+    trimesh's subdivide voxelisation (its default) splits the surface until every edge
+    is shorter than half the pitch, rounds each vertex / pitch to the nearest integer
+    (numpy's round, half to even) and keeps the hit cells; their grid starts at the
+    smallest hit index i0, placed at i0 * pitch. The face coordinates stay exact under
+    the splits, so a box covers the indices round(lo / pitch) .. round(hi / pitch) on
+    each axis. fill() closes the interior (binary hole filling), and the points are the
+    cell centres (i - i0) * pitch + i0 * pitch in C order of the grid (x slowest)."""
+    p = param.particle_radius * 2
+    lo = np.asarray(param.domain_start, np.float64) + param.padding
+    hi = np.asarray(param.domain_end, np.float64) - param.padding
+    hi = np.array([hi[0], height, hi[2]], np.float64)
+    i0 = np.round(lo / p).astype(np.int64)
+    i1 = np.round(hi / p).astype(np.int64)
+    if np.any(i1 < i0):
+        return np.zeros((0, 3), np.float64)
+    axes = [np.arange(i1[d] - i0[d] + 1, dtype=np.float64) * p + float(i0[d]) * p for d in range(3)]
     g = np.meshgrid(*axes, indexing="ij")
     return np.stack([a.ravel() for a in g], axis=1)
-
-
-def fill_tank(param: Parameter, height: float) -> np.ndarray:
-    lo = param.domain_start + param.padding
-    hi = param.domain_end - param.padding
-    hi = np.array([hi[0], height, hi[2]])
-    return lattice(lo, hi, param.particle_radius * 2)
 
 
 # ---------------------------------------------------------------- particle sets

@@ -14,7 +14,11 @@ class Trimesh:
 
     @property
     def center_mass(self):
-        return self.vertices.mean(axis=0)
+        # trimesh integrates the mass properties over the faces; a mesh without faces
+        # has zero volume, for which trimesh returns a zero center of mass
+        if self.faces is None or len(self.faces) == 0:
+            return np.zeros(3)
+        raise NotImplementedError("center_mass of a mesh with faces")
 
     def apply_translation(self, t):
         self.vertices = self.vertices + np.asarray(t, np.float64)

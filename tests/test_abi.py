@@ -161,6 +161,53 @@ def test_scene_geometry_resolves_like_the_reference_layout(tmp_path, monkeypatch
         geometry_path("./data/models/missing.ply", str(path))
 
 
+def test_transform_rotates_about_the_origin_like_trimesh():
+    """transform (SPH/main.py:133-144) rotates about trimesh's center_mass of a mesh
+    without faces, which is the origin, then translates."""
+    import numpy as np
+
+    from nonnewton_b200.scene import transform
+
+    pts = np.array([[1.0, 0.0, 0.0], [0.5, 0.5, 0.2], [2.0, 1.0, -1.0]])
+    out = transform(pts, {"rotationAxis": [0, 0, 2], "rotationAngle": 90, "translation": [0.1, 0.0, 0.0]})
+    R = np.array([[0.0, -1.0, 0.0], [1.0, 0.0, 0.0], [0.0, 0.0, 1.0]])
+    assert np.allclose(out, pts @ R.T + [0.1, 0.0, 0.0], atol=1e-15)
+    # the reference's test_transform.json: cube.ply's [0.26, 0.74]^3 turned 45 degrees
+    # about x through the origin reaches below y = 0
+    cube = np.array([[x, y, z] for x in (0.26, 0.74) for y in (0.26, 0.74) for z in (0.26, 0.74)])
+    turned = transform(cube, {"rotationAxis": [1, 0, 0], "rotationAngle": 45})
+    assert turned[:, 1].min() < -0.3 and np.allclose(turned[:, 0], cube[:, 0])
+    assert np.array_equal(transform(cube, {}), cube)
+
+
+def test_fill_tank_is_the_filled_voxelisation_of_the_box():
+    """fill_tank (SPH/main.py:147-181) as trimesh's voxelized(2r).fill().points: cell
+    centres at integer multiples of the pitch, from round(lo / pitch) to round(hi / pitch)
+    on each axis, x slowest."""
+    import numpy as np
+
+    from nonnewton_b200.config import Parameter, SimConfig
+    from nonnewton_b200.scene import fill_tank
+
+    def param(start, end):
+        conf = {"Configuration": {"domainStart": start, "domainEnd": end, "particleRadius": 0.01,
+                                  "density0": 1000, "simulationMethod": 4, "timeStepSize": 0.004},
+                "FluidParticles": [{}]}
+        return Parameter.from_config(SimConfig(config=conf))
+
+    p = 0.02
+    pts = fill_tank(param([0, 0, 0], [1, 1, 1]), 0.3)  # padding = support radius 0.04
+    i = np.rint(pts / p).astype(int)
+    assert np.allclose(pts, i * p, atol=1e-12)
+    assert [i[:, d].min() for d in range(3)] == [2, 2, 2] and [i[:, d].max() for d in range(3)] == [48, 15, 48]
+    assert len(pts) == 47 * 14 * 47
+    assert np.array_equal(i[:3], [[2, 2, 2], [2, 2, 3], [2, 2, 4]])  # z fastest
+    # a domain start off the pitch: the lattice stays on multiples of the pitch
+    pts = fill_tank(param([0.013, 0.0, 0.0], [1, 1, 1]), 0.3)
+    assert np.isclose(pts[:, 0].min(), 0.06) and np.isclose(pts[:, 0].max(), 0.96)
+    assert len(fill_tank(param([0, 0, 0], [1, 1, 1]), 0.0)) == 0
+
+
 def test_animation_file_reads_as_plyfile_gives_it(tmp_path):
     """An animeFile (SPH/main.py:283-309) is a PLY whose vertices carry frame, dx, dy and
     dz; ASCII and binary files give the same table, each column with its declared type."""
