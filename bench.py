@@ -52,21 +52,21 @@ ALG_BYTES = {
 ALG_BYTES["density_change_np"] = ALG_BYTES["density_change"] + 4 + 4 + 16 + 4 + 4 + 8
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch on the
 # 2.4M-particle dam break, from `ncu --set full` captures of the current kernels.
-NCU_TRAFFIC_2M = {"build_lists": 477530368, "density_adv": 380777216,
+NCU_TRAFFIC_2M = {"build_lists": 477530368, "density_adv": 372967680,
                   "nonpressure": 431172096, "density_factor": 371440896,
                   "density_change": 366368512, "divergence_update": 376274432,
-                  "pressure_update": 383854080, "cg_matvec": 406361600, "density_change_np": 436444416}
+                  "pressure_update": 383854080, "cg_matvec": 401365504, "density_change_np": 436444416}
 # what bounds each kernel instead of DRAM, from its ncu capture on the 2.4M scene:
 # the HBM fraction above is low because none is DRAM-bound
 LIMITER_2M = {
     "build_lists": "instruction issue: 72 % issue active, ~160 exact f32 distance tests per particle, two per packed f32x2 instruction; DRAM 13 %",
-    "density_adv": "L1 data pipe: LSU wavefronts at 84 % of peak (neighbour gathers); DRAM 18 %",
+    "density_adv": "L1 data pipe: LSU wavefronts at 78 % of peak (neighbour gathers); DRAM 19 %",
     "nonpressure": "L1 data pipe and gather latency: LSU wavefronts 62 %, 46 % warps active; DRAM 13 %",
     "density_factor": "L1 data pipe: LSU wavefronts 67 % of peak; DRAM 14 %",
     "density_change": "L1 data pipe: LSU wavefronts 85 % of peak; DRAM 18 %",
     "divergence_update": "L1 data pipe: LSU wavefronts 65 % of peak, 64 % issue active; DRAM 20 %",
     "pressure_update": "L1 data pipe: LSU wavefronts 72 % of peak; DRAM 24 %",
-    "cg_matvec": "L1 data pipe: LSU wavefronts 84 % of peak; DRAM 15 %",
+    "cg_matvec": "L1 data pipe: LSU wavefronts 78 % of peak; DRAM 16 %",
     "density_change_np": "gather latency with the folded force terms: LSU wavefronts 60 %, issue 63 %, "
                          "46 % warps active at 64 registers; DRAM 12 %",
 }
