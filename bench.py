@@ -303,6 +303,65 @@ def run_reference(args):
                               "d2h_bytes_per_step": 0}}))
 
 
+def iterating_measure(args, world, rank, steps=10, presteps=100):
+    """The 2.4M-particle scene at a state whose solver loops iterate: the fluid packed to
+    0.92 of its lattice spacing (starting near 1,027 kg/m^3) after `presteps` untimed
+    steps of its fall (through the object API's run(), which grows the neighbour lists
+    as the packing clusters), then `steps` steps with the state resident, timed with
+    CUDA events (max over ranks), and each solver loop's cost per body from its kernels'
+    own times on the same slots."""
+    import torch
+
+    from nonnewton_b200 import scene as S
+    from nonnewton_b200 import sph
+    from nonnewton_b200.config import SimConfig
+
+    sc = S.roofline_scene(seed=0, spacing_factor=0.92)
+    n = sc.particles.n
+    m = sph.initialize(SimConfig(config=sc.config), particles=sc.particles, quirks=sc.param.quirks)
+    solver = sph.build_solver()
+    solver.initialize()
+    solver.run(presteps)
+    solver.stats()  # the run's last status check
+    eng = m.engine
+    eng.step(max(args.warmup, 1), sync=False, resume=True)
+    torch.cuda.synchronize()
+    barrier(world)
+    stream = torch.cuda.current_stream()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    eng.step(steps, sync=False, resume=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1), world)
+    st = eng.stats(0)
+    folded = bool(st["nonpressure_folded"])
+    kms = {k: eng.time_kernel(KERNEL_IDS[k], reps=10)
+           for k in ("pressure_update", "density_adv", "divergence_update", "density_change", "density_change_np",
+                     "cg_matvec")}
+    eng.close()
+    sph.meta.pd = sph.meta.engine = sph.meta.ns = sph.meta.solver = None
+    del m, solver
+    torch.cuda.empty_cache()
+    bodies = {"divergence": st["iterations_v"] + 1, "pressure": st["iterations"] + 1, "cg": st["cg_iterations"]}
+    return {
+        "workload": f"roofline_2m with the fluid packed to 0.92 of its spacing, after {presteps} steps",
+        "particles": n, "steps": steps, "ms_per_step": ms / steps,
+        "value": float(n) * steps * world / (ms / 1e3), "unit": "particle-steps/s",
+        "loop_bodies_per_step": bodies, "max_neighbors_seen": st["max_neighbors_seen"],
+        "avg_density_err_pct": 100.0 * st["avg_density_err"] / sc.param.density0,
+        "nonpressure": "in the divergence loop's last density change" if folded else "force pass",
+        "kernel_ms": kms,
+        # one body of each loop: its neighbour passes (the loop checks add a few us)
+        "ms_per_loop_body": {"pressure": kms["pressure_update"] + kms["density_adv"],
+                             "divergence": kms["divergence_update"] + kms["density_change"],
+                             "divergence_last (non-pressure terms folded in)":
+                                 kms["divergence_update"] + kms["density_change_np"],
+                             "cg_matvec": kms["cg_matvec"]},
+    }
+
+
 def served_measure(args, world, rank):
     """The mixed served workload: one seeded stream of Poisson-arriving dam-break
     requests (fluid count log-uniform in [2k, 128k], box at 50 % fill, Cross law with
@@ -743,16 +802,20 @@ def run_ours(args):
     e2e_ms = max_over_ranks(t0.elapsed_time(t1), world)
     e2e_val = total_ps / (e2e_ms / 1e3)
     peaks, peak_kind = load_peaks()
-    served = None
-    if args.workload == "roofline_2m" and not args.no_served:
-        # the headline comparison of the served form with the plain loop, on the mixed
-        # workload, in the same run (every rank takes part: it has collectives)
+    served = iterating = None
+    if args.workload == "roofline_2m" and not (args.no_served and args.no_iterating):
         del st_x, st_v, st_o, h_x, h_v, h_out
         eng.close()
         sph.meta.pd = sph.meta.engine = sph.meta.ns = sph.meta.solver = None
         del m, pd, solver
         torch.cuda.empty_cache()
-        served = served_measure(args, world, rank)["block"]
+        if not args.no_iterating:
+            # the same scene at a state whose solver loops iterate several times per step
+            iterating = iterating_measure(args, world, rank)
+        if not args.no_served:
+            # the headline comparison of the served form with the plain loop, on the mixed
+            # workload, in the same run (every rank takes part: it has collectives)
+            served = served_measure(args, world, rank)["block"]
     if rank != 0:
         if world > 1:
             torch.distributed.destroy_process_group()
@@ -793,6 +856,8 @@ def run_ours(args):
                 "copies": "pinned host <-> device staging on two copy streams, overlapped with the steps"},
         "clocks": cs.summary(),
     }
+    if iterating is not None:
+        line["iterating"] = iterating
     if served is not None:
         line["served"] = served
     if not args.no_cpu_baseline and world == 1:  # the CPU baseline is an N=1 measurement
@@ -821,6 +886,8 @@ def main():
     ap.add_argument("--chunk", type=int, default=10, help="steps between admissions")
     ap.add_argument("--plain-sample", type=int, default=48)
     ap.add_argument("--no-served", action="store_true", help="leave the served block out of the default line")
+    ap.add_argument("--no-iterating", action="store_true",
+                    help="leave the iterating-state block (packed scene after 100 steps) out of the default line")
     ap.add_argument("--presteps", type=int, default=0,
                     help="untimed steps before the warm-up (to reach a later state of the scene)")
     ap.add_argument("--no-served-autotune", action="store_true",
