@@ -10,6 +10,7 @@ not on test-sized stand-ins:
   - shear-thinning drop, 135,201 particles (Cross law, implicit viscosity CG, CFL),
     20 steps in lockstep: the same, plus CG iteration counts within one and the CFL
     time step equal;
+  - the 2.4M-particle roofline scene: three steps in lockstep, the same checks;
   - fluid + elastic block, 175,870 particles, the full 200 steps: after every step
     the neighbour lists of all particles, searched on the current positions, equal
     the oracle's search (the reference's rule p_i != p_j and |x_i - x_j| < h in f32,
@@ -78,6 +79,18 @@ def test_shear_thinning_drop_135k_lockstep(cuda_lib):
     m, worst, iters = _lockstep(sc, 20, cg=True)
     assert sum(i[2] for i in iters) > 0  # the viscosity CG iterated
     print("drop 135k, 20 steps, worst per-field error:", {k: f"{v:.1e}" for k, v in worst.items()})
+
+
+def test_roofline_2m_lockstep_3_steps(cuda_lib):
+    """The 2.4M-particle scene itself (2,000,000 fluid in a 400,002-particle box; Carreau
+    law, implicit viscosity CG): three steps in lockstep with the FP32 oracle, with the
+    same checks as the drop (iteration counts equal, CG counts within one, dt equal,
+    every field within 1e-4 of its scale). The oracle takes about 1.5 s per step on 16
+    host threads."""
+    sc = S.roofline_scene(seed=0)
+    assert sc.particles.n == 2400002 and sc.particles.n_fluid == 2000000
+    m, worst, iters = _lockstep(sc, 3, cg=True)
+    print("roofline 2.4M, 3 steps, worst per-field error:", {k: f"{v:.1e}" for k, v in worst.items()})
 
 
 def _cutoff_tie(x, h, i, j, ulps=4):
