@@ -107,11 +107,6 @@ def make_workload(name, seed=0):
 
     if name == "roofline_2m":
         return [S.roofline_scene(seed=seed)]
-    if name == "roofline_2m_packed":
-        # the same scene with the fluid packed to 0.92 of its spacing: after --presteps
-        # of the column's fall the pressure solve iterates several times per step (for
-        # per-iteration costs and launch lists)
-        return [S.roofline_scene(seed=seed, spacing_factor=0.92)]
     if name == "dam_break":
         return [S.dam_break(seed=seed)]
     if name == "shear_thinning_drop":
@@ -303,20 +298,20 @@ def run_reference(args):
                               "d2h_bytes_per_step": 0}}))
 
 
-def iterating_measure(args, world, rank, steps=10, presteps=100):
-    """The 2.4M-particle scene at a state whose solver loops iterate: the fluid packed to
-    0.92 of its lattice spacing (starting near 1,027 kg/m^3) after `presteps` untimed
-    steps of its fall (through the object API's run(), which grows the neighbour lists
-    as the packing clusters), then `steps` steps with the state resident, timed with
-    CUDA events (max over ranks), and each solver loop's cost per body from its kernels'
-    own times on the same slots."""
+def iterating_measure(args, world, rank, steps=10, presteps=600):
+    """The 2.4M-particle scene at a state whose solver loops iterate: after `presteps`
+    untimed steps (0.3 s of simulated time), the fluid, which starts as a lattice below
+    the rest density, has settled to it under gravity and the pressure solve runs
+    several bodies per step. Then `steps` steps with the state resident, timed with CUDA
+    events (max over ranks), and each solver loop's cost per body from its kernels' own
+    times on the same slots."""
     import torch
 
     from nonnewton_b200 import scene as S
     from nonnewton_b200 import sph
     from nonnewton_b200.config import SimConfig
 
-    sc = S.roofline_scene(seed=0, spacing_factor=0.92)
+    sc = S.roofline_scene(seed=0)
     n = sc.particles.n
     m = sph.initialize(SimConfig(config=sc.config), particles=sc.particles, quirks=sc.param.quirks)
     solver = sph.build_solver()
@@ -346,7 +341,7 @@ def iterating_measure(args, world, rank, steps=10, presteps=100):
     torch.cuda.empty_cache()
     bodies = {"divergence": st["iterations_v"] + 1, "pressure": st["iterations"] + 1, "cg": st["cg_iterations"]}
     return {
-        "workload": f"roofline_2m with the fluid packed to 0.92 of its spacing, after {presteps} steps",
+        "workload": f"roofline_2m after {presteps} steps (settled to the rest density)",
         "particles": n, "steps": steps, "ms_per_step": ms / steps,
         "value": float(n) * steps * world / (ms / 1e3), "unit": "particle-steps/s",
         "loop_bodies_per_step": bodies, "max_neighbors_seen": st["max_neighbors_seen"],
@@ -887,7 +882,7 @@ def main():
     ap.add_argument("--plain-sample", type=int, default=48)
     ap.add_argument("--no-served", action="store_true", help="leave the served block out of the default line")
     ap.add_argument("--no-iterating", action="store_true",
-                    help="leave the iterating-state block (packed scene after 100 steps) out of the default line")
+                    help="leave the iterating-state block (the scene after 600 steps) out of the default line")
     ap.add_argument("--presteps", type=int, default=0,
                     help="untimed steps before the warm-up (to reach a later state of the scene)")
     ap.add_argument("--no-served-autotune", action="store_true",

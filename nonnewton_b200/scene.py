@@ -405,16 +405,13 @@ def fluid_elastic(seed=0, n_el=40, r=0.01, quirks=False, steps=200) -> Scene:
     return _make("fluid_elastic", conf, phases, steps, quirks)
 
 
-def roofline_scene(seed=0, counts=(200, 100, 100), r=0.005, quirks=False, steps=50, implicit=True,
-                   spacing_factor=1.0) -> Scene:
+def roofline_scene(seed=0, counts=(200, 100, 100), r=0.005, quirks=False, steps=50, implicit=True) -> Scene:
     """2M fluid particles (200 x 100 x 100 at 0.01 m, the long side along x) in the
     corner of a 4 x 2 x 2 m one-layer boundary box (401*201*201 - 399*199*199 =
     400,002 particles); Carreau mu0=1, mu_inf=0.001, lambda=0.5 (K = lambda^2 in the
-    reference form), n=0.6; h = 0.02 m. `spacing_factor` < 1 packs the fluid lattice
-    closer: the lattice at 2r sits near 800 kg/m^3 (volume0 = 0.8 (2r)^3), so the plain
-    scene has no pressure for hundreds of steps; at 0.92 it starts near 1,027 kg/m^3,
-    and once the column falls the pressure solve iterates several times per step (the
-    oracle on the same block at r = 0.02: 3 to 5 iterations per step after 80 steps)."""
+    reference form), n=0.6; h = 0.02 m, dt = 0.5 ms. The lattice at 2r sits near
+    800 kg/m^3 (volume0 = 0.8 (2r)^3), so the fluid first settles under gravity: the
+    pressure solve acts after about 400 steps and then runs several bodies per step."""
     h = 4 * r
     sp = 2 * r
     rng = np.random.default_rng(seed)
@@ -427,13 +424,12 @@ def roofline_scene(seed=0, counts=(200, 100, 100), r=0.005, quirks=False, steps=
             "FluidParticles": [fcfg], "SolidParticles": [{"solidType": "STATIC"}]}
 
     def phases(param):
-        fl = block([h + sp] * 3, counts, sp * spacing_factor, 1e-4 * 0.5, rng)
+        fl = block([h + sp] * 3, counts, sp, 1e-4 * 0.5, rng)
         bd = box_shell([h] * 3, list(h + B), sp)
         return [PhaseInfo(uid=0, material=FLUID, is_dynamic=True, pos=fl),
                 PhaseInfo(uid=1000, material=SOLID, is_dynamic=False, pos=bd, solid_type=STATIC)]
 
-    name = "roofline_2m" if spacing_factor == 1.0 else f"roofline_2m_packed{spacing_factor:g}"
-    return _make(name, conf, phases, steps, quirks)
+    return _make("roofline_2m", conf, phases, steps, quirks)
 
 
 def served_request(rng: np.random.Generator, r=0.01, steps=100) -> Scene:
