@@ -293,7 +293,9 @@ enum nn_kernel_id {
 /* Average duration in ms of `reps` launches of one kernel on the current slots,
    timed with CUDA events on the context stream (measurement hook, no reference
    counterpart). Solver masks are set to "iterating" first, so the kernel does its
-   full work; it mutates solver scratch and, for the update kernels, velocities. */
+   full work; it mutates solver scratch and, for the update kernels, velocities.
+   NN_K_BUILD_LISTS first re-sorts the slots by their current positions (one search),
+   as a step's build sees them, and times the list build alone. */
 int nn_time_kernel(nn_ctx* ctx, int32_t kernel, int32_t reps, float* ms_out);
 
 /* Neighbour search that allocates no device memory. No counterpart in the

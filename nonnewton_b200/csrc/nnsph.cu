@@ -1085,6 +1085,14 @@ int nn_time_kernel(nn_ctx* c, int32_t kernel, int32_t reps, float* ms_out) {
   if (!c->searched) return fail(c, NN_ERR_STATE, "run a step first");
   c->resident_ok = false;  // the timed update kernels change the slots' velocities
   cudaStream_t s = run_stream(c);
+  if (kernel == NN_K_BUILD_LISTS) {
+    // the slots of the last search are sorted by the positions before its step's
+    // advection: sort the current ones again (from the slots), so the timed builds see
+    // the cell ranges a step's build sees
+    CK(cudaMemsetAsync(c->d_src_flag, 0, sizeof(int32_t), s));
+    RC(launch1(c, s, k_step_reset, make_dev(c, c->cur)));
+    RC(enq_search(c, s));
+  }
   Dev d = make_dev(c, c->cur);
   RC(launch1(c, s, k_force_active, d));
   cudaEvent_t e0, e1;
