@@ -87,7 +87,7 @@ struct nn_ctx {
   int32_t* slot_of_id = nullptr;
   uint32_t *key = nullptr, *rank = nullptr, *cell_count = nullptr, *tile_sums = nullptr;
   int32_t *src = nullptr, *nbr = nullptr, *nbr_cnt = nullptr;
-  real4 *cg_x = nullptr, *cg_r = nullptr, *cg_z = nullptr, *cg_p = nullptr, *cg_Ap = nullptr, *cg_b = nullptr;
+  real4 *cg_x = nullptr, *cg_r = nullptr, *cg_z = nullptr, *cg_p = nullptr, *cg_Ap = nullptr;
   real2* cg_aux = nullptr;
   real* cg_pinv = nullptr;
   int el_cap = 64, el_stride = 0;
@@ -170,7 +170,7 @@ static Dev make_dev(nn_ctx* c, int cur) {
   d.max_nb = c->max_nb;
   d.srn = c->srn;
   d.mu = c->mu;
-  d.cg_x = c->cg_x; d.cg_r = c->cg_r; d.cg_z = c->cg_z; d.cg_p = c->cg_p; d.cg_Ap = c->cg_Ap; d.cg_b = c->cg_b;
+  d.cg_x = c->cg_x; d.cg_r = c->cg_r; d.cg_z = c->cg_z; d.cg_p = c->cg_p; d.cg_Ap = c->cg_Ap;
   d.cg_aux = c->cg_aux;
   d.cg_pinv = c->cg_pinv;
   d.el_id = c->el_id; d.el_slot = c->el_slot; d.e_of_id = c->e_of_id; d.el_x0 = c->el_x0;
@@ -663,7 +663,7 @@ int nn_ctx_create(int32_t max_particles, int32_t max_scenes, int32_t max_neighbo
   AL(c->alpha, N); AL(c->rho_adv, N); AL(c->kappa, N); AL(c->srn, N); AL(c->mu, N);
   AL(c->slot_of_id, N); AL(c->key, N); AL(c->rank, N); AL(c->src, N);
   AL(c->nbr, N * (size_t)max_neighbors); AL(c->nbr_cnt, N);
-  AL(c->cg_x, N); AL(c->cg_r, N); AL(c->cg_z, N); AL(c->cg_p, N); AL(c->cg_Ap, N); AL(c->cg_b, N); AL(c->cg_aux, N);
+  AL(c->cg_x, N); AL(c->cg_r, N); AL(c->cg_z, N); AL(c->cg_p, N); AL(c->cg_Ap, N); AL(c->cg_aux, N);
   AL(c->cg_pinv, 6 * N);
   AL(c->e_of_id, N);
   AL(c->d_any, 1); AL(c->d_body, 4);
@@ -698,7 +698,7 @@ int nn_ctx_destroy(nn_ctx* c) {
   }
   void* bufs[] = {c->d_n, c->d_sc, c->d_dyn, c->d_acc, c->d_scene_of_id, c->d_src_flag, c->acc4, c->alpha,
                   c->rho_adv, c->kappa, c->srn, c->mu, c->slot_of_id, c->key, c->rank, c->src, c->nbr,
-                  c->nbr_cnt, c->cg_x, c->cg_r, c->cg_z, c->cg_p, c->cg_Ap, c->cg_b, c->cg_aux, c->cg_pinv,
+                  c->nbr_cnt, c->cg_x, c->cg_r, c->cg_z, c->cg_p, c->cg_Ap, c->cg_aux, c->cg_pinv,
                   c->e_of_id, c->d_any, c->d_body, c->cell_count, c->tile_sums};
   for (void* b : bufs) cudaFree(b);
   free_elastic(c);

@@ -768,7 +768,6 @@ __global__ void NN_REGS64 k_cg_setup(Dev d) {
       for (int k = 0; k < 6; ++k) d.cg_pinv[(size_t)k * d.cap + i] = P[k];
       const real3 r = b - Av;
       const real3 z = sym_apply(P, r);
-      d.cg_b[i] = make_real4(b.x, b.y, b.z, 0.f);
       d.cg_x[i] = make_real4(vi.x, vi.y, vi.z, 0.f);
       d.cg_r[i] = make_real4(r.x, r.y, r.z, 0.f);
       d.cg_z[i] = make_real4(z.x, z.y, z.z, 0.f);
