@@ -46,6 +46,8 @@ ALG_BYTES = {
     "cg_matvec": 16 + 16 + 8 + 4 + 4 + 16,        # pos4, p, aux2, mass, flags -> Ap
     "nonpressure": 4 + 16 + 16 + 4 + 4 + 16 + 4 + 4 + 8,  # flags, pos4, vel4, mass, dens -> acc4, srn, mu, aux2
     "build_lists": 16 + 4 + 4,                    # pos4, flags -> count; + 4 B per list entry (added live)
+    # flags, pos4, vel4, aux2, mass, dens -> x, r, z, p, matvec positions (float4 each), preconditioner 24
+    "cg_setup": 4 + 16 + 16 + 8 + 4 + 4 + 5 * 16 + 24,
 }
 # the density change that also computes the non-pressure terms (run in the divergence
 # loop's predicted last body) reads mass and density besides and writes acc4, srn, mu, aux2
@@ -55,7 +57,8 @@ ALG_BYTES["density_change_np"] = ALG_BYTES["density_change"] + 4 + 4 + 16 + 4 + 
 NCU_TRAFFIC_2M = {"build_lists": 477530368, "density_adv": 372967680,
                   "nonpressure": 431172096, "density_factor": 371440896,
                   "density_change": 366368512, "divergence_update": 376274432,
-                  "pressure_update": 383854080, "cg_matvec": 401365504, "density_change_np": 436444416}
+                  "pressure_update": 383854080, "cg_matvec": 401365504, "density_change_np": 436444416,
+                  "cg_setup": 570425344}
 # what bounds each kernel instead of DRAM, from its ncu capture on the 2.4M scene:
 # the HBM fraction above is low because none is DRAM-bound
 LIMITER_2M = {
@@ -67,11 +70,13 @@ LIMITER_2M = {
     "divergence_update": "L1 data pipe: LSU wavefronts 65 % of peak, 64 % issue active; DRAM 20 %",
     "pressure_update": "L1 data pipe: LSU wavefronts 72 % of peak; DRAM 24 %",
     "cg_matvec": "L1 data pipe: LSU wavefronts 78 % of peak; DRAM 16 %",
+    "cg_setup": "L1 data pipe: LSU wavefronts 83 % of peak; DRAM 19 %",
     "density_change_np": "gather latency with the folded force terms: LSU wavefronts 60 %, issue 63 %, "
                          "46 % warps active at 64 registers; DRAM 12 %",
 }
 KERNEL_IDS = {"pressure_update": 0, "density_adv": 1, "divergence_update": 2, "density_change": 3,
-              "density_factor": 4, "build_lists": 5, "cg_matvec": 6, "nonpressure": 7, "density_change_np": 8}
+              "density_factor": 4, "build_lists": 5, "cg_matvec": 6, "nonpressure": 7, "density_change_np": 8,
+              "cg_setup": 9}
 
 
 def step_bytes(iters_v, iters_p, iters_cg, f_el, implicit):
@@ -727,7 +732,7 @@ def run_ours(args):
     kms = {}
     for k in ("pressure_update", "density_adv", "build_lists", "density_factor", "divergence_update",
               "density_change") + (("density_change_np",) if folded else ("nonpressure",)) + \
-             (("cg_matvec",) if implicit else ()):
+             (("cg_setup", "cg_matvec") if implicit else ()):
         kms[k] = eng.time_kernel(KERNEL_IDS[k], reps=10)
     # launches per step of each timed kernel at the iteration counts of the last step;
     # the dominant kernel is the one with the largest time per step
@@ -735,7 +740,7 @@ def run_ours(args):
     per_step = {"build_lists": 1, "density_factor": 1, "nonpressure": 0 if folded else 1,
                 "density_adv": it_p + 1, "pressure_update": it_p, "divergence_update": it_v,
                 "density_change": it_v - (1 if folded else 0), "density_change_np": 1 if folded else 0,
-                "cg_matvec": st["cg_iterations"]}
+                "cg_matvec": st["cg_iterations"], "cg_setup": 1}
     dom = max(kms, key=lambda k: kms[k] * per_step[k])
     num_nb, _ = eng.neighbors(n, 1)
     entries = int(num_nb.sum().item())
@@ -829,7 +834,7 @@ def run_ours(args):
         "data": "synthetic (seeded numpy scene generator)",
         "config": workload_config(sc, world),
         "launch": {"step_graph": "host-driven loops" if args.host_loop else "CUDA graph with while-node solver loops",
-                   "tuning": tuning or {"block": 128, "unroll": 2, "cell_factor": 1},
+                   "tuning": tuning or {"block": 128, "unroll": 0, "cell_factor": 1, "x_split": 2},
                    "nonpressure": "in the divergence loop's last density change" if folded else "force pass"},
         "autotune_ms_per_step": tune_ms,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
@@ -888,7 +893,7 @@ def main():
     ap.add_argument("--no-served-autotune", action="store_true",
                     help="serve with the default launch shape instead of tuning it on the first packing")
     ap.add_argument("--autotune", action="store_true", help="pick block size, unroll and cell factor first")
-    ap.add_argument("--tuning", default=None, help="block,unroll,cell_factor[,x_split] (e.g. 128,2,1,2)")
+    ap.add_argument("--tuning", default=None, help="block,unroll,cell_factor[,x_split] (e.g. 128,0,1,2; unroll 0: each pass its own depth)")
     ap.add_argument("--clocks-dir", default=tempfile.gettempdir(),
                     help="where the nvidia-smi clock samples of the timed region go (clocks_rank<r>.csv)")
     ap.add_argument("--host-loop", action="store_true",

@@ -288,6 +288,7 @@ enum nn_kernel_id {
   NN_K_CG_MATVEC,             /* implicit viscosity matrix-vector product */
   NN_K_NONPRESSURE,           /* surface tension + explicit viscosity */
   NN_K_DENSITY_CHANGE_NP,     /* compute_density_change with the non-pressure terms */
+  NN_K_CG_SETUP,              /* implicit viscosity setup: A v, diagonal blocks, first residual */
   NN_K_COUNT
 };
 /* Average duration in ms of `reps` launches of one kernel on the current slots,
@@ -332,7 +333,8 @@ int nn_neighbors_noalloc(const float* x, int32_t n, const double* domain_start, 
 int nn_set_block_size(nn_ctx* ctx, int32_t threads);
 
 /* All tuning knobs at once (0 = default): threads per block of the neighbour passes
-   (32..1024), neighbour chains each thread keeps in flight (2, 4 or 8), and the cell
+   (32..1024), neighbour chains each thread keeps in flight (1, 2 or 4 for every pass;
+   0 = each pass its own measured depth, the default), and the cell
    factor f (cells of edge h / f searched with a (2f+1)-cell stencil; 1 or 2). A new
    cell factor takes effect at the next nn_set_scenes, which must follow. */
 int nn_set_tuning(nn_ctx* ctx, int32_t block, int32_t unroll, int32_t cell_factor);

@@ -58,7 +58,7 @@ NN_HERSCHEL_BULKLEY = 6
  NN_PASS_SUBSTEP, NN_PASS_RIGID, NN_PASS_COUNT) = range(16)
 
 (NN_K_PRESSURE_UPDATE, NN_K_DENSITY_ADV, NN_K_DIVERGENCE_UPDATE, NN_K_DENSITY_CHANGE, NN_K_DENSITY_FACTOR,
- NN_K_BUILD_LISTS, NN_K_CG_MATVEC, NN_K_NONPRESSURE, NN_K_DENSITY_CHANGE_NP, NN_K_COUNT) = range(10)
+ NN_K_BUILD_LISTS, NN_K_CG_MATVEC, NN_K_NONPRESSURE, NN_K_DENSITY_CHANGE_NP, NN_K_CG_SETUP, NN_K_COUNT) = range(11)
 
 NN_STEP_SYNC_STATE = 1 << 0
 NN_STEP_HOST_LOOP = 1 << 1

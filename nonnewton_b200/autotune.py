@@ -2,7 +2,7 @@
 
 Knobs (see nn_set_tuning, nn_set_x_split): threads per block of the neighbour
 passes, neighbour chains each thread keeps in flight ("unroll": how many neighbours of
-a particle a thread gathers at once), the cell factor f (cells of edge h / f with a
+a particle a thread gathers at once; 0 gives each pass its own measured depth), the cell factor f (cells of edge h / f with a
 (2f+1)-cell stencil) and the x split (x cells per cell edge). The tuner times each candidate on the actual batch, from the
 batch's initial state after a few untimed steps, and keeps the fastest; results are
 cached per device, scene mix and particle count (rounded to a power of two).
@@ -16,12 +16,12 @@ import os
 import torch
 
 DEFAULT_CANDIDATES = ([dict(block=b, unroll=u, cell_factor=1, x_split=x)
-                       for b, u, x in itertools.product((128, 256, 512), (2, 4, 8), (1, 2))]
+                       for b, u, x in itertools.product((128, 256, 512), (0, 1, 2), (1, 2))]
                       + [dict(block=b, unroll=u, cell_factor=2, x_split=1)
-                         for b, u in itertools.product((128, 256, 512), (2, 4, 8))])
+                         for b, u in itertools.product((128, 256, 512), (0, 1, 2))])
 
 # a shorter list for tuning inside a served run (block x chains, cell factor 1)
-QUICK_CANDIDATES = [dict(block=b, unroll=u, cell_factor=1) for b, u in itertools.product((128, 256), (2, 4))]
+QUICK_CANDIDATES = [dict(block=b, unroll=u, cell_factor=1) for b, u in itertools.product((128, 256), (0, 2))]
 
 _cache: dict = {}
 

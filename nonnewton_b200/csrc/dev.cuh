@@ -51,7 +51,9 @@ struct Dev {
   real* srn;
   real* mu;
   // implicit viscosity CG (slot order)
-  real4* cg_x; real4* cg_r; real4* cg_z; real4* cg_p; real4* cg_Ap;
+  real4* cg_x; real4* cg_r; real4* cg_z; real4* cg_Ap;
+  real4* cg_p;                 // search direction; w = mu_i (read by the matvec)
+  real4* cg_pos;               // matvec positions: fluid (x_i, m_i / rho_i), solid (x_i, -V_i) as pos
   real2* cg_aux;               // fluid: mu_i, m_i / rho_i; solid: 0, 1 if dynamic
   real* cg_pinv;               // [6][cap] symmetric inverse of the diagonal block
   // elasticity (e-space: elastic particles in id order)

@@ -41,10 +41,11 @@ cudaError_t dalloc(T** p, size_t count) {
 }  // namespace
 
 // Default launch shape of the neighbour passes: the autotuner's pick for the
-// 2.4M-particle dam break on B200 (128 threads, 2 neighbour chains per thread was
-// the fastest of block {128, 256, 512} x chains {2, 4, 8} x cell factor {1, 2}).
+// 2.4M-particle dam break on B200 (128 threads was the fastest of {128, 256, 512};
+// cell factor 1 of {1, 2}). Neighbour chains in flight per thread (`unroll`): 0 gives
+// each pass its own depth (U_* below); 1, 2 or 4 sets all of them.
 #define NN_DEFAULT_BLOCK 128
-#define NN_DEFAULT_UNROLL 2
+#define NN_DEFAULT_UNROLL 0
 #define NN_DEFAULT_XSPLIT 2  // 2.4M scene: list build 0.66 -> 0.60 ms, step -0.7 % (x split 3 and 4: slower steps)
 
 struct nn_ctx {
@@ -57,7 +58,7 @@ struct nn_ctx {
   std::string err;
   int64_t launches = 0;
   int block = NN_DEFAULT_BLOCK;
-  int unroll = NN_DEFAULT_UNROLL;      // neighbour chains in flight per thread (2, 4, 8)
+  int unroll = NN_DEFAULT_UNROLL;      // neighbour chains in flight per thread (1, 2, 4; 0: per pass)
   int cell_factor = 1;                 // cells of edge h / cell_factor
   int x_split = NN_DEFAULT_XSPLIT;     // x cells per cell edge
   // state binding and scenes
@@ -87,7 +88,7 @@ struct nn_ctx {
   int32_t* slot_of_id = nullptr;
   uint32_t *key = nullptr, *rank = nullptr, *cell_count = nullptr, *tile_sums = nullptr;
   int32_t *src = nullptr, *nbr = nullptr, *nbr_cnt = nullptr;
-  real4 *cg_x = nullptr, *cg_r = nullptr, *cg_z = nullptr, *cg_p = nullptr, *cg_Ap = nullptr;
+  real4 *cg_x = nullptr, *cg_r = nullptr, *cg_z = nullptr, *cg_p = nullptr, *cg_Ap = nullptr, *cg_pos = nullptr;
   real2* cg_aux = nullptr;
   real* cg_pinv = nullptr;
   int el_cap = 64, el_stride = 0;
@@ -170,7 +171,7 @@ static Dev make_dev(nn_ctx* c, int cur) {
   d.max_nb = c->max_nb;
   d.srn = c->srn;
   d.mu = c->mu;
-  d.cg_x = c->cg_x; d.cg_r = c->cg_r; d.cg_z = c->cg_z; d.cg_p = c->cg_p; d.cg_Ap = c->cg_Ap;
+  d.cg_x = c->cg_x; d.cg_r = c->cg_r; d.cg_z = c->cg_z; d.cg_p = c->cg_p; d.cg_Ap = c->cg_Ap; d.cg_pos = c->cg_pos;
   d.cg_aux = c->cg_aux;
   d.cg_pinv = c->cg_pinv;
   d.el_id = c->el_id; d.el_slot = c->el_slot; d.e_of_id = c->e_of_id; d.el_x0 = c->el_x0;
@@ -221,9 +222,21 @@ static int launch1(nn_ctx* c, cudaStream_t s, void (*k)(KArgs...), Args... args)
   return NN_OK;
 }
 
-// The instantiation of a neighbour kernel for the context's neighbour-batch depth.
-#define KU(k) (c->unroll == 8 ? &k<8> : c->unroll == 2 ? &k<2> : &k<4>)
-#define KU2(k, B) (c->unroll == 8 ? &k<8, B> : c->unroll == 2 ? &k<2, B> : &k<4, B>)
+// Each pass's neighbour-batch depth at unroll 0, measured against the other depth on
+// the 2.4M-particle dam break (early and settled states): the update passes, with
+// little arithmetic per pair, keep 2 neighbours in flight (at 1: k_pressure_update
+// +17-31 %, k_density_adv +3 %); the passes with more arithmetic per pair gather one
+// at a time, with 8 list entries loaded ahead (k_density_change_np -9 %, k_cg_setup
+// -7 %, k_density_factor -6 %, k_cg_matvec -4 %, k_density_change -2 %). The force
+// pass keeps 2 (the 23k-particle dam break: 29.0 against 31.0 us at 1).
+enum : int {
+  U_PRESSURE_UPDATE = 2, U_DENSITY_ADV = 2, U_DIVERGENCE_UPDATE = 2, U_BOUNDARY_VOLUME = 2, U_FORCES = 2,
+  U_DENSITY_FACTOR = 1, U_DENSITY_CHANGE = 1, U_DENSITY_CHANGE_NP = 1, U_CG_SETUP = 1, U_CG_MATVEC = 1
+};
+static inline int ku(const nn_ctx* c, int pass_default) { return c->unroll ? c->unroll : pass_default; }
+// The instantiation of a neighbour kernel for the context's (or the pass's) batch depth.
+#define KU(k, def) (ku(c, def) == 4 ? &k<4> : ku(c, def) == 2 ? &k<2> : &k<1>)
+#define KU2(k, B, def) (ku(c, def) == 4 ? &k<4, B> : ku(c, def) == 2 ? &k<2, B> : &k<1, B>)
 
 // The force pass instance for the batch's terms (c->forces_feat) and batch depth.
 template <int U, int... F>
@@ -234,7 +247,8 @@ static void (*forces_pick(int feat, std::integer_sequence<int, F...>))(Dev, int)
 static void (*forces_kernel(const nn_ctx* c))(Dev, int) {
   using All = std::make_integer_sequence<int, 16>;
   const int f = c->forces_feat & 15;
-  return c->unroll == 8 ? forces_pick<8>(f, All{}) : c->unroll == 2 ? forces_pick<2>(f, All{}) : forces_pick<4>(f, All{});
+  const int u = ku(c, U_FORCES);
+  return u == 4 ? forces_pick<4>(f, All{}) : u == 2 ? forces_pick<2>(f, All{}) : forces_pick<1>(f, All{});
 }
 
 #define RC(x)                 \
@@ -341,13 +355,13 @@ static int enq_divergence(nn_ctx* c, cudaStream_t s, bool fused) {
   if (!fused) RC(launch1(c, s, k_solver_begin, d, 0));
   RC(solver_loop(c, s, false,
                  [&](cudaStream_t q) {
-                   return fused ? NN_OK : launch(c, q, KU(k_density_change), B, c->n, make_dev(c, c->cur), 0, 0);
+                   return fused ? NN_OK : launch(c, q, KU(k_density_change, U_DENSITY_CHANGE), B, c->n, make_dev(c, c->cur), 0, 0);
                  },
                  [&](cudaStream_t q) {
                    Dev e = make_dev(c, c->cur);
-                   RC(launch(c, q, KU(k_divergence_update), B, c->n, e));
-                   RC(launch(c, q, KU(k_density_change), B, c->n, e, 1, np ? 1 : 0));
-                   if (np) RC(launch(c, q, KU(k_density_change_np), B, c->n, e, 1, 1));
+                   RC(launch(c, q, KU(k_divergence_update, U_DIVERGENCE_UPDATE), B, c->n, e));
+                   RC(launch(c, q, KU(k_density_change, U_DENSITY_CHANGE), B, c->n, e, 1, np ? 1 : 0));
+                   if (np) RC(launch(c, q, KU(k_density_change_np, U_DENSITY_CHANGE_NP), B, c->n, e, 1, 1));
                    return launch1(c, q, k_solver_check, e, 0, np ? 1 : 0);
                  }));
   return fused ? NN_OK : launch(c, s, k_alpha_times_dt, 256, c->n, d);
@@ -361,12 +375,12 @@ static int enq_pressure(nn_ctx* c, cudaStream_t s, int init_mode) {
   RC(launch1(c, s, k_solver_begin, d, 1));
   return solver_loop(c, s, false,
                      [&](cudaStream_t q) {
-                       return launch(c, q, KU(k_density_adv), B, c->n, make_dev(c, c->cur), init_mode);
+                       return launch(c, q, KU(k_density_adv, U_DENSITY_ADV), B, c->n, make_dev(c, c->cur), init_mode);
                      },
                      [&](cudaStream_t q) {
                        Dev e = make_dev(c, c->cur);
-                       RC(launch(c, q, KU(k_pressure_update), B, c->n, e));
-                       RC(launch(c, q, KU(k_density_adv), B, c->n, e, 1));
+                       RC(launch(c, q, KU(k_pressure_update, U_PRESSURE_UPDATE), B, c->n, e));
+                       RC(launch(c, q, KU(k_density_adv, U_DENSITY_ADV), B, c->n, e, 1));
                        return launch1(c, q, k_solver_check, e, 1, 0);
                      });
 }
@@ -380,11 +394,11 @@ static int enq_nonpressure(nn_ctx* c, cudaStream_t s, int advect, int clear) {
   const int B = c->block;
   RC(launch(c, s, forces_kernel(c), B, c->n, d, clear));
   if (c->any_implicit) {
-    RC(launch(c, s, KU(k_cg_setup), B, c->n, d));
+    RC(launch(c, s, KU(k_cg_setup, U_CG_SETUP), B, c->n, d));
     RC(solver_loop(c, s, true, [&](cudaStream_t q) { return launch1(c, q, k_cg_check0, make_dev(c, c->cur)); },
                    [&](cudaStream_t q) {
                      Dev e = make_dev(c, c->cur);
-                     RC(launch(c, q, KU(k_cg_matvec), B, c->n, e));
+                     RC(launch(c, q, KU(k_cg_matvec, U_CG_MATVEC), B, c->n, e));
                      RC(launch1(c, q, k_cg_alpha, e));
                      RC(launch(c, q, k_cg_update, 256, c->n, e));
                      RC(launch1(c, q, k_cg_check, e));
@@ -429,10 +443,10 @@ static int enq_substep(nn_ctx* c, cudaStream_t s) {
   Dev d = make_dev(c, c->cur);
   if (c->any_div) {
     RC(launch1(c, s, k_solver_begin, d, 0));
-    RC(launch(c, s, KU2(k_density_factor, true), c->block, c->n, d, 1, 1));
+    RC(launch(c, s, KU2(k_density_factor, true, U_DENSITY_FACTOR), c->block, c->n, d, 1, 1));
     RC(enq_divergence(c, s, true));
   } else {
-    RC(launch(c, s, KU2(k_density_factor, false), c->block, c->n, d, 1, 1));
+    RC(launch(c, s, KU2(k_density_factor, false, U_DENSITY_FACTOR), c->block, c->n, d, 1, 1));
   }
   RC(enq_nonpressure(c, s, 1, 1));
   return enq_pressure(c, s, 2);
@@ -444,7 +458,7 @@ static int enq_step(nn_ctx* c, cudaStream_t s) {
   RC(enq_search(c, s));
   Dev d = make_dev(c, c->cur);
   RC(launch1(c, s, k_step_dt, d, 1));
-  RC(launch(c, s, KU(k_boundary_volume), c->block, c->n, d, 1));
+  RC(launch(c, s, KU(k_boundary_volume, U_BOUNDARY_VOLUME), c->block, c->n, d, 1));
   RC(launch(c, s, k_clear_acc, 256, c->n, d, c->fold_np ? 1 : 0));
   RC(enq_substep(c, s));
   RC(enq_elastic(c, s));
@@ -663,7 +677,7 @@ int nn_ctx_create(int32_t max_particles, int32_t max_scenes, int32_t max_neighbo
   AL(c->alpha, N); AL(c->rho_adv, N); AL(c->kappa, N); AL(c->srn, N); AL(c->mu, N);
   AL(c->slot_of_id, N); AL(c->key, N); AL(c->rank, N); AL(c->src, N);
   AL(c->nbr, N * (size_t)max_neighbors); AL(c->nbr_cnt, N);
-  AL(c->cg_x, N); AL(c->cg_r, N); AL(c->cg_z, N); AL(c->cg_p, N); AL(c->cg_Ap, N); AL(c->cg_aux, N);
+  AL(c->cg_x, N); AL(c->cg_r, N); AL(c->cg_z, N); AL(c->cg_p, N); AL(c->cg_Ap, N); AL(c->cg_pos, N); AL(c->cg_aux, N);
   AL(c->cg_pinv, 6 * N);
   AL(c->e_of_id, N);
   AL(c->d_any, 1); AL(c->d_body, 4);
@@ -698,7 +712,7 @@ int nn_ctx_destroy(nn_ctx* c) {
   }
   void* bufs[] = {c->d_n, c->d_sc, c->d_dyn, c->d_acc, c->d_scene_of_id, c->d_src_flag, c->acc4, c->alpha,
                   c->rho_adv, c->kappa, c->srn, c->mu, c->slot_of_id, c->key, c->rank, c->src, c->nbr,
-                  c->nbr_cnt, c->cg_x, c->cg_r, c->cg_z, c->cg_p, c->cg_Ap, c->cg_aux, c->cg_pinv,
+                  c->nbr_cnt, c->cg_x, c->cg_r, c->cg_z, c->cg_p, c->cg_Ap, c->cg_pos, c->cg_aux, c->cg_pinv,
                   c->e_of_id, c->d_any, c->d_body, c->cell_count, c->tile_sums};
   for (void* b : bufs) cudaFree(b);
   free_elastic(c);
@@ -732,9 +746,8 @@ int nn_set_block_size(nn_ctx* c, int32_t threads) {
 int nn_set_tuning(nn_ctx* c, int32_t block, int32_t unroll, int32_t cell_factor) {
   if (!c) return fail(nullptr, NN_ERR_INVALID_ARG, "null context");
   if (block == 0) block = NN_DEFAULT_BLOCK;
-  if (unroll == 0) unroll = NN_DEFAULT_UNROLL;
   if (cell_factor == 0) cell_factor = 1;
-  if (block < 32 || block > 1024 || (block % 32) || (unroll != 2 && unroll != 4 && unroll != 8) ||
+  if (block < 32 || block > 1024 || (block % 32) || (unroll != 0 && unroll != 1 && unroll != 2 && unroll != 4) ||
       (cell_factor != 1 && cell_factor != 2))
     return fail(c, NN_ERR_INVALID_ARG, "tuning: block %d, unroll %d, cell factor %d", block, unroll, cell_factor);
   if (block != c->block || unroll != c->unroll || cell_factor != c->cell_factor) drop_graphs(c);
@@ -991,8 +1004,8 @@ int nn_initialize(nn_ctx* c) {
     RC(launch(c, s, k_rigid_com, 256, c->n, d, r, 1));
     RC(launch1(c, s, k_rigid_cm, d, r, 1));
   }
-  RC(launch(c, s, KU(k_boundary_volume), c->block, c->n, d, 0));
-  RC(launch(c, s, KU(k_boundary_volume), c->block, c->n, d, 1));
+  RC(launch(c, s, KU(k_boundary_volume, U_BOUNDARY_VOLUME), c->block, c->n, d, 0));
+  RC(launch(c, s, KU(k_boundary_volume, U_BOUNDARY_VOLUME), c->block, c->n, d, 1));
   RC(enq_sync_out(c, s, SM_VOL));
   CK(cudaStreamSynchronize(s));
   c->el_stale = false;
@@ -1048,11 +1061,11 @@ int nn_run_pass(nn_ctx* c, int32_t pass) {
   RC(launch(c, s, k_sync_in, 256, c->n, d, (uint32_t)SM_ALL));
   RC(launch1(c, s, k_step_dt, d, 0));
   switch (pass) {
-    case NN_PASS_STATIC_BOUNDARY_VOLUME: RC(launch(c, s, KU(k_boundary_volume), c->block, c->n, d, 0)); break;
-    case NN_PASS_MOVING_BOUNDARY_VOLUME: RC(launch(c, s, KU(k_boundary_volume), c->block, c->n, d, 1)); break;
+    case NN_PASS_STATIC_BOUNDARY_VOLUME: RC(launch(c, s, KU(k_boundary_volume, U_BOUNDARY_VOLUME), c->block, c->n, d, 0)); break;
+    case NN_PASS_MOVING_BOUNDARY_VOLUME: RC(launch(c, s, KU(k_boundary_volume, U_BOUNDARY_VOLUME), c->block, c->n, d, 1)); break;
     case NN_PASS_CLEAR_ACCELERATIONS: RC(launch(c, s, k_clear_acc, 256, c->n, d, 0)); break;
-    case NN_PASS_DENSITIES: RC(launch(c, s, KU2(k_density_factor, false), c->block, c->n, d, 1, 0)); break;
-    case NN_PASS_DFSPH_FACTOR: RC(launch(c, s, KU2(k_density_factor, false), c->block, c->n, d, 0, 1)); break;
+    case NN_PASS_DENSITIES: RC(launch(c, s, KU2(k_density_factor, false, U_DENSITY_FACTOR), c->block, c->n, d, 1, 0)); break;
+    case NN_PASS_DFSPH_FACTOR: RC(launch(c, s, KU2(k_density_factor, false, U_DENSITY_FACTOR), c->block, c->n, d, 0, 1)); break;
     case NN_PASS_DIVERGENCE_SOLVE: if (c->any_div) RC(enq_divergence(c, s, false)); break;
     case NN_PASS_NON_PRESSURE_FORCES: if (c->any_fluid) RC(enq_nonpressure(c, s, 0, 0)); break;
     case NN_PASS_NON_PRESSURE_ADVECT: RC(launch(c, s, k_np_advect, 256, c->n, d)); break;
@@ -1101,14 +1114,17 @@ int nn_time_kernel(nn_ctx* c, int32_t kernel, int32_t reps, float* ms_out) {
   auto one = [&]() -> int {
     const int B = c->block;
     switch (kernel) {
-      case NN_K_PRESSURE_UPDATE: return launch(c, s, KU(k_pressure_update), B, c->n, d);
-      case NN_K_DENSITY_ADV: return launch(c, s, KU(k_density_adv), B, c->n, d, 1);
-      case NN_K_DIVERGENCE_UPDATE: return launch(c, s, KU(k_divergence_update), B, c->n, d);
-      case NN_K_DENSITY_CHANGE: return launch(c, s, KU(k_density_change), B, c->n, d, 1, 0);
-      case NN_K_DENSITY_CHANGE_NP: return launch(c, s, KU(k_density_change_np), B, c->n, d, 1, 0);
-      case NN_K_DENSITY_FACTOR: return launch(c, s, KU2(k_density_factor, false), B, c->n, d, 1, 1);
+      case NN_K_PRESSURE_UPDATE: return launch(c, s, KU(k_pressure_update, U_PRESSURE_UPDATE), B, c->n, d);
+      case NN_K_DENSITY_ADV: return launch(c, s, KU(k_density_adv, U_DENSITY_ADV), B, c->n, d, 1);
+      case NN_K_DIVERGENCE_UPDATE: return launch(c, s, KU(k_divergence_update, U_DIVERGENCE_UPDATE), B, c->n, d);
+      case NN_K_DENSITY_CHANGE: return launch(c, s, KU(k_density_change, U_DENSITY_CHANGE), B, c->n, d, 1, 0);
+      case NN_K_DENSITY_CHANGE_NP: return launch(c, s, KU(k_density_change_np, U_DENSITY_CHANGE_NP), B, c->n, d, 1, 0);
+      case NN_K_DENSITY_FACTOR:  // the instance the step runs (with the first density change)
+        return c->any_div ? launch(c, s, KU2(k_density_factor, true, U_DENSITY_FACTOR), B, c->n, d, 1, 1)
+                          : launch(c, s, KU2(k_density_factor, false, U_DENSITY_FACTOR), B, c->n, d, 1, 1);
       case NN_K_BUILD_LISTS: return launch(c, s, k_build_lists, NS_WARPS * 32, c->n, d);
-      case NN_K_CG_MATVEC: return launch(c, s, KU(k_cg_matvec), B, c->n, d);
+      case NN_K_CG_MATVEC: return launch(c, s, KU(k_cg_matvec, U_CG_MATVEC), B, c->n, d);
+      case NN_K_CG_SETUP: return launch(c, s, KU(k_cg_setup, U_CG_SETUP), B, c->n, d);
       default: return launch(c, s, forces_kernel(c), B, c->n, d, 0);
     }
   };

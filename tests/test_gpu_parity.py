@@ -243,7 +243,7 @@ def test_resident_run_equals_steps(cuda_lib):
     assert np.array_equal(x1, pd_field(m2, "x"))
 
 
-@pytest.mark.parametrize("tuning", [dict(block=128, unroll=8, cell_factor=2), dict(block=512, unroll=2, cell_factor=1),
+@pytest.mark.parametrize("tuning", [dict(block=128, unroll=1, cell_factor=2), dict(block=512, unroll=2, cell_factor=1),
                                     dict(block=64, unroll=4, cell_factor=2),
                                     dict(block=128, unroll=2, cell_factor=1, x_split=2),
                                     dict(block=128, unroll=2, cell_factor=1, x_split=4),
