@@ -39,6 +39,28 @@ def rel_err(a, b, scale=None):
     return float(np.abs(a - b).max() / s)
 
 
+def factor_denominator(f):
+    """-1 / dfsph_factor where the factor is set, else 0: the gradient sum the reference
+    divides by (SPH/main.py:1586-1593), up to the solver's time-step scaling."""
+    f = np.asarray(f, np.float64)
+    out = np.zeros_like(f)
+    nz = f != 0
+    out[nz] = -1.0 / f[nz]
+    return out
+
+
+def field_err(name, a, b):
+    """rel_err of one field. The DFSPH factor is compared through its denominator: a
+    particle whose few neighbours all sit near the edge of the kernel support has a
+    gradient sum of a few kernel gradients near r = h, where the f32 rounding of 1 - r/h
+    moves each term by about 1e-4 of itself; its factor, the reciprocal of that small sum,
+    is then both the field's largest value and its least accurate one. The denominators
+    carry the same information, scaled by the well-conditioned interior."""
+    if name == "dfsph_factor":
+        return rel_err(factor_denominator(a), factor_denominator(b))
+    return rel_err(a, b)
+
+
 def sorted_sets_equal(n1, l1, n2, l2):
     """Per-particle neighbour id sets equal (rows are already sorted by id)."""
     n1 = np.asarray(n1); n2 = np.asarray(n2)

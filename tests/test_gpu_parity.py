@@ -14,7 +14,7 @@ from nonnewton_b200 import _abi
 from nonnewton_b200 import scene as S
 from nonnewton_b200.config import Parameter, SimConfig
 
-from .helpers import gpu_sim, near_cutoff_pairs, oracle_sim, pd_field, rel_err
+from .helpers import field_err, gpu_sim, near_cutoff_pairs, oracle_sim, pd_field, rel_err
 
 pytestmark = pytest.mark.gpu
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
@@ -155,7 +155,7 @@ def _compare(m, o, names, nf=None, tol=TOL):
         r = o.get(name)
         if nf is not None and name in ("density", "dfsph_factor", "density_adv"):
             g, r = g[:nf], r[:nf]
-        e = rel_err(g, r)
+        e = field_err(name, g, r)
         assert e < tol, f"{name}: rel err {e:.2e}"
 
 
