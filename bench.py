@@ -42,7 +42,9 @@ ALG_BYTES = {
     "density_adv": 16 + 16 + 4 + 4 + 4 + 4 + 4,   # pos4, vel4, dens, alpha, flags -> rho_adv, kappa
     "divergence_update": 16 + 16 + 4 + 4 + 16,
     "density_change": 16 + 16 + 4 + 4 + 4 + 4,
-    "density_factor": 16 + 4 + 4 + 4,
+    # the instance the step runs with the divergence solve's first density change:
+    # pos4, vel4, flags -> dens, alpha, rho_adv, kappa
+    "density_factor": 16 + 16 + 4 + 4 + 4 + 4 + 4,
     "cg_matvec": 16 + 16 + 8 + 4 + 4 + 16,        # pos4, p, aux2, mass, flags -> Ap
     "nonpressure": 4 + 16 + 16 + 4 + 4 + 16 + 4 + 4 + 8,  # flags, pos4, vel4, mass, dens -> acc4, srn, mu, aux2
     "build_lists": 16 + 4 + 4,                    # pos4, flags -> count; + 4 B per list entry (added live)
@@ -55,24 +57,24 @@ ALG_BYTES["density_change_np"] = ALG_BYTES["density_change"] + 4 + 4 + 16 + 4 + 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch on the
 # 2.4M-particle dam break, from `ncu --set full` captures of the current kernels.
 NCU_TRAFFIC_2M = {"build_lists": 477530368, "density_adv": 372967680,
-                  "nonpressure": 431172096, "density_factor": 371440896,
+                  "nonpressure": 431172096, "density_factor": 365270272,
                   "density_change": 366368512, "divergence_update": 376274432,
-                  "pressure_update": 383854080, "cg_matvec": 401365504, "density_change_np": 436444416,
-                  "cg_setup": 570425344}
+                  "pressure_update": 383854080, "cg_matvec": 433442816, "density_change_np": 430826240,
+                  "cg_setup": 567003648}
 # what bounds each kernel instead of DRAM, from its ncu capture on the 2.4M scene:
 # the HBM fraction above is low because none is DRAM-bound
 LIMITER_2M = {
     "build_lists": "instruction issue: 72 % issue active, ~160 exact f32 distance tests per particle, two per packed f32x2 instruction; DRAM 13 %",
     "density_adv": "L1 data pipe: LSU wavefronts at 78 % of peak (neighbour gathers); DRAM 19 %",
     "nonpressure": "L1 data pipe and gather latency: LSU wavefronts 62 %, 46 % warps active; DRAM 13 %",
-    "density_factor": "L1 data pipe: LSU wavefronts 67 % of peak; DRAM 14 %",
+    "density_factor": "gather latency: LSU wavefronts 64 %, issue 64 %, 53 % warps active; DRAM 15 %",
     "density_change": "L1 data pipe: LSU wavefronts 85 % of peak; DRAM 18 %",
     "divergence_update": "L1 data pipe: LSU wavefronts 65 % of peak, 64 % issue active; DRAM 20 %",
     "pressure_update": "L1 data pipe: LSU wavefronts 72 % of peak; DRAM 24 %",
-    "cg_matvec": "L1 data pipe: LSU wavefronts 78 % of peak; DRAM 16 %",
-    "cg_setup": "L1 data pipe: LSU wavefronts 83 % of peak; DRAM 19 %",
-    "density_change_np": "gather latency with the folded force terms: LSU wavefronts 60 %, issue 63 %, "
-                         "46 % warps active at 64 registers; DRAM 12 %",
+    "cg_matvec": "gather latency: LSU wavefronts 66 %, issue 63 %, 46 % warps active at 64 registers; DRAM 20 %",
+    "cg_setup": "L1 data pipe and gather latency: LSU wavefronts 72 %, issue 64 %, 46 % warps active; DRAM 21 %",
+    "density_change_np": "gather latency with the folded force terms: LSU wavefronts 55 %, issue 68 %, "
+                         "46 % warps active at 64 registers; DRAM 13 %",
 }
 KERNEL_IDS = {"pressure_update": 0, "density_adv": 1, "divergence_update": 2, "density_change": 3,
               "density_factor": 4, "build_lists": 5, "cg_matvec": 6, "nonpressure": 7, "density_change_np": 8,
