@@ -45,11 +45,12 @@ class Request:
 # 16, mass 4, density 4, flags 4, id 4: 2 x 48), its per-slot scratch (scene of id 4,
 # acceleration 16, alpha / rho_adv / kappa / strain rate / viscosity 20, slot of id 4,
 # sort key / rank / source 12), the neighbour counts 4 and 4 B per list entry, the CG
-# vectors (5 x 16, coefficients 8, preconditioner 24) and the elastic index 4; plus
+# vectors (x, r, z, p, Ap and the matvec's positions: 6 x 16, coefficients 8,
+# preconditioner 24) and the elastic index 4; plus
 # the batch's ParticleData fields (168: x, x_0, v, a 48; six scalars 24; four int32 16;
 # color 12; strain rate and viscosity 8; stress 24; rotations 36). A grid cell costs
 # CELL_BYTES (its count / start).
-CTX_BYTES_PER_PARTICLE = 96 + 56 + 4 + 112 + 4
+CTX_BYTES_PER_PARTICLE = 96 + 56 + 4 + 128 + 4
 PD_BYTES_PER_PARTICLE = 168
 CELL_BYTES = 4
 DEFAULT_RESERVE_BYTES = 4 << 30  # left free for torch, graphs and the repack's temporaries
