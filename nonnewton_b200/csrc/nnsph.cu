@@ -270,6 +270,11 @@ static int launch_g(nn_ctx* c, cudaStream_t s, void (*k)(KArgs...), int grid, in
 // Data-dependent solver loop. In a capture, `pre` runs in the parent graph (it may
 // set the loop condition) and `body` becomes the body of a CUDA-graph while-node;
 // otherwise both run from the host with one synchronisation per iteration.
+// A loop without check_first always runs its body once (the DFSPH solves count from
+// zero and test after the body, SPH/main.py:1695-1703, 1778-1784): that first body is
+// captured straight into the parent graph, where its closing check sets the condition
+// of the while-node that runs the further bodies, so a solve that stops after one body
+// launches no body graph.
 // Body launches are counted per execution on the device (body_count).
 template <typename Pre, typename Body>
 static int solver_loop(nn_ctx* c, cudaStream_t s, bool check_first, Pre pre, Body body) {
@@ -284,6 +289,12 @@ static int solver_loop(nn_ctx* c, cudaStream_t s, bool check_first, Pre pre, Bod
     c->cur_handle = (unsigned long long)h;
     int rc = pre(s);
     if (rc != NN_OK) { c->cur_handle = 0; return rc; }
+    if (!check_first) {
+      const int64_t first = c->capture_nodes;
+      rc = body(s);
+      c->capture_nodes = first;
+      if (rc != NN_OK) { c->cur_handle = 0; return rc; }
+    }
     CK(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nd));
     cudaGraphNodeParams p{};
     p.type = cudaGraphNodeTypeConditional;
