@@ -336,13 +336,14 @@ static int solver_loop(nn_ctx* c, cudaStream_t s, bool check_first, Pre pre, Bod
 // ---- pass sequences ---------------------------------------------------------------
 // NeighborhoodSearchSparse.run_search (SPH/main.py:822-829): the new slots go into the
 // other working set; the source (caller state or previous slots) is a device flag.
-static int enq_search(nn_ctx* c, cudaStream_t s) {
+// `reset_step`: the step's first launch (k_zero_cells) also resets its per-scene counters.
+static int enq_search(nn_ctx* c, cudaStream_t s, bool reset_step = false) {
   c->cur = 1 - c->cur;
   Dev d = make_dev(c, c->cur);
   const int B = 256;
   const int64_t cells = c->in_capture ? c->max_cells : c->ncells;
   const int tiles = (int)((cells + 1 + SCAN_TILE - 1) / SCAN_TILE);
-  RC(launch(c, s, k_zero_cells, B, (int)std::min<int64_t>(cells + 1, INT32_MAX), d));
+  RC(launch(c, s, k_zero_cells, B, (int)std::min<int64_t>(cells + 1, INT32_MAX), d, reset_step ? 1 : 0));
   RC(launch(c, s, k_keys, B, c->n, d));
   RC(launch_g(c, s, k_scan_tiles, std::min(tiles, c->sms * 2), SCAN_THREADS, d));
   RC(launch_g(c, s, k_scan_sums, 1, SCAN_THREADS, d));
@@ -380,10 +381,11 @@ static int enq_divergence(nn_ctx* c, cudaStream_t s, bool fused) {
 
 // DFSPHSolver.pressure_solve (SPH/main.py:1762-1791); init_mode 2 also folds the
 // divergence solve's alpha *= dt.
-static int enq_pressure(nn_ctx* c, cudaStream_t s, int init_mode) {
+// `begun`: the loop start is done (k_clear_acc at the start of the step).
+static int enq_pressure(nn_ctx* c, cudaStream_t s, int init_mode, bool begun = false) {
   Dev d = make_dev(c, c->cur);
   const int B = c->block;
-  RC(launch1(c, s, k_solver_begin, d, 1));
+  if (!begun) RC(launch1(c, s, k_solver_begin, d, 1));
   return solver_loop(c, s, false,
                      [&](cudaStream_t q) {
                        return launch(c, q, KU(k_density_adv, U_DENSITY_ADV), B, c->n, make_dev(c, c->cur), init_mode);
@@ -449,29 +451,30 @@ static int enq_rigid(nn_ctx* c, cudaStream_t s) {
 }
 
 // DFSPHSolver.substep (SPH/main.py:1546-1555) with the fused passes.
-static int enq_substep(nn_ctx* c, cudaStream_t s) {
+// `begun`: the loops' start is done (k_clear_acc at the start of the step).
+static int enq_substep(nn_ctx* c, cudaStream_t s, bool begun = false) {
   if (!c->any_fluid) return NN_OK;
   Dev d = make_dev(c, c->cur);
   if (c->any_div) {
-    RC(launch1(c, s, k_solver_begin, d, 0));
+    if (!begun) RC(launch1(c, s, k_solver_begin, d, 0));
     RC(launch(c, s, KU2(k_density_factor, true, U_DENSITY_FACTOR), c->block, c->n, d, 1, 1));
     RC(enq_divergence(c, s, true));
   } else {
     RC(launch(c, s, KU2(k_density_factor, false, U_DENSITY_FACTOR), c->block, c->n, d, 1, 1));
   }
   RC(enq_nonpressure(c, s, 1, 1));
-  return enq_pressure(c, s, 2);
+  return enq_pressure(c, s, 2, begun);
 }
 
 // SPHBase.step (SPH/main.py:915-937)
 static int enq_step(nn_ctx* c, cudaStream_t s) {
-  RC(launch1(c, s, k_step_reset, make_dev(c, c->cur)));
-  RC(enq_search(c, s));
+  // k_step_reset rides in the search's first launch, k_step_dt and the solves' loop
+  // start in k_clear_acc's first block: one-block kernels cost a graph node each
+  RC(enq_search(c, s, true));
   Dev d = make_dev(c, c->cur);
-  RC(launch1(c, s, k_step_dt, d, 1));
   RC(launch(c, s, KU(k_boundary_volume, U_BOUNDARY_VOLUME), c->block, c->n, d, 1));
-  RC(launch(c, s, k_clear_acc, 256, c->n, d, c->fold_np ? 1 : 0));
-  RC(enq_substep(c, s));
+  RC(launch(c, s, k_clear_acc, 256, c->n, d, c->fold_np ? 1 : 0, 1));
+  RC(enq_substep(c, s, true));
   RC(enq_elastic(c, s));
   RC(enq_rigid(c, s));
   RC(launch(c, s, k_advect_boundary, 256, c->n, d, 1, 1, 1));
@@ -1074,7 +1077,7 @@ int nn_run_pass(nn_ctx* c, int32_t pass) {
   switch (pass) {
     case NN_PASS_STATIC_BOUNDARY_VOLUME: RC(launch(c, s, KU(k_boundary_volume, U_BOUNDARY_VOLUME), c->block, c->n, d, 0)); break;
     case NN_PASS_MOVING_BOUNDARY_VOLUME: RC(launch(c, s, KU(k_boundary_volume, U_BOUNDARY_VOLUME), c->block, c->n, d, 1)); break;
-    case NN_PASS_CLEAR_ACCELERATIONS: RC(launch(c, s, k_clear_acc, 256, c->n, d, 0)); break;
+    case NN_PASS_CLEAR_ACCELERATIONS: RC(launch(c, s, k_clear_acc, 256, c->n, d, 0, 0)); break;
     case NN_PASS_DENSITIES: RC(launch(c, s, KU2(k_density_factor, false, U_DENSITY_FACTOR), c->block, c->n, d, 1, 0)); break;
     case NN_PASS_DFSPH_FACTOR: RC(launch(c, s, KU2(k_density_factor, false, U_DENSITY_FACTOR), c->block, c->n, d, 0, 1)); break;
     case NN_PASS_DIVERGENCE_SOLVE: if (c->any_div) RC(enq_divergence(c, s, false)); break;
@@ -1437,7 +1440,7 @@ extern "C" int nn_neighbors_noalloc(const float* x, int32_t n, const double* dom
   const int gC = std::max(1, std::min((int)((cells + 1 + B - 1) / B), 1024));
   const int tiles = (int)((cells + 1 + SCAN_TILE - 1) / SCAN_TILE);
   k_na_setup<<<gN, B, 0, st>>>(d, s, n, (int32_t)cells);
-  k_zero_cells<<<gC, B, 0, st>>>(d);
+  k_zero_cells<<<gC, B, 0, st>>>(d, 0);
   k_keys<<<gN, B, 0, st>>>(d);
   k_scan_tiles<<<std::min(tiles, 256), SCAN_THREADS, 0, st>>>(d);
   k_scan_sums<<<1, SCAN_THREADS, 0, st>>>(d);

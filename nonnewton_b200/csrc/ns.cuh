@@ -33,7 +33,23 @@ __device__ __forceinline__ uint32_t cell_key(const SceneDev& s, real x, real y, 
   return (uint32_t)(s.cell_base + (int64_t)morton2((uint32_t)cy, (uint32_t)cz) * s.gx + cx);
 }
 
-__global__ void k_zero_cells(Dev d) {
+// Per-step counters reset (before the neighbour search).
+__device__ __forceinline__ void step_reset_scenes(const Dev& d) {
+  const int ns = d.d_n[1];
+  for (int sc = threadIdx.x; sc < ns; sc += blockDim.x) {
+    SceneDyn& y = d.dyn[sc];
+    y.max_density_bits = 0u;
+    y.max_nb = 0;
+    y.it_v = y.it_p = y.it_cg = 0;
+    y.div_ran = 0;
+    y.np_fresh = 0;
+  }
+}
+
+// `reset_step`: block 0 also resets the step's per-scene counters (the step's first
+// launch; nothing before the list build reads them).
+__global__ void k_zero_cells(Dev d, int reset_step) {
+  if (reset_step && blockIdx.x == 0) step_reset_scenes(d);
   const int nc = d.d_n[2];
   GRID_STRIDE(i, nc + 1) d.cell_count[i] = 0u;
 }

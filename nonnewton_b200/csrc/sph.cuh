@@ -45,7 +45,18 @@ __global__ void k_boundary_volume(Dev d, int moving) {
 // force pass would write for the solid slots of scenes with fluid (strain rate and
 // viscosity 0, CG coefficients (0, 1 if dynamic)): the step sets it when the fluid's
 // non-pressure terms come from the divergence loop's last density change instead.
-__global__ void k_clear_acc(Dev d, int solid_terms) {
+// `step_start`: block 0 also takes the step's time step (k_step_dt with the CFL rule)
+// and the divergence and pressure solves' loop start, which nothing reads before them.
+__device__ __forceinline__ void step_dt_scenes(const Dev& d, int do_cfl);
+__device__ __forceinline__ void solver_begin_scene(SceneDyn& y, const SceneDev& s, int which);
+__global__ void k_clear_acc(Dev d, int solid_terms, int step_start) {
+  if (step_start && blockIdx.x == 0) {
+    step_dt_scenes(d, 1);
+    for (int sc = threadIdx.x; sc < d.d_n[1]; sc += blockDim.x) {
+      solver_begin_scene(d.dyn[sc], d.sc[sc], 0);
+      solver_begin_scene(d.dyn[sc], d.sc[sc], 1);
+    }
+  }
   const int n = d.d_n[0];
   GRID_STRIDE(i, n) {
     const uint32_t fl = d.w.flags[i];
@@ -409,43 +420,28 @@ __global__ void k_solver_check(Dev d, int which /*0 div, 1 pressure*/, int fold)
   }
 }
 
-// Per-scene loop start: which scenes iterate, counters reset, dt-derived constants.
+// Per-scene loop start: which scenes iterate, counters reset.
+__device__ __forceinline__ void solver_begin_scene(SceneDyn& y, const SceneDev& s, int which) {
+  int on = s.n_fluid > 0;
+  if (which == 0) {
+    on = on && (s.flags & NN_F_DIVERGENCE);
+    y.act_v = on; y.it_v = 0; y.div_ran = on;
+    y.np_body = min(max(y.np_last, 0), max(s.max_iter_v, 1) - 1);  // as many bodies as last step
+  }
+  else if (which == 1) { y.act_p = on; y.it_p = 0; }
+  else { y.it_cg = 0; }
+}
 __global__ void k_solver_begin(Dev d, int which /*0 div, 1 pressure, 2 cg*/) {
   const int ns = d.d_n[1];
-  int any = 0;
-  for (int sc = threadIdx.x; sc < ns; sc += blockDim.x) {
-    SceneDyn& y = d.dyn[sc];
-    const SceneDev& s = d.sc[sc];
-    int on = s.n_fluid > 0;
-    if (which == 0) {
-      on = on && (s.flags & NN_F_DIVERGENCE);
-      y.act_v = on; y.it_v = 0; y.div_ran = on;
-      y.np_body = min(max(y.np_last, 0), max(s.max_iter_v, 1) - 1);  // as many bodies as last step
-    }
-    else if (which == 1) { y.act_p = on; y.it_p = 0; }
-    else { y.it_cg = 0; }
-    any |= on;
-  }
-  (void)any;
+  for (int sc = threadIdx.x; sc < ns; sc += blockDim.x) solver_begin_scene(d.dyn[sc], d.sc[sc], which);
 }
 
-// Per-step counters reset (before the neighbour search).
-__global__ void k_step_reset(Dev d) {
-  const int ns = d.d_n[1];
-  for (int sc = threadIdx.x; sc < ns; sc += blockDim.x) {
-    SceneDyn& y = d.dyn[sc];
-    y.max_density_bits = 0u;
-    y.max_nb = 0;
-    y.it_v = y.it_p = y.it_cg = 0;
-    y.div_ran = 0;
-    y.np_fresh = 0;
-  }
-}
+__global__ void k_step_reset(Dev d) { step_reset_scenes(d); }
 
 // Time step of the step: the CFL step from max |v| of the gather (extension; the
 // reference keeps dt fixed), and the f32 constants the reference passes to its
 // kernels (1/dt and 1/dt^2 computed in f64 from the f32 dt field, SPH/main.py:1687,1764).
-__global__ void k_step_dt(Dev d, int do_cfl) {
+__device__ __forceinline__ void step_dt_scenes(const Dev& d, int do_cfl) {
   const int ns = d.d_n[1];
   for (int sc = threadIdx.x; sc < ns; sc += blockDim.x) {
     SceneDyn& y = d.dyn[sc];
@@ -462,6 +458,7 @@ __global__ void k_step_dt(Dev d, int do_cfl) {
     y.vmax_bits = 0u;
   }
 }
+__global__ void k_step_dt(Dev d, int do_cfl) { step_dt_scenes(d, do_cfl); }
 
 // non_pressure_advect (SPH/main.py:1843-1848) as a pass of its own.
 __global__ void k_np_advect(Dev d) {
