@@ -346,7 +346,6 @@ static int enq_search(nn_ctx* c, cudaStream_t s, bool reset_step = false) {
   RC(launch(c, s, k_zero_cells, B, (int)std::min<int64_t>(cells + 1, INT32_MAX), d, reset_step ? 1 : 0));
   RC(launch(c, s, k_keys, B, c->n, d));
   RC(launch_g(c, s, k_scan_tiles, std::min(tiles, c->sms * 2), SCAN_THREADS, d));
-  RC(launch_g(c, s, k_scan_sums, 1, SCAN_THREADS, d));
   RC(launch_g(c, s, k_scan_apply, std::min(tiles, c->sms * 2), SCAN_THREADS, d));
   RC(launch(c, s, k_scatter, B, c->n, d));
   RC(launch(c, s, k_cell_sort, B, (int)std::min<int64_t>(cells, INT32_MAX), d));
@@ -1443,7 +1442,6 @@ extern "C" int nn_neighbors_noalloc(const float* x, int32_t n, const double* dom
   k_zero_cells<<<gC, B, 0, st>>>(d, 0);
   k_keys<<<gN, B, 0, st>>>(d);
   k_scan_tiles<<<std::min(tiles, 256), SCAN_THREADS, 0, st>>>(d);
-  k_scan_sums<<<1, SCAN_THREADS, 0, st>>>(d);
   k_scan_apply<<<std::min(tiles, 256), SCAN_THREADS, 0, st>>>(d);
   k_scatter<<<gN, B, 0, st>>>(d);
   k_cell_sort<<<gC, B, 0, st>>>(d);

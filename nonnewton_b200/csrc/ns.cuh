@@ -77,7 +77,7 @@ __global__ void k_keys(Dev d) {
   }
 }
 
-// Exclusive scan of cell_count[0 .. cells] in place (three phases over tiles).
+// Exclusive scan of cell_count[0 .. cells] in place (two phases over tiles).
 #define SCAN_TILE 4096
 #define SCAN_THREADS 1024
 __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* sh, uint32_t* total) {
@@ -127,28 +127,22 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_tiles(Dev d) {
   }
 }
 
-__global__ void __launch_bounds__(SCAN_THREADS) k_scan_sums(Dev d) {
-  __shared__ uint32_t sh[32];
-  const int len = d.d_n[2] + 1;
-  const int ntiles = (len + SCAN_TILE - 1) / SCAN_TILE;
-  uint32_t carry = 0;
-  for (int base = 0; base < ntiles; base += blockDim.x) {
-    int i = base + threadIdx.x;
-    uint32_t v = i < ntiles ? d.tile_sums[i] : 0u;
-    uint32_t tot;
-    uint32_t ex = block_excl_scan(v, sh, &tot);
-    if (i < ntiles) d.tile_sums[i] = ex + carry;
-    carry += tot;
-    __syncthreads();
-  }
-}
-
+// Second phase: each block adds up the tile sums before its tile itself (the blocks
+// walk the tiles in order, so each reads about as many tile sums as there are tiles),
+// then scans its tile. A separate one-block scan of the tile sums would cost a launch.
 __global__ void __launch_bounds__(SCAN_THREADS) k_scan_apply(Dev d) {
   __shared__ uint32_t sh[32];
   const int len = d.d_n[2] + 1;
   const int ntiles = (len + SCAN_TILE - 1) / SCAN_TILE;
   constexpr int PER = SCAN_TILE / SCAN_THREADS;
+  uint32_t before = 0;  // sum of tile_sums[0 .. done)
+  int done = 0;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    uint32_t part = 0, tot = 0;
+    for (int k = done + (int)threadIdx.x; k < t; k += blockDim.x) part += d.tile_sums[k];
+    block_excl_scan(part, sh, &tot);
+    before += tot;
+    done = t;
     uint32_t v[PER];
     uint32_t s = 0;
 #pragma unroll
@@ -157,7 +151,7 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_apply(Dev d) {
       v[k] = i < len ? d.cell_count[i] : 0u;
       s += v[k];
     }
-    uint32_t ex = block_excl_scan(s, sh, nullptr) + d.tile_sums[t];
+    uint32_t ex = block_excl_scan(s, sh, nullptr) + before;
 #pragma unroll
     for (int k = 0; k < PER; ++k) {
       int i = t * SCAN_TILE + threadIdx.x * PER + k;

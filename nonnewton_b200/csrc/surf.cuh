@@ -957,7 +957,6 @@ static int sr_scan(nn_sr_ctx* c, uint32_t* a, int64_t len, cudaStream_t st) {
   SRCK(cudaMemcpyAsync(c->d_n, hn, sizeof(hn), cudaMemcpyHostToDevice, st));
   const int tiles = (int)((len + SCAN_TILE - 1) / SCAN_TILE);
   k_scan_tiles<<<std::max(1, std::min(tiles, c->sms * 2)), SCAN_THREADS, 0, st>>>(d);
-  k_scan_sums<<<1, SCAN_THREADS, 0, st>>>(d);
   k_scan_apply<<<std::max(1, std::min(tiles, c->sms * 2)), SCAN_THREADS, 0, st>>>(d);
   SRCK(cudaGetLastError());
   return NN_OK;
