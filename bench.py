@@ -56,6 +56,9 @@ ALG_BYTES = {
 ALG_BYTES["density_change_np"] = ALG_BYTES["density_change"] + 4 + 4 + 16 + 4 + 4 + 8
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch on the
 # 2.4M-particle dam break, from `ncu --set full` captures of the current kernels.
+# list entries of the captured k_build_lists launch (step 5 of the 2.4M scene); the line
+# scales that launch's traffic to the timed launch's entries, which the bytes follow
+NCU_ENTRIES_2M = 62_580_972
 NCU_TRAFFIC_2M = {"build_lists": 477530368, "density_adv": 372967680,
                   "nonpressure": 431172096, "density_factor": 365270272,
                   "density_change": 366368512, "divergence_update": 376274432,
@@ -825,6 +828,12 @@ def run_ours(args):
     ab = ALG_BYTES[dom] * n + (4 * entries if dom == "build_lists" else 0)
     achieved = ab / (kms[dom] / 1e3) / 1e9
     traffic = NCU_TRAFFIC_2M.get(dom) if sc.name == "roofline_2m" else None
+    traffic_src = "ncu dram bytes of one launch, same kernel and workload" if traffic else None
+    if traffic and dom == "build_lists":
+        ab_capture = ALG_BYTES["build_lists"] * n + 4 * NCU_ENTRIES_2M
+        traffic = traffic * ab / ab_capture
+        traffic_src = (f"ncu dram bytes of one launch of the same kernel and workload at "
+                       f"{NCU_ENTRIES_2M} list entries, scaled to this launch's {entries} by the algorithmic bytes")
     hbm = peaks["hbm_gbs"]
     bytes_step = step_bytes(st["iterations_v"] + 1, st["iterations"] + 1, st["cg_iterations"], 0.0, implicit)
     line = {
@@ -842,7 +851,7 @@ def run_ours(args):
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "peak_source": f"{peak_kind} hbm_gbs",
                      "alg_bytes_per_launch": ab, "traffic": traffic,
-                     "traffic_source": "ncu dram bytes of one launch, same kernel and workload" if traffic else None,
+                     "traffic_source": traffic_src,
                      "kernel_ms": kms, "launches_per_step": per_step, "list_entries": entries,
                      "limiter": LIMITER_2M.get(dom) if sc.name == "roofline_2m" else None},
         "step_alg_bytes_per_particle": bytes_step,

@@ -26,6 +26,6 @@ def test_step_bytes_formula(iv, ip, icg, fel, implicit):
 def test_ncu_traffic_covers_the_algorithmic_bytes():
     import bench
 
-    n, entries = 2_400_002, 62_580_972  # the 2.4M scene and its list entries at the captured step
+    n, entries = 2_400_002, bench.NCU_ENTRIES_2M  # the 2.4M scene and its list entries at the captured step
     assert bench.NCU_TRAFFIC_2M["build_lists"] >= bench.ALG_BYTES["build_lists"] * n + 4 * entries
     assert bench.NCU_TRAFFIC_2M["density_adv"] >= bench.ALG_BYTES["density_adv"] * n
