@@ -283,7 +283,8 @@ enum nn_kernel_id {
   NN_K_DENSITY_ADV,           /* compute_density_adv + FP64 error reduction */
   NN_K_DIVERGENCE_UPDATE,     /* divergence_solver_iteration_kernel */
   NN_K_DENSITY_CHANGE,        /* compute_density_change + FP64 error reduction */
-  NN_K_DENSITY_FACTOR,        /* compute_densities + compute_DFSPH_factor */
+  NN_K_DENSITY_FACTOR,        /* compute_densities + compute_DFSPH_factor (with the divergence
+                                 solve's first density change when a scene runs it, as in the step) */
   NN_K_BUILD_LISTS,           /* store_neighbors */
   NN_K_CG_MATVEC,             /* implicit viscosity matrix-vector product */
   NN_K_NONPRESSURE,           /* surface tension + explicit viscosity */
