@@ -382,3 +382,19 @@ def test_unchecked_step_is_checked_by_the_next_call(monkeypatch):
     s.step()  # the third step overflowed (70 seen): restored to x = 2 and run again first
     assert calls == [("cap", 88), ("step", 2.0), ("stats",), ("step", 3.0), ("async",)]
     assert float(pd.x[0, 0]) == 4.0 and m.step_num == 4
+
+
+def test_kernel_ids_match_the_header_enum():
+    """_abi's NN_K_* (the ids nn_time_kernel takes) are the header's enum nn_kernel_id,
+    in order from 0."""
+    import os
+    import re
+
+    from nonnewton_b200 import _abi
+
+    hdr = open(os.path.join(os.path.dirname(__file__), "..", "include", "nnsph.h")).read()
+    body = re.search(r"enum nn_kernel_id \{(.*?)\};", hdr, re.S).group(1)
+    body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+    names = [t.split("=")[0].strip() for t in body.split(",") if t.strip()]
+    assert names[-1] == "NN_K_COUNT"
+    assert {n: getattr(_abi, n) for n in names} == {n: k for k, n in enumerate(names)}

@@ -29,3 +29,19 @@ def test_ncu_traffic_covers_the_algorithmic_bytes():
     n, entries = 2_400_002, bench.NCU_ENTRIES_2M  # the 2.4M scene and its list entries at the captured step
     assert bench.NCU_TRAFFIC_2M["build_lists"] >= bench.ALG_BYTES["build_lists"] * n + 4 * entries
     assert bench.NCU_TRAFFIC_2M["density_adv"] >= bench.ALG_BYTES["density_adv"] * n
+
+
+def test_kernel_ids_follow_the_abi():
+    """bench.py names nn_time_kernel's ids itself; they must be the header's NN_K_* values,
+    each timed kernel with a byte count."""
+    import bench
+    from nonnewton_b200 import _abi
+
+    assert bench.KERNEL_IDS == {
+        "pressure_update": _abi.NN_K_PRESSURE_UPDATE, "density_adv": _abi.NN_K_DENSITY_ADV,
+        "divergence_update": _abi.NN_K_DIVERGENCE_UPDATE, "density_change": _abi.NN_K_DENSITY_CHANGE,
+        "density_factor": _abi.NN_K_DENSITY_FACTOR, "build_lists": _abi.NN_K_BUILD_LISTS,
+        "cg_matvec": _abi.NN_K_CG_MATVEC, "nonpressure": _abi.NN_K_NONPRESSURE,
+        "density_change_np": _abi.NN_K_DENSITY_CHANGE_NP, "cg_setup": _abi.NN_K_CG_SETUP}
+    assert set(bench.KERNEL_IDS) <= set(bench.ALG_BYTES)
+    assert max(bench.KERNEL_IDS.values()) == _abi.NN_K_COUNT - 1
