@@ -398,3 +398,31 @@ def test_kernel_ids_match_the_header_enum():
     names = [t.split("=")[0].strip() for t in body.split(",") if t.strip()]
     assert names[-1] == "NN_K_COUNT"
     assert {n: getattr(_abi, n) for n in names} == {n: k for k, n in enumerate(names)}
+
+
+def test_constants_match_the_header():
+    """Every NN_* constant that _abi restates (status codes, materials, phase bases, scene
+    flags, viscosity laws, step flags, pass ids, allocation-free limits) has the header's
+    value."""
+    import os
+    import re
+
+    from nonnewton_b200 import _abi
+
+    hdr = open(os.path.join(os.path.dirname(__file__), "..", "include", "nnsph.h")).read()
+    hdr = re.sub(r"/\*.*?\*/", "", hdr, flags=re.S)
+    vals = {}
+    for name, expr in re.findall(r"^#define (NN_\w+)\s+(.+)$", hdr, re.M):
+        expr = re.sub(r"(\d+)u\b", r"\1", expr.strip())
+        if re.fullmatch(r"[\d\s()<+-]+", expr):
+            vals[name] = eval(expr)  # integer literals and shifts only
+    for body in re.findall(r"enum \w+ \{(.*?)\};", hdr, re.S):
+        k = 0
+        for item in (t.strip() for t in body.split(",") if t.strip()):
+            name, _, v = (p.strip() for p in item.partition("="))
+            k = int(v) if v else k
+            vals[name] = k
+            k += 1
+    checked = {n: v for n, v in vals.items() if hasattr(_abi, n)}
+    assert len(checked) >= 40, sorted(checked)
+    assert {n: getattr(_abi, n) for n in checked} == checked
