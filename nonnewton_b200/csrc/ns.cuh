@@ -175,6 +175,7 @@ __global__ void k_scatter(Dev d) {
 // thread. Particle ids are distinct, so the ranks are a permutation. The scratch of
 // the warp path is the key array, which nothing reads after k_scatter.
 #define NS_SORT_SMALL 24
+#define NS_SORT_REG 8
 __global__ void k_cell_sort(Dev d) {
   const int nc = d.d_n[2];
   const bool truth = *d.src_from_truth != 0;
@@ -184,7 +185,27 @@ __global__ void k_cell_sort(Dev d) {
     uint32_t b = 0, e = 0;
     if (valid) { b = d.cell_count[c]; e = d.cell_count[c + 1]; }
     const uint32_t n = e - b;
-    if (n >= 2 && n <= NS_SORT_SMALL) {
+    if (n >= 2 && n <= NS_SORT_REG) {
+      // in registers: the sources and their ids load together (no chain of dependent
+      // loads per comparison), an odd-even transposition network sorts NS_SORT_REG slots
+      // whose unused tail holds the largest key, and the sources go back in id order
+      int sv[NS_SORT_REG], kv[NS_SORT_REG];
+#pragma unroll
+      for (int q = 0; q < NS_SORT_REG; ++q) sv[q] = (uint32_t)q < n ? d.src[b + q] : 0;
+#pragma unroll
+      for (int q = 0; q < NS_SORT_REG; ++q) kv[q] = (uint32_t)q < n ? (truth ? sv[q] : d.wo.id[sv[q]]) : INT_MAX;
+#pragma unroll
+      for (int r = 0; r < NS_SORT_REG; ++r)
+#pragma unroll
+        for (int q = r & 1; q + 1 < NS_SORT_REG; q += 2)
+          if (kv[q] > kv[q + 1]) {
+            const int tk = kv[q]; kv[q] = kv[q + 1]; kv[q + 1] = tk;
+            const int ts = sv[q]; sv[q] = sv[q + 1]; sv[q + 1] = ts;
+          }
+#pragma unroll
+      for (int q = 0; q < NS_SORT_REG; ++q)
+        if ((uint32_t)q < n) d.src[b + q] = sv[q];
+    } else if (n > NS_SORT_REG && n <= NS_SORT_SMALL) {
       for (uint32_t i = b + 1; i < e; ++i) {
         int s = d.src[i];
         int ids = truth ? s : d.wo.id[s];
