@@ -168,8 +168,9 @@ __global__ void k_scatter(Dev d) {
 }
 
 // In-cell order by particle id, so that the slot order (and every neighbour sum)
-// does not depend on the atomics of k_keys. A cell of up to NS_SORT_SMALL particles
-// is sorted by its own thread (insertion sort); a crowded cell (a cluster) by the
+// does not depend on the atomics of k_keys. A cell of up to NS_SORT_REG particles is
+// sorted by its own thread in registers, one of up to NS_SORT_SMALL by its own thread
+// in place (insertion sort); a crowded cell (a cluster) by the
 // whole warp: each lane ranks some of its particles by counting the smaller ids, so
 // a cell of n particles takes n^2 / 32 steps per lane instead of about n^2 / 4 on one
 // thread. Particle ids are distinct, so the ranks are a permutation. The scratch of
